@@ -1,0 +1,140 @@
+/*
+ * ocfd_b200.h -- C ABI of the B200 (sm_100a) implementation of the
+ * OpenCFD-SCU per-RK-stage right-hand-side path.
+ *
+ * Two layers:
+ *
+ *  1. A context API (ocfd_b200_*): explicit handle, int status codes (0 ok,
+ *     negative on error, never aborts), caller-owned host buffers,
+ *     library-owned device buffers, one CUDA stream per context.
+ *
+ *  2. Reference-named entry points (du_comput, OCFD_time_advance, get_duvwT,
+ *     get_Amu, OCFD_bc, Set_Scheme_HybridAuto) acting on a context bound with
+ *     ocfd_b200_compat_bind().  These replace the reference's own objects for
+ *     the RHS path; see INTEGRATION.md.
+ *
+ * Arrays crossing the ABI are FP64, C order [nvar][nz][ny][nx] (x fastest),
+ * interior cells only -- the order of the reference's record files
+ * (src/OCFD_IO.c:157-228).  Primitive order is d,u,v,w,T; conserved order
+ * is rho, rho u, rho v, rho w, E; metric order is
+ * Axx Ayy Azz Akx Aky Akz Aix Aiy Aiz Asx Asy Asz Ajac
+ * (src/OCFD_Comput_Jacobian3d.cu:142-181).
+ */
+#ifndef OCFD_B200_H
+#define OCFD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OCFD_B200_ABI_VERSION 1
+
+/* status codes */
+#define OCFD_OK               0
+#define OCFD_ERR_ARG         -1   /* bad argument or size                   */
+#define OCFD_ERR_UNSUPPORTED -2   /* configuration outside what is built    */
+#define OCFD_ERR_CUDA        -3   /* CUDA runtime error (see last_error)     */
+#define OCFD_ERR_NOMEM       -4   /* device allocation failed                */
+#define OCFD_ERR_STATE       -5   /* call out of order (e.g. no metrics yet) */
+#define OCFD_ERR_NODEVICE    -6   /* no usable CUDA device                   */
+
+typedef struct ocfd_b200_ctx ocfd_b200_ctx;
+
+/* Replaces the globals that read_parameters() fills from opencfd-scu.in
+ * (src/parameters.c:197-345) for the keys the RHS path consumes. */
+typedef struct ocfd_b200_config {
+    int nx, ny, nz;            /* GRID_3D (single GPU holds the whole grid)      */
+    int iperiodic[3];          /* IPERIODIC                                       */
+    int jac_bound[3];          /* JAC_BOUND                                       */
+    int dif_bound[6];          /* DIF_BOUND                                       */
+    int non_reflection[6];     /* NON_REFLETION                                   */
+    int scheme_invis;          /* SCHEME_INVIS id: 301 UP7 .. 310 HYBRIDAUTO      */
+    int scheme_vis;            /* SCHEME_VIS id: 203 CD6, 204 CD8                 */
+    int charteric;             /* CHARTERIC                                       */
+    int hy_style;              /* HY_STYLE (2 = Jameson pressure sensor)          */
+    double hy_dp_intv[2];      /* HY_DP_INTV                                      */
+    double re, ama, gamma, pr, t_ref, epsl_sw, dt;   /* RE AMA GAMMA PR T_REF EPSL_SW DT */
+    int device;                /* CUDA device ordinal                             */
+} ocfd_b200_config;
+
+int  ocfd_b200_abi_version(void);
+const char *ocfd_b200_status_string(int status);
+/* Last error message of a context (or of the last failed create when ctx is NULL). */
+const char *ocfd_b200_last_error(const ocfd_b200_ctx *ctx);
+
+/* Allocate device state for one grid.  Replaces opencfd_mem_init_all()
+ * (src/OCFD_init.cu:134-235) and opencfd_para_init[_dev]()
+ * (src/OCFD_init.cu:381-410, :580-616). */
+int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out);
+int ocfd_b200_destroy(ocfd_b200_ctx *ctx);
+
+/* Use the caller's CUDA stream (cudaStream_t passed as void*); NULL = the
+ * context's own stream. */
+int ocfd_b200_set_stream(ocfd_b200_ctx *ctx, void *stream);
+void *ocfd_b200_get_stream(const ocfd_b200_ctx *ctx);
+int ocfd_b200_synchronize(ocfd_b200_ctx *ctx);
+
+/* Grid metrics, 13 interior fields (host or device memory).  Replaces the
+ * OCFD3d-Jacobi.dat branch of Init_Jacobian3d()
+ * (src/OCFD_Comput_Jacobian3d.cu:32-218): ghosts start at 1.0 and are
+ * filled periodically in periodic directions. */
+int ocfd_b200_set_metrics(ocfd_b200_ctx *ctx, const double *metrics13);
+int ocfd_b200_set_metrics_device(ocfd_b200_ctx *ctx, const double *metrics13_dev);
+
+/* Initial primitives d,u,v,w,T (host or device).  Replaces the
+ * INIT_STAT=1 part of init() (src/OCFD_init.cu:88-115): ghosts zero, then
+ * pri_to_cons; followed by the pre-loop of NS_solver_real
+ * (src/OCFD_NS_Solver.cu:45-53). */
+int ocfd_b200_set_primitives(ocfd_b200_ctx *ctx, const double *prim5, int istep, double tt);
+int ocfd_b200_set_primitives_device(ocfd_b200_ctx *ctx, const double *prim5_dev, int istep, double tt);
+
+/* nsteps full SSP-RK3 steps (time-level swap + 3 stages each),
+ * src/OCFD_NS_Solver.cu:63-89.  Asynchronous on the context stream. */
+int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps);
+
+/* End-to-end call with host buffers: copy prim5_in to the device, run
+ * nsteps, copy the primitives back into prim5_out (may alias prim5_in).
+ * Metrics must be set.  Synchronous. */
+int ocfd_b200_advance_host(ocfd_b200_ctx *ctx, const double *prim5_in, double *prim5_out,
+                           int nsteps);
+
+/* Per-stage pieces, same semantics as the reference calls of one stage. */
+int ocfd_b200_swap_time_levels(ocfd_b200_ctx *ctx);        /* src/OCFD_NS_Solver.cu:65-73 */
+int ocfd_b200_du_comput(ocfd_b200_ctx *ctx, int krk);      /* src/OCFD_Stream.cu:28-54    */
+int ocfd_b200_time_advance(ocfd_b200_ctx *ctx, int krk);   /* src/OCFD_time.cu:96-123     */
+int ocfd_b200_get_duvwT(ocfd_b200_ctx *ctx);               /* src/commen_kernel.cu:111-118 */
+int ocfd_b200_bc(ocfd_b200_ctx *ctx);                      /* src/OCFD_boundary.cu:18-92  */
+
+/* Read-back (synchronous). */
+int ocfd_b200_get_primitives(ocfd_b200_ctx *ctx, double *prim5);
+int ocfd_b200_get_primitives_device(ocfd_b200_ctx *ctx, double *prim5_dev);
+int ocfd_b200_get_conserved(ocfd_b200_ctx *ctx, double *cons5);
+int ocfd_b200_get_du(ocfd_b200_ctx *ctx, double *du5);
+int ocfd_b200_get_flags(ocfd_b200_ctx *ctx, int8_t *flag_x, int8_t *flag_y, int8_t *flag_z);
+int ocfd_b200_get_time(const ocfd_b200_ctx *ctx, int *istep, double *tt);
+
+/* Kernel timing: when enabled, step() brackets each kernel family with CUDA
+ * events on the context stream.  get_timing returns accumulated device
+ * milliseconds and launch counts per family (names by index). */
+#define OCFD_TIMER_COUNT 8
+int ocfd_b200_set_timing(ocfd_b200_ctx *ctx, int enabled);
+int ocfd_b200_get_timing(ocfd_b200_ctx *ctx, double *ms, long long *launches, int n);
+const char *ocfd_b200_timer_name(int index);
+/* number of kernel launches issued by the library so far */
+long long ocfd_b200_launch_count(const ocfd_b200_ctx *ctx);
+
+/* ---- reference-named entry points (act on the bound context) ---------- */
+int  ocfd_b200_compat_bind(ocfd_b200_ctx *ctx);
+void du_comput(int KRK);                    /* head/OCFD_Stream.h:10           */
+void OCFD_time_advance(int KRK);            /* src/OCFD_time.cu:96             */
+void get_duvwT(void);                       /* head/commen_kernel.h:17         */
+void get_Amu(void);                         /* head/commen_kernel.h:20         */
+void OCFD_bc(void);                         /* src/OCFD_boundary.cu:18         */
+void Set_Scheme_HybridAuto(void *stream);   /* head/OCFD_Schemes_hybrid_auto.h:24 (cudaStream_t*) */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

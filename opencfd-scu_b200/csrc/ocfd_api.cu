@@ -1,0 +1,575 @@
+// ocfd_api.cu -- C ABI (include/ocfd_b200.h) over the sm_100a kernels.
+//
+// State ownership follows the reference's process-global device buffers
+// (head/parameters_d.h:24-80) but lives in an explicit context: primitive
+// and metric fields on the LAP box (LAP = 4 ghost layers), conserved
+// variables f, fn and du without ghosts, hybrid flags as int8.
+#include "ocfd_b200.h"
+#include "ocfd_device.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+namespace ocfd {
+cudaError_t launch_sensor(const Params &p, cudaStream_t st);
+cudaError_t launch_ghost(const Params &p, double *const *fields, const int *dirmask, int nf, cudaStream_t st);
+cudaError_t launch_sweeps(const Params &p, cudaStream_t st);
+cudaError_t launch_viscous(const Params &p, cudaStream_t st);
+cudaError_t launch_rk(const Params &p, int krk, cudaStream_t st);
+cudaError_t launch_rk_only(const Params &p, int krk, cudaStream_t st);
+cudaError_t launch_c2p(const Params &p, cudaStream_t st);
+cudaError_t launch_bc_faces(const Params &p, cudaStream_t st);
+cudaError_t launch_p2c(const Params &p, double *out, cudaStream_t st);
+cudaError_t launch_scatter(const Params &p, const double *src, double *dst_lap, cudaStream_t st);
+cudaError_t launch_gather(const Params &p, const double *src_lap, double *dst, cudaStream_t st);
+cudaError_t launch_fill(double *f, long long n, double v, cudaStream_t st);
+}  // namespace ocfd
+
+using ocfd::Params;
+
+namespace {
+
+enum Timer { T_SENSOR = 0, T_GHOST, T_SWEEP, T_VIS, T_RK, T_OTHER1, T_OTHER2, T_OTHER3 };
+const char *kTimerNames[OCFD_TIMER_COUNT] = {
+    "sensor", "ghost_fill", "inviscid_sweeps", "viscous", "rk_update", "-", "-", "-"};
+
+thread_local std::string g_create_error;
+
+}  // namespace
+
+struct ocfd_b200_ctx {
+    ocfd_b200_config cfg;
+    Params p;
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    // allocations
+    double *prim_buf = nullptr;   // 5 LAP fields
+    double *met_buf = nullptr;    // 13 LAP fields
+    double *cons_buf = nullptr;   // f, fn, du: 15 interior fields
+    double *grad_buf = nullptr;   // 12 interior fields
+    double *ev_buf = nullptr;     // 12 LAP fields
+    int8_t *flag_buf = nullptr;
+    double *stage_buf = nullptr;  // 5 interior fields for host transfers
+    double *pinned = nullptr;     // host staging for advance_host
+    size_t pinned_bytes = 0;
+    bool have_metrics = false;
+    bool have_state = false;
+    int istep = 0;
+    double tt = 0.0;
+    long long launches = 0;
+    // timing
+    bool timing = false;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    double t_ms[OCFD_TIMER_COUNT] = {0};
+    long long t_n[OCFD_TIMER_COUNT] = {0};
+    std::string err;
+};
+
+static int fail(ocfd_b200_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg; else g_create_error = msg;
+    return code;
+}
+
+static int cuda_fail(ocfd_b200_ctx *c, cudaError_t e, const char *where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return fail(c, OCFD_ERR_CUDA, m);
+}
+
+#define CK(call, where)                                     \
+    do {                                                    \
+        cudaError_t _e = (call);                            \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, where); \
+    } while (0)
+
+extern "C" int ocfd_b200_abi_version(void) { return OCFD_B200_ABI_VERSION; }
+
+extern "C" const char *ocfd_b200_status_string(int s) {
+    switch (s) {
+    case OCFD_OK: return "ok";
+    case OCFD_ERR_ARG: return "invalid argument";
+    case OCFD_ERR_UNSUPPORTED: return "unsupported configuration";
+    case OCFD_ERR_CUDA: return "CUDA error";
+    case OCFD_ERR_NOMEM: return "device out of memory";
+    case OCFD_ERR_STATE: return "call out of order";
+    case OCFD_ERR_NODEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+extern "C" const char *ocfd_b200_last_error(const ocfd_b200_ctx *ctx) {
+    return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+static void free_all(ocfd_b200_ctx *c) {
+    cudaFree(c->prim_buf); cudaFree(c->met_buf); cudaFree(c->cons_buf);
+    cudaFree(c->grad_buf); cudaFree(c->ev_buf); cudaFree(c->flag_buf); cudaFree(c->stage_buf);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    for (auto &e : c->ev) if (e) cudaEventDestroy(e);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+}
+
+extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out) {
+    ocfd_b200_ctx *ctx = nullptr;
+    if (!cfg || !out) return fail(nullptr, OCFD_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (cfg->nx < 8 || cfg->ny < 8 || cfg->nz < 8)
+        return fail(nullptr, OCFD_ERR_ARG, "each grid dimension must be >= 8 (LAP = 4 on both sides)");
+    long long N = (long long)cfg->nx * cfg->ny * cfg->nz;
+    if (N > (1LL << 34)) return fail(nullptr, OCFD_ERR_ARG, "grid too large");
+    int si = cfg->scheme_invis;
+    if (si < 301 || si > 310) return fail(nullptr, OCFD_ERR_UNSUPPORTED, "SCHEME_INVIS id must be 301..310");
+    if (cfg->scheme_vis != 203 && cfg->scheme_vis != 204)
+        return fail(nullptr, OCFD_ERR_UNSUPPORTED, "SCHEME_VIS id must be 203 (CD6) or 204 (CD8)");
+    if (si == 310 && cfg->hy_style != 2)
+        return fail(nullptr, OCFD_ERR_UNSUPPORTED, "SCHEME_HYBRIDAUTO is built for HY_STYLE = 2 (Jameson sensor)");
+    for (int d = 0; d < 3; d++)
+        if (!cfg->iperiodic[d])
+            return fail(nullptr, OCFD_ERR_UNSUPPORTED, "non-periodic directions (boundary closures, IBC) are not built");
+    if (!(cfg->ama > 0) || !(cfg->gamma > 1) || !(cfg->re > 0) || !(cfg->pr > 0))
+        return fail(nullptr, OCFD_ERR_ARG, "AMA, GAMMA, RE, PR out of range");
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(nullptr, OCFD_ERR_NODEVICE, "no CUDA device");
+    if (cfg->device < 0 || cfg->device >= ndev) return fail(nullptr, OCFD_ERR_ARG, "device ordinal out of range");
+
+    ctx = new ocfd_b200_ctx();
+    ctx->cfg = *cfg;
+    ctx->device = cfg->device;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) { int r = cuda_fail(nullptr, e, "cudaSetDevice"); delete ctx; return r; }
+
+    Params &p = ctx->p;
+    memset(&p, 0, sizeof(p));
+    p.nx = cfg->nx; p.ny = cfg->ny; p.nz = cfg->nz;
+    int nx2 = p.nx + 2 * OCFD_LAP, ny2 = p.ny + 2 * OCFD_LAP, nz2 = p.nz + 2 * OCFD_LAP;
+    p.pitch = (nx2 + 7) / 8 * 8;                 // 64-byte rows
+    p.ys = p.pitch;
+    p.zs = (long long)p.pitch * ny2;
+    p.lapN = p.zs * nz2;
+    p.N = N;
+    // init() and opencfd_para_init() (src/OCFD_init.cu:29-31, :381-399)
+    p.hx = 1.0 / (p.nx - 1.0);
+    p.hy = 1.0 / (p.ny - 1.0);
+    p.hz = 1.0 / (p.nz - 1.0);
+    double G = cfg->gamma, Ma = cfg->ama;
+    double t_ref = cfg->t_ref > 0 ? cfg->t_ref : 288.15;
+    p.Ama = Ma; p.Gamma = G; p.epsl_sw = cfg->epsl_sw;
+    p.Cv = 1.0 / (G * (G - 1.0) * Ma * Ma);
+    double Cp = 1.0 / ((G - 1.0) * Ma * Ma);
+    p.Tsb = 110.4 / t_ref;
+    p.amu_C0 = 1.0 / cfg->re * (1.0 + 110.4 / t_ref);
+    p.tmp0 = 1.0 / (2.0 * G);
+    p.split_C1 = 2.0 * (G - 1.0);
+    p.split_C3 = (3.0 - G) / (2.0 * (G - 1.0));
+    p.vis_c = Cp / cfg->pr;
+    p.dt = cfg->dt;
+    p.p00 = 1.0 / (G * Ma * Ma);                 // Comput_P (src/OCFD_Schemes_hybrid_auto.cu:64)
+    p.tv_lim = 5.0; p.tv_max = 0.2;              // src/parameters.c:75-76
+    p.dp1 = cfg->hy_dp_intv[0]; p.dp2 = cfg->hy_dp_intv[1];
+    p.scheme_invis = si; p.scheme_vis = cfg->scheme_vis; p.charteric = cfg->charteric;
+    for (int d = 0; d < 3; d++) p.periodic[d] = cfg->iperiodic[d];
+
+    size_t lapB = sizeof(double) * (size_t)p.lapN, inB = sizeof(double) * (size_t)N;
+    size_t flagN = (size_t)(p.nx + 1) * p.ny * p.nz + (size_t)p.nx * (p.ny + 1) * p.nz + (size_t)p.nx * p.ny * (p.nz + 1);
+    auto alloc = [&](void **ptr, size_t bytes, const char *what) -> int {
+        cudaError_t ae = cudaMalloc(ptr, bytes);
+        if (ae != cudaSuccess) {
+            cudaGetLastError();
+            ctx->err = std::string("cudaMalloc(") + what + "): " + cudaGetErrorString(ae);
+            return ae == cudaErrorMemoryAllocation ? OCFD_ERR_NOMEM : OCFD_ERR_CUDA;
+        }
+        return OCFD_OK;
+    };
+    int rc;
+    if ((rc = alloc((void **)&ctx->prim_buf, 5 * lapB, "primitives")) ||
+        (rc = alloc((void **)&ctx->met_buf, 13 * lapB, "metrics")) ||
+        (rc = alloc((void **)&ctx->cons_buf, 15 * inB, "conserved")) ||
+        (rc = alloc((void **)&ctx->grad_buf, 12 * inB, "gradients")) ||
+        (rc = alloc((void **)&ctx->ev_buf, 12 * lapB, "viscous fluxes")) ||
+        (rc = alloc((void **)&ctx->flag_buf, flagN, "flags")) ||
+        (rc = alloc((void **)&ctx->stage_buf, 5 * inB, "staging"))) {
+        g_create_error = ctx->err;
+        free_all(ctx);
+        delete ctx;
+        return rc;
+    }
+    for (int m = 0; m < 5; m++) p.prim[m] = ctx->prim_buf + (size_t)m * p.lapN;
+    for (int m = 0; m < 13; m++) p.met[m] = ctx->met_buf + (size_t)m * p.lapN;
+    p.f = ctx->cons_buf; p.fn = ctx->cons_buf + 5 * N; p.du = ctx->cons_buf + 10 * N;
+    p.grad = ctx->grad_buf;
+    p.ev = ctx->ev_buf;
+    p.flag[0] = ctx->flag_buf;
+    p.flag[1] = ctx->flag_buf + (size_t)(p.nx + 1) * p.ny * p.nz;
+    p.flag[2] = p.flag[1] + (size_t)p.nx * (p.ny + 1) * p.nz;
+
+    if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&ctx->ev[0])) != cudaSuccess || (e = cudaEventCreate(&ctx->ev[1])) != cudaSuccess) {
+        cuda_fail(nullptr, e, "stream/event create");
+        free_all(ctx); delete ctx;
+        return OCFD_ERR_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    // Init_Jacobian3d: metrics 1.0 everywhere; init(): primitives and du zero
+    if ((e = ocfd::launch_fill(ctx->met_buf, 13 * p.lapN, 1.0, ctx->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(ctx->prim_buf, 0, 5 * lapB, ctx->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(ctx->cons_buf, 0, 15 * inB, ctx->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(ctx->ev_buf, 0, 12 * lapB, ctx->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(ctx->flag_buf, 0, flagN, ctx->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) {
+        cuda_fail(nullptr, e, "initialisation");
+        free_all(ctx); delete ctx;
+        return OCFD_ERR_CUDA;
+    }
+    *out = ctx;
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_destroy(ocfd_b200_ctx *ctx) {
+    if (!ctx) return OCFD_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    free_all(ctx);
+    delete ctx;
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_set_stream(ocfd_b200_ctx *ctx, void *stream) {
+    if (!ctx) return OCFD_ERR_ARG;
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return OCFD_OK;
+}
+extern "C" void *ocfd_b200_get_stream(const ocfd_b200_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+extern "C" int ocfd_b200_synchronize(ocfd_b200_ctx *ctx) {
+    if (!ctx) return OCFD_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    return OCFD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// internal helpers
+// ---------------------------------------------------------------------------
+
+static int ghost_prims(ocfd_b200_ctx *ctx) {
+    double *f[5]; int mask[5];
+    for (int m = 0; m < 5; m++) { f[m] = ctx->p.prim[m]; mask[m] = 7; }
+    CK(ocfd::launch_ghost(ctx->p, f, mask, 5, ctx->stream), "ghost fill");
+    ctx->launches += 1;
+    return OCFD_OK;
+}
+
+static int ghost_metrics(ocfd_b200_ctx *ctx) {
+    double *f[12]; int mask[12];
+    for (int m = 0; m < 12; m++) { f[m] = const_cast<double *>(ctx->p.met[m]); mask[m] = 7; }
+    CK(ocfd::launch_ghost(ctx->p, f, mask, 12, ctx->stream), "metric ghost fill");
+    double *fj[1] = { const_cast<double *>(ctx->p.met[12]) }; int mj[1] = { 7 };
+    CK(ocfd::launch_ghost(ctx->p, fj, mj, 1, ctx->stream), "metric ghost fill");
+    ctx->launches += 2;
+    return OCFD_OK;
+}
+
+struct TimerScope {
+    ocfd_b200_ctx *c; int which; bool on;
+    TimerScope(ocfd_b200_ctx *cc, int w) : c(cc), which(w), on(cc->timing) {
+        if (on) cudaEventRecord(c->ev[0], c->stream);
+    }
+    ~TimerScope() {
+        if (!on) return;
+        cudaEventRecord(c->ev[1], c->stream);
+        if (cudaEventSynchronize(c->ev[1]) == cudaSuccess) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+            c->t_ms[which] += ms;
+            c->t_n[which] += 1;
+        }
+    }
+};
+
+static int rhs(ocfd_b200_ctx *ctx, int krk) {
+    const Params &p = ctx->p;
+    if (p.scheme_invis == 310 && krk == 1) {
+        TimerScope ts(ctx, T_SENSOR);
+        CK(ocfd::launch_sensor(p, ctx->stream), "sensor");
+        ctx->launches += 1;
+    }
+    {
+        TimerScope ts(ctx, T_GHOST);
+        int rc = ghost_prims(ctx);
+        if (rc) return rc;
+    }
+    {
+        TimerScope ts(ctx, T_SWEEP);
+        CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
+        ctx->launches += 3;
+    }
+    {
+        TimerScope ts(ctx, T_VIS);
+        CK(ocfd::launch_viscous(p, ctx->stream), "viscous");
+        ctx->launches += 4;
+    }
+    return OCFD_OK;
+}
+
+static int check_ready(ocfd_b200_ctx *ctx) {
+    if (!ctx) return OCFD_ERR_ARG;
+    if (!ctx->have_metrics) return fail(ctx, OCFD_ERR_STATE, "metrics not set");
+    if (!ctx->have_state) return fail(ctx, OCFD_ERR_STATE, "primitives not set");
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+    return OCFD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// set-up
+// ---------------------------------------------------------------------------
+
+static int set_metrics_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKind kind) {
+    if (!ctx || !src) return OCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const Params &p = ctx->p;
+    size_t inB = sizeof(double) * (size_t)p.N;
+    for (int m = 0; m < 13; m++) {
+        CK(cudaMemcpyAsync(ctx->stage_buf, src + (size_t)m * p.N, inB, kind, ctx->stream), "metric copy");
+        CK(ocfd::launch_scatter(p, ctx->stage_buf, const_cast<double *>(p.met[m]), ctx->stream), "metric scatter");
+        ctx->launches += 1;
+    }
+    int rc = ghost_metrics(ctx);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream), "set_metrics");
+    ctx->have_metrics = true;
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_set_metrics(ocfd_b200_ctx *ctx, const double *m) {
+    return set_metrics_impl(ctx, m, cudaMemcpyHostToDevice);
+}
+extern "C" int ocfd_b200_set_metrics_device(ocfd_b200_ctx *ctx, const double *m) {
+    return set_metrics_impl(ctx, m, cudaMemcpyDeviceToDevice);
+}
+
+static int upload_prims(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKind kind) {
+    const Params &p = ctx->p;
+    size_t inB = sizeof(double) * (size_t)p.N;
+    CK(cudaMemcpyAsync(ctx->stage_buf, src, 5 * inB, kind, ctx->stream), "primitive copy");
+    for (int m = 0; m < 5; m++) {
+        CK(ocfd::launch_scatter(p, ctx->stage_buf + (size_t)m * p.N, p.prim[m], ctx->stream), "scatter");
+        ctx->launches += 1;
+    }
+    return OCFD_OK;
+}
+
+static int set_prims_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKind kind, int istep, double tt) {
+    if (!ctx || !src) return OCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const Params &p = ctx->p;
+    // init(): ghosts of d,u,v,w,T zero (src/OCFD_init.cu:37-41), f/fn/du zero
+    CK(cudaMemsetAsync(ctx->prim_buf, 0, 5 * sizeof(double) * (size_t)p.lapN, ctx->stream), "memset");
+    CK(cudaMemsetAsync(ctx->cons_buf, 0, 15 * sizeof(double) * (size_t)p.N, ctx->stream), "memset");
+    int rc = upload_prims(ctx, src, kind);
+    if (rc) return rc;
+    CK(ocfd::launch_p2c(p, p.f, ctx->stream), "pri_to_cons");
+    ctx->launches += 1;
+    // NS_solver_real pre-loop: exchange, OCFD_bc (re-projects the faces of f
+    // from the same primitives: no change), get_Amu (formed on the fly)
+    rc = ghost_prims(ctx);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream), "set_primitives");
+    ctx->istep = istep;
+    ctx->tt = tt;
+    ctx->have_state = true;
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_set_primitives(ocfd_b200_ctx *ctx, const double *prim5, int istep, double tt) {
+    return set_prims_impl(ctx, prim5, cudaMemcpyHostToDevice, istep, tt);
+}
+extern "C" int ocfd_b200_set_primitives_device(ocfd_b200_ctx *ctx, const double *prim5, int istep, double tt) {
+    return set_prims_impl(ctx, prim5, cudaMemcpyDeviceToDevice, istep, tt);
+}
+
+// ---------------------------------------------------------------------------
+// time stepping
+// ---------------------------------------------------------------------------
+
+extern "C" int ocfd_b200_swap_time_levels(ocfd_b200_ctx *ctx) {
+    if (!ctx) return OCFD_ERR_ARG;
+    double *t = ctx->p.f; ctx->p.f = ctx->p.fn; ctx->p.fn = t;
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (nsteps < 0) return fail(ctx, OCFD_ERR_ARG, "nsteps < 0");
+    for (int n = 0; n < nsteps; n++) {
+        ocfd_b200_swap_time_levels(ctx);
+        for (int krk = 1; krk <= 3; krk++) {
+            if ((rc = rhs(ctx, krk))) return rc;
+            TimerScope ts(ctx, T_RK);
+            CK(ocfd::launch_rk(ctx->p, krk, ctx->stream), "rk update");
+            ctx->launches += 1;
+        }
+        ctx->istep++;
+        ctx->tt += ctx->p.dt;
+    }
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_du_comput(ocfd_b200_ctx *ctx, int krk) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (krk < 1 || krk > 3) return fail(ctx, OCFD_ERR_ARG, "KRK must be 1..3");
+    return rhs(ctx, krk);
+}
+
+extern "C" int ocfd_b200_time_advance(ocfd_b200_ctx *ctx, int krk) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (krk < 1 || krk > 3) return fail(ctx, OCFD_ERR_ARG, "KRK must be 1..3");
+    CK(ocfd::launch_rk_only(ctx->p, krk, ctx->stream), "time advance");
+    ctx->launches += 1;
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_get_duvwT(ocfd_b200_ctx *ctx) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    CK(ocfd::launch_c2p(ctx->p, ctx->stream), "cons_to_pri");
+    ctx->launches += 1;
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_bc(ocfd_b200_ctx *ctx) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    CK(ocfd::launch_bc_faces(ctx->p, ctx->stream), "face re-projection");
+    ctx->launches += 1;
+    return OCFD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// read-back
+// ---------------------------------------------------------------------------
+
+extern "C" int ocfd_b200_get_primitives_device(ocfd_b200_ctx *ctx, double *out) {
+    if (!ctx || !out) return OCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    for (int m = 0; m < 5; m++) {
+        CK(ocfd::launch_gather(ctx->p, ctx->p.prim[m], out + (size_t)m * ctx->p.N, ctx->stream), "gather");
+        ctx->launches += 1;
+    }
+    CK(cudaStreamSynchronize(ctx->stream), "get_primitives");
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_get_primitives(ocfd_b200_ctx *ctx, double *out) {
+    if (!ctx || !out) return OCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    for (int m = 0; m < 5; m++) {
+        CK(ocfd::launch_gather(ctx->p, ctx->p.prim[m], ctx->stage_buf + (size_t)m * ctx->p.N, ctx->stream), "gather");
+        ctx->launches += 1;
+    }
+    CK(cudaMemcpyAsync(out, ctx->stage_buf, 5 * sizeof(double) * (size_t)ctx->p.N, cudaMemcpyDeviceToHost,
+                       ctx->stream), "primitive copy");
+    CK(cudaStreamSynchronize(ctx->stream), "get_primitives");
+    return OCFD_OK;
+}
+
+static int get_interior5(ocfd_b200_ctx *ctx, const double *src, double *out, const char *what) {
+    if (!ctx || !out) return OCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaMemcpyAsync(out, src, 5 * sizeof(double) * (size_t)ctx->p.N, cudaMemcpyDeviceToHost, ctx->stream), what);
+    CK(cudaStreamSynchronize(ctx->stream), what);
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_get_conserved(ocfd_b200_ctx *ctx, double *out) {
+    return ctx ? get_interior5(ctx, ctx->p.f, out, "get_conserved") : OCFD_ERR_ARG;
+}
+extern "C" int ocfd_b200_get_du(ocfd_b200_ctx *ctx, double *out) {
+    return ctx ? get_interior5(ctx, ctx->p.du, out, "get_du") : OCFD_ERR_ARG;
+}
+
+extern "C" int ocfd_b200_get_flags(ocfd_b200_ctx *ctx, int8_t *fx, int8_t *fy, int8_t *fz) {
+    if (!ctx || !fx || !fy || !fz) return OCFD_ERR_ARG;
+    const Params &p = ctx->p;
+    size_t nxf = (size_t)(p.nx + 1) * p.ny * p.nz, nyf = (size_t)p.nx * (p.ny + 1) * p.nz,
+           nzf = (size_t)p.nx * p.ny * (p.nz + 1);
+    CK(cudaMemcpyAsync(fx, p.flag[0], nxf, cudaMemcpyDeviceToHost, ctx->stream), "flags");
+    CK(cudaMemcpyAsync(fy, p.flag[1], nyf, cudaMemcpyDeviceToHost, ctx->stream), "flags");
+    CK(cudaMemcpyAsync(fz, p.flag[2], nzf, cudaMemcpyDeviceToHost, ctx->stream), "flags");
+    CK(cudaStreamSynchronize(ctx->stream), "flags");
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_get_time(const ocfd_b200_ctx *ctx, int *istep, double *tt) {
+    if (!ctx) return OCFD_ERR_ARG;
+    if (istep) *istep = ctx->istep;
+    if (tt) *tt = ctx->tt;
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_advance_host(ocfd_b200_ctx *ctx, const double *in, double *out, int nsteps) {
+    if (!ctx || !in || !out) return OCFD_ERR_ARG;
+    if (!ctx->have_metrics) return fail(ctx, OCFD_ERR_STATE, "metrics not set");
+    int rc = ocfd_b200_set_primitives(ctx, in, ctx->istep, ctx->tt);
+    if (rc) return rc;
+    if ((rc = ocfd_b200_step(ctx, nsteps))) return rc;
+    return ocfd_b200_get_primitives(ctx, out);
+}
+
+// ---------------------------------------------------------------------------
+// timing
+// ---------------------------------------------------------------------------
+
+extern "C" int ocfd_b200_set_timing(ocfd_b200_ctx *ctx, int enabled) {
+    if (!ctx) return OCFD_ERR_ARG;
+    ctx->timing = enabled != 0;
+    for (int i = 0; i < OCFD_TIMER_COUNT; i++) { ctx->t_ms[i] = 0; ctx->t_n[i] = 0; }
+    return OCFD_OK;
+}
+extern "C" int ocfd_b200_get_timing(ocfd_b200_ctx *ctx, double *ms, long long *n, int cnt) {
+    if (!ctx) return OCFD_ERR_ARG;
+    for (int i = 0; i < cnt && i < OCFD_TIMER_COUNT; i++) {
+        if (ms) ms[i] = ctx->t_ms[i];
+        if (n) n[i] = ctx->t_n[i];
+    }
+    return OCFD_OK;
+}
+extern "C" const char *ocfd_b200_timer_name(int i) {
+    return (i >= 0 && i < OCFD_TIMER_COUNT) ? kTimerNames[i] : "";
+}
+extern "C" long long ocfd_b200_launch_count(const ocfd_b200_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+// ---------------------------------------------------------------------------
+// reference-named entry points
+// ---------------------------------------------------------------------------
+static ocfd_b200_ctx *g_bound = nullptr;
+
+extern "C" int ocfd_b200_compat_bind(ocfd_b200_ctx *ctx) { g_bound = ctx; return OCFD_OK; }
+
+static void compat_report(int rc, const char *what) {
+    if (rc != OCFD_OK)
+        fprintf(stderr, "ocfd_b200: %s failed: %s (%s)\n", what, ocfd_b200_status_string(rc),
+                ocfd_b200_last_error(g_bound));
+}
+
+extern "C" void du_comput(int KRK) { compat_report(g_bound ? ocfd_b200_du_comput(g_bound, KRK) : OCFD_ERR_STATE, "du_comput"); }
+extern "C" void OCFD_time_advance(int KRK) { compat_report(g_bound ? ocfd_b200_time_advance(g_bound, KRK) : OCFD_ERR_STATE, "OCFD_time_advance"); }
+extern "C" void get_duvwT(void) { compat_report(g_bound ? ocfd_b200_get_duvwT(g_bound) : OCFD_ERR_STATE, "get_duvwT"); }
+// viscosity is formed from T inside the viscous kernel; nothing to store
+extern "C" void get_Amu(void) { compat_report(g_bound ? OCFD_OK : OCFD_ERR_STATE, "get_Amu"); }
+extern "C" void OCFD_bc(void) { compat_report(g_bound ? ocfd_b200_bc(g_bound) : OCFD_ERR_STATE, "OCFD_bc"); }
+extern "C" void Set_Scheme_HybridAuto(void *stream) {
+    (void)stream;
+    if (!g_bound) { compat_report(OCFD_ERR_STATE, "Set_Scheme_HybridAuto"); return; }
+    cudaError_t e = ocfd::launch_sensor(g_bound->p, g_bound->stream);
+    compat_report(e == cudaSuccess ? OCFD_OK : OCFD_ERR_CUDA, "Set_Scheme_HybridAuto");
+}

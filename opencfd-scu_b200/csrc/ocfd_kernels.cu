@@ -1,0 +1,655 @@
+// ocfd_kernels.cu -- CUDA kernels of the per-RK-stage RHS path (sm_100a, FP64).
+//
+// One stage (reference driver order, src/OCFD_NS_Solver.cu:76-89 and
+// src/OCFD_Stream.cu:28-54):
+//   [KRK=1, hybrid] sensor        -> int8 face flags            (k_sensor)
+//   ghost fill of d,u,v,w,T        (periodic wrap on device)    (k_ghost_prim)
+//   inviscid x, y, z sweeps        -> du (single writer, fixed order)  (k_sweep<DIR>)
+//   viscous gradients, Ev, Ev ghosts, divergence -> du         (k_vis_*)
+//   RK stage + cons->prim + face re-projection                 (k_rk_update)
+//
+// Each sweep block owns a tile of TS cells along the sweep direction and R
+// rows across it.  Phase A computes the Steger-Warming split of every tile
+// point once into shared memory; phase B runs one thread per
+// (face, sign, component) -- for characteristic schemes the component is the
+// characteristic field, so the 5x5 projection of the 8-point stencil is a
+// 5-term dot product per thread; phase C forms du of each tile cell from
+// the two neighbouring face fluxes (no atomics).
+#include "ocfd_device.cuh"
+
+#include <cuda_runtime.h>
+
+namespace ocfd {
+
+// ---------------------------------------------------------------------------
+// hybrid sensor, style 2: Comput_P + Comput_Scheme_point_{x,y,z}_Jameson
+// (src/OCFD_Schemes_hybrid_auto.cu:48-68, :611-703).  Flag q along DIR
+// belongs to cell q-1; P = p00*d*T is formed on the fly from the LAP-box d,T
+// as they stand before this stage's ghost fill.
+// ---------------------------------------------------------------------------
+__global__ void k_sensor(Params p) {
+    long long nfx = (long long)(p.nx + 1) * p.ny * p.nz;
+    long long nfy = (long long)p.nx * (p.ny + 1) * p.nz;
+    long long nfz = (long long)p.nx * p.ny * (p.nz + 1);
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int dir;
+    long long q;
+    if (tid < nfx) { dir = 0; q = tid; }
+    else if (tid < nfx + nfy) { dir = 1; q = tid - nfx; }
+    else if (tid < nfx + nfy + nfz) { dir = 2; q = tid - nfx - nfy; }
+    else return;
+    int ex = p.nx + (dir == 0), ey = p.ny + (dir == 1);
+    int i = (int)(q % ex);
+    long long r = q / ex;
+    int j = (int)(r % ey);
+    int k = (int)(r / ey);
+    int ci = i + OCFD_LAP - (dir == 0), cj = j + OCFD_LAP - (dir == 1), ck = k + OCFD_LAP - (dir == 2);
+    const double *d = p.prim[0], *T = p.prim[4];
+    long long c = lap_index(p, ci, cj, ck);
+    const double p00 = p.p00;
+    auto P = [&](long long o) { return p00 * d[o] * T[o]; };
+    double P0 = P(c);
+    double Pm = P(c - 1), Pp = P(c + 1);
+    double dp0 = fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
+    Pm = P(c - p.ys); Pp = P(c + p.ys);
+    dp0 += fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
+    Pm = P(c - p.zs); Pp = P(c + p.zs);
+    dp0 += fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
+    int kp = 1;
+    if (dp0 > p.dp1) kp += 1;
+    if (dp0 > p.dp2) kp += 1;
+    p.flag[dir][q] = (int8_t)kp;
+}
+
+// ---------------------------------------------------------------------------
+// periodic ghost fill of LAP-box fields, exchange_boundary_{x,y,z}_packed_dev
+// (src/OCFD_mpi_dev.cu:186-310) on one GPU: x ghosts for interior (y,z),
+// y ghosts for interior (x,z), z ghosts for interior (x,y).  The three slabs
+// read only interior cells, so one launch fills all of them.
+// fields: list of base pointers; dirmask selects directions per field.
+// ---------------------------------------------------------------------------
+struct GhostList { double *f[12]; int dirmask[12]; int n; };
+
+__global__ void k_ghost(Params p, GhostList g) {
+    const int L = OCFD_LAP;
+    long long sx = 2LL * L * p.ny * p.nz, sy = 2LL * L * p.nx * p.nz, sz = 2LL * L * p.nx * p.ny;
+    long long per = sx + sy + sz;
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= per * g.n) return;
+    int fi = (int)(tid / per);
+    long long q = tid - (long long)fi * per;
+    double *f = g.f[fi];
+    int mask = g.dirmask[fi];
+    if (q < sx) {
+        if (!(mask & 1) || !p.periodic[0]) return;
+        int i = (int)(q % (2 * L)); long long r = q / (2 * L);
+        int j = (int)(r % p.ny) + L, k = (int)(r / p.ny) + L;
+        int dst = i < L ? i : p.nx + i;              // 0..L-1  or  nx+L..nx+2L-1
+        int src = i < L ? p.nx + i : i;              // wrap
+        f[lap_index(p, dst, j, k)] = f[lap_index(p, src, j, k)];
+    } else if (q < sx + sy) {
+        if (!(mask & 2) || !p.periodic[1]) return;
+        q -= sx;
+        int i = (int)(q % p.nx) + L; long long r = q / p.nx;
+        int jj = (int)(r % (2 * L)); int k = (int)(r / (2 * L)) + L;
+        int dst = jj < L ? jj : p.ny + jj;
+        int src = jj < L ? p.ny + jj : jj;
+        f[lap_index(p, i, dst, k)] = f[lap_index(p, i, src, k)];
+    } else {
+        if (!(mask & 4) || !p.periodic[2]) return;
+        q -= sx + sy;
+        int i = (int)(q % p.nx) + L; long long r = q / p.nx;
+        int j = (int)(r % p.ny) + L; int kk = (int)(r / p.ny);
+        int dst = kk < L ? kk : p.nz + kk;
+        int src = kk < L ? p.nz + kk : kk;
+        f[lap_index(p, i, j, dst)] = f[lap_index(p, i, j, src)];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// inviscid sweep along DIR
+// ---------------------------------------------------------------------------
+template <int DIR> struct SweepShape;
+template <> struct SweepShape<0> { static constexpr int TS = 64, R = 2, THREADS = 128; };
+template <> struct SweepShape<1> { static constexpr int TS = 16, R = 16, THREADS = 256; };
+template <> struct SweepShape<2> { static constexpr int TS = 16, R = 16, THREADS = 256; };
+
+template <int DIR> __device__ __forceinline__ int ndir(const Params &p) { return DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz); }
+template <int DIR> __device__ __forceinline__ int nrow(const Params &p) { return DIR == 0 ? p.ny : p.nx; }
+template <int DIR> __device__ __forceinline__ long long sdir(const Params &p) { return DIR == 0 ? 1LL : (DIR == 1 ? p.ys : p.zs); }
+template <int DIR> __device__ __forceinline__ long long srow(const Params &p) { return DIR == 0 ? p.ys : 1LL; }
+template <int DIR> __device__ __forceinline__ long long s3rd(const Params &p) { return DIR == 2 ? p.ys : p.zs; }
+template <int DIR> __device__ __forceinline__ double hdir(const Params &p) { return DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz); }
+
+// reconstruction of one (face, sign) from the stencil v[0..7] = f(F-3..F+4)
+__device__ __forceinline__ double recon(const Params &p, int scheme, int hflag, int sign, const double *v) {
+    if (sign == 0) {
+        switch (scheme) {
+        case 301: return up7_p(v);
+        case 302: return weno5_p(v);
+        case 303: return weno7_p(v);
+        case 304: return symbo_p(0, p.tv_lim, p.tv_max, v);
+        case 305: return symbo_p(1, p.tv_lim, p.tv_max, v);
+        case 306: return nnd2_p(v);
+        case 307: return omp6_p(0, v);
+        case 308: return omp6_p(1, v);
+        case 309: return omp6_p(2, v);
+        default:  // 310, style 2 (OCFD_HybridAuto_*_Jameson_kernel)
+            if (hflag == 1) return up7_p(v);
+            if (hflag == 2) return weno7_p(v);
+            return weno5_p(v);
+        }
+    } else {
+        switch (scheme) {
+        case 301: return up7_m(v);
+        case 302: return weno5_m(v);
+        case 303: return weno7_m(v);
+        case 304: return symbo_m(0, p.tv_lim, p.tv_max, v);
+        case 305: return symbo_m(1, p.tv_lim, p.tv_max, v);
+        case 306: return nnd2_m(v);
+        case 307: return omp6_m(0, v);
+        case 308: return omp6_m(1, v);
+        case 309: return omp6_m(2, v);
+        default:
+            if (hflag == 1) return up7_m(v);
+            if (hflag == 2) return weno7_m(v);
+            return weno5_m(v);
+        }
+    }
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(SweepShape<DIR>::THREADS)
+k_sweep(Params p) {
+    constexpr int TS = SweepShape<DIR>::TS, R = SweepShape<DIR>::R;
+    constexpr int NP = (TS + 8) * R;      // split points
+    constexpr int NF = (TS + 1) * R;      // faces
+    constexpr int NC = TS * R;            // cells
+    extern __shared__ double smem[];
+    double *spl = smem;                   // [10][NP]: f+ 0..4, f- 5..9
+    double *hat = smem + 10 * NP;         // [10][NF]: sign*5 + comp
+
+    const int n = ndir<DIR>(p), nr = nrow<DIR>(p);
+    const int s0 = blockIdx.x * TS;       // first interior cell of the tile (along DIR)
+    const int r0 = blockIdx.y * R;        // first row
+    const int c3 = blockIdx.z;            // third coordinate (interior)
+    const long long sd = sdir<DIR>(p), sr = srow<DIR>(p);
+    const long long base = lap_index(p, 0, 0, 0) + (long long)(c3 + OCFD_LAP) * s3rd<DIR>(p)
+                         + (long long)(r0 + OCFD_LAP) * sr + (long long)(s0) * sd;
+    // base points at LAP coordinate (s0 along DIR), i.e. interior cell s0-4
+    const double *d = p.prim[0], *u = p.prim[1], *v = p.prim[2], *w = p.prim[3], *T = p.prim[4];
+    const double *A1 = p.met[M_AKX + 3 * DIR], *A2 = p.met[M_AKX + 3 * DIR + 1], *A3 = p.met[M_AKX + 3 * DIR + 2];
+
+    // ---- phase A: split fluxes at interior-relative points s0-4 .. s0+TS+3
+    for (int q = threadIdx.x; q < NP; q += blockDim.x) {
+        int s, r;
+        if (DIR == 0) { s = q % (TS + 8); r = q / (TS + 8); }
+        else          { r = q % R; s = q / R; }
+        if (r0 + r >= nr || s0 + s - 4 > n + 3) continue;
+        long long o = base + (long long)s * sd + (long long)r * sr;
+        double cc = sqrt(T[o]) / p.Ama;
+        double fp[5], fm[5];
+        sw_split(d[o] * p.tmp0, u[o], v[o], w[o], cc, A1[o], A2[o], A3[o], p.Gamma, p.epsl_sw,
+                 p.split_C1, p.split_C3, fp, fm);
+        int pi = s + (TS + 8) * r;
+#pragma unroll
+        for (int m = 0; m < 5; m++) { spl[m * NP + pi] = fp[m]; spl[(5 + m) * NP + pi] = fm[m]; }
+    }
+    __syncthreads();
+
+    const int scheme = p.scheme_invis;
+    const bool char_scheme = p.charteric && (scheme == 304 || scheme == 305 || scheme == 310);
+    const bool comp_none = p.charteric && !char_scheme;   // reference adds nothing
+    const int8_t *flags = p.flag[DIR];
+
+    // ---- phase B1: one thread per (face, sign, component / characteristic)
+    for (int t = threadIdx.x; t < 10 * NF; t += blockDim.x) {
+        int fi = t % NF, rem = t / NF;          // rem = sign*5 + c
+        int sign = rem / 5, c = rem - 5 * sign;
+        int fs, r;
+        if (DIR == 0) { fs = fi % (TS + 1); r = fi / (TS + 1); }
+        else          { r = fi % R; fs = fi / R; }
+        int F = s0 - 1 + fs;                    // face F+1/2, interior-relative
+        if (r0 + r >= nr || F > n - 1) continue;
+        int hflag = 0;
+        if (scheme == 310) {
+            // flag of the face's left cell F (both signs)
+            long long fq;
+            if (DIR == 0)      fq = (long long)(F + 1) + (long long)(p.nx + 1) * ((long long)(r0 + r) + (long long)p.ny * c3);
+            else if (DIR == 1) fq = (long long)(r0 + r) + (long long)p.nx * ((long long)(F + 1) + (long long)(p.ny + 1) * c3);
+            else               fq = (long long)(r0 + r) + (long long)p.nx * ((long long)c3 + (long long)p.ny * (F + 1));
+            hflag = flags[fq];
+        }
+        const double *sp = spl + (sign * 5) * NP + fs + (TS + 8) * r;   // stencil start f(F-3)
+        double vals[8];
+        double res;
+        if (comp_none) {
+            res = 0.0;
+        } else if (char_scheme && !(scheme == 310 && hflag == 1)) {
+            // face-averaged characteristic system, get_para_charteric_{p,m}_kernel
+            long long o0 = base + (long long)(fs + 3) * sd + (long long)r * sr;   // cell F
+            long long o1 = o0 + sd;                                                // cell F+1
+            CharPara cp;
+            double c0v = sqrt(T[o0]) / p.Ama, c1v = sqrt(T[o1]) / p.Ama;
+            char_para((u[o0] + u[o1]) * 0.5, (v[o0] + v[o1]) * 0.5, (w[o0] + w[o1]) * 0.5,
+                      (c0v + c1v) * 0.5, (A1[o0] + A1[o1]) * 0.5, (A2[o0] + A2[o1]) * 0.5,
+                      (A3[o0] + A3[o1]) * 0.5, p.Gamma, cp);
+            double Lr[5];
+            char_L_row(cp, c, Lr);
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                vals[k] = dot5(Lr, sp[k], sp[NP + k], sp[2 * NP + k], sp[3 * NP + k], sp[4 * NP + k]);
+            res = recon(p, scheme, hflag, sign, vals);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) vals[k] = sp[c * NP + k];
+            res = recon(p, scheme, hflag, sign, vals);
+        }
+        hat[rem * NF + fi] = res;
+    }
+    __syncthreads();
+
+    // ---- phase B2: back-projection R * F^_char (characteristic faces only)
+    if (char_scheme) {
+        double *outb = spl;   // the split values are no longer needed
+        for (int t = threadIdx.x; t < 10 * NF; t += blockDim.x) {
+            int fi = t % NF, rem = t / NF;
+            int sign = rem / 5, m = rem - 5 * sign;
+            int fs, r;
+            if (DIR == 0) { fs = fi % (TS + 1); r = fi / (TS + 1); }
+            else          { r = fi % R; fs = fi / R; }
+            int F = s0 - 1 + fs;
+            if (r0 + r >= nr || F > n - 1) continue;
+            int hflag = 2;
+            if (scheme == 310) {
+                long long fq;
+                if (DIR == 0)      fq = (long long)(F + 1) + (long long)(p.nx + 1) * ((long long)(r0 + r) + (long long)p.ny * c3);
+                else if (DIR == 1) fq = (long long)(r0 + r) + (long long)p.nx * ((long long)(F + 1) + (long long)(p.ny + 1) * c3);
+                else               fq = (long long)(r0 + r) + (long long)p.nx * ((long long)c3 + (long long)p.ny * (F + 1));
+                hflag = flags[fq];
+            }
+            const double *h = hat + (sign * 5) * NF + fi;
+            double res;
+            if (scheme == 310 && hflag == 1) {
+                res = h[m * NF];
+            } else {
+                long long o0 = base + (long long)(fs + 3) * sd + (long long)r * sr;
+                long long o1 = o0 + sd;
+                CharPara cp;
+                double c0v = sqrt(T[o0]) / p.Ama, c1v = sqrt(T[o1]) / p.Ama;
+                char_para((u[o0] + u[o1]) * 0.5, (v[o0] + v[o1]) * 0.5, (w[o0] + w[o1]) * 0.5,
+                          (c0v + c1v) * 0.5, (A1[o0] + A1[o1]) * 0.5, (A2[o0] + A2[o1]) * 0.5,
+                          (A3[o0] + A3[o1]) * 0.5, p.Gamma, cp);
+                double Rr[5];
+                char_R_row(cp, m, Rr);
+                res = dot5(Rr, h[0], h[NF], h[2 * NF], h[3 * NF], h[4 * NF]);
+            }
+            outb[rem * NF + fi] = res;
+        }
+        __syncthreads();
+    }
+    const double *fl = char_scheme ? spl : hat;
+
+    // ---- phase C: du of each tile cell (x+ then x- for every component)
+    const double *Aj = p.met[M_AJAC];
+    const double h = hdir<DIR>(p);
+    for (int t = threadIdx.x; t < NC; t += blockDim.x) {
+        int s, r;
+        if (DIR == 0) { s = t % TS; r = t / TS; }
+        else          { r = t % R; s = t / R; }
+        int X = s0 + s;
+        if (r0 + r >= nr || X > n - 1) continue;
+        long long o = base + (long long)(s + 4) * sd + (long long)r * sr;
+        double aj = Aj[o];
+        int i, j, k;
+        if (DIR == 0)      { i = X; j = r0 + r; k = c3; }
+        else if (DIR == 1) { i = r0 + r; j = X; k = c3; }
+        else               { i = r0 + r; j = c3; k = X; }
+        long long ci = in_index(p, i, j, k);
+        int fr = (DIR == 0) ? (s + 1) + (TS + 1) * r : r + R * (s + 1);
+        int fl_ = (DIR == 0) ? s + (TS + 1) * r : r + R * s;
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            double acc = (DIR == 0) ? 0.0 : p.du[m * p.N + ci];
+            acc += -aj * (fl[m * NF + fr] - fl[m * NF + fl_]) / h;
+            acc += -aj * (fl[(5 + m) * NF + fr] - fl[(5 + m) * NF + fl_]) / h;
+            p.du[m * p.N + ci] = acc;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// viscous terms, src/OCFD_NS_Jacobian3d.cu:58-440
+// ---------------------------------------------------------------------------
+
+// 12 first derivatives of u,v,w,T (du_viscous_Jacobian3d_init, OCFD_d?0)
+__global__ void k_vis_grad(Params p) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    int i = (int)(tid % p.nx); long long r = tid / p.nx;
+    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+    const long long st[3] = { 1LL, p.ys, p.zs };
+    const double hh[3] = { p.hx, p.hy, p.hz };
+    const bool c8 = p.scheme_vis == 204;
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        const double *f = p.prim[m == 3 ? 4 : m + 1];
+#pragma unroll
+        for (int dd = 0; dd < 3; dd++) {
+            long long s = st[dd];
+            double t;
+            if (c8) t = cd8(f[o - 4 * s], f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s], f[o + 4 * s]);
+            else    t = cd6(f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s]);
+            p.grad[(3 * m + dd) * p.N + tid] = t / hh[dd];
+        }
+    }
+}
+
+// Ev1..4 of all three directions (vis_flux_ker :178-236; the stress and heat
+// flux are direction independent, so they are formed once per cell)
+__global__ void k_vis_ev(Params p) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    int i = (int)(tid % p.nx); long long r = tid / p.nx;
+    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+    const double *g = p.grad;
+    const long long N = p.N;
+    double Akx = p.met[M_AKX][o], Aix = p.met[M_AIX][o], Asx = p.met[M_ASX][o];
+    double Aky = p.met[M_AKY][o], Aiy = p.met[M_AIY][o], Asy = p.met[M_ASY][o];
+    double Akz = p.met[M_AKZ][o], Aiz = p.met[M_AIZ][o], Asz = p.met[M_ASZ][o];
+    double Tc = p.prim[4][o];
+    double Amu = p.amu_C0 * sqrt(Tc * Tc * Tc) / (p.Tsb + Tc);      // get_Amu_kernal
+    double uk = g[0 * N + tid], ui = g[1 * N + tid], us = g[2 * N + tid];
+    double vk = g[3 * N + tid], vi = g[4 * N + tid], vs = g[5 * N + tid];
+    double wk = g[6 * N + tid], wi = g[7 * N + tid], ws = g[8 * N + tid];
+    double Tk = g[9 * N + tid], Ti = g[10 * N + tid], Ts = g[11 * N + tid];
+    double ux = uk*Akx + ui*Aix + us*Asx;
+    double vx = vk*Akx + vi*Aix + vs*Asx;
+    double wx = wk*Akx + wi*Aix + ws*Asx;
+    double uy = uk*Aky + ui*Aiy + us*Asy;
+    double vy = vk*Aky + vi*Aiy + vs*Asy;
+    double wy = wk*Aky + wi*Aiy + ws*Asy;
+    double uz = uk*Akz + ui*Aiz + us*Asz;
+    double vz = vk*Akz + vi*Aiz + vs*Asz;
+    double wz = wk*Akz + wi*Aiz + ws*Asz;
+    double div = ux + vy + wz;
+    double s11 = (2.0*ux - 2.0/3.0*div) * Amu;
+    double s22 = (2.0*vy - 2.0/3.0*div) * Amu;
+    double s33 = (2.0*wz - 2.0/3.0*div) * Amu;
+    double s12 = (uy + vx) * Amu;
+    double s13 = (uz + wx) * Amu;
+    double s23 = (vz + wy) * Amu;
+    double uu = p.prim[1][o], vv = p.prim[2][o], ww = p.prim[3][o];
+    double Amuk = Amu * p.vis_c;
+    double Tx = Tk*Akx + Ti*Aix + Ts*Asx;
+    double Ty = Tk*Aky + Ti*Aiy + Ts*Asy;
+    double Tz = Tk*Akz + Ti*Aiz + Ts*Asz;
+    double E1 = uu*s11 + vv*s12 + ww*s13 + Amuk*Tx;
+    double E2 = uu*s12 + vv*s22 + ww*s23 + Amuk*Ty;
+    double E3 = uu*s13 + vv*s23 + ww*s33 + Amuk*Tz;
+    double Aj1 = p.met[M_AJAC][o];
+#pragma unroll
+    for (int dd = 0; dd < 3; dd++) {
+        double akx = p.met[M_AKX + 3 * dd][o] * Aj1;
+        double aky = p.met[M_AKX + 3 * dd + 1][o] * Aj1;
+        double akz = p.met[M_AKX + 3 * dd + 2][o] * Aj1;
+        double *ev = p.ev + (long long)(4 * dd) * p.lapN;
+        ev[o]              = (akx*s11 + aky*s12 + akz*s13);
+        ev[p.lapN + o]     = (akx*s12 + aky*s22 + akz*s23);
+        ev[2 * p.lapN + o] = (akx*s13 + aky*s23 + akz*s33);
+        ev[3 * p.lapN + o] = (akx*E1  + aky*E2  + akz*E3);
+    }
+}
+
+// du[1..4] += Ajac * d(Ev)/d(xi) for x, then y, then z
+// (du_viscous_Jacobian3d_{x,y,z}_final + YF_Pe_XF, src/commen_kernel.cu:158-169)
+__global__ void k_vis_div(Params p) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    int i = (int)(tid % p.nx); long long r = tid / p.nx;
+    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+    const long long st[3] = { 1LL, p.ys, p.zs };
+    const double hh[3] = { p.hx, p.hy, p.hz };
+    const bool c8 = p.scheme_vis == 204;
+    double ajac = p.met[M_AJAC][o];
+    double acc[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) acc[m] = p.du[(m + 1) * p.N + tid];
+#pragma unroll
+    for (int dd = 0; dd < 3; dd++) {
+        long long s = st[dd];
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const double *f = p.ev + (long long)(4 * dd + m) * p.lapN;
+            double t;
+            if (c8) t = cd8(f[o - 4 * s], f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s], f[o + 4 * s]);
+            else    t = cd6(f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s]);
+            acc[m] += ajac * (t / hh[dd]);
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 4; m++) p.du[(m + 1) * p.N + tid] = acc[m];
+}
+
+// ---------------------------------------------------------------------------
+// RK stage (src/OCFD_time.cu:44-94) + cons_to_pri (src/commen_kernel.cu:77-109)
+// + face re-projection pri_to_cons on the six faces (src/OCFD_boundary.cu:40-91)
+// ---------------------------------------------------------------------------
+__global__ void k_rk_update(Params p, int krk) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    int i = (int)(tid % p.nx); long long r = tid / p.nx;
+    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    const long long N = p.N;
+    double f[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+        double fn = p.fn[m * N + tid], du = p.du[m * N + tid];
+        if (krk == 1) {
+            f[m] = fn + p.dt * du;
+        } else if (krk == 2) {
+            double t1 = 3.0 / 4.0, t2 = 1.0 / 4.0;
+            f[m] = t1 * fn + t2 * (p.f[m * N + tid] + p.dt * du);
+        } else {
+            double t1 = 1.0 / 3.0, t2 = 2.0 / 3.0;
+            f[m] = t1 * fn + t2 * (p.f[m * N + tid] + p.dt * du);
+        }
+    }
+    double d1 = f[0];
+    double u1 = f[1] / d1;
+    double v1 = f[2] / d1;
+    double w1 = f[3] / d1;
+    double T2 = (f[4] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1)) / (d1 * p.Cv);
+    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+    p.prim[0][o] = d1; p.prim[1][o] = u1; p.prim[2][o] = v1; p.prim[3][o] = w1; p.prim[4][o] = T2;
+    bool face = (i == 0) || (i == p.nx - 1) || (j == 0) || (j == p.ny - 1) || (k == 0) || (k == p.nz - 1);
+    if (face) {
+        f[0] = d1;
+        f[1] = u1 * d1;
+        f[2] = v1 * d1;
+        f[3] = w1 * d1;
+        f[4] = d1 * ((u1 * u1 + v1 * v1 + w1 * w1) * 0.5 + p.Cv * T2);
+    }
+#pragma unroll
+    for (int m = 0; m < 5; m++) p.f[m * N + tid] = f[m];
+}
+
+// Unfused pieces of the same update for the reference-named per-stage API:
+// RK stage only, cons->prim only, face re-projection only.
+__global__ void k_rk_only(Params p, int krk) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= 5 * p.N) return;
+    double fn = p.fn[tid], du = p.du[tid];
+    if (krk == 1) p.f[tid] = fn + p.dt * du;
+    else if (krk == 2) { double t1 = 3.0 / 4.0, t2 = 1.0 / 4.0; p.f[tid] = t1 * fn + t2 * (p.f[tid] + p.dt * du); }
+    else { double t1 = 1.0 / 3.0, t2 = 2.0 / 3.0; p.f[tid] = t1 * fn + t2 * (p.f[tid] + p.dt * du); }
+}
+__global__ void k_c2p(Params p) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    int i = (int)(tid % p.nx); long long r = tid / p.nx;
+    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    const long long N = p.N;
+    double d1 = p.f[tid];
+    double u1 = p.f[N + tid] / d1;
+    double v1 = p.f[2 * N + tid] / d1;
+    double w1 = p.f[3 * N + tid] / d1;
+    double T2 = (p.f[4 * N + tid] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1)) / (d1 * p.Cv);
+    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+    p.prim[0][o] = d1; p.prim[1][o] = u1; p.prim[2][o] = v1; p.prim[3][o] = w1; p.prim[4][o] = T2;
+}
+__global__ void k_bc_faces(Params p) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    int i = (int)(tid % p.nx); long long r = tid / p.nx;
+    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    bool face = (i == 0) || (i == p.nx - 1) || (j == 0) || (j == p.ny - 1) || (k == 0) || (k == p.nz - 1);
+    if (!face) return;
+    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+    double d = p.prim[0][o], u = p.prim[1][o], v = p.prim[2][o], w = p.prim[3][o], T = p.prim[4][o];
+    const long long N = p.N;
+    p.f[tid] = d;
+    p.f[N + tid] = u * d;
+    p.f[2 * N + tid] = v * d;
+    p.f[3 * N + tid] = w * d;
+    p.f[4 * N + tid] = d * ((u * u + v * v + w * w) * 0.5 + p.Cv * T);
+}
+
+// pri_to_cons over the interior (init, src/OCFD_init.cu:108-115)
+__global__ void k_p2c(Params p, double *out) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    int i = (int)(tid % p.nx); long long r = tid / p.nx;
+    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+    double d = p.prim[0][o], u = p.prim[1][o], v = p.prim[2][o], w = p.prim[3][o], T = p.prim[4][o];
+    const long long N = p.N;
+    out[tid] = d;
+    out[N + tid] = u * d;
+    out[2 * N + tid] = v * d;
+    out[3 * N + tid] = w * d;
+    out[4 * N + tid] = d * ((u * u + v * v + w * w) * 0.5 + p.Cv * T);
+}
+
+// interior <-> LAP-box copy of one field (dense [nz][ny][nx] <-> LAP box)
+__global__ void k_scatter_interior(Params p, const double *src, double *dst_lap) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    int i = (int)(tid % p.nx); long long r = tid / p.nx;
+    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    dst_lap[lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP)] = src[tid];
+}
+__global__ void k_gather_interior(Params p, const double *src_lap, double *dst) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    int i = (int)(tid % p.nx); long long r = tid / p.nx;
+    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    dst[tid] = src_lap[lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP)];
+}
+__global__ void k_fill(double *f, long long n, double v) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid < n) f[tid] = v;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static inline unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+template <int DIR>
+static cudaError_t launch_sweep(const Params &p, cudaStream_t st) {
+    using S = SweepShape<DIR>;
+    constexpr int NP = (S::TS + 8) * S::R, NF = (S::TS + 1) * S::R;
+    size_t smem = sizeof(double) * (10 * NP + 10 * NF);
+    int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
+    int nr = DIR == 0 ? p.ny : p.nx;
+    int n3 = DIR == 2 ? p.ny : p.nz;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_sweep<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set = true;
+    }
+    dim3 grid((n + S::TS - 1) / S::TS, (nr + S::R - 1) / S::R, n3);
+    k_sweep<DIR><<<grid, S::THREADS, smem, st>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sensor(const Params &p, cudaStream_t st) {
+    long long n = (long long)(p.nx + 1) * p.ny * p.nz + (long long)p.nx * (p.ny + 1) * p.nz
+                + (long long)p.nx * p.ny * (p.nz + 1);
+    k_sensor<<<blocks_for(n, 256), 256, 0, st>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ghost(const Params &p, double *const *fields, const int *dirmask, int nf, cudaStream_t st) {
+    GhostList g;
+    g.n = nf;
+    for (int i = 0; i < nf; i++) { g.f[i] = fields[i]; g.dirmask[i] = dirmask[i]; }
+    long long per = 2LL * OCFD_LAP * ((long long)p.ny * p.nz + (long long)p.nx * p.nz + (long long)p.nx * p.ny);
+    k_ghost<<<blocks_for(per * nf, 256), 256, 0, st>>>(p, g);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweeps(const Params &p, cudaStream_t st) {
+    cudaError_t e;
+    if ((e = launch_sweep<0>(p, st)) != cudaSuccess) return e;
+    if ((e = launch_sweep<1>(p, st)) != cudaSuccess) return e;
+    return launch_sweep<2>(p, st);
+}
+
+cudaError_t launch_viscous(const Params &p, cudaStream_t st) {
+    unsigned nb = blocks_for(p.N, 256);
+    k_vis_grad<<<nb, 256, 0, st>>>(p);
+    k_vis_ev<<<nb, 256, 0, st>>>(p);
+    double *evf[12]; int mask[12];
+    for (int dd = 0; dd < 3; dd++)
+        for (int m = 0; m < 4; m++) { evf[4 * dd + m] = p.ev + (long long)(4 * dd + m) * p.lapN; mask[4 * dd + m] = 1 << dd; }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if ((e = launch_ghost(p, evf, mask, 12, st)) != cudaSuccess) return e;
+    k_vis_div<<<nb, 256, 0, st>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rk(const Params &p, int krk, cudaStream_t st) {
+    k_rk_update<<<blocks_for(p.N, 256), 256, 0, st>>>(p, krk);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_p2c(const Params &p, double *out, cudaStream_t st) {
+    k_p2c<<<blocks_for(p.N, 256), 256, 0, st>>>(p, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(const Params &p, const double *src, double *dst_lap, cudaStream_t st) {
+    k_scatter_interior<<<blocks_for(p.N, 256), 256, 0, st>>>(p, src, dst_lap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather(const Params &p, const double *src_lap, double *dst, cudaStream_t st) {
+    k_gather_interior<<<blocks_for(p.N, 256), 256, 0, st>>>(p, src_lap, dst);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill(double *f, long long n, double v, cudaStream_t st) {
+    k_fill<<<blocks_for(n, 256), 256, 0, st>>>(f, n, v);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rk_only(const Params &p, int krk, cudaStream_t st) {
+    k_rk_only<<<blocks_for(5 * p.N, 256), 256, 0, st>>>(p, krk);
+    return cudaGetLastError();
+}
+cudaError_t launch_c2p(const Params &p, cudaStream_t st) {
+    k_c2p<<<blocks_for(p.N, 256), 256, 0, st>>>(p);
+    return cudaGetLastError();
+}
+cudaError_t launch_bc_faces(const Params &p, cudaStream_t st) {
+    k_bc_faces<<<blocks_for(p.N, 256), 256, 0, st>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace ocfd

@@ -1,0 +1,285 @@
+"""ctypes binding of libocfd_b200.so (include/ocfd_b200.h).
+
+The library is the product; this module only marshals numpy arrays (host)
+or raw device pointers across the C ABI.  Loading fails loudly when the
+shared object is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+from .formats import CaseConfig
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))   # opencfd-scu_b200/
+LIB_PATH = os.path.join(PKG_DIR, "libocfd_b200.so")
+
+OCFD_OK = 0
+STATUS = {0: "ok", -1: "invalid argument", -2: "unsupported configuration", -3: "CUDA error",
+          -4: "device out of memory", -5: "call out of order", -6: "no CUDA device"}
+TIMER_COUNT = 8
+
+# every function the header declares (the non-GPU tests check the exports)
+EXPORTED = (
+    "ocfd_b200_abi_version", "ocfd_b200_status_string", "ocfd_b200_last_error",
+    "ocfd_b200_create", "ocfd_b200_destroy", "ocfd_b200_set_stream", "ocfd_b200_get_stream",
+    "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
+    "ocfd_b200_set_primitives", "ocfd_b200_set_primitives_device", "ocfd_b200_step",
+    "ocfd_b200_advance_host", "ocfd_b200_swap_time_levels", "ocfd_b200_du_comput",
+    "ocfd_b200_time_advance", "ocfd_b200_get_duvwT", "ocfd_b200_bc",
+    "ocfd_b200_get_primitives", "ocfd_b200_get_primitives_device", "ocfd_b200_get_conserved",
+    "ocfd_b200_get_du", "ocfd_b200_get_flags", "ocfd_b200_get_time", "ocfd_b200_set_timing",
+    "ocfd_b200_get_timing", "ocfd_b200_timer_name", "ocfd_b200_launch_count",
+    "ocfd_b200_compat_bind", "du_comput", "OCFD_time_advance", "get_duvwT", "get_Amu",
+    "OCFD_bc", "Set_Scheme_HybridAuto",
+)
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("iperiodic", ctypes.c_int * 3),
+        ("jac_bound", ctypes.c_int * 3),
+        ("dif_bound", ctypes.c_int * 6),
+        ("non_reflection", ctypes.c_int * 6),
+        ("scheme_invis", ctypes.c_int),
+        ("scheme_vis", ctypes.c_int),
+        ("charteric", ctypes.c_int),
+        ("hy_style", ctypes.c_int),
+        ("hy_dp_intv", ctypes.c_double * 2),
+        ("re", ctypes.c_double), ("ama", ctypes.c_double), ("gamma", ctypes.c_double),
+        ("pr", ctypes.c_double), ("t_ref", ctypes.c_double), ("epsl_sw", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("device", ctypes.c_int),
+    ]
+
+
+class OcfdError(RuntimeError):
+    def __init__(self, status: int, what: str, detail: str = ""):
+        super().__init__(f"{what}: {STATUS.get(status, status)} {detail}".strip())
+        self.status = status
+
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", PKG_DIR], check=True)
+    return LIB_PATH
+
+
+def load(path: Optional[str] = None):
+    """Load the shared library (never builds implicitly on a GPU box)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise OSError(f"{path} not found: build it with `make -C opencfd-scu_b200` "
+                      "(the CUDA library is required; there is no CPU fallback)")
+    L = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    D = ctypes.POINTER(ctypes.c_double)
+    I8 = ctypes.POINTER(ctypes.c_int8)
+    sig = {
+        "ocfd_b200_abi_version": (ctypes.c_int, []),
+        "ocfd_b200_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+        "ocfd_b200_last_error": (ctypes.c_char_p, [P]),
+        "ocfd_b200_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(P)]),
+        "ocfd_b200_destroy": (ctypes.c_int, [P]),
+        "ocfd_b200_set_stream": (ctypes.c_int, [P, P]),
+        "ocfd_b200_get_stream": (P, [P]),
+        "ocfd_b200_synchronize": (ctypes.c_int, [P]),
+        "ocfd_b200_set_metrics": (ctypes.c_int, [P, D]),
+        "ocfd_b200_set_metrics_device": (ctypes.c_int, [P, P]),
+        "ocfd_b200_set_primitives": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_double]),
+        "ocfd_b200_set_primitives_device": (ctypes.c_int, [P, P, ctypes.c_int, ctypes.c_double]),
+        "ocfd_b200_step": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_advance_host": (ctypes.c_int, [P, D, D, ctypes.c_int]),
+        "ocfd_b200_swap_time_levels": (ctypes.c_int, [P]),
+        "ocfd_b200_du_comput": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_time_advance": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_get_duvwT": (ctypes.c_int, [P]),
+        "ocfd_b200_bc": (ctypes.c_int, [P]),
+        "ocfd_b200_get_primitives": (ctypes.c_int, [P, D]),
+        "ocfd_b200_get_primitives_device": (ctypes.c_int, [P, P]),
+        "ocfd_b200_get_conserved": (ctypes.c_int, [P, D]),
+        "ocfd_b200_get_du": (ctypes.c_int, [P, D]),
+        "ocfd_b200_get_flags": (ctypes.c_int, [P, I8, I8, I8]),
+        "ocfd_b200_get_time": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_int), D]),
+        "ocfd_b200_set_timing": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_get_timing": (ctypes.c_int, [P, D, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
+        "ocfd_b200_timer_name": (ctypes.c_char_p, [ctypes.c_int]),
+        "ocfd_b200_launch_count": (ctypes.c_longlong, [P]),
+        "ocfd_b200_compat_bind": (ctypes.c_int, [P]),
+        "du_comput": (None, [ctypes.c_int]),
+        "OCFD_time_advance": (None, [ctypes.c_int]),
+        "get_duvwT": (None, []),
+        "get_Amu": (None, []),
+        "OCFD_bc": (None, []),
+        "Set_Scheme_HybridAuto": (None, [P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def make_config(cfg: CaseConfig, device: int = 0) -> Config:
+    c = Config()
+    c.nx, c.ny, c.nz = cfg.nx, cfg.ny, cfg.nz
+    c.iperiodic[:] = list(cfg.iperiodic)
+    c.jac_bound[:] = list(cfg.jac_bound)
+    c.dif_bound[:] = list(cfg.dif_bound)
+    c.non_reflection[:] = list(cfg.non_ref)
+    c.scheme_invis = cfg.scheme_invis_id
+    c.scheme_vis = cfg.scheme_vis_id
+    c.charteric = cfg.charteric
+    c.hy_style = cfg.hy_style
+    c.hy_dp_intv[:] = list(cfg.hy_dp_intv)
+    c.re, c.ama, c.gamma, c.pr = cfg.re, cfg.ama, cfg.gamma, cfg.pr
+    c.t_ref, c.epsl_sw, c.dt = cfg.t_ref, cfg.epsl_sw, cfg.dt
+    c.device = device
+    return c
+
+
+class Solver:
+    """One B200 solver context.  Same call surface as the reference driver."""
+
+    def __init__(self, cfg: CaseConfig, prims: Optional[Sequence[np.ndarray]] = None,
+                 metrics: Optional[Sequence[np.ndarray]] = None, device: int = 0,
+                 istep: int = 0, tt: float = 0.0):
+        self.L = load()
+        self.cfg = cfg
+        self.shape = (cfg.nz, cfg.ny, cfg.nx)
+        self._c = make_config(cfg, device)
+        h = ctypes.c_void_p()
+        rc = self.L.ocfd_b200_create(ctypes.byref(self._c), ctypes.byref(h))
+        if rc != OCFD_OK:
+            raise OcfdError(rc, "ocfd_b200_create", (self.L.ocfd_b200_last_error(None) or b"").decode())
+        self.h = h
+        if metrics is not None:
+            self.set_metrics(metrics)
+        if prims is not None:
+            self.set_primitives(prims, istep, tt)
+
+    def _check(self, rc: int, what: str):
+        if rc != OCFD_OK:
+            raise OcfdError(rc, what, (self.L.ocfd_b200_last_error(self.h) or b"").decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ocfd_b200_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # set-up -----------------------------------------------------------
+    def set_metrics(self, metrics: Sequence[np.ndarray]):
+        a = np.ascontiguousarray(np.stack([np.asarray(m, np.float64) for m in metrics]))
+        if a.shape != (13,) + self.shape:
+            raise ValueError(f"metrics shape {a.shape} != {(13,) + self.shape}")
+        self._check(self.L.ocfd_b200_set_metrics(self.h, _dp(a)), "set_metrics")
+
+    def set_primitives(self, prims: Sequence[np.ndarray], istep: int = 0, tt: float = 0.0):
+        a = np.ascontiguousarray(np.stack([np.asarray(p, np.float64) for p in prims]))
+        if a.shape != (5,) + self.shape:
+            raise ValueError(f"primitives shape {a.shape} != {(5,) + self.shape}")
+        self._check(self.L.ocfd_b200_set_primitives(self.h, _dp(a), istep, tt), "set_primitives")
+
+    def set_primitives_device(self, ptr: int, istep: int = 0, tt: float = 0.0):
+        self._check(self.L.ocfd_b200_set_primitives_device(self.h, ctypes.c_void_p(ptr), istep, tt),
+                    "set_primitives_device")
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        self._check(self.L.ocfd_b200_set_stream(self.h, ctypes.c_void_p(stream_ptr or 0)), "set_stream")
+
+    # stepping ---------------------------------------------------------
+    def step(self, n: int = 1):
+        self._check(self.L.ocfd_b200_step(self.h, n), "step")
+
+    def synchronize(self):
+        self._check(self.L.ocfd_b200_synchronize(self.h), "synchronize")
+
+    def advance_host(self, prims_in: np.ndarray, prims_out: np.ndarray, n: int):
+        self._check(self.L.ocfd_b200_advance_host(self.h, _dp(prims_in), _dp(prims_out), n),
+                    "advance_host")
+
+    def swap(self):
+        self._check(self.L.ocfd_b200_swap_time_levels(self.h), "swap")
+
+    def du_comput(self, krk: int):
+        self._check(self.L.ocfd_b200_du_comput(self.h, krk), "du_comput")
+
+    def time_advance(self, krk: int):
+        self._check(self.L.ocfd_b200_time_advance(self.h, krk), "time_advance")
+
+    def get_duvwT(self):
+        self._check(self.L.ocfd_b200_get_duvwT(self.h), "get_duvwT")
+
+    def bc(self):
+        self._check(self.L.ocfd_b200_bc(self.h), "bc")
+
+    # read-back --------------------------------------------------------
+    def _get5(self, fn, what) -> np.ndarray:
+        out = np.empty((5,) + self.shape, dtype=np.float64)
+        self._check(fn(self.h, _dp(out)), what)
+        return out
+
+    def primitives(self) -> np.ndarray:
+        return self._get5(self.L.ocfd_b200_get_primitives, "get_primitives")
+
+    def conserved(self) -> np.ndarray:
+        return self._get5(self.L.ocfd_b200_get_conserved, "get_conserved")
+
+    def du(self) -> np.ndarray:
+        return self._get5(self.L.ocfd_b200_get_du, "get_du")
+
+    def flags(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        nz, ny, nx = self.shape
+        fx = np.empty((nz, ny, nx + 1), dtype=np.int8)
+        fy = np.empty((nz, ny + 1, nx), dtype=np.int8)
+        fz = np.empty((nz + 1, ny, nx), dtype=np.int8)
+        I8 = ctypes.POINTER(ctypes.c_int8)
+        self._check(self.L.ocfd_b200_get_flags(self.h, fx.ctypes.data_as(I8), fy.ctypes.data_as(I8),
+                                               fz.ctypes.data_as(I8)), "get_flags")
+        return fx, fy, fz
+
+    def time(self) -> Tuple[int, float]:
+        i = ctypes.c_int()
+        t = ctypes.c_double()
+        self._check(self.L.ocfd_b200_get_time(self.h, ctypes.byref(i), ctypes.byref(t)), "get_time")
+        return i.value, t.value
+
+    # timing -----------------------------------------------------------
+    def set_timing(self, on: bool):
+        self._check(self.L.ocfd_b200_set_timing(self.h, int(on)), "set_timing")
+
+    def timing(self):
+        ms = (ctypes.c_double * TIMER_COUNT)()
+        n = (ctypes.c_longlong * TIMER_COUNT)()
+        self._check(self.L.ocfd_b200_get_timing(self.h, ms, n, TIMER_COUNT), "get_timing")
+        out = {}
+        for i in range(TIMER_COUNT):
+            name = self.L.ocfd_b200_timer_name(i).decode()
+            if name != "-":
+                out[name] = (ms[i], n[i])
+        return out
+
+    def launch_count(self) -> int:
+        return int(self.L.ocfd_b200_launch_count(self.h))

@@ -1,0 +1,83 @@
+"""Run the reference's own CUDA build (oracle/_ref/opencfd-scu.out) on a case.
+
+TEST / BENCH INFRASTRUCTURE ONLY.  The binary is compiled from the reference
+sources by oracle/ref.mk; this module only writes the reference's input files
+(opencfd-scu.in, opencfd.dat, OCFD3d-Jacobi.dat), runs it in a scratch
+directory and parses what it prints or saves.
+"""
+from __future__ import annotations
+
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+from typing import Optional, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+REF_BIN = os.path.join(HERE, "_ref", "opencfd-scu.out")
+
+sys.path.insert(0, os.path.join(ROOT, "opencfd-scu_b200"))
+from ocfd_b200 import formats  # noqa: E402
+
+
+def available() -> bool:
+    return os.path.exists(REF_BIN) and os.access(REF_BIN, os.X_OK)
+
+
+def _write_inputs(case, workdir: str) -> None:
+    formats.write_config(os.path.join(workdir, "opencfd-scu.in"), case.cfg)
+    formats.write_field_file(os.path.join(workdir, "opencfd.dat"), case.prims, 0, 0.0)
+    formats.write_metric_file(os.path.join(workdir, "OCFD3d-Jacobi.dat"), case.metrics)
+
+
+def run_and_read(case, nsteps: int, timeout: float = 900.0):
+    """Run nsteps steps and return (prims[5,nz,ny,nx], Istep, tt, wall_s, stdout)."""
+    cfg = case.cfg
+    cfg.set_steps(nsteps)
+    cfg.kstep_save = nsteps
+    cfg.kstep_show = 10 ** 8
+    wd = tempfile.mkdtemp(prefix="ocfd_ref_")
+    try:
+        _write_inputs(case, wd)
+        t0 = time.time()
+        p = subprocess.run([REF_BIN], cwd=wd, capture_output=True, text=True, timeout=timeout)
+        wall = time.time() - t0
+        if p.returncode != 0:
+            raise RuntimeError(f"reference exited {p.returncode}:\n{p.stdout[-3000:]}\n{p.stderr[-3000:]}")
+        fields, istep, tt = formats.read_field_file(os.path.join(wd, "OCFD%08d.dat" % nsteps),
+                                                    case.shape)
+        return np.stack(fields), istep, tt, wall, p.stdout
+    finally:
+        shutil.rmtree(wd, ignore_errors=True)
+
+
+_INTERVAL = re.compile(r"^(\d+) steps GPU time ([0-9.eE+-]+)", re.M)
+
+
+def time_steps(case, warmup: int, steps: int, timeout: float = 1800.0) -> Tuple[float, str]:
+    """Seconds for `steps` RK3 steps after `warmup` steps, from the reference's
+    own MPI_Wtime interval print (src/OCFD_NS_Solver.cu:104-153).  The show
+    interval is `steps`; warmup is rounded up to a multiple of it."""
+    cfg = case.cfg
+    nwarm = max(1, -(-warmup // steps)) * steps
+    cfg.set_steps(nwarm + steps)
+    cfg.kstep_show = steps
+    cfg.kstep_save = 10 ** 8
+    wd = tempfile.mkdtemp(prefix="ocfd_ref_")
+    try:
+        _write_inputs(case, wd)
+        p = subprocess.run([REF_BIN], cwd=wd, capture_output=True, text=True, timeout=timeout)
+        if p.returncode != 0:
+            raise RuntimeError(f"reference exited {p.returncode}:\n{p.stdout[-3000:]}\n{p.stderr[-3000:]}")
+        m = _INTERVAL.findall(p.stdout)
+        if not m:
+            raise RuntimeError("no interval timing in reference output:\n" + p.stdout[-3000:])
+        return float(m[-1][1]), p.stdout
+    finally:
+        shutil.rmtree(wd, ignore_errors=True)

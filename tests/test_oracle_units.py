@@ -1,0 +1,126 @@
+"""Unit checks of the CPU oracle's point formulas (the checker itself).
+
+Exactness properties of the reference schemes (src/OCFD_Schemes.cu) on
+polynomial data, the Steger-Warming split identity (src/OCFD_split.cu), and
+L*R = I for the characteristic matrices (src/OCFD_flux_charteric.cu).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as oro
+
+
+def _poly_cells(coef, x):
+    return sum(c * x**k for k, c in enumerate(coef))
+
+
+def _flux_diff(name, coef, sign, args=()):
+    """(F(i+1/2) - F(i-1/2)) at i = 0 on a unit grid from point values f(x_j)."""
+    h = 1.0
+    xs = np.arange(-8, 9) * h
+    f = _poly_cells(coef, xs)
+    off = 8
+
+    def face(F):
+        s8 = f[off + F - 3: off + F + 5]
+        if name in ("weno7_p", "up7_p", "omp6_p", "weno7_symbo_p"):
+            return oro.point(name, s8, *args)
+        if name == "weno5_p":
+            return oro.point(name, s8[1:6], *args)
+        if name == "weno7_m":
+            return oro.point(name, s8[1:8], *args)
+        if name == "weno5_m":
+            return oro.point(name, s8[2:7], *args)
+        if name in ("up7_m", "omp6_m", "weno7_symbo_m"):
+            return oro.point(name, s8, *args)
+        raise KeyError(name)
+    return face(0) - face(-1)
+
+
+def _exact_derivative(coef):
+    return coef[1] if len(coef) > 1 else 0.0
+
+
+@pytest.mark.parametrize("name,deg", [("up7_p", 7), ("up7_m", 7), ("weno7_p", 3), ("weno7_m", 3),
+                                      ("weno5_p", 2), ("weno5_m", 2)])
+def test_scheme_polynomial_exactness(name, deg):
+    rng = np.random.default_rng(deg)
+    for trial in range(5):
+        coef = list(rng.uniform(-1, 1, size=deg + 1) * 1e-2)
+        got = _flux_diff(name, coef, 0)
+        assert abs(got - _exact_derivative(coef)) < 1e-12, (name, coef, got)
+
+
+def test_weno7_smooth_order():
+    # on a smooth sine the WENO7 face difference converges at high order
+    errs = []
+    for n in (16, 32, 64):
+        h = 2 * math.pi / n
+        xs = np.arange(-8, 9) * h + 0.3
+        f = np.sin(xs)
+        s = lambda F: oro.point("weno7_p", f[8 + F - 3: 8 + F + 4])
+        d = (s(0) - s(-1)) / h
+        errs.append(abs(d - math.cos(0.3)))
+    assert errs[2] < errs[1] < errs[0]
+    assert errs[1] / errs[2] > 30   # better than 5th order on this range
+
+
+@pytest.mark.parametrize("name,n,deg", [("cd6", 7, 6), ("cd8", 9, 8)])
+def test_central_derivative_exactness(name, n, deg):
+    rng = np.random.default_rng(n)
+    half = n // 2
+    xs = np.arange(-half, half + 1, dtype=float)
+    for _ in range(5):
+        coef = rng.uniform(-1, 1, size=deg + 1)
+        f = _poly_cells(coef, xs)
+        assert abs(oro.point(name, f) - coef[1]) < 1e-10
+
+
+def test_steger_warming_split_identity():
+    rng = np.random.default_rng(3)
+    gamma, ama = 1.4, 0.5
+    for _ in range(20):
+        d = rng.uniform(0.5, 2.0)
+        u, v, w = rng.uniform(-1, 1, size=3)
+        T = rng.uniform(0.5, 2.0)
+        c = math.sqrt(T) / ama
+        A = rng.uniform(-2, 2, size=3)
+        out = oro.sw_split(d, u, v, w, c, *A, gamma=gamma, eps=0.0)
+        fsum = out[:5] + out[5:]
+        U = A @ np.array([u, v, w])
+        p = d * c * c / gamma
+        E = p / (gamma - 1) + 0.5 * d * (u * u + v * v + w * w)
+        exact = np.array([d * U, d * u * U + p * A[0], d * v * U + p * A[1],
+                          d * w * U + p * A[2], (E + p) * U])
+        assert np.allclose(fsum, exact, rtol=1e-12, atol=1e-12)
+
+
+def test_split_upwinding_signs():
+    # supersonic to the right: all flux in f+, none in f-
+    gamma, ama = 1.4, 1.0
+    out = oro.sw_split(1.0, 3.0, 0.0, 0.0, 1.0, 1.0, 0.0, 0.0, gamma=gamma, eps=0.0)
+    assert np.all(np.abs(out[5:]) < 1e-15)
+
+
+def test_characteristic_matrices_are_inverse():
+    rng = np.random.default_rng(5)
+    for _ in range(20):
+        u, v, w = rng.uniform(-1, 1, size=3)
+        c = rng.uniform(0.5, 3.0)
+        A = rng.uniform(-2, 2, size=3)
+        L, R = oro.char_matrices(u, v, w, c, *A, gamma=1.4)
+        assert np.allclose(L @ R, np.eye(5), atol=1e-12)
+
+
+def test_symbo_limiter_linear_branch_p_only():
+    # a linear ramp has equal total variation in every substencil: the
+    # limited positive side takes the linear weights, the negative side
+    # never does (its TVmin is never computed in the reference)
+    s = np.linspace(0, 0.07, 8)
+    lp = oro.point("weno7_symbo_p", s, 1, 5.0, 0.2)
+    np_ = oro.point("weno7_symbo_p", s, 0, 5.0, 0.2)
+    assert np.isfinite(lp) and np.isfinite(np_)
+    # linear data: every candidate stencil is exact, so both give the face value
+    assert abs(lp - np_) < 1e-12
