@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the per-RK-stage RHS path on B200.
+
+Workload (default): decaying compressible isotropic turbulence on a 256^3
+periodic grid, SCHEME_HYBRIDAUTO (style 2 Jameson sensor: UP7 / WENO7 /
+WENO5) with characteristic projection, CD6 viscous terms, SSP-RK3, plain
+FP64.  Synthetic, seeded input (no dataset).  One "step" is one RK3 time
+step (3 stages) over the whole grid.
+
+Metric: Gcell-RK-stage/s = cells x 3 x steps / seconds / 1e9.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank runs an independent replica of the same
+grid on its own GPU (the path has no exchange step on one grid per GPU);
+value = all ranks' cell-stages / max-over-ranks time ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "opencfd-scu_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Gcell-RK-stage/s"
+B_ALG = 120.0          # algorithmic bytes per cell-stage (read U^k, U^n, write U^k+1; FP64)
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"ocfd_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def make_case(n: int):
+    from ocfd_b200 import cases
+    return cases.isotropic_turbulence(n, seed=2024, charteric=1)
+
+
+def cpu_baseline(n_sample: int = 64, steps: int = 1):
+    """The OpenMP FP64 oracle timed on this host on a bounded sample."""
+    from oracle.oracle import Oracle
+    c = make_case(n_sample)
+    cores = os.cpu_count() or 1
+    o = Oracle(c.cfg, c.prims, c.metrics, nthreads=cores)
+    o.step(1)                                   # warm-up
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    v = n_sample ** 3 * 3 * steps / dt / 1e9
+    return {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+            "sample": f"{steps} RK3 step(s) of the same case at {n_sample}^3 "
+                      f"(OpenMP FP64 oracle, {cores} threads, {dt:.2f} s)"}
+
+
+def max_over_ranks(x: float, dist, device=None) -> float:
+    """Max of a per-rank float over all ranks (the slowest replica sets the
+    time); works for the nccl (device tensor) and gloo (CPU tensor) groups."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(cells: int, stages: int, seconds_max: float, world: int) -> float:
+    """Whole-job Gcell-RK-stage/s: every replica processes `cells` x `stages`."""
+    return world * cells * stages / seconds_max / 1e9
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+    from ocfd_b200 import lib
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    n = args.n
+    case = make_case(n)
+    solver = lib.Solver(case.cfg, case.prims, case.metrics, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    solver.set_stream(stream.cuda_stream)
+    cells = n ** 3
+
+    # warm-up
+    solver.step(args.warmup)
+    solver.synchronize()
+
+    # per-kernel timing pass (untimed region): device time per family
+    solver.set_timing(True)
+    solver.step(1)
+    solver.synchronize()
+    fam = solver.timing()
+    solver.set_timing(False)
+
+    # timed region
+    sampler = ClockSampler(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    l0 = solver.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    solver.step(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    launches = solver.launch_count() - l0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, dist, f"cuda:{dev}")
+    value = aggregate_rate(cells, 3 * args.steps, ms_max / 1e3, world)
+
+    # end to end through the C ABI with host buffers (pinned), one RK3 step
+    # per call: H2D of the primitives, the step, D2H of the primitives
+    shape = (5, n, n, n)
+    hin = torch.empty(shape, dtype=torch.float64).pin_memory()
+    hout = torch.empty(shape, dtype=torch.float64).pin_memory()
+    a_in = hin.numpy()
+    a_in[:] = np.stack(case.prims)
+    a_out = hout.numpy()
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    solver.advance_host(a_in, a_out, 1)        # warm-up of the path
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        solver.advance_host(a_in, a_out, 1)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{dev}")
+    e2e_val = aggregate_rate(cells, 3 * e2e_steps, e2e_s, world)
+    nbytes = 5 * cells * 8
+
+    if rank != 0:
+        return None
+    hbm, peak_kind = peaks()
+    # dominant kernel family and its roofline (HBM, algorithmic bytes)
+    fam_ms = {k: v[0] / max(v[1], 1) for k, v in fam.items() if v[1] > 0}
+    dom = max(fam, key=lambda k: fam[k][0])
+    dom_ms_per_stage = fam[dom][0] / 3.0                  # one step = 3 stages
+    dom_bytes = DOM_BYTES.get(dom, B_ALG) * cells
+    achieved = dom_bytes / (dom_ms_per_stage / 1e3) / 1e9
+    stage_ms = ms_max / args.steps / 3.0
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"isotropic turbulence {n}^3, hybrid UP7/WENO7/WENO5 (Jameson "
+                               f"sensor) + characteristic projection, CD6 viscous, SSP-RK3, plain FP64",
+                   "grid": [n, n, n], "stages_per_step": 3, "scheme": "SCHEME_HYBRIDAUTO style 2, CHARTERIC=1",
+                   "seed": 2024, "l2": "inputs larger than L2 (state ~8 GB/GPU)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None,
+                     "algorithmic_bytes_per_cell": DOM_BYTES.get(dom, B_ALG),
+                     "launch_ms": dom_ms_per_stage},
+        "stage_roofline": {"bytes_per_cell_stage": B_ALG, "achieved_gbs": B_ALG * cells / (stage_ms / 1e3) / 1e9,
+                           "frac": B_ALG * cells / (stage_ms / 1e3) / 1e9 / hbm},
+        "kernel_ms_per_stage": {k: fam[k][0] / 3.0 for k in fam},
+        "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                "steps": e2e_steps, "api": "ocfd_b200_advance_host"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    return line
+
+
+# Algorithmic bytes per cell for one stage's launches of each kernel family
+# (every input and output field touched once, FP64):
+#   inviscid_sweeps: x, y, z sweeps each read d,u,v,w,T + 3 direction metrics
+#                    + Ajac (9 fields); x writes du (5), y and z read and write
+#                    du (10 each)                              -> 52 words
+#   viscous: gradients 4 in / 12 out; Ev 12 grads + u,v,w,T + 10 metrics in,
+#            12 out; divergence 12 Ev + Ajac + du[1..4] in, du[1..4] out -> 75 words
+#   rk_update: fn, f, du in, f and d,u,v,w,T out              -> 25 words
+#   sensor: d,T in, three int8 flags out                       -> 19 bytes
+DOM_BYTES = {
+    "inviscid_sweeps": 52 * 8.0,
+    "viscous": 75 * 8.0,
+    "rk_update": 25 * 8.0,
+    "ghost_fill": 0.0,
+    "sensor": 19.0,
+}
+
+
+def run_reference(args, rank, world):
+    """The reference's own CUDA build on the same workload (rank 0 only)."""
+    if rank != 0:
+        return None
+    from oracle import ref_runner
+    n = args.n
+    if not ref_runner.available():
+        c = cpu_baseline(64, 1)
+        return {"impl": "reference", "metric": METRIC, "value": c["value"], "unit": METRIC,
+                "n_gpus": world, "steps": 1, "warmup": 1, "higher_is_better": True,
+                "note": "reference build missing; CPU oracle port timed instead",
+                "cpu_baseline": c, "e2e": {"value": c["value"], "unit": METRIC,
+                                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    case = make_case(n)
+    ref_steps = max(1, min(args.steps, args.ref_steps))
+    secs, out = ref_runner.time_steps(case, args.warmup, ref_steps)
+    v = n ** 3 * 3 * ref_steps / secs / 1e9
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": 1,
+            "steps": ref_steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / ref_steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"isotropic turbulence {n}^3, hybrid + characteristic, CD6, SSP-RK3, FP64",
+                       "grid": [n, n, n], "build": "reference sources, nvcc -O3 sm_100a, single-rank MPI shim",
+                       "timing": "reference's own MPI_Wtime interval print"},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": 1, "kind": "reference",
+                             "sample": f"{ref_steps} steps of the reference CUDA build on 1 B200, "
+                                       f"driven by 1 host thread"},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=256, help="grid points per direction")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--ref-steps", type=int, default=4)
+    ap.add_argument("--cpu-sample", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        dist = tdist
+
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        line = run_ours(args, rank, world, dist)
+        if line is not None and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_sample, 1)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

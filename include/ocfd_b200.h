@@ -81,6 +81,12 @@ int ocfd_b200_synchronize(ocfd_b200_ctx *ctx);
  * (src/OCFD_Comput_Jacobian3d.cu:32-218): ghosts start at 1.0 and are
  * filled periodically in periodic directions. */
 int ocfd_b200_set_metrics(ocfd_b200_ctx *ctx, const double *metrics13);
+/* Metric storage: 0 (default) detects grids whose conservative metrics and
+ * Jacobian are single values and keeps those in registers instead of
+ * reading 10 fields (same arithmetic); 1 always reads the fields.  Takes
+ * effect at the next set_metrics.  uniform_metrics reports the choice. */
+int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode);
+int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx);
 int ocfd_b200_set_metrics_device(ocfd_b200_ctx *ctx, const double *metrics13_dev);
 
 /* Initial primitives d,u,v,w,T (host or device).  Replaces the
@@ -114,6 +120,13 @@ int ocfd_b200_get_conserved(ocfd_b200_ctx *ctx, double *cons5);
 int ocfd_b200_get_du(ocfd_b200_ctx *ctx, double *du5);
 int ocfd_b200_get_flags(ocfd_b200_ctx *ctx, int8_t *flag_x, int8_t *flag_y, int8_t *flag_z);
 int ocfd_b200_get_time(const ocfd_b200_ctx *ctx, int *istep, double *tt);
+
+/* FP64 interior mean of E (which = 0) or T (which = 1); replaces
+ * ana_residual() (src/OCFD_ana.cu:76-105), deterministic on any warp width. */
+int ocfd_b200_ana_residual(ocfd_b200_ctx *ctx, int which, double *mean);
+/* Counts cells with a NaN in d,u,v,w,T and cells with T < 0 (the checks of
+ * ana_NAN_and_NT, src/OCFD_ana.cu:107-222) and returns the mean T. */
+int ocfd_b200_check_state(ocfd_b200_ctx *ctx, long long *n_nan, long long *n_neg_t, double *mean_t);
 
 /* Kernel timing: when enabled, step() brackets each kernel family with CUDA
  * events on the context stream.  get_timing returns accumulated device

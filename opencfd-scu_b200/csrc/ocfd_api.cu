@@ -28,6 +28,9 @@ cudaError_t launch_p2c(const Params &p, double *out, cudaStream_t st);
 cudaError_t launch_scatter(const Params &p, const double *src, double *dst_lap, cudaStream_t st);
 cudaError_t launch_gather(const Params &p, const double *src_lap, double *dst, cudaStream_t st);
 cudaError_t launch_fill(double *f, long long n, double v, cudaStream_t st);
+cudaError_t launch_mean(const Params &p, int which, double *scratch, unsigned long long *counts,
+                        cudaStream_t st);
+int reduce_scratch_doubles();
 }  // namespace ocfd
 
 using ocfd::Params;
@@ -56,9 +59,11 @@ struct ocfd_b200_ctx {
     double *ev_buf = nullptr;     // 12 LAP fields
     int8_t *flag_buf = nullptr;
     double *stage_buf = nullptr;  // 5 interior fields for host transfers
+    double *red_buf = nullptr;    // reduction partials + result, then two counters
     double *pinned = nullptr;     // host staging for advance_host
     size_t pinned_bytes = 0;
     bool have_metrics = false;
+    int metric_mode = 0;          // 0 auto-detect uniform grids, 1 always read the fields
     bool have_state = false;
     int istep = 0;
     double tt = 0.0;
@@ -109,6 +114,7 @@ extern "C" const char *ocfd_b200_last_error(const ocfd_b200_ctx *ctx) {
 static void free_all(ocfd_b200_ctx *c) {
     cudaFree(c->prim_buf); cudaFree(c->met_buf); cudaFree(c->cons_buf);
     cudaFree(c->grad_buf); cudaFree(c->ev_buf); cudaFree(c->flag_buf); cudaFree(c->stage_buf);
+    cudaFree(c->red_buf);
     if (c->pinned) cudaFreeHost(c->pinned);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -194,7 +200,8 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
         (rc = alloc((void **)&ctx->grad_buf, 12 * inB, "gradients")) ||
         (rc = alloc((void **)&ctx->ev_buf, 12 * lapB, "viscous fluxes")) ||
         (rc = alloc((void **)&ctx->flag_buf, flagN, "flags")) ||
-        (rc = alloc((void **)&ctx->stage_buf, 5 * inB, "staging"))) {
+        (rc = alloc((void **)&ctx->stage_buf, 5 * inB, "staging")) ||
+        (rc = alloc((void **)&ctx->red_buf, sizeof(double) * (ocfd::reduce_scratch_doubles() + 2), "reduction"))) {
         g_create_error = ctx->err;
         free_all(ctx);
         delete ctx;
@@ -330,11 +337,37 @@ static int check_ready(ocfd_b200_ctx *ctx) {
 // set-up
 // ---------------------------------------------------------------------------
 
+// A grid whose nine conservative metrics and Jacobian are each one value
+// everywhere (uniform Cartesian) lets the kernels take them from the
+// parameter block; the arithmetic is the same as reading the fields.
+static void detect_uniform(ocfd_b200_ctx *ctx, const double *host13) {
+    Params &p = ctx->p;
+    bool uni = ctx->metric_mode == 0;
+    for (int m = 0; m < 13 && uni; m++) {
+        const double *f = host13 + (size_t)m * p.N;
+        p.mc[m] = f[0];
+        if (m < ocfd::M_AKX) continue;          // coordinates are not read by the RHS
+        for (long long q = 1; q < p.N; q++)
+            if (f[q] != f[0]) { uni = false; break; }
+    }
+    p.uniform_metrics = uni ? 1 : 0;
+}
+
 static int set_metrics_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKind kind) {
     if (!ctx || !src) return OCFD_ERR_ARG;
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     const Params &p = ctx->p;
     size_t inB = sizeof(double) * (size_t)p.N;
+    if (kind == cudaMemcpyHostToDevice) {
+        detect_uniform(ctx, src);
+    } else {
+        double *h = (double *)malloc(13 * inB);
+        if (!h) return fail(ctx, OCFD_ERR_NOMEM, "host buffer for metric check");
+        cudaError_t e = cudaMemcpy(h, src, 13 * inB, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { free(h); return cuda_fail(ctx, e, "metric read-back"); }
+        detect_uniform(ctx, h);
+        free(h);
+    }
     for (int m = 0; m < 13; m++) {
         CK(cudaMemcpyAsync(ctx->stage_buf, src + (size_t)m * p.N, inB, kind, ctx->stream), "metric copy");
         CK(ocfd::launch_scatter(p, ctx->stage_buf, const_cast<double *>(p.met[m]), ctx->stream), "metric scatter");
@@ -346,6 +379,14 @@ static int set_metrics_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKin
     ctx->have_metrics = true;
     return OCFD_OK;
 }
+
+extern "C" int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode) {
+    if (!ctx || mode < 0 || mode > 1) return OCFD_ERR_ARG;
+    ctx->metric_mode = mode;
+    if (mode == 1) ctx->p.uniform_metrics = 0;
+    return OCFD_OK;
+}
+extern "C" int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx) { return ctx ? ctx->p.uniform_metrics : 0; }
 
 extern "C" int ocfd_b200_set_metrics(ocfd_b200_ctx *ctx, const double *m) {
     return set_metrics_impl(ctx, m, cudaMemcpyHostToDevice);
@@ -506,6 +547,40 @@ extern "C" int ocfd_b200_get_flags(ocfd_b200_ctx *ctx, int8_t *fx, int8_t *fy, i
     CK(cudaMemcpyAsync(fy, p.flag[1], nyf, cudaMemcpyDeviceToHost, ctx->stream), "flags");
     CK(cudaMemcpyAsync(fz, p.flag[2], nzf, cudaMemcpyDeviceToHost, ctx->stream), "flags");
     CK(cudaStreamSynchronize(ctx->stream), "flags");
+    return OCFD_OK;
+}
+
+// ana_residual (src/OCFD_ana.cu:76-105): mean of E (which = 0) or T (which = 1)
+extern "C" int ocfd_b200_ana_residual(ocfd_b200_ctx *ctx, int which, double *mean) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (!mean || which < 0 || which > 1) return fail(ctx, OCFD_ERR_ARG, "which must be 0 (E) or 1 (T)");
+    CK(ocfd::launch_mean(ctx->p, which, ctx->red_buf, nullptr, ctx->stream), "reduction");
+    ctx->launches += 2;
+    CK(cudaMemcpyAsync(mean, ctx->red_buf + ocfd::reduce_scratch_doubles() - 1, sizeof(double),
+                       cudaMemcpyDeviceToHost, ctx->stream), "reduction read-back");
+    CK(cudaStreamSynchronize(ctx->stream), "reduction");
+    return OCFD_OK;
+}
+
+// ana_NAN_and_NT (src/OCFD_ana.cu:107-222) as counts: cells with a NaN in
+// d,u,v,w,T and cells with T < 0; the mean of T is returned alongside.
+extern "C" int ocfd_b200_check_state(ocfd_b200_ctx *ctx, long long *n_nan, long long *n_neg_t, double *mean_t) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    int nd = ocfd::reduce_scratch_doubles();
+    unsigned long long *counts = reinterpret_cast<unsigned long long *>(ctx->red_buf + nd);
+    CK(ocfd::launch_mean(ctx->p, 1, ctx->red_buf, counts, ctx->stream), "state check");
+    ctx->launches += 2;
+    double host[3];
+    CK(cudaMemcpyAsync(host, ctx->red_buf + nd - 1, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+       "state check read-back");
+    CK(cudaStreamSynchronize(ctx->stream), "state check");
+    unsigned long long c[2];
+    memcpy(c, host + 1, sizeof(c));
+    if (n_nan) *n_nan = (long long)c[0];
+    if (n_neg_t) *n_neg_t = (long long)c[1];
+    if (mean_t) *mean_t = host[0];
     return OCFD_OK;
 }
 

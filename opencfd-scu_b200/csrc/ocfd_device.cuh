@@ -33,6 +33,9 @@ struct Params {
     double *grad;           // [12][nz][ny][nx]: uk ui us vk vi vs wk wi ws Tk Ti Ts
     double *ev;             // [12] LAP-box fields: Ev1..4 of x, then y, then z
     int8_t *flag[3];        // hybrid scheme flags (nx+1)ny nz, nx(ny+1)nz, nx ny(nz+1)
+    // uniform grids: every metric field is one value; kernels read mc[] instead
+    int uniform_metrics;
+    double mc[13];
 };
 
 enum { M_AXX = 0, M_AYY, M_AZZ, M_AKX, M_AKY, M_AKZ, M_AIX, M_AIY, M_AIZ,
@@ -42,6 +45,14 @@ __device__ __forceinline__ long long lap_index(const Params &p, int i, int j, in
     // i,j,k are LAP-box coordinates (0 .. n+2*LAP-1)
     return (long long)i + p.ys * j + p.zs * k;
 }
+// metric m at LAP offset o; UNI selects the constant of a uniform grid (the
+// same value every cell would hold, so the arithmetic is unchanged)
+template <bool UNI>
+__device__ __forceinline__ double metric(const Params &p, int m, long long o) {
+    if (UNI) return p.mc[m];
+    return p.met[m][o];
+}
+
 __device__ __forceinline__ long long in_index(const Params &p, int i, int j, int k) {
     return (long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * k);
 }
@@ -423,6 +434,21 @@ __device__ __forceinline__ void char_para(double u1, double v1, double w1, doubl
     p.n1 = n1; p.n2 = n2; p.n3 = n3; p.l1 = l1; p.l2 = l2; p.l3 = l3;
     p.m1 = n2*l3 - n3*l2; p.m2 = n3*l1 - n1*l3; p.m3 = n1*l2 - n2*l1;
     p.KK = (G - 1.0)/(c1*c1);
+}
+
+// face eigen-system kept in shared memory as NCP planes of nf faces
+constexpr int NCP = 14;
+__device__ __forceinline__ void store_para(const CharPara &p, double *b, int i, int nf) {
+    b[0 * nf + i] = p.u1; b[1 * nf + i] = p.v1; b[2 * nf + i] = p.w1; b[3 * nf + i] = p.c1;
+    b[4 * nf + i] = p.n1; b[5 * nf + i] = p.n2; b[6 * nf + i] = p.n3;
+    b[7 * nf + i] = p.l1; b[8 * nf + i] = p.l2; b[9 * nf + i] = p.l3;
+    b[10 * nf + i] = p.m1; b[11 * nf + i] = p.m2; b[12 * nf + i] = p.m3; b[13 * nf + i] = p.KK;
+}
+__device__ __forceinline__ void load_para(CharPara &p, const double *b, int i, int nf) {
+    p.u1 = b[0 * nf + i]; p.v1 = b[1 * nf + i]; p.w1 = b[2 * nf + i]; p.c1 = b[3 * nf + i];
+    p.n1 = b[4 * nf + i]; p.n2 = b[5 * nf + i]; p.n3 = b[6 * nf + i];
+    p.l1 = b[7 * nf + i]; p.l2 = b[8 * nf + i]; p.l3 = b[9 * nf + i];
+    p.m1 = b[10 * nf + i]; p.m2 = b[11 * nf + i]; p.m3 = b[12 * nf + i]; p.KK = b[13 * nf + i];
 }
 
 // row r of the left eigenvector matrix (flux_charteric_ptoc_kernel :617-676)

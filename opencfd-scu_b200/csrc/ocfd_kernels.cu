@@ -158,7 +158,7 @@ __device__ __forceinline__ double recon(const Params &p, int scheme, int hflag, 
     }
 }
 
-template <int DIR>
+template <int DIR, bool UNI>
 __global__ void __launch_bounds__(SweepShape<DIR>::THREADS)
 k_sweep(Params p) {
     constexpr int TS = SweepShape<DIR>::TS, R = SweepShape<DIR>::R;
@@ -168,6 +168,7 @@ k_sweep(Params p) {
     extern __shared__ double smem[];
     double *spl = smem;                   // [10][NP]: f+ 0..4, f- 5..9
     double *hat = smem + 10 * NP;         // [10][NF]: sign*5 + comp
+    double *cps = hat + 10 * NF;          // [NCP][NF]: face eigen-system (characteristic schemes)
 
     const int n = ndir<DIR>(p), nr = nrow<DIR>(p);
     const int s0 = blockIdx.x * TS;       // first interior cell of the tile (along DIR)
@@ -178,7 +179,7 @@ k_sweep(Params p) {
                          + (long long)(r0 + OCFD_LAP) * sr + (long long)(s0) * sd;
     // base points at LAP coordinate (s0 along DIR), i.e. interior cell s0-4
     const double *d = p.prim[0], *u = p.prim[1], *v = p.prim[2], *w = p.prim[3], *T = p.prim[4];
-    const double *A1 = p.met[M_AKX + 3 * DIR], *A2 = p.met[M_AKX + 3 * DIR + 1], *A3 = p.met[M_AKX + 3 * DIR + 2];
+    const int mA = M_AKX + 3 * DIR;
 
     // ---- phase A: split fluxes at interior-relative points s0-4 .. s0+TS+3
     for (int q = threadIdx.x; q < NP; q += blockDim.x) {
@@ -189,18 +190,40 @@ k_sweep(Params p) {
         long long o = base + (long long)s * sd + (long long)r * sr;
         double cc = sqrt(T[o]) / p.Ama;
         double fp[5], fm[5];
-        sw_split(d[o] * p.tmp0, u[o], v[o], w[o], cc, A1[o], A2[o], A3[o], p.Gamma, p.epsl_sw,
-                 p.split_C1, p.split_C3, fp, fm);
+        sw_split(d[o] * p.tmp0, u[o], v[o], w[o], cc, metric<UNI>(p, mA, o), metric<UNI>(p, mA + 1, o),
+                 metric<UNI>(p, mA + 2, o), p.Gamma, p.epsl_sw, p.split_C1, p.split_C3, fp, fm);
         int pi = s + (TS + 8) * r;
 #pragma unroll
         for (int m = 0; m < 5; m++) { spl[m * NP + pi] = fp[m]; spl[(5 + m) * NP + pi] = fm[m]; }
     }
-    __syncthreads();
 
     const int scheme = p.scheme_invis;
     const bool char_scheme = p.charteric && (scheme == 304 || scheme == 305 || scheme == 310);
     const bool comp_none = p.charteric && !char_scheme;   // reference adds nothing
     const int8_t *flags = p.flag[DIR];
+
+    // ---- phase A2: face-averaged eigen-system, once per face
+    //      (get_para_charteric_{p,m}_kernel, src/OCFD_flux_charteric.cu:321-520)
+    if (char_scheme) {
+        for (int fi = threadIdx.x; fi < NF; fi += blockDim.x) {
+            int fs, r;
+            if (DIR == 0) { fs = fi % (TS + 1); r = fi / (TS + 1); }
+            else          { r = fi % R; fs = fi / R; }
+            int F = s0 - 1 + fs;
+            if (r0 + r >= nr || F > n - 1) continue;
+            long long o0 = base + (long long)(fs + 3) * sd + (long long)r * sr;   // cell F
+            long long o1 = o0 + sd;                                                // cell F+1
+            CharPara cp;
+            double c0v = sqrt(T[o0]) / p.Ama, c1v = sqrt(T[o1]) / p.Ama;
+            char_para((u[o0] + u[o1]) * 0.5, (v[o0] + v[o1]) * 0.5, (w[o0] + w[o1]) * 0.5,
+                      (c0v + c1v) * 0.5,
+                      (metric<UNI>(p, mA, o0) + metric<UNI>(p, mA, o1)) * 0.5,
+                      (metric<UNI>(p, mA + 1, o0) + metric<UNI>(p, mA + 1, o1)) * 0.5,
+                      (metric<UNI>(p, mA + 2, o0) + metric<UNI>(p, mA + 2, o1)) * 0.5, p.Gamma, cp);
+            store_para(cp, cps, fi, NF);
+        }
+    }
+    __syncthreads();
 
     // ---- phase B1: one thread per (face, sign, component / characteristic)
     for (int t = threadIdx.x; t < 10 * NF; t += blockDim.x) {
@@ -226,14 +249,9 @@ k_sweep(Params p) {
         if (comp_none) {
             res = 0.0;
         } else if (char_scheme && !(scheme == 310 && hflag == 1)) {
-            // face-averaged characteristic system, get_para_charteric_{p,m}_kernel
-            long long o0 = base + (long long)(fs + 3) * sd + (long long)r * sr;   // cell F
-            long long o1 = o0 + sd;                                                // cell F+1
+            // project the 8-point stencil on characteristic field c
             CharPara cp;
-            double c0v = sqrt(T[o0]) / p.Ama, c1v = sqrt(T[o1]) / p.Ama;
-            char_para((u[o0] + u[o1]) * 0.5, (v[o0] + v[o1]) * 0.5, (w[o0] + w[o1]) * 0.5,
-                      (c0v + c1v) * 0.5, (A1[o0] + A1[o1]) * 0.5, (A2[o0] + A2[o1]) * 0.5,
-                      (A3[o0] + A3[o1]) * 0.5, p.Gamma, cp);
+            load_para(cp, cps, fi, NF);
             double Lr[5];
             char_L_row(cp, c, Lr);
 #pragma unroll
@@ -273,13 +291,8 @@ k_sweep(Params p) {
             if (scheme == 310 && hflag == 1) {
                 res = h[m * NF];
             } else {
-                long long o0 = base + (long long)(fs + 3) * sd + (long long)r * sr;
-                long long o1 = o0 + sd;
                 CharPara cp;
-                double c0v = sqrt(T[o0]) / p.Ama, c1v = sqrt(T[o1]) / p.Ama;
-                char_para((u[o0] + u[o1]) * 0.5, (v[o0] + v[o1]) * 0.5, (w[o0] + w[o1]) * 0.5,
-                          (c0v + c1v) * 0.5, (A1[o0] + A1[o1]) * 0.5, (A2[o0] + A2[o1]) * 0.5,
-                          (A3[o0] + A3[o1]) * 0.5, p.Gamma, cp);
+                load_para(cp, cps, fi, NF);
                 double Rr[5];
                 char_R_row(cp, m, Rr);
                 res = dot5(Rr, h[0], h[NF], h[2 * NF], h[3 * NF], h[4 * NF]);
@@ -291,7 +304,6 @@ k_sweep(Params p) {
     const double *fl = char_scheme ? spl : hat;
 
     // ---- phase C: du of each tile cell (x+ then x- for every component)
-    const double *Aj = p.met[M_AJAC];
     const double h = hdir<DIR>(p);
     for (int t = threadIdx.x; t < NC; t += blockDim.x) {
         int s, r;
@@ -300,7 +312,7 @@ k_sweep(Params p) {
         int X = s0 + s;
         if (r0 + r >= nr || X > n - 1) continue;
         long long o = base + (long long)(s + 4) * sd + (long long)r * sr;
-        double aj = Aj[o];
+        double aj = metric<UNI>(p, M_AJAC, o);
         int i, j, k;
         if (DIR == 0)      { i = X; j = r0 + r; k = c3; }
         else if (DIR == 1) { i = r0 + r; j = X; k = c3; }
@@ -348,6 +360,7 @@ __global__ void k_vis_grad(Params p) {
 
 // Ev1..4 of all three directions (vis_flux_ker :178-236; the stress and heat
 // flux are direction independent, so they are formed once per cell)
+template <bool UNI>
 __global__ void k_vis_ev(Params p) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= p.N) return;
@@ -356,9 +369,9 @@ __global__ void k_vis_ev(Params p) {
     long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     const double *g = p.grad;
     const long long N = p.N;
-    double Akx = p.met[M_AKX][o], Aix = p.met[M_AIX][o], Asx = p.met[M_ASX][o];
-    double Aky = p.met[M_AKY][o], Aiy = p.met[M_AIY][o], Asy = p.met[M_ASY][o];
-    double Akz = p.met[M_AKZ][o], Aiz = p.met[M_AIZ][o], Asz = p.met[M_ASZ][o];
+    double Akx = metric<UNI>(p, M_AKX, o), Aix = metric<UNI>(p, M_AIX, o), Asx = metric<UNI>(p, M_ASX, o);
+    double Aky = metric<UNI>(p, M_AKY, o), Aiy = metric<UNI>(p, M_AIY, o), Asy = metric<UNI>(p, M_ASY, o);
+    double Akz = metric<UNI>(p, M_AKZ, o), Aiz = metric<UNI>(p, M_AIZ, o), Asz = metric<UNI>(p, M_ASZ, o);
     double Tc = p.prim[4][o];
     double Amu = p.amu_C0 * sqrt(Tc * Tc * Tc) / (p.Tsb + Tc);      // get_Amu_kernal
     double uk = g[0 * N + tid], ui = g[1 * N + tid], us = g[2 * N + tid];
@@ -389,12 +402,12 @@ __global__ void k_vis_ev(Params p) {
     double E1 = uu*s11 + vv*s12 + ww*s13 + Amuk*Tx;
     double E2 = uu*s12 + vv*s22 + ww*s23 + Amuk*Ty;
     double E3 = uu*s13 + vv*s23 + ww*s33 + Amuk*Tz;
-    double Aj1 = p.met[M_AJAC][o];
+    double Aj1 = metric<UNI>(p, M_AJAC, o);
 #pragma unroll
     for (int dd = 0; dd < 3; dd++) {
-        double akx = p.met[M_AKX + 3 * dd][o] * Aj1;
-        double aky = p.met[M_AKX + 3 * dd + 1][o] * Aj1;
-        double akz = p.met[M_AKX + 3 * dd + 2][o] * Aj1;
+        double akx = metric<UNI>(p, M_AKX + 3 * dd, o) * Aj1;
+        double aky = metric<UNI>(p, M_AKX + 3 * dd + 1, o) * Aj1;
+        double akz = metric<UNI>(p, M_AKX + 3 * dd + 2, o) * Aj1;
         double *ev = p.ev + (long long)(4 * dd) * p.lapN;
         ev[o]              = (akx*s11 + aky*s12 + akz*s13);
         ev[p.lapN + o]     = (akx*s12 + aky*s22 + akz*s23);
@@ -405,6 +418,7 @@ __global__ void k_vis_ev(Params p) {
 
 // du[1..4] += Ajac * d(Ev)/d(xi) for x, then y, then z
 // (du_viscous_Jacobian3d_{x,y,z}_final + YF_Pe_XF, src/commen_kernel.cu:158-169)
+template <bool UNI>
 __global__ void k_vis_div(Params p) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= p.N) return;
@@ -414,7 +428,7 @@ __global__ void k_vis_div(Params p) {
     const long long st[3] = { 1LL, p.ys, p.zs };
     const double hh[3] = { p.hx, p.hy, p.hz };
     const bool c8 = p.scheme_vis == 204;
-    double ajac = p.met[M_AJAC][o];
+    double ajac = metric<UNI>(p, M_AJAC, o);
     double acc[4];
 #pragma unroll
     for (int m = 0; m < 4; m++) acc[m] = p.du[(m + 1) * p.N + tid];
@@ -559,21 +573,23 @@ __global__ void k_fill(double *f, long long n, double v) {
 // ---------------------------------------------------------------------------
 static inline unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
-template <int DIR>
+template <int DIR, bool UNI>
 static cudaError_t launch_sweep(const Params &p, cudaStream_t st) {
     using S = SweepShape<DIR>;
     constexpr int NP = (S::TS + 8) * S::R, NF = (S::TS + 1) * S::R;
-    size_t smem = sizeof(double) * (10 * NP + 10 * NF);
+    const bool chars = p.charteric && (p.scheme_invis == 304 || p.scheme_invis == 305 || p.scheme_invis == 310);
+    size_t smem = sizeof(double) * (10 * NP + 10 * NF + (chars ? NCP * NF : 0));
     int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
     int nr = DIR == 0 ? p.ny : p.nx;
     int n3 = DIR == 2 ? p.ny : p.nz;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_sweep<DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
+    static size_t attr_bytes = 0;
+    if (smem > attr_bytes) {
+        cudaError_t e = cudaFuncSetAttribute(k_sweep<DIR, UNI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_bytes = smem;
     }
     dim3 grid((n + S::TS - 1) / S::TS, (nr + S::R - 1) / S::R, n3);
-    k_sweep<DIR><<<grid, S::THREADS, smem, st>>>(p);
+    k_sweep<DIR, UNI><<<grid, S::THREADS, smem, st>>>(p);
     return cudaGetLastError();
 }
 
@@ -593,24 +609,30 @@ cudaError_t launch_ghost(const Params &p, double *const *fields, const int *dirm
     return cudaGetLastError();
 }
 
-cudaError_t launch_sweeps(const Params &p, cudaStream_t st) {
+template <bool UNI>
+static cudaError_t launch_sweeps_t(const Params &p, cudaStream_t st) {
     cudaError_t e;
-    if ((e = launch_sweep<0>(p, st)) != cudaSuccess) return e;
-    if ((e = launch_sweep<1>(p, st)) != cudaSuccess) return e;
-    return launch_sweep<2>(p, st);
+    if ((e = launch_sweep<0, UNI>(p, st)) != cudaSuccess) return e;
+    if ((e = launch_sweep<1, UNI>(p, st)) != cudaSuccess) return e;
+    return launch_sweep<2, UNI>(p, st);
+}
+cudaError_t launch_sweeps(const Params &p, cudaStream_t st) {
+    return p.uniform_metrics ? launch_sweeps_t<true>(p, st) : launch_sweeps_t<false>(p, st);
 }
 
 cudaError_t launch_viscous(const Params &p, cudaStream_t st) {
     unsigned nb = blocks_for(p.N, 256);
     k_vis_grad<<<nb, 256, 0, st>>>(p);
-    k_vis_ev<<<nb, 256, 0, st>>>(p);
+    if (p.uniform_metrics) k_vis_ev<true><<<nb, 256, 0, st>>>(p);
+    else                   k_vis_ev<false><<<nb, 256, 0, st>>>(p);
     double *evf[12]; int mask[12];
     for (int dd = 0; dd < 3; dd++)
         for (int m = 0; m < 4; m++) { evf[4 * dd + m] = p.ev + (long long)(4 * dd + m) * p.lapN; mask[4 * dd + m] = 1 << dd; }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if ((e = launch_ghost(p, evf, mask, 12, st)) != cudaSuccess) return e;
-    k_vis_div<<<nb, 256, 0, st>>>(p);
+    if (p.uniform_metrics) k_vis_div<true><<<nb, 256, 0, st>>>(p);
+    else                   k_vis_div<false><<<nb, 256, 0, st>>>(p);
     return cudaGetLastError();
 }
 
@@ -651,5 +673,84 @@ cudaError_t launch_bc_faces(const Params &p, cudaStream_t st) {
     k_bc_faces<<<blocks_for(p.N, 256), 256, 0, st>>>(p);
     return cudaGetLastError();
 }
+
+// ---------------------------------------------------------------------------
+// FP64 mean of an interior field (ana_residual, src/OCFD_ana.cu:50-105) and
+// the NaN / negative-T scan (ana_NAN_and_NT, src/OCFD_ana.cu:107-222).
+// Deterministic: a fixed grid of RED_BLOCKS blocks, each summing a fixed
+// strided subset in a fixed order and reducing in a fixed tree; one block
+// then sums the partials in order.  (The reference's reduction assumes
+// 64-wide warps and is wrong on 32-wide ones; this one is not.)
+// ---------------------------------------------------------------------------
+constexpr int RED_BLOCKS = 592;     // 4 x 148 SMs
+constexpr int RED_THREADS = 256;
+
+// src: which = 0 conserved energy f[4] (dense), 1 temperature (LAP box)
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_partial(Params p, int which, double *partial,
+                                                               unsigned long long *counts) {
+    __shared__ double sh[RED_THREADS];
+    __shared__ unsigned int nn[2];
+    if (threadIdx.x < 2) nn[threadIdx.x] = 0;
+    __syncthreads();
+    double acc = 0.0;
+    unsigned int nnan = 0, nneg = 0;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < p.N; q += stride) {
+        int i = (int)(q % p.nx); long long r = q / p.nx;
+        int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+        double v;
+        if (which == 0) {
+            v = p.f[4 * p.N + q];
+        } else {
+            v = p.prim[4][lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP)];
+        }
+        acc += v;
+        if (counts) {
+            long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+            bool bad = false;
+            for (int m = 0; m < 5; m++) bad |= isnan(p.prim[m][o]);
+            nnan += bad;
+            nneg += p.prim[4][o] < 0.0;
+        }
+    }
+    sh[threadIdx.x] = acc;
+    if (counts && (nnan | nneg)) { atomicAdd(&nn[0], nnan); atomicAdd(&nn[1], nneg); }
+    __syncthreads();
+    for (int h = RED_THREADS / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = sh[0];
+        if (counts && (nn[0] | nn[1])) { atomicAdd(&counts[0], nn[0]); atomicAdd(&counts[1], nn[1]); }
+    }
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_final(const double *partial, int n, double ncell,
+                                                             double *out) {
+    __shared__ double sh[RED_THREADS];
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) acc += partial[q];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = RED_THREADS / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = sh[0] / ncell;       // E0 /= NX*NY*NZ (src/OCFD_ana.cu:103)
+}
+
+// scratch: RED_BLOCKS + 1 doubles and two counters
+cudaError_t launch_mean(const Params &p, int which, double *scratch, unsigned long long *counts,
+                        cudaStream_t st) {
+    if (counts) {
+        cudaError_t e = cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return e;
+    }
+    k_reduce_partial<<<RED_BLOCKS, RED_THREADS, 0, st>>>(p, which, scratch, counts);
+    k_reduce_final<<<1, RED_THREADS, 0, st>>>(scratch, RED_BLOCKS, (double)p.N, scratch + RED_BLOCKS);
+    return cudaGetLastError();
+}
+int reduce_scratch_doubles() { return RED_BLOCKS + 1; }
 
 }  // namespace ocfd

