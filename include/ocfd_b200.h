@@ -57,6 +57,12 @@ typedef struct ocfd_b200_config {
     double hy_dp_intv[2];      /* HY_DP_INTV                                      */
     double re, ama, gamma, pr, t_ref, epsl_sw, dt;   /* RE AMA GAMMA PR T_REF EPSL_SW DT */
     int device;                /* CUDA device ordinal                             */
+    /* SCHEME_HYBRIDAUTO with CHARTERIC = 0: the reference's per-component
+     * kernels read an uninitialised scheme flag for components 1-4
+     * (src/OCFD_Schemes_hybrid_auto.cu:907,1005); its sm_100a build then
+     * uses WENO5 there.  0 (default) reproduces that build; 1 gives every
+     * component the face's flag. */
+    int hybrid_nochar_same_flag;
 } ocfd_b200_config;
 
 int  ocfd_b200_abi_version(void);

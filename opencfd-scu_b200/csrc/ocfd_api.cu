@@ -180,6 +180,7 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     p.tv_lim = 5.0; p.tv_max = 0.2;              // src/parameters.c:75-76
     p.dp1 = cfg->hy_dp_intv[0]; p.dp2 = cfg->hy_dp_intv[1];
     p.scheme_invis = si; p.scheme_vis = cfg->scheme_vis; p.charteric = cfg->charteric;
+    p.nochar_comp_flag = cfg->hybrid_nochar_same_flag ? 0 : 3;
     for (int d = 0; d < 3; d++) p.periodic[d] = cfg->iperiodic[d];
 
     size_t lapB = sizeof(double) * (size_t)p.lapN, inB = sizeof(double) * (size_t)N;

@@ -25,6 +25,7 @@ struct Params {
     double tv_lim, tv_max;
     double dp1, dp2;
     int scheme_invis, scheme_vis, charteric;
+    int nochar_comp_flag;   // flag of components 1-4, non-characteristic hybrid (0 = face flag)
     int periodic[3];
     // state
     double *prim[5];        // d u v w T on the LAP box

@@ -261,7 +261,9 @@ k_sweep(Params p) {
         } else {
 #pragma unroll
             for (int k = 0; k < 8; k++) vals[k] = sp[c * NP + k];
-            res = recon(p, scheme, hflag, sign, vals);
+            int hf = hflag;
+            if (scheme == 310 && !char_scheme && c > 0 && p.nochar_comp_flag) hf = p.nochar_comp_flag;
+            res = recon(p, scheme, hf, sign, vals);
         }
         hat[rem * NF + fi] = res;
     }

@@ -57,6 +57,7 @@ class Config(ctypes.Structure):
         ("pr", ctypes.c_double), ("t_ref", ctypes.c_double), ("epsl_sw", ctypes.c_double),
         ("dt", ctypes.c_double),
         ("device", ctypes.c_int),
+        ("hybrid_nochar_same_flag", ctypes.c_int),
     ]
 
 

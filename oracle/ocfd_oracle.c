@@ -944,8 +944,10 @@ static void invis_sweep(oro_state *s, int dir) {
                         mat5_apply(Rm, outp); mat5_apply(Rm, outm);
                     } else {
                         for (int m = 0; m < 5; m++) {
-                            outp[m] = face_p(s, scheme, hflag, s8p[m]);
-                            outm[m] = face_m(s, scheme, hflag, s8m[m]);
+                            int hf = hflag;
+                            if (scheme == 310 && !chart && m > 0 && s->c.hy_nochar_fixed) hf = s->c.hy_nochar_fixed;
+                            outp[m] = face_p(s, scheme, hf, s8p[m]);
+                            outm[m] = face_m(s, scheme, hf, s8m[m]);
                         }
                     }
                     for (int m = 0; m < 5; m++) {

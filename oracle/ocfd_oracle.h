@@ -42,6 +42,9 @@ typedef struct oro_config {
     double weno_tv_limiter;    /* src/parameters.c:75 (5.0)                     */
     double weno_tv_max;        /* src/parameters.c:76 (0.2)                     */
     int nthreads;              /* OpenMP threads (<=0: runtime default)         */
+    int hy_nochar_fixed;       /* CHARTERIC=0 hybrid, components 1-4: 0 = use the
+                                  face flag (intent); 1/2/3 = force that flag
+                                  (what an uninitialised register yields)       */
 } oro_config;
 
 typedef struct oro_state oro_state;

@@ -34,6 +34,7 @@ class OroConfig(ctypes.Structure):
         ("dt", ctypes.c_double),
         ("weno_tv_limiter", ctypes.c_double), ("weno_tv_max", ctypes.c_double),
         ("nthreads", ctypes.c_int),
+        ("hy_nochar_fixed", ctypes.c_int),
     ]
 
 
@@ -93,7 +94,7 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-def make_config(cfg, nthreads: int = 0) -> OroConfig:
+def make_config(cfg, nthreads: int = 0, hy_nochar_fixed: int = 3) -> OroConfig:
     """OroConfig from an ocfd_b200.formats.CaseConfig."""
     c = OroConfig()
     c.nx, c.ny, c.nz = cfg.nx, cfg.ny, cfg.nz
@@ -110,18 +111,25 @@ def make_config(cfg, nthreads: int = 0) -> OroConfig:
     c.t_ref, c.epsl_sw, c.dt = cfg.t_ref, cfg.epsl_sw, cfg.dt
     c.weno_tv_limiter, c.weno_tv_max = 5.0, 0.2
     c.nthreads = nthreads
+    c.hy_nochar_fixed = hy_nochar_fixed
     return c
 
 
 class Oracle:
-    """One solver instance; mirrors the reference driver's call sequence."""
+    """One solver instance; mirrors the reference driver's call sequence.
+
+    hy_nochar_fixed: scheme flag that components 1-4 of the non-characteristic
+    hybrid kernels use.  The reference reads an uninitialised variable there
+    (src/OCFD_Schemes_hybrid_auto.cu:907,1005); its sm_100a build behaves as
+    flag 3 (WENO5), measured against the golden fixtures, hence the default.
+    0 gives the face flag to every component."""
 
     def __init__(self, cfg, prims: Sequence[np.ndarray], metrics: Sequence[np.ndarray],
-                 nthreads: int = 0, istep: int = 0, tt: float = 0.0):
+                 nthreads: int = 0, istep: int = 0, tt: float = 0.0, hy_nochar_fixed: int = 3):
         if cfg.hy_style != 2 and cfg.scheme_invis_id == 310:
             raise NotImplementedError("oracle covers HY_STYLE=2 only")
         self.cfg = cfg
-        self._c = make_config(cfg, nthreads)
+        self._c = make_config(cfg, nthreads, hy_nochar_fixed)
         self.L = lib()
         self.h = self.L.oro_create(ctypes.byref(self._c))
         self.shape = (cfg.nz, cfg.ny, cfg.nx)

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import os
 import re
+import resource
 import shutil
 import subprocess
 import sys
@@ -24,6 +25,17 @@ REF_BIN = os.path.join(HERE, "_ref", "opencfd-scu.out")
 
 sys.path.insert(0, os.path.join(ROOT, "opencfd-scu_b200"))
 from ocfd_b200 import formats  # noqa: E402
+
+
+def _big_stack():
+    # The reference's host halo exchange keeps four LAP*n*n double arrays on
+    # the stack (src/OCFD_mpi.c:304-306): 8 MB at 256^3, past the default
+    # limit.  Raise the child's soft limit to its hard limit.
+    soft, hard = resource.getrlimit(resource.RLIMIT_STACK)
+    try:
+        resource.setrlimit(resource.RLIMIT_STACK, (hard, hard))
+    except (ValueError, OSError):
+        pass
 
 
 def available() -> bool:
@@ -46,7 +58,8 @@ def run_and_read(case, nsteps: int, timeout: float = 900.0):
     try:
         _write_inputs(case, wd)
         t0 = time.time()
-        p = subprocess.run([REF_BIN], cwd=wd, capture_output=True, text=True, timeout=timeout)
+        p = subprocess.run([REF_BIN], cwd=wd, capture_output=True, text=True, timeout=timeout,
+                           preexec_fn=_big_stack)
         wall = time.time() - t0
         if p.returncode != 0:
             raise RuntimeError(f"reference exited {p.returncode}:\n{p.stdout[-3000:]}\n{p.stderr[-3000:]}")
@@ -72,7 +85,8 @@ def time_steps(case, warmup: int, steps: int, timeout: float = 1800.0) -> Tuple[
     wd = tempfile.mkdtemp(prefix="ocfd_ref_")
     try:
         _write_inputs(case, wd)
-        p = subprocess.run([REF_BIN], cwd=wd, capture_output=True, text=True, timeout=timeout)
+        p = subprocess.run([REF_BIN], cwd=wd, capture_output=True, text=True, timeout=timeout,
+                           preexec_fn=_big_stack)
         if p.returncode != 0:
             raise RuntimeError(f"reference exited {p.returncode}:\n{p.stdout[-3000:]}\n{p.stderr[-3000:]}")
         m = _INTERVAL.findall(p.stdout)

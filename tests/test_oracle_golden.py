@@ -39,8 +39,6 @@ def test_oracle_matches_reference(path):
     got = o.primitives()
     ref = z["out_run0"]
     err = rel_l2(got, ref)
-    if "nochar" in os.path.basename(path):
-        pytest.skip(f"reference reads an uninitialised flag in this mode; rel L2 = {err}")
     assert np.all(err <= TOL), err
     assert o.istep == int(z["istep"])
 
