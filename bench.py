@@ -244,18 +244,16 @@ def run_ours(args, rank, world, dist):
 
 
 # Algorithmic bytes per cell for one stage's launches of each kernel family
-# (every input and output field touched once, FP64):
-#   inviscid_sweeps: x, y, z sweeps each read d,u,v,w,T + 3 direction metrics
-#                    + Ajac (9 fields); x writes du (5), y and z read and write
-#                    du (10 each)                              -> 52 words
-#   viscous: gradients 4 in / 12 out; Ev 12 grads + u,v,w,T + 10 metrics in,
-#            12 out; divergence 12 Ev + Ajac + du[1..4] in, du[1..4] out -> 75 words
-#   rk_update: fn, f, du in, f and d,u,v,w,T out              -> 25 words
-#   sensor: d,T in, three int8 flags out                       -> 19 bytes
+# on a uniform grid (metrics are constants there; every field touched once):
+#   inviscid_sweeps: each of the x, y, z sweeps reads d,u,v,w,T; x writes du
+#                    (5), y and z read and write du (10 each)      -> 40 words
+#   viscous_rk_update: Ev kernel reads u,v,w,T, writes 12 Ev; divergence +
+#                    RK kernel reads 12 Ev, du, fn, f and writes f and
+#                    d,u,v,w,T                                     -> 53 words
+#   sensor: d,T in, three int8 flags out                           -> 19 bytes
 DOM_BYTES = {
-    "inviscid_sweeps": 52 * 8.0,
-    "viscous": 75 * 8.0,
-    "rk_update": 25 * 8.0,
+    "inviscid_sweeps": 40 * 8.0,
+    "viscous_rk_update": 53 * 8.0,
     "ghost_fill": 0.0,
     "sensor": 19.0,
 }

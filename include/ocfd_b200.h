@@ -93,6 +93,10 @@ int ocfd_b200_set_metrics(ocfd_b200_ctx *ctx, const double *metrics13);
  * effect at the next set_metrics.  uniform_metrics reports the choice. */
 int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode);
 int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx);
+/* Inviscid sweep kernel variant: 2 (default) one thread per (face, sign)
+ * with the five characteristic fields in registers; 1 one thread per
+ * (face, sign, field).  Both give the same result. */
+int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl);
 int ocfd_b200_set_metrics_device(ocfd_b200_ctx *ctx, const double *metrics13_dev);
 
 /* Initial primitives d,u,v,w,T (host or device).  Replaces the

@@ -19,7 +19,7 @@ namespace ocfd {
 cudaError_t launch_sensor(const Params &p, cudaStream_t st);
 cudaError_t launch_ghost(const Params &p, double *const *fields, const int *dirmask, int nf, cudaStream_t st);
 cudaError_t launch_sweeps(const Params &p, cudaStream_t st);
-cudaError_t launch_viscous(const Params &p, cudaStream_t st);
+cudaError_t launch_viscous(const Params &p, int krk, cudaStream_t st);
 cudaError_t launch_rk(const Params &p, int krk, cudaStream_t st);
 cudaError_t launch_rk_only(const Params &p, int krk, cudaStream_t st);
 cudaError_t launch_c2p(const Params &p, cudaStream_t st);
@@ -31,6 +31,8 @@ cudaError_t launch_fill(double *f, long long n, double v, cudaStream_t st);
 cudaError_t launch_mean(const Params &p, int which, double *scratch, unsigned long long *counts,
                         cudaStream_t st);
 int reduce_scratch_doubles();
+cudaError_t launch_sweeps2(const Params &p, cudaStream_t st);
+cudaError_t compute_dirconst(Params &p, DirConst *dev_scratch, cudaStream_t st);
 }  // namespace ocfd
 
 using ocfd::Params;
@@ -39,7 +41,7 @@ namespace {
 
 enum Timer { T_SENSOR = 0, T_GHOST, T_SWEEP, T_VIS, T_RK, T_OTHER1, T_OTHER2, T_OTHER3 };
 const char *kTimerNames[OCFD_TIMER_COUNT] = {
-    "sensor", "ghost_fill", "inviscid_sweeps", "viscous", "rk_update", "-", "-", "-"};
+    "sensor", "ghost_fill", "inviscid_sweeps", "viscous_rk_update", "rk_update", "-", "-", "-"};
 
 thread_local std::string g_create_error;
 
@@ -55,7 +57,6 @@ struct ocfd_b200_ctx {
     double *prim_buf = nullptr;   // 5 LAP fields
     double *met_buf = nullptr;    // 13 LAP fields
     double *cons_buf = nullptr;   // f, fn, du: 15 interior fields
-    double *grad_buf = nullptr;   // 12 interior fields
     double *ev_buf = nullptr;     // 12 LAP fields
     int8_t *flag_buf = nullptr;
     double *stage_buf = nullptr;  // 5 interior fields for host transfers
@@ -113,7 +114,7 @@ extern "C" const char *ocfd_b200_last_error(const ocfd_b200_ctx *ctx) {
 
 static void free_all(ocfd_b200_ctx *c) {
     cudaFree(c->prim_buf); cudaFree(c->met_buf); cudaFree(c->cons_buf);
-    cudaFree(c->grad_buf); cudaFree(c->ev_buf); cudaFree(c->flag_buf); cudaFree(c->stage_buf);
+    cudaFree(c->ev_buf); cudaFree(c->flag_buf); cudaFree(c->stage_buf);
     cudaFree(c->red_buf);
     if (c->pinned) cudaFreeHost(c->pinned);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
@@ -181,6 +182,7 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     p.dp1 = cfg->hy_dp_intv[0]; p.dp2 = cfg->hy_dp_intv[1];
     p.scheme_invis = si; p.scheme_vis = cfg->scheme_vis; p.charteric = cfg->charteric;
     p.nochar_comp_flag = cfg->hybrid_nochar_same_flag ? 0 : 3;
+    p.sweep_impl = 2;
     for (int d = 0; d < 3; d++) p.periodic[d] = cfg->iperiodic[d];
 
     size_t lapB = sizeof(double) * (size_t)p.lapN, inB = sizeof(double) * (size_t)N;
@@ -198,7 +200,6 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     if ((rc = alloc((void **)&ctx->prim_buf, 5 * lapB, "primitives")) ||
         (rc = alloc((void **)&ctx->met_buf, 13 * lapB, "metrics")) ||
         (rc = alloc((void **)&ctx->cons_buf, 15 * inB, "conserved")) ||
-        (rc = alloc((void **)&ctx->grad_buf, 12 * inB, "gradients")) ||
         (rc = alloc((void **)&ctx->ev_buf, 12 * lapB, "viscous fluxes")) ||
         (rc = alloc((void **)&ctx->flag_buf, flagN, "flags")) ||
         (rc = alloc((void **)&ctx->stage_buf, 5 * inB, "staging")) ||
@@ -211,7 +212,6 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     for (int m = 0; m < 5; m++) p.prim[m] = ctx->prim_buf + (size_t)m * p.lapN;
     for (int m = 0; m < 13; m++) p.met[m] = ctx->met_buf + (size_t)m * p.lapN;
     p.f = ctx->cons_buf; p.fn = ctx->cons_buf + 5 * N; p.du = ctx->cons_buf + 10 * N;
-    p.grad = ctx->grad_buf;
     p.ev = ctx->ev_buf;
     p.flag[0] = ctx->flag_buf;
     p.flag[1] = ctx->flag_buf + (size_t)(p.nx + 1) * p.ny * p.nz;
@@ -300,7 +300,10 @@ struct TimerScope {
     }
 };
 
-static int rhs(ocfd_b200_ctx *ctx, int krk) {
+// One stage's RHS.  fused_rk = 0: du_comput semantics (du complete on
+// return).  fused_rk = KRK: the viscous divergence kernel also applies the
+// RK stage, cons->prim and the face re-projection (step() path).
+static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
     const Params &p = ctx->p;
     if (p.scheme_invis == 310 && krk == 1) {
         TimerScope ts(ctx, T_SENSOR);
@@ -314,13 +317,14 @@ static int rhs(ocfd_b200_ctx *ctx, int krk) {
     }
     {
         TimerScope ts(ctx, T_SWEEP);
-        CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
+        if (p.sweep_impl == 1) CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
+        else                   CK(ocfd::launch_sweeps2(p, ctx->stream), "inviscid sweeps");
         ctx->launches += 3;
     }
     {
         TimerScope ts(ctx, T_VIS);
-        CK(ocfd::launch_viscous(p, ctx->stream), "viscous");
-        ctx->launches += 4;
+        CK(ocfd::launch_viscous(p, fused_rk, ctx->stream), "viscous");
+        ctx->launches += 3;
     }
     return OCFD_OK;
 }
@@ -376,6 +380,9 @@ static int set_metrics_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKin
     }
     int rc = ghost_metrics(ctx);
     if (rc) return rc;
+    if (ctx->p.uniform_metrics)
+        CK(ocfd::compute_dirconst(ctx->p, reinterpret_cast<ocfd::DirConst *>(ctx->red_buf), ctx->stream),
+           "direction constants");
     CK(cudaStreamSynchronize(ctx->stream), "set_metrics");
     ctx->have_metrics = true;
     return OCFD_OK;
@@ -388,6 +395,12 @@ extern "C" int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode) {
     return OCFD_OK;
 }
 extern "C" int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx) { return ctx ? ctx->p.uniform_metrics : 0; }
+
+extern "C" int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl) {
+    if (!ctx || impl < 1 || impl > 2) return OCFD_ERR_ARG;
+    ctx->p.sweep_impl = impl;
+    return OCFD_OK;
+}
 
 extern "C" int ocfd_b200_set_metrics(ocfd_b200_ctx *ctx, const double *m) {
     return set_metrics_impl(ctx, m, cudaMemcpyHostToDevice);
@@ -452,12 +465,8 @@ extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
     if (nsteps < 0) return fail(ctx, OCFD_ERR_ARG, "nsteps < 0");
     for (int n = 0; n < nsteps; n++) {
         ocfd_b200_swap_time_levels(ctx);
-        for (int krk = 1; krk <= 3; krk++) {
-            if ((rc = rhs(ctx, krk))) return rc;
-            TimerScope ts(ctx, T_RK);
-            CK(ocfd::launch_rk(ctx->p, krk, ctx->stream), "rk update");
-            ctx->launches += 1;
-        }
+        for (int krk = 1; krk <= 3; krk++)
+            if ((rc = rhs(ctx, krk, krk))) return rc;
         ctx->istep++;
         ctx->tt += ctx->p.dt;
     }
@@ -468,7 +477,7 @@ extern "C" int ocfd_b200_du_comput(ocfd_b200_ctx *ctx, int krk) {
     int rc = check_ready(ctx);
     if (rc) return rc;
     if (krk < 1 || krk > 3) return fail(ctx, OCFD_ERR_ARG, "KRK must be 1..3");
-    return rhs(ctx, krk);
+    return rhs(ctx, krk, 0);
 }
 
 extern "C" int ocfd_b200_time_advance(ocfd_b200_ctx *ctx, int krk) {

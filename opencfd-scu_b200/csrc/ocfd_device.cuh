@@ -11,6 +11,14 @@
 
 namespace ocfd {
 
+// per-direction constants of a uniform grid (see k_dirconst)
+struct DirConst {
+    double A[3];       // metric row of the direction (Akx Aky Akz for x, ...)
+    double ss;         // |A|
+    double An[3];      // A / |A|
+    double n[3], l[3], m[3];   // characteristic basis of a face
+};
+
 // ---------------------------------------------------------------------------
 // kernel parameter block (passed by value to every kernel)
 // ---------------------------------------------------------------------------
@@ -31,12 +39,13 @@ struct Params {
     double *prim[5];        // d u v w T on the LAP box
     const double *met[13];  // Axx Ayy Azz Akx Aky Akz Aix Aiy Aiz Asx Asy Asz Ajac (LAP box)
     double *f, *fn, *du;    // [5][nz][ny][nx]
-    double *grad;           // [12][nz][ny][nx]: uk ui us vk vi vs wk wi ws Tk Ti Ts
     double *ev;             // [12] LAP-box fields: Ev1..4 of x, then y, then z
     int8_t *flag[3];        // hybrid scheme flags (nx+1)ny nz, nx(ny+1)nz, nx ny(nz+1)
     // uniform grids: every metric field is one value; kernels read mc[] instead
     int uniform_metrics;
     double mc[13];
+    DirConst dc[3];
+    int sweep_impl;         // 1: per-(face,sign,field) threads; 2: per-(face,sign) threads
 };
 
 enum { M_AXX = 0, M_AYY, M_AZZ, M_AKX, M_AKY, M_AKZ, M_AIX, M_AIY, M_AIZ,

@@ -336,32 +336,19 @@ k_sweep(Params p) {
 // viscous terms, src/OCFD_NS_Jacobian3d.cu:58-440
 // ---------------------------------------------------------------------------
 
-// 12 first derivatives of u,v,w,T (du_viscous_Jacobian3d_init, OCFD_d?0)
-__global__ void k_vis_grad(Params p) {
-    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= p.N) return;
-    int i = (int)(tid % p.nx); long long r = tid / p.nx;
-    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
-    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
-    const long long st[3] = { 1LL, p.ys, p.zs };
-    const double hh[3] = { p.hx, p.hy, p.hz };
-    const bool c8 = p.scheme_vis == 204;
-#pragma unroll
-    for (int m = 0; m < 4; m++) {
-        const double *f = p.prim[m == 3 ? 4 : m + 1];
-#pragma unroll
-        for (int dd = 0; dd < 3; dd++) {
-            long long s = st[dd];
-            double t;
-            if (c8) t = cd8(f[o - 4 * s], f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s], f[o + 4 * s]);
-            else    t = cd6(f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s]);
-            p.grad[(3 * m + dd) * p.N + tid] = t / hh[dd];
-        }
-    }
+// first derivative of a LAP field along stride s at o (OCFD_d?0 with CD6 or
+// CD8, src/OCFD_Schemes.cu:96-156; put_d0_kernel divides by h)
+__device__ __forceinline__ double d0(const double *f, long long o, long long s, double h, bool c8) {
+    double t;
+    if (c8) t = cd8(f[o - 4 * s], f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s], f[o + 4 * s]);
+    else    t = cd6(f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s]);
+    return t / h;
 }
 
-// Ev1..4 of all three directions (vis_flux_ker :178-236; the stress and heat
-// flux are direction independent, so they are formed once per cell)
+// Ev1..4 of all three directions (vis_flux_ker :178-236).  The 12 velocity
+// and temperature derivatives (du_viscous_Jacobian3d_init :58-77) are formed
+// here from the LAP-box primitives instead of being stored; the stress and
+// heat flux do not depend on the direction, so they are formed once per cell.
 template <bool UNI>
 __global__ void k_vis_ev(Params p) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -369,17 +356,17 @@ __global__ void k_vis_ev(Params p) {
     int i = (int)(tid % p.nx); long long r = tid / p.nx;
     int j = (int)(r % p.ny); int k = (int)(r / p.ny);
     long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
-    const double *g = p.grad;
-    const long long N = p.N;
+    const bool c8 = p.scheme_vis == 204;
     double Akx = metric<UNI>(p, M_AKX, o), Aix = metric<UNI>(p, M_AIX, o), Asx = metric<UNI>(p, M_ASX, o);
     double Aky = metric<UNI>(p, M_AKY, o), Aiy = metric<UNI>(p, M_AIY, o), Asy = metric<UNI>(p, M_ASY, o);
     double Akz = metric<UNI>(p, M_AKZ, o), Aiz = metric<UNI>(p, M_AIZ, o), Asz = metric<UNI>(p, M_ASZ, o);
     double Tc = p.prim[4][o];
     double Amu = p.amu_C0 * sqrt(Tc * Tc * Tc) / (p.Tsb + Tc);      // get_Amu_kernal
-    double uk = g[0 * N + tid], ui = g[1 * N + tid], us = g[2 * N + tid];
-    double vk = g[3 * N + tid], vi = g[4 * N + tid], vs = g[5 * N + tid];
-    double wk = g[6 * N + tid], wi = g[7 * N + tid], ws = g[8 * N + tid];
-    double Tk = g[9 * N + tid], Ti = g[10 * N + tid], Ts = g[11 * N + tid];
+    const double *U = p.prim[1], *V = p.prim[2], *W = p.prim[3], *TT = p.prim[4];
+    double uk = d0(U, o, 1, p.hx, c8), ui = d0(U, o, p.ys, p.hy, c8), us = d0(U, o, p.zs, p.hz, c8);
+    double vk = d0(V, o, 1, p.hx, c8), vi = d0(V, o, p.ys, p.hy, c8), vs = d0(V, o, p.zs, p.hz, c8);
+    double wk = d0(W, o, 1, p.hx, c8), wi = d0(W, o, p.ys, p.hy, c8), ws = d0(W, o, p.zs, p.hz, c8);
+    double Tk = d0(TT, o, 1, p.hx, c8), Ti = d0(TT, o, p.ys, p.hy, c8), Ts = d0(TT, o, p.zs, p.hz, c8);
     double ux = uk*Akx + ui*Aix + us*Asx;
     double vx = vk*Akx + vi*Aix + vs*Asx;
     double wx = wk*Akx + wi*Aix + ws*Asx;
@@ -418,60 +405,24 @@ __global__ void k_vis_ev(Params p) {
     }
 }
 
-// du[1..4] += Ajac * d(Ev)/d(xi) for x, then y, then z
-// (du_viscous_Jacobian3d_{x,y,z}_final + YF_Pe_XF, src/commen_kernel.cu:158-169)
-template <bool UNI>
-__global__ void k_vis_div(Params p) {
-    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= p.N) return;
-    int i = (int)(tid % p.nx); long long r = tid / p.nx;
-    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
-    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
-    const long long st[3] = { 1LL, p.ys, p.zs };
-    const double hh[3] = { p.hx, p.hy, p.hz };
-    const bool c8 = p.scheme_vis == 204;
-    double ajac = metric<UNI>(p, M_AJAC, o);
-    double acc[4];
-#pragma unroll
-    for (int m = 0; m < 4; m++) acc[m] = p.du[(m + 1) * p.N + tid];
-#pragma unroll
-    for (int dd = 0; dd < 3; dd++) {
-        long long s = st[dd];
-#pragma unroll
-        for (int m = 0; m < 4; m++) {
-            const double *f = p.ev + (long long)(4 * dd + m) * p.lapN;
-            double t;
-            if (c8) t = cd8(f[o - 4 * s], f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s], f[o + 4 * s]);
-            else    t = cd6(f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s]);
-            acc[m] += ajac * (t / hh[dd]);
-        }
-    }
-#pragma unroll
-    for (int m = 0; m < 4; m++) p.du[(m + 1) * p.N + tid] = acc[m];
-}
-
-// ---------------------------------------------------------------------------
 // RK stage (src/OCFD_time.cu:44-94) + cons_to_pri (src/commen_kernel.cu:77-109)
-// + face re-projection pri_to_cons on the six faces (src/OCFD_boundary.cu:40-91)
-// ---------------------------------------------------------------------------
-__global__ void k_rk_update(Params p, int krk) {
-    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= p.N) return;
-    int i = (int)(tid % p.nx); long long r = tid / p.nx;
-    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+// + pri_to_cons re-projection on the six faces (src/OCFD_boundary.cu:40-91)
+// for one cell, given its final du
+__device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid, int i, int j, int k,
+                                        const double du[5]) {
     const long long N = p.N;
     double f[5];
 #pragma unroll
     for (int m = 0; m < 5; m++) {
-        double fn = p.fn[m * N + tid], du = p.du[m * N + tid];
+        double fn = p.fn[m * N + tid];
         if (krk == 1) {
-            f[m] = fn + p.dt * du;
+            f[m] = fn + p.dt * du[m];
         } else if (krk == 2) {
             double t1 = 3.0 / 4.0, t2 = 1.0 / 4.0;
-            f[m] = t1 * fn + t2 * (p.f[m * N + tid] + p.dt * du);
+            f[m] = t1 * fn + t2 * (p.f[m * N + tid] + p.dt * du[m]);
         } else {
             double t1 = 1.0 / 3.0, t2 = 2.0 / 3.0;
-            f[m] = t1 * fn + t2 * (p.f[m * N + tid] + p.dt * du);
+            f[m] = t1 * fn + t2 * (p.f[m * N + tid] + p.dt * du[m]);
         }
     }
     double d1 = f[0];
@@ -491,6 +442,52 @@ __global__ void k_rk_update(Params p, int krk) {
     }
 #pragma unroll
     for (int m = 0; m < 5; m++) p.f[m * N + tid] = f[m];
+}
+
+// du[1..4] += Ajac * d(Ev)/d(xi) for x, then y, then z
+// (du_viscous_Jacobian3d_{x,y,z}_final + YF_Pe_XF, src/commen_kernel.cu:158-169).
+// RK = true: the stage's du is complete here, so the RK update, cons->prim
+// and the face re-projection follow in the same thread and du is not stored.
+template <bool UNI, bool RK>
+__global__ void k_vis_div(Params p, int krk) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    int i = (int)(tid % p.nx); long long r = tid / p.nx;
+    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+    const long long st[3] = { 1LL, p.ys, p.zs };
+    const double hh[3] = { p.hx, p.hy, p.hz };
+    const bool c8 = p.scheme_vis == 204;
+    double ajac = metric<UNI>(p, M_AJAC, o);
+    double acc[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) acc[m] = (RK || m > 0) ? p.du[m * p.N + tid] : 0.0;
+#pragma unroll
+    for (int dd = 0; dd < 3; dd++) {
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const double *f = p.ev + (long long)(4 * dd + m) * p.lapN;
+            acc[m + 1] += ajac * d0(f, o, st[dd], hh[dd], c8);
+        }
+    }
+    if (RK) {
+        rk_cell(p, krk, tid, i, j, k, acc);
+    } else {
+#pragma unroll
+        for (int m = 0; m < 4; m++) p.du[(m + 1) * p.N + tid] = acc[m + 1];
+    }
+}
+
+// RK stage + cons->prim + face re-projection over the whole grid (du given)
+__global__ void k_rk_update(Params p, int krk) {
+    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    int i = (int)(tid % p.nx); long long r = tid / p.nx;
+    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    double du[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) du[m] = p.du[m * p.N + tid];
+    rk_cell(p, krk, tid, i, j, k, du);
 }
 
 // Unfused pieces of the same update for the reference-named per-stage API:
@@ -622,9 +619,10 @@ cudaError_t launch_sweeps(const Params &p, cudaStream_t st) {
     return p.uniform_metrics ? launch_sweeps_t<true>(p, st) : launch_sweeps_t<false>(p, st);
 }
 
-cudaError_t launch_viscous(const Params &p, cudaStream_t st) {
+// krk = 0: viscous terms into du; krk = 1..3: viscous terms, then the RK
+// stage update in the same kernel (du is not written)
+cudaError_t launch_viscous(const Params &p, int krk, cudaStream_t st) {
     unsigned nb = blocks_for(p.N, 256);
-    k_vis_grad<<<nb, 256, 0, st>>>(p);
     if (p.uniform_metrics) k_vis_ev<true><<<nb, 256, 0, st>>>(p);
     else                   k_vis_ev<false><<<nb, 256, 0, st>>>(p);
     double *evf[12]; int mask[12];
@@ -633,8 +631,13 @@ cudaError_t launch_viscous(const Params &p, cudaStream_t st) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if ((e = launch_ghost(p, evf, mask, 12, st)) != cudaSuccess) return e;
-    if (p.uniform_metrics) k_vis_div<true><<<nb, 256, 0, st>>>(p);
-    else                   k_vis_div<false><<<nb, 256, 0, st>>>(p);
+    if (krk == 0) {
+        if (p.uniform_metrics) k_vis_div<true, false><<<nb, 256, 0, st>>>(p, 0);
+        else                   k_vis_div<false, false><<<nb, 256, 0, st>>>(p, 0);
+    } else {
+        if (p.uniform_metrics) k_vis_div<true, true><<<nb, 256, 0, st>>>(p, krk);
+        else                   k_vis_div<false, true><<<nb, 256, 0, st>>>(p, krk);
+    }
     return cudaGetLastError();
 }
 

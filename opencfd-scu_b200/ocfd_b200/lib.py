@@ -28,7 +28,7 @@ EXPORTED = (
     "ocfd_b200_abi_version", "ocfd_b200_status_string", "ocfd_b200_last_error",
     "ocfd_b200_create", "ocfd_b200_destroy", "ocfd_b200_set_stream", "ocfd_b200_get_stream",
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
-    "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics",
+    "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics", "ocfd_b200_set_sweep_impl",
     "ocfd_b200_set_primitives", "ocfd_b200_set_primitives_device", "ocfd_b200_step",
     "ocfd_b200_advance_host", "ocfd_b200_swap_time_levels", "ocfd_b200_du_comput",
     "ocfd_b200_time_advance", "ocfd_b200_get_duvwT", "ocfd_b200_bc",
@@ -102,6 +102,7 @@ def load(path: Optional[str] = None):
         "ocfd_b200_set_metrics_device": (ctypes.c_int, [P, P]),
         "ocfd_b200_set_metric_mode": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_uniform_metrics": (ctypes.c_int, [P]),
+        "ocfd_b200_set_sweep_impl": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_set_primitives": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_double]),
         "ocfd_b200_set_primitives_device": (ctypes.c_int, [P, P, ctypes.c_int, ctypes.c_double]),
         "ocfd_b200_step": (ctypes.c_int, [P, ctypes.c_int]),
@@ -205,6 +206,9 @@ class Solver:
         if a.shape != (13,) + self.shape:
             raise ValueError(f"metrics shape {a.shape} != {(13,) + self.shape}")
         self._check(self.L.ocfd_b200_set_metrics(self.h, _dp(a)), "set_metrics")
+
+    def set_sweep_impl(self, impl: int):
+        self._check(self.L.ocfd_b200_set_sweep_impl(self.h, impl), "set_sweep_impl")
 
     @property
     def uniform_metrics(self) -> bool:

@@ -62,3 +62,22 @@ def test_calls_out_of_order_return_status(gpu_lib):
     with pytest.raises(lib.OcfdError) as ei:
         s.du_comput(4)
     assert ei.value.status in (-1, -5)
+
+
+@pytest.mark.parametrize("maker", [
+    lambda: cases.isotropic_turbulence(16, seed=41, charteric=1),
+    lambda: cases.random_smooth_case(13, 17, 11, seed=4, scheme_invis="SCHEME_HYBRIDAUTO",
+                                     charteric=1, shock=True, curvilinear=True),
+    lambda: cases.taylor_green(16, seed=2),
+    lambda: cases.random_smooth_case(12, 11, 10, seed=23, scheme_invis="WENO7_SYMBO_LIM", charteric=1, shock=True),
+], ids=["iso_char", "shock_char_curv", "tgv_weno7", "symbo_lim_char"])
+def test_sweep_variants_agree(maker, gpu_lib):
+    case = maker()
+    a = lib.Solver(case.cfg, case.prims, case.metrics)
+    b = lib.Solver(case.cfg, case.prims, case.metrics)
+    b.set_sweep_impl(1)
+    a.step(2)
+    b.step(2)
+    pa, pb = a.primitives(), b.primitives()
+    err = max(np.linalg.norm(pa[m] - pb[m]) / np.linalg.norm(pb[m]) for m in range(5))
+    assert err <= 1e-14, err
