@@ -94,8 +94,9 @@ int ocfd_b200_set_metrics(ocfd_b200_ctx *ctx, const double *metrics13);
 int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode);
 int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx);
 /* Inviscid sweep kernel variant: 2 (default) one thread per (face, sign)
- * with the five characteristic fields in registers; 1 one thread per
- * (face, sign, field).  Both give the same result. */
+ * with the five characteristic fields in registers, register budget for 4
+ * blocks per SM; 3 the same with a budget for 3 blocks; 1 one thread per
+ * (face, sign, field).  All give the same result to the last few ulps. */
 int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl);
 int ocfd_b200_set_metrics_device(ocfd_b200_ctx *ctx, const double *metrics13_dev);
 

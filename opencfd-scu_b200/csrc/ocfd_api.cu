@@ -183,6 +183,8 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     p.scheme_invis = si; p.scheme_vis = cfg->scheme_vis; p.charteric = cfg->charteric;
     p.nochar_comp_flag = cfg->hybrid_nochar_same_flag ? 0 : 3;
     p.sweep_impl = 2;
+    p.inv_h[0] = 1.0 / p.hx; p.inv_h[1] = 1.0 / p.hy; p.inv_h[2] = 1.0 / p.hz;
+    p.inv_Ama = 1.0 / Ma;
     for (int d = 0; d < 3; d++) p.periodic[d] = cfg->iperiodic[d];
 
     size_t lapB = sizeof(double) * (size_t)p.lapN, inB = sizeof(double) * (size_t)N;
@@ -397,7 +399,7 @@ extern "C" int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode) {
 extern "C" int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx) { return ctx ? ctx->p.uniform_metrics : 0; }
 
 extern "C" int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl) {
-    if (!ctx || impl < 1 || impl > 2) return OCFD_ERR_ARG;
+    if (!ctx || impl < 1 || impl > 3) return OCFD_ERR_ARG;
     ctx->p.sweep_impl = impl;
     return OCFD_OK;
 }

@@ -42,6 +42,10 @@ template <int DIR> __device__ __forceinline__ double t_h(const Params &p) { retu
 
 // Steger-Warming split with the direction's |A| and A/|A| already formed
 // (same operations as sw_split, src/OCFD_split.cu:92-142)
+// EPS0: EPSL_SW = 0, where sqrt(E*E + 0) is exactly |E| (the square root of
+// a correctly rounded square returns the operand's magnitude), so the three
+// square roots reduce to fabs with the same result.
+template <bool EPS0>
 __device__ __forceinline__ void sw_split_pre(double tmp0, double u, double v, double w, double cc,
                                              double A1, double A2, double A3, double ss,
                                              double An1, double An2, double An3,
@@ -50,9 +54,9 @@ __device__ __forceinline__ void sw_split_pre(double tmp0, double u, double v, do
     double E1 = A1 * u + A2 * v + A3 * w;
     double E2 = E1 - cc * ss;
     double E3 = E1 + cc * ss;
-    double E1P = (E1 + sqrt(E1 * E1 + eps * eps)) * 0.50;
-    double E2P = (E2 + sqrt(E2 * E2 + eps * eps)) * 0.50;
-    double E3P = (E3 + sqrt(E3 * E3 + eps * eps)) * 0.50;
+    double E1P = (E1 + (EPS0 ? fabs(E1) : sqrt(E1 * E1 + eps * eps))) * 0.50;
+    double E2P = (E2 + (EPS0 ? fabs(E2) : sqrt(E2 * E2 + eps * eps))) * 0.50;
+    double E3P = (E3 + (EPS0 ? fabs(E3) : sqrt(E3 * E3 + eps * eps))) * 0.50;
     double E1M = E1 - E1P, E2M = E2 - E2P, E3M = E3 - E3P;
     double uc1 = u - cc * An1, uc2 = u + cc * An1;
     double vc1 = v - cc * An2, vc2 = v + cc * An2;
@@ -141,11 +145,21 @@ __device__ __forceinline__ void make_record(double u1, double v1, double w1, dou
     r[FM1 * nf] = cp.m1; r[FM2 * nf] = cp.m2; r[FM3 * nf] = cp.m3;
 }
 
+// UP7 (src/OCFD_Schemes.cu:865-907) with the /420 done by div_const
+__device__ __forceinline__ double up7_p_q(const double *s) {
+    return div_const(-3.0*s[0] + 25.0*s[1] - 101.0*s[2] + 319.0*s[3] + 214.0*s[4]
+                     - 38.0*s[5] + 4.0*s[6], 420.0, 1.0 / 420.0);
+}
+__device__ __forceinline__ double up7_m_q(const double *s) {
+    return div_const(-3.0*s[7] + 25.0*s[6] - 101.0*s[5] + 319.0*s[4] + 214.0*s[3]
+                     - 38.0*s[2] + 4.0*s[1], 420.0, 1.0 / 420.0);
+}
+
 // reconstruction of one (face, sign) of one field from v[0..7] = f(F-3..F+4)
 __device__ __forceinline__ double recon_one(const Params &p, int scheme, int hflag, int sign, const double *v) {
     if (sign == 0) {
         switch (scheme) {
-        case 301: return up7_p(v);
+        case 301: return up7_p_q(v);
         case 302: return weno5_p(v);
         case 303: return weno7_p(v);
         case 304: return symbo_p(0, p.tv_lim, p.tv_max, v);
@@ -155,13 +169,13 @@ __device__ __forceinline__ double recon_one(const Params &p, int scheme, int hfl
         case 308: return omp6_p(1, v);
         case 309: return omp6_p(2, v);
         default:
-            if (hflag == 1) return up7_p(v);
+            if (hflag == 1) return up7_p_q(v);
             if (hflag == 2) return weno7_p(v);
             return weno5_p(v);
         }
     }
     switch (scheme) {
-    case 301: return up7_m(v);
+    case 301: return up7_m_q(v);
     case 302: return weno5_m(v);
     case 303: return weno7_m(v);
     case 304: return symbo_m(0, p.tv_lim, p.tv_max, v);
@@ -171,14 +185,24 @@ __device__ __forceinline__ double recon_one(const Params &p, int scheme, int hfl
     case 308: return omp6_m(1, v);
     case 309: return omp6_m(2, v);
     default:
-        if (hflag == 1) return up7_m(v);
+        if (hflag == 1) return up7_m_q(v);
         if (hflag == 2) return weno7_m(v);
         return weno5_m(v);
     }
 }
 
-template <int DIR, bool UNI>
-__global__ void __launch_bounds__(Tile<DIR>::THREADS)
+// shared-memory position of tile point (s along DIR, row r): unit stride
+// along the direction the consecutive threads of phase B walk
+template <int DIR> __device__ __forceinline__ int spos(int s, int r) {
+    constexpr int TS = Tile<DIR>::TS, R = Tile<DIR>::R;
+    return DIR == 0 ? s + (TS + 8) * r : r + R * s;
+}
+
+// MINB: resident blocks per SM the register budget is fitted to (4 caps a
+// thread at 128 registers and spills part of the characteristic path;
+// 3 allows 170 and does not spill)
+template <int DIR, bool UNI, bool EPS0, int MINB>
+__global__ void __launch_bounds__(Tile<DIR>::THREADS, MINB)
 k_sweep2(Params p) {
     constexpr int TS = Tile<DIR>::TS, R = Tile<DIR>::R;
     constexpr int NP = (TS + 8) * R;      // split points
@@ -213,17 +237,17 @@ k_sweep2(Params p) {
         else          { r = q % R; s = q / R; }
         if (r0 + r >= nr || s0 + s - 4 > n + 3) continue;
         long long o = base + (long long)s * sd + (long long)r * sr;
-        double cc = sqrt(T[o]) / p.Ama;
+        double cc = div_const(sqrt(T[o]), p.Ama, p.inv_Ama);
         double fp[5], fm[5];
         if (UNI) {
             const DirConst &dc = p.dc[DIR];
-            sw_split_pre(d[o] * p.tmp0, u[o], v[o], w[o], cc, dc.A[0], dc.A[1], dc.A[2], dc.ss,
+            sw_split_pre<EPS0>(d[o] * p.tmp0, u[o], v[o], w[o], cc, dc.A[0], dc.A[1], dc.A[2], dc.ss,
                          dc.An[0], dc.An[1], dc.An[2], p, fp, fm);
         } else {
             sw_split(d[o] * p.tmp0, u[o], v[o], w[o], cc, metric<false>(p, mA, o), metric<false>(p, mA + 1, o),
                      metric<false>(p, mA + 2, o), p.Gamma, p.epsl_sw, p.split_C1, p.split_C3, fp, fm);
         }
-        int pi = s + (TS + 8) * r;
+        int pi = spos<DIR>(s, r);
 #pragma unroll
         for (int m = 0; m < 5; m++) { spl[m * NP + pi] = fp[m]; spl[(5 + m) * NP + pi] = fm[m]; }
     }
@@ -248,7 +272,8 @@ k_sweep2(Params p) {
         if (proj) {
             long long o0 = base + (long long)(fs + 3) * sd + (long long)r * sr;   // cell F
             long long o1 = o0 + sd;                                                // cell F+1
-            double c0v = sqrt(T[o0]) / p.Ama, c1v = sqrt(T[o1]) / p.Ama;
+            double c0v = div_const(sqrt(T[o0]), p.Ama, p.inv_Ama);
+            double c1v = div_const(sqrt(T[o1]), p.Ama, p.inv_Ama);
             double u1 = (u[o0] + u[o1]) * 0.5, v1 = (v[o0] + v[o1]) * 0.5, w1 = (w[o0] + w[o1]) * 0.5;
             double c1 = (c0v + c1v) * 0.5;
             if (UNI) {
@@ -272,26 +297,31 @@ k_sweep2(Params p) {
                             p, rec + fi, NF);
             }
         }
-        // face code: bits 0-9 index, bit 14 = projected, bits 10-13 = flag
+        // face code: bits 0-9 index, bits 10-13 flag, bit 14 projected; -1 = no face
         short code = (short)(fi | (hflag << 10) | (proj ? (1 << 14) : 0));
         if (!valid) code = -1;
         list[NF + fi] = code;
         if (proj) atomicAdd(&nchar, 1);
     }
     __syncthreads();
-    // stable partition of the faces: projected ones first (order inside the
-    // lists does not change any result; each face writes its own slot)
-    if (threadIdx.x == 0) {
-        int a = 0, b = nchar;
-        for (int fi = 0; fi < NF; fi++) {
-            short code = list[NF + fi];
-            if (code < 0) continue;
-            if (code & (1 << 14)) list[a++] = code; else list[b++] = code;
-        }
-        list[NF] = (short)b;      // number of valid faces (the copy above is consumed)
+    // Faces with a projection go first so the two costs do not share warps.
+    // Slots come from shared counters; the order inside each class does not
+    // change any result (every face writes its own flux slot).
+    const int nproj = nchar;
+    __shared__ int cnt[2];
+    if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (int fi = threadIdx.x; fi < NF; fi += blockDim.x) {
+        short code = list[NF + fi];
+        int slot;
+        if (code < 0) continue;
+        if (nproj == 0) slot = atomicAdd(&cnt[1], 1);
+        else if (code & (1 << 14)) slot = atomicAdd(&cnt[0], 1);
+        else slot = nproj + atomicAdd(&cnt[1], 1);
+        list[slot] = code;
     }
     __syncthreads();
-    const int nvalid = list[NF];
+    const int nvalid = cnt[0] + cnt[1];
 
     // ---- B: one thread per (face, sign)
     for (int t = threadIdx.x; t < 2 * nvalid; t += blockDim.x) {
@@ -302,7 +332,8 @@ k_sweep2(Params p) {
         int fs, r;
         if (DIR == 0) { fs = fi % (TS + 1); r = fi / (TS + 1); }
         else          { r = fi % R; fs = fi / R; }
-        const double *sp = spl + (sign * 5) * NP + fs + (TS + 8) * r;
+        const double *sp = spl + (sign * 5) * NP + spos<DIR>(fs, r);
+        constexpr int KS = DIR == 0 ? 1 : R;     // stencil stride in shared memory
         double out[5];
         if (comp_none) {
 #pragma unroll
@@ -312,7 +343,7 @@ k_sweep2(Params p) {
 #pragma unroll
             for (int m = 0; m < 5; m++)
 #pragma unroll
-                for (int k = 0; k < 8; k++) fv[m][k] = sp[m * NP + k];
+                for (int k = 0; k < 8; k++) fv[m][k] = sp[m * NP + k * KS];
             const double *rr = rec + fi;
 #pragma unroll
             for (int c = 0; c < 5; c++) {
@@ -335,7 +366,7 @@ k_sweep2(Params p) {
             for (int m = 0; m < 5; m++) {
                 double vals[8];
 #pragma unroll
-                for (int k = 0; k < 8; k++) vals[k] = sp[m * NP + k];
+                for (int k = 0; k < 8; k++) vals[k] = sp[m * NP + k * KS];
                 int hf = hflag;
                 if (hybrid && !char_scheme && m > 0 && p.nochar_comp_flag) hf = p.nochar_comp_flag;
                 out[m] = recon_one(p, scheme, hf, sign, vals);
@@ -347,7 +378,7 @@ k_sweep2(Params p) {
     __syncthreads();
 
     // ---- C: du of each tile cell (x+ then x- for every component)
-    const double h = t_h<DIR>(p);
+    const double h = t_h<DIR>(p), ih = p.inv_h[DIR];
     for (int t = threadIdx.x; t < NC; t += blockDim.x) {
         int s, r;
         if (DIR == 0) { s = t % TS; r = t / TS; }
@@ -366,14 +397,14 @@ k_sweep2(Params p) {
 #pragma unroll
         for (int m = 0; m < 5; m++) {
             double acc = (DIR == 0) ? 0.0 : p.du[m * p.N + ci];
-            acc += -aj * (hat[m * NF + fr] - hat[m * NF + fl]) / h;
-            acc += -aj * (hat[(5 + m) * NF + fr] - hat[(5 + m) * NF + fl]) / h;
+            acc += div_const(-aj * (hat[m * NF + fr] - hat[m * NF + fl]), h, ih);
+            acc += div_const(-aj * (hat[(5 + m) * NF + fr] - hat[(5 + m) * NF + fl]), h, ih);
             p.du[m * p.N + ci] = acc;
         }
     }
 }
 
-template <int DIR, bool UNI>
+template <int DIR, bool UNI, bool EPS0, int MINB>
 static cudaError_t launch_sweep2(const Params &p, cudaStream_t st) {
     using S = Tile<DIR>;
     constexpr int NP = (S::TS + 8) * S::R, NF = (S::TS + 1) * S::R;
@@ -384,25 +415,32 @@ static cudaError_t launch_sweep2(const Params &p, cudaStream_t st) {
     int n3 = DIR == 2 ? p.ny : p.nz;
     static size_t attr_bytes = 0;
     if (smem > attr_bytes) {
-        cudaError_t e = cudaFuncSetAttribute(k_sweep2<DIR, UNI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(k_sweep2<DIR, UNI, EPS0, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_bytes = smem;
     }
     dim3 grid((n + S::TS - 1) / S::TS, (nr + S::R - 1) / S::R, n3);
-    k_sweep2<DIR, UNI><<<grid, S::THREADS, smem, st>>>(p);
+    k_sweep2<DIR, UNI, EPS0, MINB><<<grid, S::THREADS, smem, st>>>(p);
     return cudaGetLastError();
 }
 
-template <bool UNI>
-static cudaError_t launch_sweeps2_t(const Params &p, cudaStream_t st) {
+template <bool UNI, bool EPS0, int MINB>
+static cudaError_t launch_sweeps2_m(const Params &p, cudaStream_t st) {
     cudaError_t e;
-    if ((e = launch_sweep2<0, UNI>(p, st)) != cudaSuccess) return e;
-    if ((e = launch_sweep2<1, UNI>(p, st)) != cudaSuccess) return e;
-    return launch_sweep2<2, UNI>(p, st);
+    if ((e = launch_sweep2<0, UNI, EPS0, MINB>(p, st)) != cudaSuccess) return e;
+    if ((e = launch_sweep2<1, UNI, EPS0, MINB>(p, st)) != cudaSuccess) return e;
+    return launch_sweep2<2, UNI, EPS0, MINB>(p, st);
+}
+template <bool UNI, bool EPS0>
+static cudaError_t launch_sweeps2_t(const Params &p, cudaStream_t st) {
+    return p.sweep_impl == 3 ? launch_sweeps2_m<UNI, EPS0, 3>(p, st) : launch_sweeps2_m<UNI, EPS0, 4>(p, st);
 }
 
 cudaError_t launch_sweeps2(const Params &p, cudaStream_t st) {
-    return p.uniform_metrics ? launch_sweeps2_t<true>(p, st) : launch_sweeps2_t<false>(p, st);
+    // the EPSL_SW = 0 shortcut only exists on the precomputed (uniform) path
+    if (p.uniform_metrics)
+        return p.epsl_sw == 0.0 ? launch_sweeps2_t<true, true>(p, st) : launch_sweeps2_t<true, false>(p, st);
+    return launch_sweeps2_t<false, false>(p, st);
 }
 
 // per-direction constants of a uniform grid, formed on the device with the

@@ -1,0 +1,92 @@
+"""Parity at the benchmark sizes.
+
+* C1 as configured: Taylor-Green vortex 64^3, WENO7 + CD6, 100 RK3 steps,
+  against the CPU oracle and against the reference's own CUDA build
+  (oracle/_ref, run live when it is present on the box).
+* C2 shape: isotropic turbulence 256^3, hybrid + characteristic projection,
+  a few steps against the reference build, and size-independent properties:
+  conservation of mass, momentum and energy on the periodic box, finite
+  state, bitwise repeatability.
+Tolerance: relative L2 <= 1e-12 per variable.
+"""
+import numpy as np
+import pytest
+
+from ocfd_b200 import cases, lib
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def rel_l2(a, b):
+    return np.array([np.linalg.norm(a[m] - b[m]) / np.linalg.norm(b[m]) for m in range(a.shape[0])])
+
+
+def _ref_runner():
+    from oracle import ref_runner
+    if not ref_runner.available():
+        pytest.skip("reference build (oracle/_ref) not present on this machine")
+    return ref_runner
+
+
+@pytest.fixture(scope="module")
+def tgv64():
+    case = cases.taylor_green(64, seed=1234)
+    s = lib.Solver(case.cfg, case.prims, case.metrics)
+    s.step(100)
+    return case, s.primitives(), s.conserved()
+
+
+def test_c1_tgv64_100_steps_vs_oracle(tgv64):
+    from oracle.oracle import Oracle
+    case, prims, cons = tgv64
+    o = Oracle(case.cfg, case.prims, case.metrics)
+    o.step(100)
+    assert np.all(rel_l2(prims, o.primitives()) <= TOL)
+    assert np.all(rel_l2(cons, o.conserved()) <= TOL)
+
+
+def test_c1_tgv64_100_steps_vs_reference(tgv64):
+    rr = _ref_runner()
+    case, prims, _ = tgv64
+    ref, istep, tt, wall, _ = rr.run_and_read(cases.taylor_green(64, seed=1234), 100)
+    assert istep == 100
+    err = rel_l2(prims, ref)
+    assert np.all(err <= TOL), err
+
+
+@pytest.fixture(scope="module")
+def iso256():
+    case = cases.isotropic_turbulence(256, seed=2024, charteric=1)
+    s = lib.Solver(case.cfg, case.prims, case.metrics)
+    f0 = s.conserved()
+    s.step(3)
+    return case, s, f0
+
+
+def test_c2_iso256_conservation_and_finite(iso256):
+    case, s, f0 = iso256
+    f3 = s.conserved()
+    assert np.isfinite(f3).all()
+    nnan, nneg, _ = s.check_state()
+    assert nnan == 0 and nneg == 0
+    for m in range(5):
+        scale = np.abs(f0[m]).sum()
+        drift = abs(f3[m].sum() - f0[m].sum()) / scale
+        assert drift < 1e-12, (m, drift)
+
+
+def test_c2_iso256_repeatable(iso256):
+    case, s, _ = iso256
+    s2 = lib.Solver(case.cfg, case.prims, case.metrics)
+    s2.step(3)
+    assert np.array_equal(s2.primitives(), s.primitives())
+
+
+def test_c2_iso256_vs_reference(iso256):
+    rr = _ref_runner()
+    case, s, _ = iso256
+    ref, istep, tt, wall, _ = rr.run_and_read(cases.isotropic_turbulence(256, seed=2024, charteric=1), 3)
+    err = rel_l2(s.primitives(), ref)
+    assert np.all(err <= TOL), err
