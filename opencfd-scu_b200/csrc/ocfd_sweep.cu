@@ -472,4 +472,142 @@ cudaError_t compute_dirconst(Params &p, DirConst *dev_scratch, cudaStream_t st) 
     return cudaStreamSynchronize(st);
 }
 
+
+// ===========================================================================
+// Third-generation sweeps: no block barriers.
+//   x: a warp owns 32 consecutive faces of one row; its lanes compute the
+//      40 split points of the strip into warp-private shared memory
+//      (__syncwarp only), then each lane forms its face flux (both signs,
+//      all five fields) and the du of its cell.
+//   y, z: each lane owns one x column and marches along the sweep direction,
+//      keeping the split values of the last 8 points in a lane-private ring
+//      in shared memory; every point is split once, every face is formed
+//      once, and du(X) uses the face kept from the previous step.
+// Boundary closures of non-periodic directions (src/OCFD_bound_Scheme.cu)
+// are applied per face; non-reflecting faces and the characteristic
+// kernels' first-order boundary fluxes per cell.
+// ===========================================================================
+
+// one-sided WENO5 candidates used by the closures, src/OCFD_bound_Scheme.cu:554-745;
+// s[0..4] = f(i-2..i+2)
+__device__ __forceinline__ double w5_p_left(const double *s) {
+    double S0 = 0.0, tmp; const double ep = 1e-6;
+    tmp = s[2] - 2.0*s[3] + s[4]; S0 += 13*tmp*tmp;
+    tmp = 3.0*s[2] - 4.0*s[3] + s[4]; S0 += 3*tmp*tmp;
+    double a0 = 1.0/((12.0*ep + S0)*(12.0*ep + S0));
+    double q03 = (2.0*s[2] + 5.0*s[3] - s[4]);
+    return a0*q03/(6.0*a0);
+}
+__device__ __forceinline__ double w5_m_left(const double *s) {
+    double S2 = 0.0, tmp; const double ep = 1e-6;
+    tmp = s[4] - 2.0*s[3] + s[2]; S2 += 13*tmp*tmp;
+    tmp = s[4] - 4.0*s[3] + 3.0*s[2]; S2 += 3*tmp*tmp;
+    double a2 = 1.0/((12.0*ep + S2)*(12.0*ep + S2));
+    double q23 = (2.0*s[4] - 7.0*s[3] + 11.0*s[2]);
+    return a2*q23/(6.0*a2);
+}
+__device__ __forceinline__ double w5_p_right_plus(const double *s) {
+    double S1 = 0.0, S2 = 0.0, tmp; const double ep = 1e-6;
+    tmp = s[1] - 2.0*s[2] + s[3]; S1 += 13*tmp*tmp;
+    tmp = s[1] - s[3]; S1 += 3*tmp*tmp;
+    double a1 = 6.0/((12.0*ep + S1)*(12.0*ep + S1));
+    double q13 = (-s[1] + 5.0*s[2] + 2.0*s[3]);
+    tmp = s[0] - 2.0*s[1] + s[2]; S2 += 13*tmp*tmp;
+    tmp = s[0] - 4.0*s[1] + 3.0*s[2]; S2 += 3*tmp*tmp;
+    double a2 = 1.0/((12.0*ep + S2)*(12.0*ep + S2));
+    double q23 = (2.0*s[0] - 7.0*s[1] + 11.0*s[2]);
+    return (a1*q13 + a2*q23)/(6.0*(a1 + a2));
+}
+__device__ __forceinline__ double w5_p_left_plus(const double *s) {
+    double S0 = 0.0, S1 = 0.0, tmp; const double ep = 1e-6;
+    tmp = s[2] - 2.0*s[3] + s[4]; S0 += 13*tmp*tmp;
+    tmp = 3.0*s[2] - 4.0*s[3] + s[4]; S0 += 3*tmp*tmp;
+    double a0 = 3.0/((12.0*ep + S0)*(12.0*ep + S0));
+    double q03 = (2.0*s[2] + 5.0*s[3] - s[4]);
+    tmp = s[1] - 2.0*s[2] + s[3]; S1 += 13*tmp*tmp;
+    tmp = s[1] - s[3]; S1 += 3*tmp*tmp;
+    double a1 = 6.0/((12.0*ep + S1)*(12.0*ep + S1));
+    double q13 = (-s[1] + 5.0*s[2] + 2.0*s[3]);
+    return (a0*q03 + a1*q13)/(6.0*(a0 + a1));
+}
+__device__ __forceinline__ double w5_m_right_plus(const double *s) {
+    double S0 = 0.0, S1 = 0.0, tmp; const double ep = 1e-6;
+    tmp = s[2] - 2.0*s[1] + s[0]; S0 += 13*tmp*tmp;
+    tmp = 3.0*s[2] - 4.0*s[1] + s[0]; S0 += 3*tmp*tmp;
+    double a0 = 3.0/((12.0*ep + S0)*(12.0*ep + S0));
+    double q03 = (2.0*s[2] + 5.0*s[1] - s[0]);
+    tmp = s[3] - 2.0*s[2] + s[1]; S1 += 13*tmp*tmp;
+    tmp = s[3] - s[1]; S1 += 3*tmp*tmp;
+    double a1 = 6.0/((12.0*ep + S1)*(12.0*ep + S1));
+    double q13 = (-s[3] + 5.0*s[2] + 2.0*s[1]);
+    return (a0*q03 + a1*q13)/(6.0*(a0 + a1));
+}
+__device__ __forceinline__ double w5_m_left_plus(const double *s) {
+    double S1 = 0.0, S2 = 0.0, tmp; const double ep = 1e-6;
+    tmp = s[3] - 2.0*s[2] + s[1]; S1 += 13*tmp*tmp;
+    tmp = s[3] - s[1]; S1 += 3*tmp*tmp;
+    double a1 = 6.0/((12.0*ep + S1)*(12.0*ep + S1));
+    double q13 = (-s[3] + 5.0*s[2] + 2.0*s[1]);
+    tmp = s[4] - 2.0*s[3] + s[2]; S2 += 13*tmp*tmp;
+    tmp = s[4] - 4.0*s[3] + 3.0*s[2]; S2 += 3*tmp*tmp;
+    double a2 = 1.0/((12.0*ep + S2)*(12.0*ep + S2));
+    double q23 = (2.0*s[4] - 7.0*s[3] + 11.0*s[2]);
+    return (a1*q13 + a2*q23)/(6.0*(a1 + a2));
+}
+
+// Closure of face F+1/2 of a line of n cells, v[t] = f(F-3+t); returns true
+// when it replaces the interior scheme (OCFD_bound_scheme_kernel_p / _m with
+// boundp1/boundp2/boundm1/boundm2, :748-944).  KA, KB: stencil extents
+// (-ia1, ib1) of the reference kernel of this sign.
+__device__ __forceinline__ bool closure(int sign, bool lo, bool hi, int KA, int KB, int F, int n,
+                                        const double *v, double &out) {
+    int c = F + 1;
+    if (sign == 0) {
+        if (lo && c <= KA) {
+            if (c == 0) out = v[4];
+            else if (c == 1) out = w5_p_left(v + 1);
+            else if (c == 2) out = w5_p_left_plus(v + 1);
+            else out = weno5_p(v);
+            return true;
+        }
+        if (hi) {
+            int t = c - (n + 1);
+            if (t >= -KB) {
+                if (t == -1) out = v[3] + 0.5 * minmod2(v[3] - v[2], v[3] - v[2]);
+                else if (t == -2) out = w5_p_right_plus(v + 1);
+                else out = weno5_p(v);
+                return true;
+            }
+        }
+        return false;
+    }
+    if (lo && c < KA) {
+        if (c == 0) out = w5_m_left(v + 2);
+        else if (c == 1) out = w5_m_left_plus(v + 2);
+        else out = weno5_m(v);
+        return true;
+    }
+    if (hi) {
+        int t = c - (n + 1);
+        if (t >= -KB - 1) {
+            if (t == -1) out = v[3];
+            else if (t == -2) out = v[4] - 0.5 * minmod2(v[4] - v[3], v[4] - v[3]);
+            else if (t == -3) out = w5_m_right_plus(v + 2);
+            else out = weno5_m(v);
+            return true;
+        }
+    }
+    return false;
+}
+
+// stencil extents of the reference kernels per scheme and sign (P: -ia1, ib1)
+__device__ __forceinline__ void extents(int scheme, bool chart, int sign, int &KA, int &KB) {
+    if (chart) { KA = sign ? 4 : 3; KB = sign ? 3 : 4; return; }
+    switch (scheme) {
+    case 302: case 306: KA = 2; KB = 2; break;
+    case 303: KA = 3; KB = 3; break;
+    default: KA = sign ? 4 : 3; KB = sign ? 3 : 4; break;
+    }
+}
+
 }  // namespace ocfd

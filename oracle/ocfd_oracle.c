@@ -833,6 +833,149 @@ static inline int face_flag(const oro_state *s, int dir, int i, int j, int k) {
 /* inviscid sweeps                                                           */
 /* ------------------------------------------------------------------------ */
 
+/* ------------------------------------------------------------------------ */
+/* boundary closures on non-periodic directions, src/OCFD_bound_Scheme.cu    */
+/* ------------------------------------------------------------------------ */
+
+/* one-sided WENO5 candidates, :554-745; s[0..4] = f(i-2..i+2) (P) */
+static double w5_p_right(const double *s) {
+    double S2 = 0.0, tmp, ep = 1e-6;
+    tmp = s[0] - 2.0*s[1] +     s[2]; S2 += 13*tmp*tmp;
+    tmp = s[0] - 4.0*s[1] + 3.0*s[2]; S2 +=  3*tmp*tmp;
+    double a2 = 1.0/((12.0*ep + S2)*(12.0*ep + S2));
+    double q23 = (2.0*s[0] - 7.0*s[1] + 11.0*s[2]);
+    return a2*q23/(6.0*a2);
+}
+static double w5_p_left(const double *s) {
+    double S0 = 0.0, tmp, ep = 1e-6;
+    tmp =     s[2] - 2.0*s[3] + s[4]; S0 += 13*tmp*tmp;
+    tmp = 3.0*s[2] - 4.0*s[3] + s[4]; S0 +=  3*tmp*tmp;
+    double a0 = 1.0/((12.0*ep + S0)*(12.0*ep + S0));
+    double q03 = (2.0*s[2] + 5.0*s[3] - s[4]);
+    return a0*q03/(6.0*a0);
+}
+static double w5_m_right(const double *s) {
+    double S0 = 0.0, tmp, ep = 1e-6;
+    tmp =     s[2] - 2.0*s[1] + s[0]; S0 += 13*tmp*tmp;
+    tmp = 3.0*s[2] - 4.0*s[1] + s[0]; S0 +=  3*tmp*tmp;
+    double a0 = 1.0/((12.0*ep + S0)*(12.0*ep + S0));
+    double q03 = (2.0*s[2] + 5.0*s[1] - s[0]);
+    return a0*q03/(6.0*a0);
+}
+static double w5_m_left(const double *s) {
+    double S2 = 0.0, tmp, ep = 1e-6;
+    tmp = s[4] - 2.0*s[3] +     s[2]; S2 += 13*tmp*tmp;
+    tmp = s[4] - 4.0*s[3] + 3.0*s[2]; S2 +=  3*tmp*tmp;
+    double a2 = 1.0/((12.0*ep + S2)*(12.0*ep + S2));
+    double q23 = (2.0*s[4] - 7.0*s[3] + 11.0*s[2]);
+    return a2*q23/(6.0*a2);
+}
+static double w5_p_right_plus(const double *s) {
+    double S1 = 0.0, S2 = 0.0, tmp, ep = 1e-6;
+    tmp = s[1] - 2.0*s[2] + s[3]; S1 += 13*tmp*tmp;
+    tmp =             s[1] - s[3]; S1 +=  3*tmp*tmp;
+    double a1 = 6.0/((12.0*ep + S1)*(12.0*ep + S1));
+    double q13 = (-s[1] + 5.0*s[2] + 2.0*s[3]);
+    tmp = s[0] - 2.0*s[1] +     s[2]; S2 += 13*tmp*tmp;
+    tmp = s[0] - 4.0*s[1] + 3.0*s[2]; S2 +=  3*tmp*tmp;
+    double a2 = 1.0/((12.0*ep + S2)*(12.0*ep + S2));
+    double q23 = (2.0*s[0] - 7.0*s[1] + 11.0*s[2]);
+    return (a1*q13 + a2*q23)/(6.0*(a1 + a2));
+}
+static double w5_p_left_plus(const double *s) {
+    double S0 = 0.0, S1 = 0.0, tmp, ep = 1e-6;
+    tmp =     s[2] - 2.0*s[3] + s[4]; S0 += 13*tmp*tmp;
+    tmp = 3.0*s[2] - 4.0*s[3] + s[4]; S0 +=  3*tmp*tmp;
+    double a0 = 3.0/((12.0*ep + S0)*(12.0*ep + S0));
+    double q03 = (2.0*s[2] + 5.0*s[3] - s[4]);
+    tmp = s[1] - 2.0*s[2] + s[3]; S1 += 13*tmp*tmp;
+    tmp =             s[1] - s[3]; S1 +=  3*tmp*tmp;
+    double a1 = 6.0/((12.0*ep + S1)*(12.0*ep + S1));
+    double q13 = (-s[1] + 5.0*s[2] + 2.0*s[3]);
+    return (a0*q03 + a1*q13)/(6.0*(a0 + a1));
+}
+static double w5_m_right_plus(const double *s) {
+    double S0 = 0.0, S1 = 0.0, tmp, ep = 1e-6;
+    tmp =     s[2] - 2.0*s[1] + s[0]; S0 += 13*tmp*tmp;
+    tmp = 3.0*s[2] - 4.0*s[1] + s[0]; S0 +=  3*tmp*tmp;
+    double a0 = 3.0/((12.0*ep + S0)*(12.0*ep + S0));
+    double q03 = (2.0*s[2] + 5.0*s[1] - s[0]);
+    tmp = s[3] - 2.0*s[2] + s[1]; S1 += 13*tmp*tmp;
+    tmp =             s[3] - s[1]; S1 +=  3*tmp*tmp;
+    double a1 = 6.0/((12.0*ep + S1)*(12.0*ep + S1));
+    double q13 = (-s[3] + 5.0*s[2] + 2.0*s[1]);
+    return (a0*q03 + a1*q13)/(6.0*(a0 + a1));
+}
+static double w5_m_left_plus(const double *s) {
+    double S1 = 0.0, S2 = 0.0, tmp, ep = 1e-6;
+    tmp = s[3] - 2.0*s[2] + s[1]; S1 += 13*tmp*tmp;
+    tmp =             s[3] - s[1]; S1 +=  3*tmp*tmp;
+    double a1 = 6.0/((12.0*ep + S1)*(12.0*ep + S1));
+    double q13 = (-s[3] + 5.0*s[2] + 2.0*s[1]);
+    tmp = s[4] - 2.0*s[3] +     s[2]; S2 += 13*tmp*tmp;
+    tmp = s[4] - 4.0*s[3] + 3.0*s[2]; S2 +=  3*tmp*tmp;
+    double a2 = 1.0/((12.0*ep + S2)*(12.0*ep + S2));
+    double q23 = (2.0*s[4] - 7.0*s[3] + 11.0*s[2]);
+    return (a1*q13 + a2*q23)/(6.0*(a1 + a2));
+}
+
+/* Stencil extents (-ia1, ib1) of the reference kernels, which decide how far
+ * the closures reach: P kernels and M kernels of each scheme. */
+static void closure_extent(int scheme, int chart, int *kap, int *kbp, int *kam, int *kbm) {
+    if (chart) { *kap = 3; *kbp = 4; *kam = 4; *kbm = 3; return; }
+    switch (scheme) {
+    case 302: case 306: *kap = 2; *kbp = 2; *kam = 2; *kbm = 2; break;   /* WENO5, NND2 */
+    case 303: *kap = 3; *kbp = 3; *kam = 3; *kbm = 3; break;             /* WENO7 */
+    default:  *kap = 3; *kbp = 4; *kam = 4; *kbm = 3; break;             /* UP7, SYMBO, OMP6, hybrid */
+    }
+}
+
+/* P-side closure of face F+1/2 on a line of n cells, s8[t] = f(F-3+t):
+ * OCFD_bound_scheme_kernel_p with boundp1 / boundp2 (:748-848).
+ * Returns 1 when the closure replaces the interior scheme. */
+static int closure_p(int lo, int hi, int KA, int KB, int F, int n, const double *s8, double *out) {
+    int c = F + 1;
+    if (lo && c <= KA) {
+        if (c == 0) *out = s8[4];
+        if (c == 1) *out = w5_p_left(s8 + 1);
+        if (c == 2) *out = w5_p_left_plus(s8 + 1);
+        if (c == 3) *out = oro_weno5_p(s8 + 1);
+        return 1;
+    }
+    if (hi) {
+        int t = c - (n + 1);
+        if (t >= -KB) {
+            if (t == -1) *out = s8[3] + 0.5*minmod2(s8[3] - s8[2], s8[3] - s8[2]);
+            if (t == -2) *out = w5_p_right_plus(s8 + 1);
+            if (t <= -3) *out = oro_weno5_p(s8 + 1);
+            return 1;
+        }
+    }
+    return 0;
+}
+
+/* M-side closure, OCFD_bound_scheme_kernel_m with boundm1 / boundm2 (:850-944) */
+static int closure_m(int lo, int hi, int KA, int KB, int F, int n, const double *s8, double *out) {
+    int c = F + 1;
+    if (lo && c < KA) {
+        if (c == 0) *out = w5_m_left(s8 + 2);
+        if (c == 1) *out = w5_m_left_plus(s8 + 2);
+        if (c >= 2) *out = oro_weno5_m(s8 + 2);
+        return 1;
+    }
+    if (hi) {
+        int t = c - (n + 1);
+        if (t >= -KB - 1) {
+            if (t == -1) *out = s8[3];
+            if (t == -2) *out = s8[4] - 0.5*minmod2(s8[4] - s8[3], s8[4] - s8[3]);
+            if (t == -3) *out = w5_m_right_plus(s8 + 2);
+            if (t == -4) *out = oro_weno5_m(s8 + 2);
+            return 1;
+        }
+    }
+    return 0;
+}
+
 /* face flux of one component from the 8-point stencil s8[k] = f(F-3+k) */
 static double face_p(const oro_state *s, int scheme, int hflag, const double *s8) {
     switch (scheme) {
