@@ -149,6 +149,26 @@ const char *ocfd_b200_timer_name(int index);
 /* number of kernel launches issued by the library so far */
 long long ocfd_b200_launch_count(const ocfd_b200_ctx *ctx);
 
+/* ---- allocation-free field means (no counterpart in the reference) ---- */
+/* FP64 means of nfield dense fields of n doubles each, laid out one after
+ * another at `fields`; means[f] = sum(field f) / n.  Both pointers are
+ * device memory on the calling thread's current device; the call is
+ * asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream).
+ * It allocates nothing, for callers that keep their fields in their own
+ * device buffers and may not allocate between steps (no context is
+ * created; no cudaMalloc/cudaFree and their implicit synchronisation).
+ * Partial sums go to one fixed device array shared by every call on a
+ * device: at most OCFD_NOALLOC_MAX_FIELDS fields x 592 partials (37,888
+ * bytes); nfield above the maximum returns OCFD_ERR_ARG with the reason in
+ * ocfd_b200_last_error(NULL).  The first call on a device looks up that
+ * array's address, so make it before any stream capture on that device.
+ * Calls that overlap in time on one device (other streams, other threads)
+ * race on the shared array; order them.  For the same values the mean is
+ * bitwise that of ocfd_b200_ana_residual. */
+#define OCFD_NOALLOC_MAX_FIELDS 8
+int ocfd_b200_field_means_noalloc(const double *fields, int nfield, long long n, double *means,
+                                  void *stream);
+
 /* ---- reference-named entry points (act on the bound context) ---------- */
 int  ocfd_b200_compat_bind(ocfd_b200_ctx *ctx);
 void du_comput(int KRK);                    /* head/OCFD_Stream.h:10           */

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 namespace ocfd {
@@ -659,4 +660,111 @@ extern "C" void Set_Scheme_HybridAuto(void *stream) {
     if (!g_bound) { compat_report(OCFD_ERR_STATE, "Set_Scheme_HybridAuto"); return; }
     cudaError_t e = ocfd::launch_sensor(g_bound->p, g_bound->stream);
     compat_report(e == cudaSuccess ? OCFD_OK : OCFD_ERR_CUDA, "Set_Scheme_HybridAuto");
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free field means (no counterpart in the reference).
+//
+// For callers that own their device arrays and cannot allocate: a host code
+// that keeps its fields in its own device buffers (the reference sizes its
+// arrays to the whole GPU) and wants the FP64 residual means between steps
+// without creating a solver context, which allocates the whole state, and
+// without cudaMalloc/cudaFree, whose implicit device synchronisation would
+// stall its pipeline.  The partial sums live in one file-scope device array
+// that every call on a device shares; nothing is allocated per call.
+//
+// Same blocks, same per-thread order and same tree as the context reduction
+// (launch_mean), so the mean of a field equals ocfd_b200_ana_residual's to
+// the last bit when it is given the same values.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int NA_BLOCKS = 592;        // partial sums per field (4 x 148 SMs)
+constexpr int NA_THREADS = 256;
+constexpr int NA_MAX_FIELDS = OCFD_NOALLOC_MAX_FIELDS;
+constexpr int NA_MAX_DEVICES = 64;
+
+// 8 fields x 592 partials x 8 bytes = 37,888 bytes per device.  Host code
+// never names this array directly; it reaches it through the address that
+// cudaGetSymbolAddress returns on each device.
+static __device__ __align__(256) double g_mean_scratch[NA_MAX_FIELDS * NA_BLOCKS];
+
+__global__ void __launch_bounds__(NA_THREADS) k_field_mean_partial(const double *fields, long long n,
+                                                                  double *partial) {
+    __shared__ double sh[NA_THREADS];
+    const double *src = fields + (long long)blockIdx.y * n;
+    double acc = 0.0;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) acc += src[q];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = NA_THREADS / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.y * NA_BLOCKS + blockIdx.x] = sh[0];
+}
+
+__global__ void __launch_bounds__(NA_THREADS) k_field_mean_final(const double *partial, long long n,
+                                                                double *means) {
+    __shared__ double sh[NA_THREADS];
+    const double *src = partial + blockIdx.x * NA_BLOCKS;
+    double acc = 0.0;
+    for (int q = threadIdx.x; q < NA_BLOCKS; q += blockDim.x) acc += src[q];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = NA_THREADS / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) sh[threadIdx.x] += sh[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) means[blockIdx.x] = sh[0] / (double)n;
+}
+
+std::mutex g_na_mutex;
+double *g_na_scratch[NA_MAX_DEVICES] = {};
+
+// Address of this device's copy of g_mean_scratch, looked up once per device
+// (on the first call made with that device current) and cached.
+int noalloc_scratch(int dev, double **out) {
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_scratch[dev]) {
+        double *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_mean_scratch);
+        if (e != cudaSuccess) return cuda_fail(nullptr, e, "field_means_noalloc: cudaGetSymbolAddress");
+        g_na_scratch[dev] = ptr;
+    }
+    *out = g_na_scratch[dev];
+    return OCFD_OK;
+}
+
+}  // namespace
+
+extern "C" int ocfd_b200_field_means_noalloc(const double *fields, int nfield, long long n, double *means,
+                                             void *stream) {
+    if (!fields || !means) return fail(nullptr, OCFD_ERR_ARG, "field_means_noalloc: null fields or means");
+    if (nfield < 1 || nfield > NA_MAX_FIELDS)
+        return fail(nullptr, OCFD_ERR_ARG,
+                    "field_means_noalloc: nfield = " + std::to_string(nfield) + " is outside 1.." +
+                        std::to_string(NA_MAX_FIELDS) + " (the fixed scratch holds " +
+                        std::to_string(NA_MAX_FIELDS) + " x " + std::to_string(NA_BLOCKS) + " partial sums)");
+    if (n < 1 || n > (1LL << 40))
+        return fail(nullptr, OCFD_ERR_ARG, "field_means_noalloc: n = " + std::to_string(n) + " is outside 1..2^40");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "field_means_noalloc: cudaGetDevice");
+    if (dev < 0 || dev >= NA_MAX_DEVICES)
+        return fail(nullptr, OCFD_ERR_ARG, "field_means_noalloc: device ordinal above 63");
+    double *scratch = nullptr;
+    int rc = noalloc_scratch(dev, &scratch);
+    if (rc) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // every partial slot the final kernel reads is written by the first
+    // kernel of the same call, so nothing in the scratch needs clearing
+    k_field_mean_partial<<<dim3(NA_BLOCKS, nfield), NA_THREADS, 0, st>>>(fields, n, scratch);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "field_means_noalloc: partial sums");
+    k_field_mean_final<<<nfield, NA_THREADS, 0, st>>>(scratch, n, means);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "field_means_noalloc: final sums");
+    return OCFD_OK;
 }

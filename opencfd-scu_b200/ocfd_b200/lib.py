@@ -36,7 +36,7 @@ EXPORTED = (
     "ocfd_b200_get_du", "ocfd_b200_get_flags", "ocfd_b200_get_time", "ocfd_b200_set_timing",
     "ocfd_b200_ana_residual", "ocfd_b200_check_state",
     "ocfd_b200_get_timing", "ocfd_b200_timer_name", "ocfd_b200_launch_count",
-    "ocfd_b200_compat_bind", "du_comput", "OCFD_time_advance", "get_duvwT", "get_Amu",
+    "ocfd_b200_compat_bind", "ocfd_b200_field_means_noalloc", "du_comput", "OCFD_time_advance", "get_duvwT", "get_Amu",
     "OCFD_bc", "Set_Scheme_HybridAuto",
 )
 
@@ -126,6 +126,7 @@ def load(path: Optional[str] = None):
         "ocfd_b200_timer_name": (ctypes.c_char_p, [ctypes.c_int]),
         "ocfd_b200_launch_count": (ctypes.c_longlong, [P]),
         "ocfd_b200_compat_bind": (ctypes.c_int, [P]),
+        "ocfd_b200_field_means_noalloc": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_longlong, P, P]),
         "du_comput": (None, [ctypes.c_int]),
         "OCFD_time_advance": (None, [ctypes.c_int]),
         "get_duvwT": (None, []),
