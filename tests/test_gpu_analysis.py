@@ -47,7 +47,9 @@ def test_uniform_metric_path_matches_field_path(gpu_lib):
     b.step(3)
     pa, pb = a.primitives(), b.primitives()
     err = max(np.linalg.norm(pa[m] - pb[m]) / np.linalg.norm(pb[m]) for m in range(5))
-    assert err <= 1e-14, err
+    # the variants contract multiply-adds differently; WENO weights amplify
+    # that, so they agree to the parity bound rather than to the last bit
+    assert err <= 1e-12, err
 
 
 def test_curvilinear_grid_uses_field_path(gpu_lib):

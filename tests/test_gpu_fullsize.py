@@ -5,8 +5,8 @@
   (oracle/_ref, run live when it is present on the box).
 * C2 shape: isotropic turbulence 256^3, hybrid + characteristic projection,
   a few steps against the reference build, and size-independent properties:
-  conservation of mass, momentum and energy on the periodic box, finite
-  state, bitwise repeatability.
+  finite state, bitwise repeatability, and (on a single-scheme run) exact
+  conservation of mass, momentum and energy on the periodic box.
 Tolerance: relative L2 <= 1e-12 per variable.
 """
 import numpy as np
@@ -65,16 +65,30 @@ def iso256():
     return case, s, f0
 
 
-def test_c2_iso256_conservation_and_finite(iso256):
+def test_c2_iso256_finite(iso256):
     case, s, f0 = iso256
     f3 = s.conserved()
     assert np.isfinite(f3).all()
     nnan, nneg, _ = s.check_state()
     assert nnan == 0 and nneg == 0
+
+
+def test_iso256_weno7_conserves_mass_momentum_energy():
+    # The hybrid scheme is not discretely conservative in the reference: the
+    # sensor reads ghost cells that are one stage old and ghost corners that
+    # are never filled, so the two images of a periodic seam face can get
+    # different schemes (the oracle drifts by ~1e-5 in mass at 32^3 after 3
+    # steps).  A single-scheme run conserves to round-off.
+    case = cases.isotropic_turbulence(256, seed=2024, charteric=0)
+    case.cfg.scheme_invis = "WENO7"
+    s = lib.Solver(case.cfg, case.prims, case.metrics)
+    f0 = s.conserved()
+    s.step(2)
+    f2 = s.conserved()
     for m in range(5):
         scale = np.abs(f0[m]).sum()
-        drift = abs(f3[m].sum() - f0[m].sum()) / scale
-        assert drift < 1e-12, (m, drift)
+        drift = abs(f2[m].sum() - f0[m].sum()) / scale
+        assert drift < 1e-13, (m, drift)
 
 
 def test_c2_iso256_repeatable(iso256):
