@@ -93,10 +93,13 @@ int ocfd_b200_set_metrics(ocfd_b200_ctx *ctx, const double *metrics13);
  * effect at the next set_metrics.  uniform_metrics reports the choice. */
 int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode);
 int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx);
-/* Inviscid sweep kernel variant: 2 (default) one thread per (face, sign)
+/* Inviscid sweep kernel variant: 4 (default) no block barriers: each warp
+ * walks its own lines (one x row, or 8 y or z lines) through a ring of
+ * split values in shared memory; 2 one thread per (face, sign) in tiles
  * with the five characteristic fields in registers, register budget for 4
  * blocks per SM; 3 the same with a budget for 3 blocks; 1 one thread per
- * (face, sign, field).  All give the same result to the last few ulps. */
+ * (face, sign, field).  All agree to the parity bound (WENO weights
+ * amplify the different multiply-add contractions). */
 int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl);
 int ocfd_b200_set_metrics_device(ocfd_b200_ctx *ctx, const double *metrics13_dev);
 

@@ -33,6 +33,7 @@ cudaError_t launch_mean(const Params &p, int which, double *scratch, unsigned lo
                         cudaStream_t st);
 int reduce_scratch_doubles();
 cudaError_t launch_sweeps2(const Params &p, cudaStream_t st);
+cudaError_t launch_sweeps3(const Params &p, cudaStream_t st);
 cudaError_t compute_dirconst(Params &p, DirConst *dev_scratch, cudaStream_t st);
 }  // namespace ocfd
 
@@ -183,7 +184,7 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     p.dp1 = cfg->hy_dp_intv[0]; p.dp2 = cfg->hy_dp_intv[1];
     p.scheme_invis = si; p.scheme_vis = cfg->scheme_vis; p.charteric = cfg->charteric;
     p.nochar_comp_flag = cfg->hybrid_nochar_same_flag ? 0 : 3;
-    p.sweep_impl = 2;
+    p.sweep_impl = 4;
     p.inv_h[0] = 1.0 / p.hx; p.inv_h[1] = 1.0 / p.hy; p.inv_h[2] = 1.0 / p.hz;
     p.inv_Ama = 1.0 / Ma;
     for (int d = 0; d < 3; d++) p.periodic[d] = cfg->iperiodic[d];
@@ -320,8 +321,9 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
     }
     {
         TimerScope ts(ctx, T_SWEEP);
-        if (p.sweep_impl == 1) CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
-        else                   CK(ocfd::launch_sweeps2(p, ctx->stream), "inviscid sweeps");
+        if (p.sweep_impl == 1)      CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
+        else if (p.sweep_impl == 4) CK(ocfd::launch_sweeps3(p, ctx->stream), "inviscid sweeps");
+        else                        CK(ocfd::launch_sweeps2(p, ctx->stream), "inviscid sweeps");
         ctx->launches += 3;
     }
     {
@@ -400,7 +402,7 @@ extern "C" int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode) {
 extern "C" int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx) { return ctx ? ctx->p.uniform_metrics : 0; }
 
 extern "C" int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl) {
-    if (!ctx || impl < 1 || impl > 3) return OCFD_ERR_ARG;
+    if (!ctx || impl < 1 || impl > 4) return OCFD_ERR_ARG;
     ctx->p.sweep_impl = impl;
     return OCFD_OK;
 }

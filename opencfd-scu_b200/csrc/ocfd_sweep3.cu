@@ -1,0 +1,325 @@
+// ocfd_sweep3.cu -- inviscid flux sweeps without block barriers (sm_100a, FP64).
+//
+// Same results as the reference's OCFD_d{x,y,z}1/2 chain (src/OCFD_Schemes_Choose.cu:88-764,
+// src/OCFD_Schemes.cu, src/OCFD_flux_charteric.cu, src/OCFD_Schemes_hybrid_auto.cu:862-1023),
+// organised so that every split point and every face flux is formed once and
+// nothing waits on other warps: each warp walks its own lines through a ring
+// of split values in shared memory, synchronising only itself.
+//
+// Faces that need more than the upwind UP7 formula (WENO/SYMBO/OMP/NND,
+// characteristic projection, hybrid flags other than 1) go through one
+// out-of-line routine that reads the face's 8-point window from the ring.
+#include "ocfd_face.cuh"
+
+#include <cuda_runtime.h>
+
+namespace ocfd {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// window over the split values of one face: at(sv, k) = value sv
+// (sign * 5 + field) of stencil point k (face F+1/2: point F-3+k)
+struct Win {
+    const double *b;
+    int ks, vs, mask, s0;
+    __device__ __forceinline__ double at(int sv, int k) const { return b[((s0 + k) & mask) * ks + sv * vs]; }
+};
+
+// Steger-Warming split of LAP point o along direction DIR into fp/fm
+template <int DIR, bool UNI, bool EPS0>
+__device__ __forceinline__ void split_point(const Params &p, long long o, double d, double u, double v,
+                                            double w, double T, double *fp, double *fm) {
+    double cc = div_const(sqrt(T), p.Ama, p.inv_Ama);
+    if constexpr (UNI) {
+        const DirConst &dc = p.dc[DIR];
+        sw_split_pre<EPS0>(d * p.tmp0, u, v, w, cc, dc.A[0], dc.A[1], dc.A[2], dc.ss,
+                           dc.An[0], dc.An[1], dc.An[2], p, fp, fm);
+    } else {
+        const int mA = M_AKX + 3 * DIR;
+        sw_split(d * p.tmp0, u, v, w, cc, p.met[mA][o], p.met[mA + 1][o], p.met[mA + 2][o], p.Gamma,
+                 p.epsl_sw, p.split_C1, p.split_C3, fp, fm);
+    }
+}
+
+// characteristic face record between LAP cells o0 and o1 (get_para_charteric_*,
+// src/OCFD_flux_charteric.cu:330-418)
+template <bool UNI>
+__device__ __forceinline__ void face_record(const Params &p, int dir, long long o0, long long o1, double *rec) {
+    const double *u = p.prim[1], *v = p.prim[2], *w = p.prim[3], *T = p.prim[4];
+    double c0v = div_const(sqrt(T[o0]), p.Ama, p.inv_Ama);
+    double c1v = div_const(sqrt(T[o1]), p.Ama, p.inv_Ama);
+    double u1 = (u[o0] + u[o1]) * 0.5, v1 = (v[o0] + v[o1]) * 0.5, w1 = (w[o0] + w[o1]) * 0.5;
+    double c1 = (c0v + c1v) * 0.5;
+    if (UNI) {
+        const DirConst &dc = p.dc[dir];
+        double KK = (p.Gamma - 1.0) / (c1 * c1);
+        rec[FU] = u1; rec[FV] = v1; rec[FW] = w1; rec[FC] = c1; rec[FKK] = KK;
+        rec[FX1] = 1.0 / (2.0 * c1);
+        double v2 = (u1 * u1 + v1 * v1 + w1 * w1) * 0.5;
+        rec[FV2] = v2;
+        rec[FUN] = u1 * dc.n[0] + v1 * dc.n[1] + w1 * dc.n[2];
+        rec[FH] = v2 + 1.0 / KK;
+        rec[FN1] = dc.n[0]; rec[FN2] = dc.n[1]; rec[FN3] = dc.n[2];
+        rec[FL1] = dc.l[0]; rec[FL2] = dc.l[1]; rec[FL3] = dc.l[2];
+        rec[FM1] = dc.m[0]; rec[FM2] = dc.m[1]; rec[FM3] = dc.m[2];
+    } else {
+        const int mA = M_AKX + 3 * dir;
+        make_record(u1, v1, w1, c1, (p.met[mA][o0] + p.met[mA][o1]) * 0.5,
+                    (p.met[mA + 1][o0] + p.met[mA + 1][o1]) * 0.5,
+                    (p.met[mA + 2][o0] + p.met[mA + 2][o1]) * 0.5, p, rec, 1);
+    }
+}
+
+// Flux of one face (both signs, all fields) from its 8-point window, any
+// scheme: component-wise reconstruction, or projection on the face's
+// characteristic fields, reconstruction and back-projection.  o0 is the LAP
+// offset of the cell left of the face, sd the LAP stride of the direction.
+template <bool UNI>
+__device__ __noinline__ void face_generic(const Params &p, int dir, Win w, int hflag, long long o0,
+                                          long long sd, double *out) {
+    const int scheme = p.scheme_invis;
+    const bool char_scheme = p.charteric && (scheme == 304 || scheme == 305 || scheme == 310);
+    const bool hybrid = scheme == 310;
+    if (p.charteric && !char_scheme) {          // the reference adds nothing
+        for (int m = 0; m < 10; m++) out[m] = 0.0;
+        return;
+    }
+    if (char_scheme && !(hybrid && hflag == 1)) {
+        double rec[FP_N];
+        face_record<UNI>(p, dir, o0, o0 + sd, rec);
+        for (int sign = 0; sign < 2; sign++) {
+            double fv[5][8];
+#pragma unroll
+            for (int m = 0; m < 5; m++)
+#pragma unroll
+                for (int k = 0; k < 8; k++) fv[m][k] = w.at(sign * 5 + m, k);
+            double o5[5];
+#pragma unroll
+            for (int c = 0; c < 5; c++) {
+                double Lr[5], vals[8], Rc[5];
+                L_row(rec, 1, c, Lr);
+#pragma unroll
+                for (int k = 0; k < 8; k++) vals[k] = dot5(Lr, fv[0][k], fv[1][k], fv[2][k], fv[3][k], fv[4][k]);
+                double res = recon_one(p, scheme, hflag, sign, vals);
+                R_col(rec, 1, c, Rc);
+                if (c == 0) {
+#pragma unroll
+                    for (int m = 0; m < 5; m++) o5[m] = Rc[m] * res;
+                } else {
+#pragma unroll
+                    for (int m = 0; m < 5; m++) o5[m] = o5[m] + Rc[m] * res;
+                }
+            }
+#pragma unroll
+            for (int m = 0; m < 5; m++) out[sign * 5 + m] = o5[m];
+        }
+        return;
+    }
+    for (int sv = 0; sv < 10; sv++) {
+        const int sign = sv >= 5, m = sv - 5 * sign;
+        double vals[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) vals[k] = w.at(sv, k);
+        int hf = hflag;
+        if (hybrid && !char_scheme && m > 0 && p.nochar_comp_flag) hf = p.nochar_comp_flag;
+        out[sv] = recon_one(p, scheme, hf, sign, vals);
+    }
+}
+
+// the face takes the inline UP7 path: UP7 everywhere, or a hybrid face with
+// flag 1 whose fields all use UP7
+__device__ __forceinline__ bool up7_face(const Params &p, int hflag) {
+    if (p.scheme_invis == 301) return !p.charteric;
+    return p.scheme_invis == 310 && hflag == 1 && (p.charteric || !p.nochar_comp_flag);
+}
+
+// du of one cell from the face fluxes on its right (cur) and left (prv):
+// x+ then x- for every field, as the reference's single-writer order
+template <bool FIRST>
+__device__ __forceinline__ void add_du(double *__restrict__ du, long long N, long long ci, double aj,
+                                       double h, double ih, const double *cur, const double *prv,
+                                       const double *old) {
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+        double acc = FIRST ? 0.0 : old[m];
+        acc += div_const(-aj * (cur[m] - prv[m]), h, ih);
+        acc += div_const(-aj * (cur[5 + m] - prv[5 + m]), h, ih);
+        du[m * N + ci] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The sweep kernel.  A warp covers LC lines (consecutive x for y and z; one
+// row for x) and LY = 32 / LC consecutive cells of each line, and walks its
+// lines LY cells at a time.  Per pass every lane splits one new point into
+// the warp's ring (RING points per line, value-major, line-minor, so a warp
+// access is 32 consecutive doubles), then forms the flux of the face on the
+// right of its cell and the du of its cell; the face on the left comes from
+// the lane below it (a shuffle) or, for the first row of lanes, from the
+// face kept from the previous pass.
+// ---------------------------------------------------------------------------
+constexpr int SW = 4;          // warps per block
+
+template <int DIR> struct Shape;
+template <> struct Shape<0> { static constexpr int LC = 1, RING = 64; };
+template <> struct Shape<1> { static constexpr int LC = 8, RING = 16; };
+template <> struct Shape<2> { static constexpr int LC = 8, RING = 16; };
+
+template <int DIR, bool UNI, bool EPS0>
+__global__ void __launch_bounds__(32 * SW, 6) k_sweep3(Params p, int seg_len) {
+    constexpr int LC = Shape<DIR>::LC, LY = 32 / LC, RING = Shape<DIR>::RING;
+    // the next pass's points overwrite slots this pass reads unless the
+    // ring spans both windows
+    constexpr bool SYNC2 = 2 * LY + 6 >= RING;
+    __shared__ double ring_all[SW][10 * RING * LC];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int col = lane % LC, ly = lane / LC;
+    const long long grp = (long long)blockIdx.x * SW + wid;     // line group of this warp
+    const int ngx = (p.nx + LC - 1) / LC;
+    const long long ngroups = DIR == 0 ? (long long)p.ny * p.nz : (long long)ngx * (DIR == 1 ? p.nz : p.ny);
+    if (grp >= ngroups) return;                                 // the whole warp
+    double *ring = ring_all[wid];
+    const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
+    const int y0 = blockIdx.y * seg_len;
+    const int y1 = min(n, y0 + seg_len);
+
+    long long base, cb, cst, fst, sd;
+    const int8_t *fl;
+    bool colok = true;
+    if (DIR == 0) {
+        const int j = (int)(grp % p.ny), k = (int)(grp / p.ny);
+        base = (long long)(k + OCFD_LAP) * p.zs + (long long)(j + OCFD_LAP) * p.ys + OCFD_LAP;
+        sd = 1;
+        cb = in_index(p, 0, j, k); cst = 1;
+        fl = p.flag[0] + (long long)(p.nx + 1) * ((long long)j + (long long)p.ny * k); fst = 1;
+    } else {
+        const int x = (int)(grp % ngx) * LC + col, c3 = (int)(grp / ngx);
+        colok = x < p.nx;
+        const int xs = colok ? x : p.nx - 1;                    // keep addresses in range
+        if (DIR == 1) {
+            base = (long long)(xs + OCFD_LAP) + (long long)OCFD_LAP * p.ys + (long long)(c3 + OCFD_LAP) * p.zs;
+            sd = p.ys;
+            cb = (long long)xs + (long long)p.nx * p.ny * c3; cst = p.nx;
+            fl = p.flag[1] + (long long)xs + (long long)p.nx * (p.ny + 1) * c3; fst = p.nx;
+        } else {
+            base = (long long)(xs + OCFD_LAP) + (long long)(c3 + OCFD_LAP) * p.ys + (long long)OCFD_LAP * p.zs;
+            sd = p.zs;
+            cb = (long long)xs + (long long)p.nx * c3; cst = (long long)p.nx * p.ny;
+            fl = p.flag[2] + (long long)xs + (long long)p.nx * c3; fst = (long long)p.nx * p.ny;
+        }
+    }
+    const double *__restrict__ d = p.prim[0], *__restrict__ u = p.prim[1], *__restrict__ v = p.prim[2],
+                 *__restrict__ w = p.prim[3], *__restrict__ T = p.prim[4];
+    double *__restrict__ du = p.du;
+    const long long N = p.N;
+    const bool hybrid = p.scheme_invis == 310;
+    const double h = DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz), ih = p.inv_h[DIR];
+
+    auto put = [&](int P) {                                     // split point P of the line
+        long long o = base + (long long)P * sd;
+        double fp[5], fm[5];
+        split_point<DIR, UNI, EPS0>(p, o, __ldg(d + o), __ldg(u + o), __ldg(v + o), __ldg(w + o), __ldg(T + o), fp, fm);
+        const int q = P & (RING - 1);
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            ring[(m * RING + q) * LC + col] = fp[m];
+            ring[((5 + m) * RING + q) * LC + col] = fm[m];
+        }
+    };
+    auto face = [&](int F, double *out) {                      // flux of face F+1/2
+        const int hflag = hybrid ? (int)fl[(long long)(F + 1) * fst] : 2;
+        if (up7_face(p, hflag)) {
+#pragma unroll
+            for (int sv = 0; sv < 10; sv++) {
+                double vals[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) vals[t] = ring[(sv * RING + ((F - 3 + t) & (RING - 1))) * LC + col];
+                out[sv] = sv < 5 ? up7_p_q(vals) : up7_m_q(vals);
+            }
+        } else {
+            face_generic<UNI>(p, DIR, Win{ring + col, LC, RING * LC, RING - 1, F - 3}, hflag,
+                              base + (long long)F * sd, sd, out);
+        }
+    };
+
+    // points y0-4 .. y0+3 and the face left of cell y0
+    for (int r = ly; r < 8; r += LY)
+        if (colok) put(y0 - 4 + r);
+    __syncwarp();
+    double carry[10], cur[10];
+#pragma unroll
+    for (int m = 0; m < 10; m++) cur[m] = 0.0;
+    if (ly == 0 && colok) face(y0 - 1, cur);
+#pragma unroll
+    for (int m = 0; m < 10; m++) carry[m] = __shfl_sync(FULL, cur[m], col);
+
+    for (int Y0 = y0; Y0 < y1; Y0 += LY) {
+        const int P = Y0 + 4 + ly;
+        if (colok && P <= y1 + 3) put(P);
+        __syncwarp();
+        const int F = Y0 + ly;
+        const bool valid = colok && F < y1;
+        const long long ci = cb + (long long)F * cst;
+        double old[5];
+        if (DIR != 0 && valid) {
+#pragma unroll
+            for (int m = 0; m < 5; m++) old[m] = du[m * N + ci];
+        }
+        if (valid) face(F, cur);
+        double prv[10];
+#pragma unroll
+        for (int m = 0; m < 10; m++) {
+            double t = __shfl_up_sync(FULL, cur[m], LC);
+            prv[m] = ly == 0 ? carry[m] : t;
+            carry[m] = __shfl_sync(FULL, cur[m], (LY - 1) * LC + col);
+        }
+        if (valid) {
+            double aj = metric<UNI>(p, M_AJAC, base + (long long)F * sd);
+            if (DIR == 0) add_du<true>(du, N, ci, aj, h, ih, cur, prv, old);
+            else          add_du<false>(du, N, ci, aj, h, ih, cur, prv, old);
+        }
+        if (SYNC2) __syncwarp();
+    }
+}
+
+template <int DIR, bool UNI, bool EPS0>
+cudaError_t launch_dir(const Params &p, cudaStream_t st) {
+    constexpr int LC = Shape<DIR>::LC, LY = 32 / LC;
+    const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
+    const long long ngx = (p.nx + LC - 1) / LC;
+    const long long groups = DIR == 0 ? (long long)p.ny * p.nz : ngx * (DIR == 1 ? p.nz : p.ny);
+    // split lines into segments when there are fewer than about four waves
+    // of warps (6 blocks of 4 warps per SM); a segment re-splits 8 points
+    // and re-forms one face
+    const long long want = 4LL * 148 * 6 * SW;
+    long long nseg = (want + groups - 1) / groups;
+    long long maxseg = n / (4 * LY) > 0 ? n / (4 * LY) : 1;
+    if (nseg > maxseg) nseg = maxseg;
+    if (nseg < 1) nseg = 1;
+    int seg_len = (int)((n + nseg - 1) / nseg);
+    seg_len = (seg_len + LY - 1) / LY * LY;
+    nseg = (n + seg_len - 1) / seg_len;
+    dim3 grid((unsigned)((groups + SW - 1) / SW), (unsigned)nseg);
+    k_sweep3<DIR, UNI, EPS0><<<grid, 32 * SW, 0, st>>>(p, seg_len);
+    return cudaGetLastError();
+}
+
+template <bool UNI, bool EPS0>
+cudaError_t launch3(const Params &p, cudaStream_t st) {
+    cudaError_t e;
+    if ((e = launch_dir<0, UNI, EPS0>(p, st)) != cudaSuccess) return e;
+    if ((e = launch_dir<1, UNI, EPS0>(p, st)) != cudaSuccess) return e;
+    return launch_dir<2, UNI, EPS0>(p, st);
+}
+
+}  // namespace
+
+cudaError_t launch_sweeps3(const Params &p, cudaStream_t st) {
+    if (p.uniform_metrics)
+        return p.epsl_sw == 0.0 ? launch3<true, true>(p, st) : launch3<true, false>(p, st);
+    return launch3<false, false>(p, st);
+}
+
+}  // namespace ocfd

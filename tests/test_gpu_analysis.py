@@ -47,9 +47,7 @@ def test_uniform_metric_path_matches_field_path(gpu_lib):
     b.step(3)
     pa, pb = a.primitives(), b.primitives()
     err = max(np.linalg.norm(pa[m] - pb[m]) / np.linalg.norm(pb[m]) for m in range(5))
-    # the variants contract multiply-adds differently; WENO weights amplify
-    # that, so they agree to the parity bound rather than to the last bit
-    assert err <= 1e-12, err
+    assert err <= 1e-14, err
 
 
 def test_curvilinear_grid_uses_field_path(gpu_lib):
@@ -76,13 +74,17 @@ def test_calls_out_of_order_return_status(gpu_lib):
     lambda: cases.taylor_green(16, seed=2),
     lambda: cases.random_smooth_case(12, 11, 10, seed=23, scheme_invis="WENO7_SYMBO_LIM", charteric=1, shock=True),
 ], ids=["iso_char", "shock_char_curv", "tgv_weno7", "symbo_lim_char"])
-def test_sweep_variants_agree(maker, gpu_lib):
+@pytest.mark.parametrize("impl", [2, 3, 4])
+def test_sweep_variants_agree(maker, impl, gpu_lib):
     case = maker()
     a = lib.Solver(case.cfg, case.prims, case.metrics)
+    a.set_sweep_impl(impl)
     b = lib.Solver(case.cfg, case.prims, case.metrics)
     b.set_sweep_impl(1)
     a.step(2)
     b.step(2)
     pa, pb = a.primitives(), b.primitives()
     err = max(np.linalg.norm(pa[m] - pb[m]) / np.linalg.norm(pb[m]) for m in range(5))
-    assert err <= 1e-14, err
+    # the variants contract multiply-adds differently; WENO weights amplify
+    # that, so they agree to the parity bound rather than to the last bit
+    assert err <= 1e-12, err
