@@ -95,7 +95,10 @@ int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode);
 int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx);
 /* Inviscid sweep kernel variant: 4 (default) no block barriers: each warp
  * walks its own lines (one x row, or 8 y or z lines) through a ring of
- * split values in shared memory; 2 one thread per (face, sign) in tiles
+ * split values in shared memory; for UP7 and the hybrid scheme the loop
+ * makes no calls and the cells next to non-UP7 faces are finished by a
+ * second kernel with the same arithmetic; 5 the same walk with every face
+ * through one in-loop dispatch; 2 one thread per (face, sign) in tiles
  * with the five characteristic fields in registers, register budget for 4
  * blocks per SM; 3 the same with a budget for 3 blocks; 1 one thread per
  * (face, sign, field).  All agree to the parity bound (WENO weights

@@ -34,6 +34,7 @@ cudaError_t launch_mean(const Params &p, int which, double *scratch, unsigned lo
 int reduce_scratch_doubles();
 cudaError_t launch_sweeps2(const Params &p, cudaStream_t st);
 cudaError_t launch_sweeps3(const Params &p, cudaStream_t st);
+int sweeps3_kernels(const Params &p);
 cudaError_t compute_dirconst(Params &p, DirConst *dev_scratch, cudaStream_t st);
 }  // namespace ocfd
 
@@ -63,6 +64,7 @@ struct ocfd_b200_ctx {
     int8_t *flag_buf = nullptr;
     double *stage_buf = nullptr;  // 5 interior fields for host transfers
     double *red_buf = nullptr;    // reduction partials + result, then two counters
+    unsigned *defer_buf = nullptr;  // three counters (padded to 256 B), then 3 deferred-cell lists
     double *pinned = nullptr;     // host staging for advance_host
     size_t pinned_bytes = 0;
     bool have_metrics = false;
@@ -117,7 +119,7 @@ extern "C" const char *ocfd_b200_last_error(const ocfd_b200_ctx *ctx) {
 static void free_all(ocfd_b200_ctx *c) {
     cudaFree(c->prim_buf); cudaFree(c->met_buf); cudaFree(c->cons_buf);
     cudaFree(c->ev_buf); cudaFree(c->flag_buf); cudaFree(c->stage_buf);
-    cudaFree(c->red_buf);
+    cudaFree(c->red_buf); cudaFree(c->defer_buf);
     if (c->pinned) cudaFreeHost(c->pinned);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -207,7 +209,10 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
         (rc = alloc((void **)&ctx->ev_buf, 12 * lapB, "viscous fluxes")) ||
         (rc = alloc((void **)&ctx->flag_buf, flagN, "flags")) ||
         (rc = alloc((void **)&ctx->stage_buf, 5 * inB, "staging")) ||
-        (rc = alloc((void **)&ctx->red_buf, sizeof(double) * (ocfd::reduce_scratch_doubles() + 2), "reduction"))) {
+        (rc = alloc((void **)&ctx->red_buf, sizeof(double) * (ocfd::reduce_scratch_doubles() + 2), "reduction")) ||
+        // deferred-cell lists of the call-free sweep (cell indices fit 32 bits)
+        (N < (1LL << 32) && (rc = alloc((void **)&ctx->defer_buf, sizeof(unsigned) * (64 + 3 * (size_t)N),
+                                        "deferred cells")))) {
         g_create_error = ctx->err;
         free_all(ctx);
         delete ctx;
@@ -220,6 +225,8 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     p.flag[0] = ctx->flag_buf;
     p.flag[1] = ctx->flag_buf + (size_t)(p.nx + 1) * p.ny * p.nz;
     p.flag[2] = p.flag[1] + (size_t)p.nx * (p.ny + 1) * p.nz;
+    p.defer_count = ctx->defer_buf;
+    for (int d = 0; d < 3; d++) p.defer[d] = ctx->defer_buf ? ctx->defer_buf + 64 + (size_t)d * N : nullptr;
 
     if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreate(&ctx->ev[0])) != cudaSuccess || (e = cudaEventCreate(&ctx->ev[1])) != cudaSuccess) {
@@ -322,9 +329,9 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
     {
         TimerScope ts(ctx, T_SWEEP);
         if (p.sweep_impl == 1)      CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
-        else if (p.sweep_impl == 4) CK(ocfd::launch_sweeps3(p, ctx->stream), "inviscid sweeps");
+        else if (p.sweep_impl >= 4) CK(ocfd::launch_sweeps3(p, ctx->stream), "inviscid sweeps");
         else                        CK(ocfd::launch_sweeps2(p, ctx->stream), "inviscid sweeps");
-        ctx->launches += 3;
+        ctx->launches += p.sweep_impl >= 4 ? ocfd::sweeps3_kernels(p) : 3;
     }
     {
         TimerScope ts(ctx, T_VIS);
@@ -402,7 +409,7 @@ extern "C" int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode) {
 extern "C" int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx) { return ctx ? ctx->p.uniform_metrics : 0; }
 
 extern "C" int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl) {
-    if (!ctx || impl < 1 || impl > 4) return OCFD_ERR_ARG;
+    if (!ctx || impl < 1 || impl > 5) return OCFD_ERR_ARG;
     ctx->p.sweep_impl = impl;
     return OCFD_OK;
 }

@@ -46,7 +46,11 @@ struct Params {
     double mc[13];
     DirConst dc[3];
     double inv_h[3], inv_Ama;   // reciprocals for div_const
-    int sweep_impl;         // 1: per-(face,sign,field) threads; 2, 3: per-(face,sign) threads; 4: marching
+    int sweep_impl;         // 1: per-(face,sign,field) threads; 2, 3: per-(face,sign) threads; 4, 5: warp rings
+    // cells whose du the call-free sweep leaves to the fix-up kernel, per
+    // direction (interior cell indices; capacity N each), and their counts
+    unsigned *defer[3];
+    unsigned *defer_count;
 };
 
 enum { M_AXX = 0, M_AYY, M_AZZ, M_AKX, M_AKY, M_AKZ, M_AIX, M_AIY, M_AIZ,

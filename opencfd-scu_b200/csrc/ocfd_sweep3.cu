@@ -167,8 +167,62 @@ template <> struct Shape<0> { static constexpr int LC = 1, RING = 64; };
 template <> struct Shape<1> { static constexpr int LC = 8, RING = 16; };
 template <> struct Shape<2> { static constexpr int LC = 8, RING = 16; };
 
-template <int DIR, bool UNI, bool EPS0>
-__global__ void __launch_bounds__(32 * SW, 6) k_sweep3(Params p, int seg_len) {
+// UP7 flux of face F+1/2 (both signs, all fields) from the ring
+template <int RING, int LC>
+__device__ __forceinline__ void face_up7(const double *ring, int col, int F, double (&out)[10]) {
+#pragma unroll
+    for (int sv = 0; sv < 10; sv++) {
+        double vals[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) vals[t] = ring[(sv * RING + ((F - 3 + t) & (RING - 1))) * LC + col];
+        out[sv] = sv < 5 ? up7_p_q(vals) : up7_m_q(vals);
+    }
+}
+
+// flux of face F+1/2 of one lane's line: UP7 inline, anything else out of line
+template <int RING, int LC, bool UNI>
+__device__ __forceinline__ void face_flux(const Params &p, int dir, const double *ring, int col, int F, int hflag,
+                                          long long o0, long long sd, double (&out)[10]) {
+    if (up7_face(p, hflag)) {
+        face_up7<RING, LC>(ring, col, F, out);
+    } else {
+        double tmp[10];      // a separate array, so that out stays in registers
+        face_generic<UNI>(p, dir, Win{ring + col, LC, RING * LC, RING - 1, F - 3}, hflag, o0, sd, tmp);
+#pragma unroll
+        for (int sv = 0; sv < 10; sv++) out[sv] = tmp[sv];
+    }
+}
+
+// split of one point (primitives q5, LAP offset o) into ring slot P
+template <int DIR, int RING, int LC, bool UNI, bool EPS0>
+__device__ __forceinline__ void ring_put(const Params &p, double *ring, int col, int P, long long o,
+                                         const double (&q5)[5]) {
+    double fp[5], fm[5];
+    split_point<DIR, UNI, EPS0>(p, o, q5[0], q5[1], q5[2], q5[3], q5[4], fp, fm);
+    const int q = P & (RING - 1);
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+        ring[(m * RING + q) * LC + col] = fp[m];
+        ring[((5 + m) * RING + q) * LC + col] = fm[m];
+    }
+}
+
+__device__ __forceinline__ void load5(const Params &p, long long o, double (&q5)[5]) {
+#pragma unroll
+    for (int m = 0; m < 5; m++) q5[m] = __ldg(p.prim[m] + o);
+}
+
+// The parameter block is __grid_constant__ so that passing it by reference
+// to the out-of-line face routine does not copy it to local memory.
+// FAST: the kernel makes no calls.  A face that is not plain UP7 gets no
+// flux here; the cells on both sides of it are left for k_sweep3_fix, which
+// recomputes them with the same arithmetic (their indices go to the
+// direction's deferred-cell list).  Keeping the call out of this loop keeps
+// its live values in registers.
+// MINB: resident blocks per SM the register budget is fitted to (5: 96
+// registers; 4: 128).
+template <int DIR, bool UNI, bool EPS0, int MINB, bool FAST>
+__global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant__ Params p, int seg_len) {
     constexpr int LC = Shape<DIR>::LC, LY = 32 / LC, RING = Shape<DIR>::RING;
     // the next pass's points overwrite slots this pass reads unless the
     // ring spans both windows
@@ -210,64 +264,66 @@ __global__ void __launch_bounds__(32 * SW, 6) k_sweep3(Params p, int seg_len) {
             fl = p.flag[2] + (long long)xs + (long long)p.nx * c3; fst = (long long)p.nx * p.ny;
         }
     }
-    const double *__restrict__ d = p.prim[0], *__restrict__ u = p.prim[1], *__restrict__ v = p.prim[2],
-                 *__restrict__ w = p.prim[3], *__restrict__ T = p.prim[4];
     double *__restrict__ du = p.du;
     const long long N = p.N;
     const bool hybrid = p.scheme_invis == 310;
     const double h = DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz), ih = p.inv_h[DIR];
 
-    auto put = [&](int P) {                                     // split point P of the line
-        long long o = base + (long long)P * sd;
-        double fp[5], fm[5];
-        split_point<DIR, UNI, EPS0>(p, o, __ldg(d + o), __ldg(u + o), __ldg(v + o), __ldg(w + o), __ldg(T + o), fp, fm);
-        const int q = P & (RING - 1);
-#pragma unroll
-        for (int m = 0; m < 5; m++) {
-            ring[(m * RING + q) * LC + col] = fp[m];
-            ring[((5 + m) * RING + q) * LC + col] = fm[m];
-        }
-    };
-    auto face = [&](int F, double *out) {                      // flux of face F+1/2
-        const int hflag = hybrid ? (int)fl[(long long)(F + 1) * fst] : 2;
-        if (up7_face(p, hflag)) {
-#pragma unroll
-            for (int sv = 0; sv < 10; sv++) {
-                double vals[8];
-#pragma unroll
-                for (int t = 0; t < 8; t++) vals[t] = ring[(sv * RING + ((F - 3 + t) & (RING - 1))) * LC + col];
-                out[sv] = sv < 5 ? up7_p_q(vals) : up7_m_q(vals);
-            }
-        } else {
-            face_generic<UNI>(p, DIR, Win{ring + col, LC, RING * LC, RING - 1, F - 3}, hflag,
-                              base + (long long)F * sd, sd, out);
-        }
-    };
-
     // points y0-4 .. y0+3 and the face left of cell y0
-    for (int r = ly; r < 8; r += LY)
-        if (colok) put(y0 - 4 + r);
+    for (int r = ly; r < 8; r += LY) {
+        if (colok) {
+            double q5[5];
+            const long long o = base + (long long)(y0 - 4 + r) * sd;
+            load5(p, o, q5);
+            ring_put<DIR, RING, LC, UNI, EPS0>(p, ring, col, y0 - 4 + r, o, q5);
+        }
+    }
     __syncwarp();
     double carry[10], cur[10];
 #pragma unroll
     for (int m = 0; m < 10; m++) cur[m] = 0.0;
-    if (ly == 0 && colok) face(y0 - 1, cur);
+    int slow = 0, carry_slow = 0;
+    if (ly == 0 && colok) {
+        const int hf = hybrid ? (int)fl[(long long)y0 * fst] : 2;
+        if constexpr (FAST) {
+            slow = !up7_face(p, hf);
+            if (!slow) face_up7<RING, LC>(ring, col, y0 - 1, cur);
+        } else {
+            face_flux<RING, LC, UNI>(p, DIR, ring, col, y0 - 1, hf, base + (long long)(y0 - 1) * sd, sd, cur);
+        }
+    }
 #pragma unroll
     for (int m = 0; m < 10; m++) carry[m] = __shfl_sync(FULL, cur[m], col);
+    if constexpr (FAST) carry_slow = __shfl_sync(FULL, slow, col);
+
+    // the primitives of this lane's next point and the flag of its next
+    // face are loaded one pass ahead
+    double nq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    int nflag = 2;
+    if (colok && y0 + 4 + ly <= y1 + 3) load5(p, base + (long long)(y0 + 4 + ly) * sd, nq);
+    if (hybrid && colok && y0 + ly < y1) nflag = fl[(long long)(y0 + ly + 1) * fst];
 
     for (int Y0 = y0; Y0 < y1; Y0 += LY) {
         const int P = Y0 + 4 + ly;
-        if (colok && P <= y1 + 3) put(P);
-        __syncwarp();
         const int F = Y0 + ly;
         const bool valid = colok && F < y1;
+        if (colok && P <= y1 + 3) ring_put<DIR, RING, LC, UNI, EPS0>(p, ring, col, P, base + (long long)P * sd, nq);
+        const int hflag = nflag;
+        if (colok && P + LY <= y1 + 3) load5(p, base + (long long)(P + LY) * sd, nq);
+        if (hybrid && colok && F + LY < y1) nflag = fl[(long long)(F + LY + 1) * fst];
+        __syncwarp();
         const long long ci = cb + (long long)F * cst;
         double old[5];
         if (DIR != 0 && valid) {
 #pragma unroll
             for (int m = 0; m < 5; m++) old[m] = du[m * N + ci];
         }
-        if (valid) face(F, cur);
+        if constexpr (FAST) {
+            slow = valid && !up7_face(p, hflag);
+            if (valid && !slow) face_up7<RING, LC>(ring, col, F, cur);
+        } else {
+            if (valid) face_flux<RING, LC, UNI>(p, DIR, ring, col, F, hflag, base + (long long)F * sd, sd, cur);
+        }
         double prv[10];
 #pragma unroll
         for (int m = 0; m < 10; m++) {
@@ -275,7 +331,22 @@ __global__ void __launch_bounds__(32 * SW, 6) k_sweep3(Params p, int seg_len) {
             prv[m] = ly == 0 ? carry[m] : t;
             carry[m] = __shfl_sync(FULL, cur[m], (LY - 1) * LC + col);
         }
-        if (valid) {
+        bool defer = false;
+        if constexpr (FAST) {
+            const int up = __shfl_up_sync(FULL, slow, LC);
+            const int prv_slow = ly == 0 ? carry_slow : up;
+            carry_slow = __shfl_sync(FULL, slow, (LY - 1) * LC + col);
+            defer = valid && (slow || prv_slow);
+            const unsigned mask = __ballot_sync(FULL, defer);
+            if (mask) {                       // one atomic per warp
+                const int leader = __ffs(mask) - 1;
+                unsigned slot = 0;
+                if (lane == leader) slot = atomicAdd(p.defer_count + DIR, (unsigned)__popc(mask));
+                slot = __shfl_sync(FULL, slot, leader);
+                if (defer) p.defer[DIR][slot + __popc(mask & ((1u << lane) - 1u))] = (unsigned)ci;
+            }
+        }
+        if (valid && !defer) {
             double aj = metric<UNI>(p, M_AJAC, base + (long long)F * sd);
             if (DIR == 0) add_du<true>(du, N, ci, aj, h, ih, cur, prv, old);
             else          add_du<false>(du, N, ci, aj, h, ih, cur, prv, old);
@@ -284,16 +355,75 @@ __global__ void __launch_bounds__(32 * SW, 6) k_sweep3(Params p, int seg_len) {
     }
 }
 
+// Cells the FAST sweep deferred: each thread takes one cell, splits the 9
+// points X-4 .. X+4 of its line, forms the fluxes of faces X-1/2 and X+1/2
+// (UP7 or the out-of-line routine, as the inline path would) and adds the
+// cell's du in the same order.
 template <int DIR, bool UNI, bool EPS0>
+__global__ void __launch_bounds__(128) k_sweep3_fix(const __grid_constant__ Params p) {
+    const unsigned cnt = p.defer_count[DIR];
+    const long long sd = DIR == 0 ? 1LL : (DIR == 1 ? p.ys : p.zs);
+    const bool hybrid = p.scheme_invis == 310;
+    const double h = DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz), ih = p.inv_h[DIR];
+    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
+        const long long ci = p.defer[DIR][e];
+        const int i = (int)(ci % p.nx);
+        const long long r = ci / p.nx;
+        const int j = (int)(r % p.ny), k = (int)(r / p.ny);
+        const int X = DIR == 0 ? i : (DIR == 1 ? j : k);
+        const long long oX = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+        double win[90];                       // [point X-4+t][sign * 5 + field]
+        for (int t = 0; t < 9; t++) {
+            const long long o = oX + (long long)(t - 4) * sd;
+            double q5[5], fp[5], fm[5];
+            load5(p, o, q5);
+            split_point<DIR, UNI, EPS0>(p, o, q5[0], q5[1], q5[2], q5[3], q5[4], fp, fm);
+#pragma unroll
+            for (int m = 0; m < 5; m++) { win[t * 10 + m] = fp[m]; win[t * 10 + 5 + m] = fm[m]; }
+        }
+        // flag of face F+1/2 is entry F+1 of the direction's flag array
+        auto flag_at = [&](int e1) -> int {
+            if (!hybrid) return 2;
+            long long q = DIR == 0 ? (long long)e1 + (long long)(p.nx + 1) * ((long long)j + (long long)p.ny * k)
+                        : DIR == 1 ? (long long)i + (long long)p.nx * ((long long)e1 + (long long)(p.ny + 1) * k)
+                                   : (long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * e1);
+            return p.flag[DIR][q];
+        };
+        double cur[10], prv[10];
+        for (int side = 0; side < 2; side++) {          // 0: face X-1/2, 1: face X+1/2
+            const int hf = flag_at(X + side);
+            double *out = side ? cur : prv;
+            if (up7_face(p, hf)) {
+                for (int sv = 0; sv < 10; sv++) {
+                    double vals[8];
+#pragma unroll
+                    for (int t = 0; t < 8; t++) vals[t] = win[(side + t) * 10 + sv];
+                    out[sv] = sv < 5 ? up7_p_q(vals) : up7_m_q(vals);
+                }
+            } else {
+                face_generic<UNI>(p, DIR, Win{win, 10, 1, 15, side}, hf, oX + (long long)(side - 1) * sd, sd, out);
+            }
+        }
+        double old[5];
+        if (DIR != 0) {
+#pragma unroll
+            for (int m = 0; m < 5; m++) old[m] = p.du[m * p.N + ci];
+        }
+        const double aj = metric<UNI>(p, M_AJAC, oX);
+        if (DIR == 0) add_du<true>(p.du, p.N, ci, aj, h, ih, cur, prv, old);
+        else          add_du<false>(p.du, p.N, ci, aj, h, ih, cur, prv, old);
+    }
+}
+
+template <int DIR, bool UNI, bool EPS0, int MINB, bool FAST>
 cudaError_t launch_dir(const Params &p, cudaStream_t st) {
     constexpr int LC = Shape<DIR>::LC, LY = 32 / LC;
     const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
     const long long ngx = (p.nx + LC - 1) / LC;
     const long long groups = DIR == 0 ? (long long)p.ny * p.nz : ngx * (DIR == 1 ? p.nz : p.ny);
     // split lines into segments when there are fewer than about four waves
-    // of warps (6 blocks of 4 warps per SM); a segment re-splits 8 points
-    // and re-forms one face
-    const long long want = 4LL * 148 * 6 * SW;
+    // of warps; a segment re-splits 8 points and re-forms one face
+    const long long want = 4LL * 148 * MINB * SW;
     long long nseg = (want + groups - 1) / groups;
     long long maxseg = n / (4 * LY) > 0 ? n / (4 * LY) : 1;
     if (nseg > maxseg) nseg = maxseg;
@@ -302,19 +432,40 @@ cudaError_t launch_dir(const Params &p, cudaStream_t st) {
     seg_len = (seg_len + LY - 1) / LY * LY;
     nseg = (n + seg_len - 1) / seg_len;
     dim3 grid((unsigned)((groups + SW - 1) / SW), (unsigned)nseg);
-    k_sweep3<DIR, UNI, EPS0><<<grid, 32 * SW, 0, st>>>(p, seg_len);
+    k_sweep3<DIR, UNI, EPS0, MINB, FAST><<<grid, 32 * SW, 0, st>>>(p, seg_len);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !FAST) return e;
+    // the deferred-cell count is only known on the device: a fixed grid
+    // that strides over it (usually a few thousand cells, often none)
+    k_sweep3_fix<DIR, UNI, EPS0><<<2 * 148, 128, 0, st>>>(p);
     return cudaGetLastError();
 }
 
+template <bool UNI, bool EPS0, int MINB, bool FAST>
+cudaError_t launch3m(const Params &p, cudaStream_t st) {
+    cudaError_t e;
+    if (FAST && (e = cudaMemsetAsync(p.defer_count, 0, 3 * sizeof(unsigned), st)) != cudaSuccess) return e;
+    if ((e = launch_dir<0, UNI, EPS0, MINB, FAST>(p, st)) != cudaSuccess) return e;
+    if ((e = launch_dir<1, UNI, EPS0, MINB, FAST>(p, st)) != cudaSuccess) return e;
+    return launch_dir<2, UNI, EPS0, MINB, FAST>(p, st);
+}
+// impl 4: the call-free kernel with deferred cells where the scheme has a
+// UP7 fast path; impl 5 (and every other scheme): every face through the
+// in-kernel dispatch
+bool use_fast(const Params &p) {
+    const bool fast_scheme = (p.scheme_invis == 301 && !p.charteric) || p.scheme_invis == 310;
+    return p.sweep_impl == 4 && fast_scheme && p.defer[0];
+}
 template <bool UNI, bool EPS0>
 cudaError_t launch3(const Params &p, cudaStream_t st) {
-    cudaError_t e;
-    if ((e = launch_dir<0, UNI, EPS0>(p, st)) != cudaSuccess) return e;
-    if ((e = launch_dir<1, UNI, EPS0>(p, st)) != cudaSuccess) return e;
-    return launch_dir<2, UNI, EPS0>(p, st);
+    if (use_fast(p)) return launch3m<UNI, EPS0, 4, true>(p, st);
+    return launch3m<UNI, EPS0, 5, false>(p, st);
 }
 
 }  // namespace
+
+// kernels one launch_sweeps3 issues
+int sweeps3_kernels(const Params &p) { return use_fast(p) ? 6 : 3; }
 
 cudaError_t launch_sweeps3(const Params &p, cudaStream_t st) {
     if (p.uniform_metrics)
