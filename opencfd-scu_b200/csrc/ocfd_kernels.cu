@@ -338,11 +338,25 @@ k_sweep(Params p) {
 
 // first derivative of a LAP field along stride s at o (OCFD_d?0 with CD6 or
 // CD8, src/OCFD_Schemes.cu:96-156; put_d0_kernel divides by h)
-__device__ __forceinline__ double d0(const double *f, long long o, long long s, double h, bool c8) {
+// (the division by h is the corrected product with RN(1/h), div_const)
+__device__ __forceinline__ double d0(const double *f, long long o, long long s, double h, double ih, bool c8) {
     double t;
     if (c8) t = cd8(f[o - 4 * s], f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s], f[o + 4 * s]);
     else    t = cd6(f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s]);
-    return t / h;
+    return div_const(t, h, ih);
+}
+
+// cons_to_pri of one cell (src/commen_kernel.cu:77-109): one reciprocal of
+// rho and one of rho*Cv, each quotient formed as the corrected product
+__device__ __forceinline__ void cons_to_prim(const Params &p, const double f[5], double &d1, double &u1,
+                                             double &v1, double &w1, double &T2) {
+    d1 = f[0];
+    const double id = 1.0 / d1;
+    u1 = div_const(f[1], d1, id);
+    v1 = div_const(f[2], d1, id);
+    w1 = div_const(f[3], d1, id);
+    const double dcv = d1 * p.Cv;
+    T2 = div_const(f[4] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1), dcv, 1.0 / dcv);
 }
 
 // Ev1..4 of all three directions (vis_flux_ker :178-236).  The 12 velocity
@@ -350,7 +364,7 @@ __device__ __forceinline__ double d0(const double *f, long long o, long long s, 
 // here from the LAP-box primitives instead of being stored; the stress and
 // heat flux do not depend on the direction, so they are formed once per cell.
 template <bool UNI>
-__global__ void k_vis_ev(Params p) {
+__global__ void __launch_bounds__(256, 5) k_vis_ev(Params p) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= p.N) return;
     int i = (int)(tid % p.nx); long long r = tid / p.nx;
@@ -363,10 +377,11 @@ __global__ void k_vis_ev(Params p) {
     double Tc = p.prim[4][o];
     double Amu = p.amu_C0 * sqrt(Tc * Tc * Tc) / (p.Tsb + Tc);      // get_Amu_kernal
     const double *U = p.prim[1], *V = p.prim[2], *W = p.prim[3], *TT = p.prim[4];
-    double uk = d0(U, o, 1, p.hx, c8), ui = d0(U, o, p.ys, p.hy, c8), us = d0(U, o, p.zs, p.hz, c8);
-    double vk = d0(V, o, 1, p.hx, c8), vi = d0(V, o, p.ys, p.hy, c8), vs = d0(V, o, p.zs, p.hz, c8);
-    double wk = d0(W, o, 1, p.hx, c8), wi = d0(W, o, p.ys, p.hy, c8), ws = d0(W, o, p.zs, p.hz, c8);
-    double Tk = d0(TT, o, 1, p.hx, c8), Ti = d0(TT, o, p.ys, p.hy, c8), Ts = d0(TT, o, p.zs, p.hz, c8);
+    const double ihx = p.inv_h[0], ihy = p.inv_h[1], ihz = p.inv_h[2];
+    double uk = d0(U, o, 1, p.hx, ihx, c8), ui = d0(U, o, p.ys, p.hy, ihy, c8), us = d0(U, o, p.zs, p.hz, ihz, c8);
+    double vk = d0(V, o, 1, p.hx, ihx, c8), vi = d0(V, o, p.ys, p.hy, ihy, c8), vs = d0(V, o, p.zs, p.hz, ihz, c8);
+    double wk = d0(W, o, 1, p.hx, ihx, c8), wi = d0(W, o, p.ys, p.hy, ihy, c8), ws = d0(W, o, p.zs, p.hz, ihz, c8);
+    double Tk = d0(TT, o, 1, p.hx, ihx, c8), Ti = d0(TT, o, p.ys, p.hy, ihy, c8), Ts = d0(TT, o, p.zs, p.hz, ihz, c8);
     double ux = uk*Akx + ui*Aix + us*Asx;
     double vx = vk*Akx + vi*Aix + vs*Asx;
     double wx = wk*Akx + wi*Aix + ws*Asx;
@@ -425,11 +440,8 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
             f[m] = t1 * fn + t2 * (p.f[m * N + tid] + p.dt * du[m]);
         }
     }
-    double d1 = f[0];
-    double u1 = f[1] / d1;
-    double v1 = f[2] / d1;
-    double w1 = f[3] / d1;
-    double T2 = (f[4] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1)) / (d1 * p.Cv);
+    double d1, u1, v1, w1, T2;
+    cons_to_prim(p, f, d1, u1, v1, w1, T2);
     long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     p.prim[0][o] = d1; p.prim[1][o] = u1; p.prim[2][o] = v1; p.prim[3][o] = w1; p.prim[4][o] = T2;
     bool face = (i == 0) || (i == p.nx - 1) || (j == 0) || (j == p.ny - 1) || (k == 0) || (k == p.nz - 1);
@@ -449,7 +461,7 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
 // RK = true: the stage's du is complete here, so the RK update, cons->prim
 // and the face re-projection follow in the same thread and du is not stored.
 template <bool UNI, bool RK>
-__global__ void k_vis_div(Params p, int krk) {
+__global__ void __launch_bounds__(256, 5) k_vis_div(Params p, int krk) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= p.N) return;
     int i = (int)(tid % p.nx); long long r = tid / p.nx;
@@ -467,7 +479,7 @@ __global__ void k_vis_div(Params p, int krk) {
 #pragma unroll
         for (int m = 0; m < 4; m++) {
             const double *f = p.ev + (long long)(4 * dd + m) * p.lapN;
-            acc[m + 1] += ajac * d0(f, o, st[dd], hh[dd], c8);
+            acc[m + 1] += ajac * d0(f, o, st[dd], hh[dd], p.inv_h[dd], c8);
         }
     }
     if (RK) {
@@ -506,11 +518,9 @@ __global__ void k_c2p(Params p) {
     int i = (int)(tid % p.nx); long long r = tid / p.nx;
     int j = (int)(r % p.ny); int k = (int)(r / p.ny);
     const long long N = p.N;
-    double d1 = p.f[tid];
-    double u1 = p.f[N + tid] / d1;
-    double v1 = p.f[2 * N + tid] / d1;
-    double w1 = p.f[3 * N + tid] / d1;
-    double T2 = (p.f[4 * N + tid] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1)) / (d1 * p.Cv);
+    const double f[5] = {p.f[tid], p.f[N + tid], p.f[2 * N + tid], p.f[3 * N + tid], p.f[4 * N + tid]};
+    double d1, u1, v1, w1, T2;
+    cons_to_prim(p, f, d1, u1, v1, w1, T2);
     long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     p.prim[0][o] = d1; p.prim[1][o] = u1; p.prim[2][o] = v1; p.prim[3][o] = w1; p.prim[4][o] = T2;
 }
