@@ -229,7 +229,8 @@ def run_ours(args, rank, world, dist):
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None,
+                     "traffic": (TRAFFIC_PER_CELL[dom] * cells if dom in TRAFFIC_PER_CELL else None),
+                     "traffic_source": TRAFFIC_SOURCE,
                      "algorithmic_bytes_per_cell": DOM_BYTES.get(dom, B_ALG),
                      "launch_ms": dom_ms_per_stage},
         "stage_roofline": {"bytes_per_cell_stage": B_ALG, "achieved_gbs": B_ALG * cells / (stage_ms / 1e3) / 1e9,
@@ -257,6 +258,16 @@ DOM_BYTES = {
     "ghost_fill": 0.0,
     "sensor": 19.0,
 }
+
+# Measured DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell
+# for one stage's launches of each family, from one ncu capture of the same
+# kernels at 160^3 (profiles/stage_kernels_iso160.txt); the traffic scales with
+# the cells processed, so the bench line reports it times the cells of a launch.
+TRAFFIC_PER_CELL = {
+    "inviscid_sweeps": 307.8,       # 3 sweeps + 3 fix-ups
+    "viscous_rk_update": 377.6,     # k_vis_ev + k_vis_div (Ev ghost fill not captured)
+}
+TRAFFIC_SOURCE = "ncu capture at 160^3 scaled by cells (profiles/stage_kernels_iso160.txt)"
 
 
 def run_reference(args, rank, world):
