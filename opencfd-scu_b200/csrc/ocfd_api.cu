@@ -139,9 +139,6 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
         return fail(nullptr, OCFD_ERR_UNSUPPORTED, "SCHEME_VIS id must be 203 (CD6) or 204 (CD8)");
     if (si == 310 && cfg->hy_style != 2)
         return fail(nullptr, OCFD_ERR_UNSUPPORTED, "SCHEME_HYBRIDAUTO is built for HY_STYLE = 2 (Jameson sensor)");
-    for (int d = 0; d < 3; d++)
-        if (!cfg->iperiodic[d])
-            return fail(nullptr, OCFD_ERR_UNSUPPORTED, "non-periodic directions (boundary closures, IBC) are not built");
     if (!(cfg->ama > 0) || !(cfg->gamma > 1) || !(cfg->re > 0) || !(cfg->pr > 0))
         return fail(nullptr, OCFD_ERR_ARG, "AMA, GAMMA, RE, PR out of range");
 
@@ -190,6 +187,14 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     p.inv_h[0] = 1.0 / p.hx; p.inv_h[1] = 1.0 / p.hy; p.inv_h[2] = 1.0 / p.hz;
     p.inv_Ama = 1.0 / Ma;
     for (int d = 0; d < 3; d++) p.periodic[d] = cfg->iperiodic[d];
+    p.has_bnd = 0;
+    for (int d = 0; d < 3; d++) {
+        p.bnd_lo[d] = cfg->dif_bound[2 * d] == 1;
+        p.bnd_hi[d] = cfg->dif_bound[2 * d + 1] == 1;
+        p.nonref_lo[d] = cfg->non_reflection[2 * d];
+        p.nonref_hi[d] = cfg->non_reflection[2 * d + 1];
+        p.has_bnd |= p.bnd_lo[d] | p.bnd_hi[d] | (p.nonref_lo[d] == 1) | (p.nonref_hi[d] == 1);
+    }
 
     size_t lapB = sizeof(double) * (size_t)p.lapN, inB = sizeof(double) * (size_t)N;
     size_t flagN = (size_t)(p.nx + 1) * p.ny * p.nz + (size_t)p.nx * (p.ny + 1) * p.nz + (size_t)p.nx * p.ny * (p.nz + 1);
@@ -328,6 +333,8 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
     }
     {
         TimerScope ts(ctx, T_SWEEP);
+        if (p.has_bnd && p.sweep_impl < 4)
+            return fail(ctx, OCFD_ERR_UNSUPPORTED, "sweep variants 1-3 have no boundary closures (use 4 or 5)");
         if (p.sweep_impl == 1)      CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
         else if (p.sweep_impl >= 4) CK(ocfd::launch_sweeps3(p, ctx->stream), "inviscid sweeps");
         else                        CK(ocfd::launch_sweeps2(p, ctx->stream), "inviscid sweeps");
@@ -359,7 +366,9 @@ static int check_ready(ocfd_b200_ctx *ctx) {
 // parameter block; the arithmetic is the same as reading the fields.
 static void detect_uniform(ocfd_b200_ctx *ctx, const double *host13) {
     Params &p = ctx->p;
-    bool uni = ctx->metric_mode == 0;
+    // ghosts of a non-periodic direction keep the initial 1.0, which the
+    // characteristic record of a boundary face averages in: field path
+    bool uni = ctx->metric_mode == 0 && p.periodic[0] && p.periodic[1] && p.periodic[2];
     for (int m = 0; m < 13 && uni; m++) {
         const double *f = host13 + (size_t)m * p.N;
         p.mc[m] = f[0];

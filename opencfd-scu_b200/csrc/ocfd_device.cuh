@@ -35,6 +35,12 @@ struct Params {
     int scheme_invis, scheme_vis, charteric;
     int nochar_comp_flag;   // flag of components 1-4, non-characteristic hybrid (0 = face flag)
     int periodic[3];
+    // faces of each direction: boundary closures where DIF_BOUND is 1
+    // (OCFD_bound, src/OCFD_bound_Scheme.cu:436-469) and the NON_REFLETION
+    // value (OCFD_bound_non_ref, :352-433); has_bnd: any of them is set
+    int bnd_lo[3], bnd_hi[3];
+    int nonref_lo[3], nonref_hi[3];
+    int has_bnd;
     // state
     double *prim[5];        // d u v w T on the LAP box
     const double *met[13];  // Axx Ayy Azz Akx Aky Akz Aix Aiy Aiz Asx Asy Asz Ajac (LAP box)

@@ -346,6 +346,34 @@ __device__ __forceinline__ double d0(const double *f, long long o, long long s, 
     return div_const(t, h, ih);
 }
 
+// The same derivative at point X of a line of n cells whose faces may be
+// closed (DIF_BOUND = 1): the one-sided and lower-order formulas of
+// OCFD_D0bound_scheme_kernel (src/OCFD_bound_Scheme.cu:79-186) on the four
+// points next to a closed face, the lower face first as in its case 7/8/9.
+__device__ __forceinline__ double d0b(const double *f, long long o, long long s, double h, double ih, bool c8,
+                                      int X, int n, bool lo, bool hi) {
+    if (lo && X <= 3) {
+        double t;
+        if (X == 0)      t = (f[o + s] - f[o]);
+        else if (X == 1) t = (f[o + s] - f[o - s]) * 0.5;
+        else if (X == 2) t = (f[o - 2 * s] - 8.0 * f[o - s] + 8.0 * f[o + s] - f[o + 2 * s]) / 12.0;
+        else             t = (f[o + 3 * s] - f[o - 3 * s] - 9.0 * (f[o + 2 * s] - f[o - 2 * s])
+                             + 45.0 * (f[o + s] - f[o - s])) / 60.0;
+        return div_const(t, h, ih);
+    }
+    if (hi && X >= n - 4) {
+        double t;
+        const int q = X - n;
+        if (q == -1)      t = (f[o] - f[o - s]);
+        else if (q == -2) t = (f[o + s] - f[o - s]) * 0.5;
+        else if (q == -3) t = (f[o - 2 * s] - 8.0 * f[o - s] + 8.0 * f[o + s] - f[o + 2 * s]) / 12.0;
+        else              t = (f[o + 3 * s] - f[o - 3 * s] - 9.0 * (f[o + 2 * s] - f[o - 2 * s])
+                              + 45.0 * (f[o + s] - f[o - s])) / 60.0;
+        return div_const(t, h, ih);
+    }
+    return d0(f, o, s, h, ih, c8);
+}
+
 // cons_to_pri of one cell (src/commen_kernel.cu:77-109): one reciprocal of
 // rho and one of rho*Cv, each quotient formed as the corrected product
 __device__ __forceinline__ void cons_to_prim(const Params &p, const double f[5], double &d1, double &u1,
@@ -378,10 +406,24 @@ __global__ void __launch_bounds__(256, 5) k_vis_ev(Params p) {
     double Amu = p.amu_C0 * sqrt(Tc * Tc * Tc) / (p.Tsb + Tc);      // get_Amu_kernal
     const double *U = p.prim[1], *V = p.prim[2], *W = p.prim[3], *TT = p.prim[4];
     const double ihx = p.inv_h[0], ihy = p.inv_h[1], ihz = p.inv_h[2];
-    double uk = d0(U, o, 1, p.hx, ihx, c8), ui = d0(U, o, p.ys, p.hy, ihy, c8), us = d0(U, o, p.zs, p.hz, ihz, c8);
-    double vk = d0(V, o, 1, p.hx, ihx, c8), vi = d0(V, o, p.ys, p.hy, ihy, c8), vs = d0(V, o, p.zs, p.hz, ihz, c8);
-    double wk = d0(W, o, 1, p.hx, ihx, c8), wi = d0(W, o, p.ys, p.hy, ihy, c8), ws = d0(W, o, p.zs, p.hz, ihz, c8);
-    double Tk = d0(TT, o, 1, p.hx, ihx, c8), Ti = d0(TT, o, p.ys, p.hy, ihy, c8), Ts = d0(TT, o, p.zs, p.hz, ihz, c8);
+    double uk, ui, us, vk, vi, vs, wk, wi, ws, Tk, Ti, Ts;
+    if (!p.has_bnd) {
+        uk = d0(U, o, 1, p.hx, ihx, c8); ui = d0(U, o, p.ys, p.hy, ihy, c8); us = d0(U, o, p.zs, p.hz, ihz, c8);
+        vk = d0(V, o, 1, p.hx, ihx, c8); vi = d0(V, o, p.ys, p.hy, ihy, c8); vs = d0(V, o, p.zs, p.hz, ihz, c8);
+        wk = d0(W, o, 1, p.hx, ihx, c8); wi = d0(W, o, p.ys, p.hy, ihy, c8); ws = d0(W, o, p.zs, p.hz, ihz, c8);
+        Tk = d0(TT, o, 1, p.hx, ihx, c8); Ti = d0(TT, o, p.ys, p.hy, ihy, c8); Ts = d0(TT, o, p.zs, p.hz, ihz, c8);
+    } else {
+        const bool lx = p.bnd_lo[0], hx = p.bnd_hi[0], ly = p.bnd_lo[1], hy = p.bnd_hi[1];
+        const bool lz = p.bnd_lo[2], hz = p.bnd_hi[2];
+        uk = d0b(U, o, 1, p.hx, ihx, c8, i, p.nx, lx, hx); ui = d0b(U, o, p.ys, p.hy, ihy, c8, j, p.ny, ly, hy);
+        us = d0b(U, o, p.zs, p.hz, ihz, c8, k, p.nz, lz, hz);
+        vk = d0b(V, o, 1, p.hx, ihx, c8, i, p.nx, lx, hx); vi = d0b(V, o, p.ys, p.hy, ihy, c8, j, p.ny, ly, hy);
+        vs = d0b(V, o, p.zs, p.hz, ihz, c8, k, p.nz, lz, hz);
+        wk = d0b(W, o, 1, p.hx, ihx, c8, i, p.nx, lx, hx); wi = d0b(W, o, p.ys, p.hy, ihy, c8, j, p.ny, ly, hy);
+        ws = d0b(W, o, p.zs, p.hz, ihz, c8, k, p.nz, lz, hz);
+        Tk = d0b(TT, o, 1, p.hx, ihx, c8, i, p.nx, lx, hx); Ti = d0b(TT, o, p.ys, p.hy, ihy, c8, j, p.ny, ly, hy);
+        Ts = d0b(TT, o, p.zs, p.hz, ihz, c8, k, p.nz, lz, hz);
+    }
     double ux = uk*Akx + ui*Aix + us*Asx;
     double vx = vk*Akx + vi*Aix + vs*Asx;
     double wx = wk*Akx + wi*Aix + ws*Asx;
@@ -479,7 +521,12 @@ __global__ void __launch_bounds__(256, 5) k_vis_div(Params p, int krk) {
 #pragma unroll
         for (int m = 0; m < 4; m++) {
             const double *f = p.ev + (long long)(4 * dd + m) * p.lapN;
-            acc[m + 1] += ajac * d0(f, o, st[dd], hh[dd], p.inv_h[dd], c8);
+            if (!p.has_bnd) {
+                acc[m + 1] += ajac * d0(f, o, st[dd], hh[dd], p.inv_h[dd], c8);
+            } else {
+                const int X = dd == 0 ? i : (dd == 1 ? j : k), n = dd == 0 ? p.nx : (dd == 1 ? p.ny : p.nz);
+                acc[m + 1] += ajac * d0b(f, o, st[dd], hh[dd], p.inv_h[dd], c8, X, n, p.bnd_lo[dd], p.bnd_hi[dd]);
+            }
         }
     }
     if (RK) {

@@ -72,13 +72,16 @@ __device__ __forceinline__ void face_record(const Params &p, int dir, long long 
     }
 }
 
-// Flux of one face (both signs, all fields) from its 8-point window, any
-// scheme: component-wise reconstruction, or projection on the face's
-// characteristic fields, reconstruction and back-projection.  o0 is the LAP
-// offset of the cell left of the face, sd the LAP stride of the direction.
+// Flux of face F+1/2 of a line of n cells (both signs, all fields) from its
+// 8-point window, any scheme: component-wise reconstruction, or projection on
+// the face's characteristic fields, reconstruction and back-projection.  Near
+// a face whose DIF_BOUND is 1 the boundary closure replaces the
+// reconstruction, after the projection when there is one, as the reference's
+// kernels call OCFD_bound_scheme_kernel_{p,m} (src/OCFD_bound_Scheme.cu:739-944).
+// o0 is the LAP offset of the cell left of the face, sd the LAP stride.
 template <bool UNI>
 __device__ __noinline__ void face_generic(const Params &p, int dir, Win w, int hflag, long long o0,
-                                          long long sd, double *out) {
+                                          long long sd, int F, int n, double *out) {
     const int scheme = p.scheme_invis;
     const bool char_scheme = p.charteric && (scheme == 304 || scheme == 305 || scheme == 310);
     const bool hybrid = scheme == 310;
@@ -86,6 +89,11 @@ __device__ __noinline__ void face_generic(const Params &p, int dir, Win w, int h
         for (int m = 0; m < 10; m++) out[m] = 0.0;
         return;
     }
+    const bool lo = p.bnd_lo[dir], hi = p.bnd_hi[dir];
+    const bool bnd = lo || hi;
+    int KA[2], KB[2];
+    extents(scheme, char_scheme, 0, KA[0], KB[0]);
+    extents(scheme, char_scheme, 1, KA[1], KB[1]);
     if (char_scheme && !(hybrid && hflag == 1)) {
         double rec[FP_N];
         face_record<UNI>(p, dir, o0, o0 + sd, rec);
@@ -102,7 +110,9 @@ __device__ __noinline__ void face_generic(const Params &p, int dir, Win w, int h
                 L_row(rec, 1, c, Lr);
 #pragma unroll
                 for (int k = 0; k < 8; k++) vals[k] = dot5(Lr, fv[0][k], fv[1][k], fv[2][k], fv[3][k], fv[4][k]);
-                double res = recon_one(p, scheme, hflag, sign, vals);
+                double res;
+                if (!(bnd && closure(sign, lo, hi, KA[sign], KB[sign], F, n, vals, res)))
+                    res = recon_one(p, scheme, hflag, sign, vals);
                 R_col(rec, 1, c, Rc);
                 if (c == 0) {
 #pragma unroll
@@ -124,8 +134,22 @@ __device__ __noinline__ void face_generic(const Params &p, int dir, Win w, int h
         for (int k = 0; k < 8; k++) vals[k] = w.at(sv, k);
         int hf = hflag;
         if (hybrid && !char_scheme && m > 0 && p.nochar_comp_flag) hf = p.nochar_comp_flag;
-        out[sv] = recon_one(p, scheme, hf, sign, vals);
+        if (!(bnd && closure(sign, lo, hi, KA[sign], KB[sign], F, n, vals, out[sv])))
+            out[sv] = recon_one(p, scheme, hf, sign, vals);
     }
+}
+
+// the face is within reach of a boundary closure (closure_p reaches F <= 2
+// and F >= n-4, closure_m F <= 2 and F >= n-4; one more on each side here)
+__device__ __forceinline__ bool near_closure(const Params &p, int dir, int F, int n) {
+    return (p.bnd_lo[dir] && F <= 3) || (p.bnd_hi[dir] && F >= n - 5);
+}
+
+// the first / last cell of a line, where non-reflecting faces and the
+// characteristic kernels' first-order boundary fluxes change du
+__device__ __forceinline__ bool rule_cell(const Params &p, int dir, int X, int n) {
+    return (X == 0 && (p.bnd_lo[dir] || p.nonref_lo[dir] == 1)) ||
+           (X == n - 1 && (p.bnd_hi[dir] || p.nonref_hi[dir] == 1));
 }
 
 // the face takes the inline UP7 path: UP7 everywhere, or a hybrid face with
@@ -181,13 +205,13 @@ __device__ __forceinline__ void face_up7(const double *ring, int col, int F, dou
 
 // flux of face F+1/2 of one lane's line: UP7 inline, anything else out of line
 template <int RING, int LC, bool UNI>
-__device__ __forceinline__ void face_flux(const Params &p, int dir, const double *ring, int col, int F, int hflag,
-                                          long long o0, long long sd, double (&out)[10]) {
-    if (up7_face(p, hflag)) {
+__device__ __forceinline__ void face_flux(const Params &p, int dir, const double *ring, int col, int F, int n,
+                                          int hflag, long long o0, long long sd, double (&out)[10]) {
+    if (up7_face(p, hflag) && !near_closure(p, dir, F, n)) {
         face_up7<RING, LC>(ring, col, F, out);
     } else {
         double tmp[10];      // a separate array, so that out stays in registers
-        face_generic<UNI>(p, dir, Win{ring + col, LC, RING * LC, RING - 1, F - 3}, hflag, o0, sd, tmp);
+        face_generic<UNI>(p, dir, Win{ring + col, LC, RING * LC, RING - 1, F - 3}, hflag, o0, sd, F, n, tmp);
 #pragma unroll
         for (int sv = 0; sv < 10; sv++) out[sv] = tmp[sv];
     }
@@ -286,10 +310,10 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
     if (ly == 0 && colok) {
         const int hf = hybrid ? (int)fl[(long long)y0 * fst] : 2;
         if constexpr (FAST) {
-            slow = !up7_face(p, hf);
+            slow = !up7_face(p, hf) || near_closure(p, DIR, y0 - 1, n);
             if (!slow) face_up7<RING, LC>(ring, col, y0 - 1, cur);
         } else {
-            face_flux<RING, LC, UNI>(p, DIR, ring, col, y0 - 1, hf, base + (long long)(y0 - 1) * sd, sd, cur);
+            face_flux<RING, LC, UNI>(p, DIR, ring, col, y0 - 1, n, hf, base + (long long)(y0 - 1) * sd, sd, cur);
         }
     }
 #pragma unroll
@@ -319,10 +343,10 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
             for (int m = 0; m < 5; m++) old[m] = du[m * N + ci];
         }
         if constexpr (FAST) {
-            slow = valid && !up7_face(p, hflag);
+            slow = valid && (!up7_face(p, hflag) || near_closure(p, DIR, F, n));
             if (valid && !slow) face_up7<RING, LC>(ring, col, F, cur);
         } else {
-            if (valid) face_flux<RING, LC, UNI>(p, DIR, ring, col, F, hflag, base + (long long)F * sd, sd, cur);
+            if (valid) face_flux<RING, LC, UNI>(p, DIR, ring, col, F, n, hflag, base + (long long)F * sd, sd, cur);
         }
         double prv[10];
 #pragma unroll
@@ -337,6 +361,10 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
             const int prv_slow = ly == 0 ? carry_slow : up;
             carry_slow = __shfl_sync(FULL, slow, (LY - 1) * LC + col);
             defer = valid && (slow || prv_slow);
+        }
+        // the first and last cells of a bounded line go to the fix-up kernel
+        if (p.has_bnd) defer = defer || (valid && rule_cell(p, DIR, F, n));
+        if (FAST || p.has_bnd) {
             const unsigned mask = __ballot_sync(FULL, defer);
             if (mask) {                       // one atomic per warp
                 const int leader = __ffs(mask) - 1;
@@ -389,11 +417,13 @@ __global__ void __launch_bounds__(128) k_sweep3_fix(const __grid_constant__ Para
                                    : (long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * e1);
             return p.flag[DIR][q];
         };
+        const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
         double cur[10], prv[10];
         for (int side = 0; side < 2; side++) {          // 0: face X-1/2, 1: face X+1/2
             const int hf = flag_at(X + side);
+            const int F = X - 1 + side;
             double *out = side ? cur : prv;
-            if (up7_face(p, hf)) {
+            if (up7_face(p, hf) && !near_closure(p, DIR, F, n)) {
                 for (int sv = 0; sv < 10; sv++) {
                     double vals[8];
 #pragma unroll
@@ -401,17 +431,59 @@ __global__ void __launch_bounds__(128) k_sweep3_fix(const __grid_constant__ Para
                     out[sv] = sv < 5 ? up7_p_q(vals) : up7_m_q(vals);
                 }
             } else {
-                face_generic<UNI>(p, DIR, Win{win, 10, 1, 15, side}, hf, oX + (long long)(side - 1) * sd, sd, out);
+                face_generic<UNI>(p, DIR, Win{win, 10, 1, 15, side}, hf, oX + (long long)(side - 1) * sd, sd,
+                                  F, n, out);
             }
         }
-        double old[5];
-        if (DIR != 0) {
-#pragma unroll
-            for (int m = 0; m < 5; m++) old[m] = p.du[m * p.N + ci];
-        }
         const double aj = metric<UNI>(p, M_AJAC, oX);
-        if (DIR == 0) add_du<true>(p.du, p.N, ci, aj, h, ih, cur, prv, old);
-        else          add_du<false>(p.du, p.N, ci, aj, h, ih, cur, prv, old);
+        // du of the cell: x+ then x- for every field (put_du_p_kernel /
+        // put_du_m_kernel, src/OCFD_Schemes.cu:293-381; the characteristic
+        // kernels' put_du_character_{p,m}_kernel, src/OCFD_flux_charteric.cu:16-118,
+        // and OCFD_bound_character_kernel_{p,m}, :121-319)
+        const int scheme = p.scheme_invis;
+        const bool char_kernel = p.charteric && (scheme == 304 || scheme == 305 || scheme == 310);
+        const bool lo = p.bnd_lo[DIR], hi = p.bnd_hi[DIR];
+        const bool only_lo = lo && !hi, only_hi = hi && !lo;     // flag 1..6, not 7..9
+        const bool first = X == 0, last = X == n - 1;
+        for (int m = 0; m < 5; m++) {
+            double acc = DIR == 0 ? 0.0 : p.du[m * p.N + ci];
+            // P side
+            if (!char_kernel ? (first && p.nonref_lo[DIR] == 1) : (only_lo && p.nonref_lo[DIR] == 1 && first)) {
+                acc += 0.0;
+            } else if (char_kernel && ((only_lo && first) || (only_hi && last))) {
+                double tmp;
+                if (first) {
+                    tmp = (win[5 * 10 + m] - win[4 * 10 + m]);
+                } else {
+                    const double f0 = win[4 * 10 + m], f1 = win[3 * 10 + m], f2 = win[2 * 10 + m];
+                    const double tr = f0 + 0.5 * minmod2(f0 - f1, f0 - f1);
+                    const double tl = f1 + 0.5 * minmod2(f0 - f1, f1 - f2);
+                    tmp = tr - tl;
+                }
+                acc += div_const(-aj * tmp, h, ih);
+            } else {
+                acc += div_const(-aj * (cur[m] - prv[m]), h, ih);
+            }
+            // M side; the reference's y kernel tests flag 3 for its lower
+            // face, so that first-order flux never applies on y
+            if (!char_kernel ? (last && p.nonref_hi[DIR] == 1) : (only_hi && p.nonref_hi[DIR] == 1 && last)) {
+                acc += 0.0;
+            } else if (char_kernel && ((DIR != 1 && only_lo && first) || (only_hi && last))) {
+                double tmp;
+                if (first) {
+                    const double f0 = win[4 * 10 + 5 + m], f1 = win[5 * 10 + 5 + m], f2 = win[6 * 10 + 5 + m];
+                    const double tr = f1 - 0.5 * minmod2(f2 - f1, f1 - f0);
+                    const double tl = f0 - 0.5 * minmod2(f1 - f0, f1 - f0);
+                    tmp = tr - tl;
+                } else {
+                    tmp = (win[4 * 10 + 5 + m] - win[3 * 10 + 5 + m]);
+                }
+                acc += div_const(-aj * tmp, h, ih);
+            } else {
+                acc += div_const(-aj * (cur[5 + m] - prv[5 + m]), h, ih);
+            }
+            p.du[m * p.N + ci] = acc;
+        }
     }
 }
 
@@ -434,7 +506,7 @@ cudaError_t launch_dir(const Params &p, cudaStream_t st) {
     dim3 grid((unsigned)((groups + SW - 1) / SW), (unsigned)nseg);
     k_sweep3<DIR, UNI, EPS0, MINB, FAST><<<grid, 32 * SW, 0, st>>>(p, seg_len);
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess || !FAST) return e;
+    if (e != cudaSuccess || !(FAST || p.has_bnd)) return e;
     // the deferred-cell count is only known on the device: a fixed grid
     // that strides over it (usually a few thousand cells, often none)
     k_sweep3_fix<DIR, UNI, EPS0><<<2 * 148, 128, 0, st>>>(p);
@@ -444,7 +516,8 @@ cudaError_t launch_dir(const Params &p, cudaStream_t st) {
 template <bool UNI, bool EPS0, int MINB, bool FAST>
 cudaError_t launch3m(const Params &p, cudaStream_t st) {
     cudaError_t e;
-    if (FAST && (e = cudaMemsetAsync(p.defer_count, 0, 3 * sizeof(unsigned), st)) != cudaSuccess) return e;
+    if ((FAST || p.has_bnd) && (e = cudaMemsetAsync(p.defer_count, 0, 3 * sizeof(unsigned), st)) != cudaSuccess)
+        return e;
     if ((e = launch_dir<0, UNI, EPS0, MINB, FAST>(p, st)) != cudaSuccess) return e;
     if ((e = launch_dir<1, UNI, EPS0, MINB, FAST>(p, st)) != cudaSuccess) return e;
     return launch_dir<2, UNI, EPS0, MINB, FAST>(p, st);
@@ -458,6 +531,7 @@ bool use_fast(const Params &p) {
 }
 template <bool UNI, bool EPS0>
 cudaError_t launch3(const Params &p, cudaStream_t st) {
+    if (p.has_bnd && !p.defer[0]) return cudaErrorNotSupported;   // boundary cells need the lists
     if (use_fast(p)) return launch3m<UNI, EPS0, 4, true>(p, st);
     return launch3m<UNI, EPS0, 5, false>(p, st);
 }
@@ -465,7 +539,7 @@ cudaError_t launch3(const Params &p, cudaStream_t st) {
 }  // namespace
 
 // kernels one launch_sweeps3 issues
-int sweeps3_kernels(const Params &p) { return use_fast(p) ? 6 : 3; }
+int sweeps3_kernels(const Params &p) { return (use_fast(p) || p.has_bnd) ? 6 : 3; }
 
 cudaError_t launch_sweeps3(const Params &p, cudaStream_t st) {
     if (p.uniform_metrics)

@@ -152,11 +152,15 @@ def isotropic_turbulence(n: int = 256, mach_t: float = 0.6, re_lambda: float = 1
 def random_smooth_case(nx: int, ny: int, nz: int, seed: int = 7, scheme_invis: str = "WENO7",
                        scheme_vis: str = "CD6", charteric: int = 0, ama: float = 0.5,
                        amp: float = 0.2, shock: bool = False, curvilinear: bool = False,
-                       dt: float = 2e-3) -> Case:
-    """Odd-sized periodic box with a few random Fourier modes (optionally a
-    steep tanh front so the hybrid sensor switches) for kernel parity tests.
-    ``curvilinear`` gives a smoothly sheared, periodic metric field so that
-    every metric entry is non-zero."""
+                       dt: float = 2e-3, iperiodic=(1, 1, 1), dif_bound=(0, 0, 0, 0, 0, 0),
+                       non_ref=(0, 0, 0, 0, 0, 0)) -> Case:
+    """Odd-sized box with a few random Fourier modes (optionally a steep tanh
+    front so the hybrid sensor switches) for kernel parity tests.
+    ``curvilinear`` gives a smoothly sheared metric field so that every metric
+    entry is non-zero.  ``iperiodic`` / ``dif_bound`` / ``non_ref`` are the
+    IPERIODIC / DIF_BOUND / NON_REFLETION keys: a non-periodic direction with
+    DIF_BOUND = 1 uses the boundary closures (no boundary-condition family,
+    IBC = 0, so the faces only get the re-projection)."""
     rng = np.random.default_rng(seed)
     Lx, Ly, Lz = 2 * math.pi, 2 * math.pi, 2 * math.pi
     dx, dy, dz = Lx / nx, Ly / ny, Lz / nz
@@ -184,9 +188,10 @@ def random_smooth_case(nx: int, ny: int, nz: int, seed: int = 7, scheme_invis: s
         d = d * (1.0 + 0.8 * front)
         T = T * (1.0 + 0.5 * front)
     prims = [d, u, v, w, T]
-    cfg = CaseConfig(nx=nx, ny=ny, nz=nz, iperiodic=(1, 1, 1), scheme_invis=scheme_invis,
+    cfg = CaseConfig(nx=nx, ny=ny, nz=nz, iperiodic=tuple(iperiodic), scheme_invis=scheme_invis,
                      scheme_vis=scheme_vis, charteric=charteric, re=500.0, ama=ama,
-                     gamma=1.4, pr=0.72, epsl_sw=0.0, dt=dt)
+                     gamma=1.4, pr=0.72, epsl_sw=0.0, dt=dt, dif_bound=tuple(dif_bound),
+                     non_ref=tuple(non_ref))
     met = cartesian_metrics(nx, ny, nz, dx, dy, dz)
     if curvilinear:
         # smooth periodic perturbation of all nine conservative metrics and of Ajac

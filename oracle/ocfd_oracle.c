@@ -838,28 +838,12 @@ static inline int face_flag(const oro_state *s, int dir, int i, int j, int k) {
 /* ------------------------------------------------------------------------ */
 
 /* one-sided WENO5 candidates, :554-745; s[0..4] = f(i-2..i+2) (P) */
-static double w5_p_right(const double *s) {
-    double S2 = 0.0, tmp, ep = 1e-6;
-    tmp = s[0] - 2.0*s[1] +     s[2]; S2 += 13*tmp*tmp;
-    tmp = s[0] - 4.0*s[1] + 3.0*s[2]; S2 +=  3*tmp*tmp;
-    double a2 = 1.0/((12.0*ep + S2)*(12.0*ep + S2));
-    double q23 = (2.0*s[0] - 7.0*s[1] + 11.0*s[2]);
-    return a2*q23/(6.0*a2);
-}
 static double w5_p_left(const double *s) {
     double S0 = 0.0, tmp, ep = 1e-6;
     tmp =     s[2] - 2.0*s[3] + s[4]; S0 += 13*tmp*tmp;
     tmp = 3.0*s[2] - 4.0*s[3] + s[4]; S0 +=  3*tmp*tmp;
     double a0 = 1.0/((12.0*ep + S0)*(12.0*ep + S0));
     double q03 = (2.0*s[2] + 5.0*s[3] - s[4]);
-    return a0*q03/(6.0*a0);
-}
-static double w5_m_right(const double *s) {
-    double S0 = 0.0, tmp, ep = 1e-6;
-    tmp =     s[2] - 2.0*s[1] + s[0]; S0 += 13*tmp*tmp;
-    tmp = 3.0*s[2] - 4.0*s[1] + s[0]; S0 +=  3*tmp*tmp;
-    double a0 = 1.0/((12.0*ep + S0)*(12.0*ep + S0));
-    double q03 = (2.0*s[2] + 5.0*s[1] - s[0]);
     return a0*q03/(6.0*a0);
 }
 static double w5_m_left(const double *s) {
@@ -1015,7 +999,8 @@ static double face_m(const oro_state *s, int scheme, int hflag, const double *s8
 }
 
 /* One direction, both signs: OCFD_d{x,y,z}1 and OCFD_d{x,y,z}2
- * (src/OCFD_Schemes_Choose.cu:88-764) on a periodic single-rank domain.
+ * (src/OCFD_Schemes_Choose.cu:88-764) on a single-rank domain, with the
+ * boundary closures of faces whose DIF_BOUND is 1.
  * du(X) += -Ajac(X)*(F+(X+1/2) - F+(X-1/2))/h, then the same for F-. */
 static void invis_sweep(oro_state *s, int dir) {
     int n[3] = { s->nx, s->ny, s->nz };
@@ -1029,6 +1014,17 @@ static void invis_sweep(oro_state *s, int dir) {
     double G = s->c.gamma;
     const double *Aj = s->A[AJAC];
     const double *Ax = s->A[AKX + 3 * dir], *Ay = s->A[AKX + 3 * dir + 1], *Az = s->A[AKX + 3 * dir + 2];
+    /* boundary handling of this direction (OCFD_bound / OCFD_bound_non_ref,
+     * src/OCFD_bound_Scheme.cu:352-469): flagxyzb.y is LOWER, UPPER or both
+     * (7/8/9) when DIF_BOUND of the face is 1; flagxyzb.z is NON_REFLETION */
+    const int lo = s->c.d0_bound[2 * dir] == 1, hi = s->c.d0_bound[2 * dir + 1] == 1;
+    const int LOWER = 1 + dir, UPPER = 4 + dir;
+    const int flagy = lo ? (hi ? 7 + dir : LOWER) : (hi ? UPPER : 0);
+    const int nr_lo = s->c.non_ref[2 * dir], nr_hi = s->c.non_ref[2 * dir + 1];
+    /* the characteristic kernels (304, 305, 310 with CHARTERIC=1) */
+    const int char_kernel = chart && (scheme == 304 || scheme == 305 || scheme == 310);
+    int kap, kbp, kam, kbm;
+    closure_extent(scheme, char_kernel, &kap, &kbp, &kam, &kbm);
 
 #pragma omp parallel
     {
@@ -1075,13 +1071,16 @@ static void invis_sweep(oro_state *s, int dir) {
                             mat5_apply(Lm, xp); mat5_apply(Lm, xm);
                             for (int m = 0; m < 5; m++) { s8p[m][t] = xp[m]; s8m[m][t] = xm[m]; }
                         }
+                        /* closures act on the characteristic stencils (the
+                         * kernels call OCFD_bound_scheme_kernel_{p,m} after ptoc) */
                         for (int m = 0; m < 5; m++) {
-                            if (scheme == 310) {
-                                outp[m] = face_p(s, 310, hflag, s8p[m]);
-                                outm[m] = face_m(s, 310, hflag, s8m[m]);
-                            } else {
-                                outp[m] = oro_weno7_symbo_p(scheme == 305, s->c.weno_tv_limiter, s->c.weno_tv_max, s8p[m]);
-                                outm[m] = oro_weno7_symbo_m(scheme == 305, s->c.weno_tv_limiter, s->c.weno_tv_max, s8m[m]);
+                            if (!closure_p(lo, hi, kap, kbp, F, len, s8p[m], &outp[m])) {
+                                if (scheme == 310) outp[m] = face_p(s, 310, hflag, s8p[m]);
+                                else outp[m] = oro_weno7_symbo_p(scheme == 305, s->c.weno_tv_limiter, s->c.weno_tv_max, s8p[m]);
+                            }
+                            if (!closure_m(lo, hi, kam, kbm, F, len, s8m[m], &outm[m])) {
+                                if (scheme == 310) outm[m] = face_m(s, 310, hflag, s8m[m]);
+                                else outm[m] = oro_weno7_symbo_m(scheme == 305, s->c.weno_tv_limiter, s->c.weno_tv_max, s8m[m]);
                             }
                         }
                         mat5_apply(Rm, outp); mat5_apply(Rm, outm);
@@ -1089,8 +1088,10 @@ static void invis_sweep(oro_state *s, int dir) {
                         for (int m = 0; m < 5; m++) {
                             int hf = hflag;
                             if (scheme == 310 && !chart && m > 0 && s->c.hy_nochar_fixed) hf = s->c.hy_nochar_fixed;
-                            outp[m] = face_p(s, scheme, hf, s8p[m]);
-                            outm[m] = face_m(s, scheme, hf, s8m[m]);
+                            if (!closure_p(lo, hi, kap, kbp, F, len, s8p[m], &outp[m]))
+                                outp[m] = face_p(s, scheme, hf, s8p[m]);
+                            if (!closure_m(lo, hi, kam, kbm, F, len, s8m[m], &outm[m]))
+                                outm[m] = face_m(s, scheme, hf, s8m[m]);
                         }
                     }
                     for (int m = 0; m < 5; m++) {
@@ -1104,13 +1105,62 @@ static void invis_sweep(oro_state *s, int dir) {
                     int ci[3] = { idx[0] - LAP, idx[1] - LAP, idx[2] - LAP };
                     size_t c = I(s, ci[0], ci[1], ci[2]);
                     double aj = Aj[q];
+                    /* put_du_p_kernel (src/OCFD_Schemes.cu:293-338) and
+                     * put_du_character_p_kernel (src/OCFD_flux_charteric.cu:16-64) */
                     for (int m = 0; m < 5; m++) {
                         double r = fpp[(size_t)m * (len + 1) + X + 1], l = fpp[(size_t)m * (len + 1) + X];
-                        s->du[(size_t)m * nin + c] += -aj*(r - l)/h;
+                        double *du = &s->du[(size_t)m * nin + c];
+                        if (!char_kernel) {
+                            if (X == 0 && nr_lo == 1) *du += 0.0;
+                            else *du += -aj*(r - l)/h;
+                        } else if (flagy == LOWER && nr_lo == 1 && X == 0) {
+                            *du += 0.0;
+                        } else if ((flagy == LOWER && X == 0) || (flagy == UPPER && X == len - 1)) {
+                            /* OCFD_bound_character_kernel_p (:121-210) on the split fluxes */
+                            const double *fl = s->fp[dir] + (size_t)m * nl;
+                            size_t q0 = q;
+                            double tmp;
+                            if (X == 0) {
+                                tmp = (fl[q0 + sdir] - fl[q0]);
+                            } else {
+                                double f0 = fl[q0], f1 = fl[q0 - sdir], f2 = fl[q0 - 2 * sdir];
+                                double tr = f0 + 0.5*minmod2(f0 - f1, f0 - f1);
+                                double tl = f1 + 0.5*minmod2(f0 - f1, f1 - f2);
+                                tmp = tr - tl;
+                            }
+                            *du += -aj*tmp/h;
+                        } else {
+                            *du += -aj*(r - l)/h;
+                        }
                     }
+                    /* put_du_m_kernel (:340-381) and put_du_character_m_kernel
+                     * (:67-118; its y case tests flag 3, so the lower special
+                     * never applies on y) */
+                    const int mlower = dir == 1 ? 3 : LOWER;
                     for (int m = 0; m < 5; m++) {
                         double r = fmm[(size_t)m * (len + 1) + X + 1], l = fmm[(size_t)m * (len + 1) + X];
-                        s->du[(size_t)m * nin + c] += -aj*(r - l)/h;
+                        double *du = &s->du[(size_t)m * nin + c];
+                        if (!char_kernel) {
+                            if (X == len - 1 && nr_hi == 1) *du += 0.0;
+                            else *du += -aj*(r - l)/h;
+                        } else if (flagy == UPPER && nr_hi == 1 && X == len - 1) {
+                            *du += 0.0;
+                        } else if ((flagy == mlower && X == 0) || (flagy == UPPER && X == len - 1)) {
+                            /* OCFD_bound_character_kernel_m (:214-319) */
+                            const double *fl = s->fm[dir] + (size_t)m * nl;
+                            double tmp;
+                            if (X == 0) {
+                                double f0 = fl[q], f1 = fl[q + sdir], f2 = fl[q + 2 * sdir];
+                                double tr = f1 - 0.5*minmod2(f2 - f1, f1 - f0);
+                                double tl = f0 - 0.5*minmod2(f1 - f0, f1 - f0);
+                                tmp = tr - tl;
+                            } else {
+                                tmp = (fl[q] - fl[q - sdir]);
+                            }
+                            *du += -aj*tmp/h;
+                        } else {
+                            *du += -aj*(r - l)/h;
+                        }
                     }
                 }
             }
@@ -1126,25 +1176,46 @@ static void invis_sweep(oro_state *s, int dir) {
 /* viscous terms, src/OCFD_NS_Jacobian3d.cu:58-440                            */
 /* ------------------------------------------------------------------------ */
 
-/* OCFD_d{x,y,z}0 with CD6/CD8 over the interior of a LAP field (periodic). */
+/* Derivative closures of OCFD_D0bound_scheme_kernel (src/OCFD_bound_Scheme.cu:79-186)
+ * for point i of a line of n cells, c[k] = f(i+k).  lo / hi: DIF_BOUND of the
+ * lower / upper face is 1 (OCFD_bound, :436-469).  The lower closure is tried
+ * first, as in the reference's case 7/8/9.  Returns 1 when a closure applies. */
+static int d0_closure(int lo, int hi, int i, int n, const double *c, double *out) {
+    if (lo) {
+        if (i == 0) { *out = (c[1] - c[0]); return 1; }
+        if (i == 1) { *out = (c[1] - c[-1])*0.5; return 1; }
+        if (i == 2) { *out = (c[-2] - 8.0*c[-1] + 8.0*c[1] - c[2])/12.0; return 1; }
+        if (i == 3) { *out = (c[3] - c[-3] - 9.0*(c[2] - c[-2]) + 45.0*(c[1] - c[-1]))/60.0; return 1; }
+    }
+    if (hi) {
+        int t = i - n;
+        if (t == -1) { *out = (c[0] - c[-1]); return 1; }
+        if (t == -2) { *out = (c[1] - c[-1])*0.5; return 1; }
+        if (t == -3) { *out = (c[-2] - 8.0*c[-1] + 8.0*c[1] - c[2])/12.0; return 1; }
+        if (t == -4) { *out = (c[3] - c[-3] - 9.0*(c[2] - c[-2]) + 45.0*(c[1] - c[-1]))/60.0; return 1; }
+    }
+    return 0;
+}
+
+/* OCFD_d{x,y,z}0 (src/OCFD_Schemes_Choose.cu:19-84) with CD6/CD8 over the
+ * interior of a LAP field, closures on faces whose DIF_BOUND is 1. */
 static void d0(oro_state *s, const double *f, double *out, int dir) {
     size_t st[3] = { 1, (size_t)s->nx2, (size_t)s->nx2 * s->ny2 };
     size_t sd = st[dir];
     double h = dir == 0 ? s->hx : (dir == 1 ? s->hy : s->hz);
     int cd8 = s->c.scheme_vis == 204;
+    int n = dir == 0 ? s->nx : (dir == 1 ? s->ny : s->nz);
+    int lo = s->c.d0_bound[2 * dir] == 1, hi = s->c.d0_bound[2 * dir + 1] == 1;
 #pragma omp parallel for
     for (int k = 0; k < s->nz; k++)
         for (int j = 0; j < s->ny; j++)
             for (int i = 0; i < s->nx; i++) {
                 size_t q = L(s, i + LAP, j + LAP, k + LAP);
+                int X = dir == 0 ? i : (dir == 1 ? j : k);
                 double st9[9], tmp;
-                if (cd8) {
-                    for (int t = 0; t < 9; t++) st9[t] = f[q + (size_t)((long)(t - 4) * (long)sd)];
-                    tmp = oro_cd8(st9);
-                } else {
-                    for (int t = 0; t < 7; t++) st9[t] = f[q + (size_t)((long)(t - 3) * (long)sd)];
-                    tmp = oro_cd6(st9);
-                }
+                for (int t = 0; t < 9; t++) st9[t] = f[q + (size_t)((long)(t - 4) * (long)sd)];
+                if (!d0_closure(lo, hi, X, n, st9 + 4, &tmp))
+                    tmp = cd8 ? oro_cd8(st9) : oro_cd6(st9 + 1);
                 out[I(s, i, j, k)] = tmp/h;   /* put_d0_kernel :75-94 */
             }
 }

@@ -54,6 +54,38 @@ def golden_cases():
     for sch in ("WENO7_SYMBO", "WENO7_SYMBO_LIM"):
         c = cases.random_smooth_case(12, 11, 10, seed=23, scheme_invis=sch, charteric=1, shock=True)
         out.append((f"rnd12x11x10_{sch.lower()}_char", c, 3))
+    out.extend(bounded_cases())
+    return out
+
+
+def bounded_cases():
+    """Non-periodic directions with the boundary closures (DIF_BOUND = 1) and
+    non-reflecting faces, no boundary-condition family (IBC = 0): both faces
+    closed (flag 7/8/9), one face closed (1..6), and closures on a periodic
+    direction, for component-wise and characteristic kernels."""
+    out = []
+    both = dict(iperiodic=(0, 0, 0), dif_bound=(1, 1, 1, 1, 1, 1))
+    one = dict(iperiodic=(0, 0, 0), dif_bound=(1, 0, 0, 1, 1, 0), non_ref=(1, 0, 0, 1, 0, 0))
+    for sch in ("UP7", "WENO7", "WENO5", "NND2", "WENO7_SYMBO", "OMP6_HR"):
+        c = cases.random_smooth_case(14, 13, 12, seed=31, scheme_invis=sch, **both)
+        out.append((f"bnd14x13x12_{sch.lower()}_both", c, 3))
+    c = cases.random_smooth_case(14, 13, 12, seed=32, scheme_invis="UP7", **one)
+    out.append(("bnd14x13x12_up7_one_nonref", c, 3))
+    c = cases.random_smooth_case(14, 13, 12, seed=33, scheme_invis="WENO7", scheme_vis="CD8", **one)
+    out.append(("bnd14x13x12_weno7_cd8_one_nonref", c, 3))
+    for tag, kw in (("both", both), ("one_nonref", one)):
+        c = cases.random_smooth_case(13, 14, 12, seed=34, scheme_invis="SCHEME_HYBRIDAUTO",
+                                     charteric=1, shock=True, **kw)
+        c.cfg.hy_dp_intv = (0.01, 0.2)
+        out.append((f"bnd13x14x12_hybrid_char_{tag}", c, 3))
+        c = cases.random_smooth_case(12, 13, 11, seed=35, scheme_invis="WENO7_SYMBO_LIM",
+                                     charteric=1, shock=True, **kw)
+        out.append((f"bnd12x13x11_symbo_lim_char_{tag}", c, 3))
+    c = cases.random_smooth_case(13, 12, 11, seed=36, scheme_invis="SCHEME_HYBRIDAUTO", charteric=1,
+                                 shock=True, curvilinear=True, iperiodic=(1, 0, 1),
+                                 dif_bound=(1, 1, 1, 1, 0, 0), non_ref=(0, 1, 1, 0, 0, 0))
+    c.cfg.hy_dp_intv = (0.01, 0.2)
+    out.append(("bnd13x12x11_hybrid_char_curv_mixed", c, 3))
     return out
 
 

@@ -50,6 +50,7 @@ def test_create_rejects_bad_arguments_without_a_gpu():
     c.scheme_invis = 399
     assert L.ocfd_b200_create(ctypes.byref(c), ctypes.byref(h)) == -2
     c = lib.make_config(cfg)
-    c.iperiodic[0] = 0
+    c.scheme_invis = 310
+    c.hy_style = 1
     assert L.ocfd_b200_create(ctypes.byref(c), ctypes.byref(h)) == -2
-    assert b"non-periodic" in L.ocfd_b200_last_error(None)
+    assert b"HY_STYLE" in L.ocfd_b200_last_error(None)

@@ -56,6 +56,29 @@ def small_cases():
     for sch in ("WENO7_SYMBO", "WENO7_SYMBO_LIM"):
         out.append((f"rnd_{sch.lower()}_char", cases.random_smooth_case(12, 11, 10, seed=23, scheme_invis=sch,
                                                                         charteric=1, shock=True)))
+    out.extend(bounded_cases())
+    return out
+
+
+def bounded_cases():
+    """Non-periodic directions with boundary closures (DIF_BOUND = 1) and
+    non-reflecting faces: both faces closed, or one face of each direction."""
+    both = dict(iperiodic=(0, 0, 0), dif_bound=(1, 1, 1, 1, 1, 1))
+    one = dict(iperiodic=(0, 0, 0), dif_bound=(1, 0, 0, 1, 1, 0), non_ref=(1, 0, 0, 1, 0, 0))
+    out = [
+        ("bnd_up7_both", cases.random_smooth_case(14, 13, 12, seed=41, scheme_invis="UP7", **both)),
+        ("bnd_up7_one", cases.random_smooth_case(14, 13, 12, seed=42, scheme_invis="UP7", **one)),
+        ("bnd_weno7_cd8_one", cases.random_smooth_case(13, 12, 11, seed=43, scheme_vis="CD8", **one)),
+        ("bnd_hybrid_char_both", cases.random_smooth_case(13, 14, 12, seed=44, scheme_invis="SCHEME_HYBRIDAUTO",
+                                                          charteric=1, shock=True, **both)),
+        ("bnd_hybrid_char_one", cases.random_smooth_case(13, 14, 12, seed=45, scheme_invis="SCHEME_HYBRIDAUTO",
+                                                         charteric=1, shock=True, **one)),
+        ("bnd_symbo_char_one", cases.random_smooth_case(12, 13, 11, seed=46, scheme_invis="WENO7_SYMBO",
+                                                        charteric=1, shock=True, **one)),
+    ]
+    for _, c in out:
+        if c.cfg.scheme_invis == "SCHEME_HYBRIDAUTO":
+            c.cfg.hy_dp_intv = (0.01, 0.2)
     return out
 
 
@@ -136,3 +159,21 @@ def test_matches_reference_golden(path, gpu_lib):
     err = rel_l2(got, ref)
     name = os.path.basename(path)
     assert np.all(err <= TOL_TRAJ), (name, err)
+
+
+@pytest.mark.parametrize("name,case", bounded_cases(), ids=[n for n, _ in bounded_cases()])
+def test_bounded_sweep_variants(name, case, gpu_lib):
+    """Cells next to closed faces go through the fix-up kernel (variant 4) or
+    the in-loop dispatch (variant 5): same results; the tiled variants have
+    no closures and refuse the case."""
+    a = lib.Solver(case.cfg, case.prims, case.metrics)
+    b = lib.Solver(case.cfg, case.prims, case.metrics)
+    b.set_sweep_impl(5)
+    a.step(2)
+    b.step(2)
+    assert np.all(rel_l2(a.primitives(), b.primitives()) <= 1e-13), name
+    c = lib.Solver(case.cfg, case.prims, case.metrics)
+    c.set_sweep_impl(2)
+    with pytest.raises(lib.OcfdError) as ei:
+        c.step(1)
+    assert ei.value.status == -2
