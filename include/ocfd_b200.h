@@ -105,6 +105,19 @@ int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx);
  * amplify the different multiply-add contractions). */
 int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl);
 int ocfd_b200_set_metrics_device(ocfd_b200_ctx *ctx, const double *metrics13_dev);
+/* Mesh coordinates x,y,z, 3 interior fields (host or device memory), from
+ * which the 13 metric fields are computed on the GPU.  Replaces the
+ * OCFD3d-Mesh.dat branch of Init_Jacobian3d
+ * (src/OCFD_Comput_Jacobian3d.cu:119-141) and Comput_Jacobian3d (:221-246):
+ * CD6 derivatives of the coordinates, one-sided closures at both ends of a
+ * direction whose JAC_BOUND is non-zero, cross products and the inverse
+ * determinant, constant extrapolation into the ghosts, periodic exchange.
+ * Returns OCFD_ERR_ARG on a negative Jacobian (ana_Jac, src/OCFD_ana.cu:24-48). */
+int ocfd_b200_set_mesh(ocfd_b200_ctx *ctx, const double *xyz3);
+int ocfd_b200_set_mesh_device(ocfd_b200_ctx *ctx, const double *xyz3_dev);
+/* The 13 metric fields the kernels use, interior, OCFD3d-Jacobi.dat order
+ * (synchronous; metrics must be set). */
+int ocfd_b200_get_metrics(ocfd_b200_ctx *ctx, double *metrics13);
 
 /* Initial primitives d,u,v,w,T (host or device).  Replaces the
  * INIT_STAT=1 part of init() (src/OCFD_init.cu:88-115): ghosts zero, then

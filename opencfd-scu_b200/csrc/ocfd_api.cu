@@ -34,6 +34,8 @@ cudaError_t launch_mean(const Params &p, int which, double *scratch, unsigned lo
 int reduce_scratch_doubles();
 cudaError_t launch_sweeps2(const Params &p, cudaStream_t st);
 cudaError_t launch_sweeps3(const Params &p, cudaStream_t st);
+cudaError_t launch_mesh_metrics(const Params &p, const int jac_bound[3], double *scratch, cudaStream_t st);
+cudaError_t launch_negative_jacobian(const Params &p, unsigned *flag, cudaStream_t st);
 int sweeps3_kernels(const Params &p);
 cudaError_t compute_dirconst(Params &p, DirConst *dev_scratch, cudaStream_t st);
 }  // namespace ocfd
@@ -394,6 +396,9 @@ static int set_metrics_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKin
         detect_uniform(ctx, h);
         free(h);
     }
+    // Init_Jacobian3d starts every metric field at 1.0, ghosts included
+    CK(ocfd::launch_fill(ctx->met_buf, 13 * p.lapN, 1.0, ctx->stream), "metric init");
+    ctx->launches += 1;
     for (int m = 0; m < 13; m++) {
         CK(cudaMemcpyAsync(ctx->stage_buf, src + (size_t)m * p.N, inB, kind, ctx->stream), "metric copy");
         CK(ocfd::launch_scatter(p, ctx->stage_buf, const_cast<double *>(p.met[m]), ctx->stream), "metric scatter");
@@ -428,6 +433,72 @@ extern "C" int ocfd_b200_set_metrics(ocfd_b200_ctx *ctx, const double *m) {
 }
 extern "C" int ocfd_b200_set_metrics_device(ocfd_b200_ctx *ctx, const double *m) {
     return set_metrics_impl(ctx, m, cudaMemcpyDeviceToDevice);
+}
+
+// The OCFD3d-Mesh.dat branch of Init_Jacobian3d (src/OCFD_Comput_Jacobian3d.cu:119-141)
+// followed by Comput_Jacobian3d (:221-246) and ana_Jac (src/OCFD_ana.cu:24-48).
+static int set_mesh_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKind kind) {
+    if (!ctx || !src) return OCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    Params &p = ctx->p;
+    size_t inB = sizeof(double) * (size_t)p.N;
+    CK(ocfd::launch_fill(ctx->met_buf, 13 * p.lapN, 1.0, ctx->stream), "metric init");
+    ctx->launches += 1;
+    for (int m = 0; m < 3; m++) {
+        CK(cudaMemcpyAsync(ctx->stage_buf, src + (size_t)m * p.N, inB, kind, ctx->stream), "mesh copy");
+        CK(ocfd::launch_scatter(p, ctx->stage_buf, const_cast<double *>(p.met[m]), ctx->stream), "mesh scatter");
+        ctx->launches += 1;
+    }
+    {   // periodic exchange of the coordinates
+        double *f[3]; int mask[3];
+        for (int m = 0; m < 3; m++) { f[m] = const_cast<double *>(p.met[m]); mask[m] = 7; }
+        CK(ocfd::launch_ghost(p, f, mask, 3, ctx->stream), "mesh ghost fill");
+        ctx->launches += 1;
+    }
+    // the Ev scratch (12 LAP fields) holds the nine coordinate derivatives
+    CK(ocfd::launch_mesh_metrics(p, ctx->cfg.jac_bound, ctx->ev_buf, ctx->stream), "metrics from mesh");
+    ctx->launches += 10;
+    {   // periodic exchange of the ten computed fields
+        double *f[10]; int mask[10];
+        for (int m = 0; m < 10; m++) { f[m] = const_cast<double *>(p.met[ocfd::M_AKX + m]); mask[m] = 7; }
+        CK(ocfd::launch_ghost(p, f, mask, 10, ctx->stream), "metric ghost fill");
+        ctx->launches += 1;
+    }
+    unsigned *flag = reinterpret_cast<unsigned *>(ctx->red_buf);
+    CK(ocfd::launch_negative_jacobian(p, flag, ctx->stream), "Jacobian check");
+    ctx->launches += 1;
+    unsigned neg = 0;
+    CK(cudaMemcpyAsync(&neg, flag, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream), "Jacobian check");
+    CK(cudaStreamSynchronize(ctx->stream), "set_mesh");
+    if (neg) return fail(ctx, OCFD_ERR_ARG, "negative Jacobian computed from the mesh (the reference stops here)");
+    p.uniform_metrics = 0;          // metrics vary; kernels read the fields
+    ctx->have_metrics = true;
+    return OCFD_OK;
+}
+
+// the 13 metric fields as the kernels read them (interior), e.g. to write
+// OCFD3d-Jacobi.dat after a mesh was given
+extern "C" int ocfd_b200_get_metrics(ocfd_b200_ctx *ctx, double *metrics13) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (!metrics13) return OCFD_ERR_ARG;
+    const Params &p = ctx->p;
+    size_t inB = sizeof(double) * (size_t)p.N;
+    for (int m = 0; m < 13; m++) {
+        CK(ocfd::launch_gather(p, p.met[m], ctx->stage_buf, ctx->stream), "metric gather");
+        ctx->launches += 1;
+        CK(cudaMemcpyAsync(metrics13 + (size_t)m * p.N, ctx->stage_buf, inB, cudaMemcpyDeviceToHost, ctx->stream),
+           "metric read-back");
+    }
+    CK(cudaStreamSynchronize(ctx->stream), "get_metrics");
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_set_mesh(ocfd_b200_ctx *ctx, const double *xyz3) {
+    return set_mesh_impl(ctx, xyz3, cudaMemcpyHostToDevice);
+}
+extern "C" int ocfd_b200_set_mesh_device(ocfd_b200_ctx *ctx, const double *xyz3_dev) {
+    return set_mesh_impl(ctx, xyz3_dev, cudaMemcpyDeviceToDevice);
 }
 
 static int upload_prims(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKind kind) {

@@ -201,3 +201,30 @@ def random_smooth_case(nx: int, ny: int, nz: int, seed: int = 7, scheme_invis: s
             scale = float(np.max(np.abs(met[3])))
             met[m] = base + (scale if m != 12 else float(met[12].max())) * pert
     return Case(cfg, prims, met, f"random {nx}x{ny}x{nz} seed={seed} shock={shock}")
+
+
+def mesh_case(nx: int, ny: int, nz: int, seed: int = 7, scheme_invis: str = "WENO7",
+              charteric: int = 0, shock: bool = False, jac_bound=(1, 1, 1),
+              iperiodic=(0, 0, 1), dif_bound=(1, 1, 1, 1, 0, 0), non_ref=(0, 0, 0, 0, 0, 0),
+              skew: float = 0.08) -> Case:
+    """A case whose metrics the solver computes from mesh coordinates
+    (OCFD3d-Mesh.dat: x, y, z; JAC_BOUND selects the derivative closures at
+    both ends of each direction).  The grid is a smoothly skewed and
+    stretched box, the flow the random fields of random_smooth_case.
+    ``Case.metrics`` holds the three coordinate fields."""
+    base = random_smooth_case(nx, ny, nz, seed=seed, scheme_invis=scheme_invis, charteric=charteric,
+                              shock=shock, iperiodic=iperiodic, dif_bound=dif_bound, non_ref=non_ref)
+    rng = np.random.default_rng(seed + 1000)
+    xi = np.arange(nx) / (nx - 1.0)
+    eta = np.arange(ny) / (ny - 1.0)
+    zeta = np.arange(nz) / float(nz)
+    Z, Y, X = np.meshgrid(zeta, eta, xi, indexing="ij")
+    Lx, Ly, Lz = 2 * math.pi, 2 * math.pi, 2 * math.pi
+    a = skew * rng.uniform(0.5, 1.0, size=3)
+    x = Lx * X + a[0] * Lx * np.sin(math.pi * Y) * np.sin(2 * math.pi * Z)
+    y = Ly * Y * (1.0 + 0.3 * X * (1.0 - X)) + a[1] * Ly * np.sin(math.pi * X)
+    z = Lz * Z + a[2] * Lz * np.sin(math.pi * X) * np.sin(math.pi * Y)
+    cfg = base.cfg
+    cfg.jac_bound = tuple(jac_bound)
+    return Case(cfg, base.prims, [x, y, z],
+                f"mesh {nx}x{ny}x{nz} seed={seed} skew={skew} scheme={scheme_invis}")

@@ -29,6 +29,7 @@ EXPORTED = (
     "ocfd_b200_create", "ocfd_b200_destroy", "ocfd_b200_set_stream", "ocfd_b200_get_stream",
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
     "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics", "ocfd_b200_set_sweep_impl",
+    "ocfd_b200_set_mesh", "ocfd_b200_set_mesh_device", "ocfd_b200_get_metrics",
     "ocfd_b200_set_primitives", "ocfd_b200_set_primitives_device", "ocfd_b200_step",
     "ocfd_b200_advance_host", "ocfd_b200_swap_time_levels", "ocfd_b200_du_comput",
     "ocfd_b200_time_advance", "ocfd_b200_get_duvwT", "ocfd_b200_bc",
@@ -100,6 +101,9 @@ def load(path: Optional[str] = None):
         "ocfd_b200_synchronize": (ctypes.c_int, [P]),
         "ocfd_b200_set_metrics": (ctypes.c_int, [P, D]),
         "ocfd_b200_set_metrics_device": (ctypes.c_int, [P, P]),
+        "ocfd_b200_set_mesh": (ctypes.c_int, [P, D]),
+        "ocfd_b200_set_mesh_device": (ctypes.c_int, [P, P]),
+        "ocfd_b200_get_metrics": (ctypes.c_int, [P, D]),
         "ocfd_b200_set_metric_mode": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_uniform_metrics": (ctypes.c_int, [P]),
         "ocfd_b200_set_sweep_impl": (ctypes.c_int, [P, ctypes.c_int]),
@@ -203,10 +207,20 @@ class Solver:
 
     # set-up -----------------------------------------------------------
     def set_metrics(self, metrics: Sequence[np.ndarray]):
+        """13 fields: the metrics (OCFD3d-Jacobi.dat); 3 fields: mesh
+        coordinates (OCFD3d-Mesh.dat), from which the GPU computes them."""
         a = np.ascontiguousarray(np.stack([np.asarray(m, np.float64) for m in metrics]))
+        if a.shape == (3,) + self.shape:
+            self._check(self.L.ocfd_b200_set_mesh(self.h, _dp(a)), "set_mesh")
+            return
         if a.shape != (13,) + self.shape:
-            raise ValueError(f"metrics shape {a.shape} != {(13,) + self.shape}")
+            raise ValueError(f"metrics shape {a.shape} != {(13,) + self.shape} (or 3 mesh fields)")
         self._check(self.L.ocfd_b200_set_metrics(self.h, _dp(a)), "set_metrics")
+
+    def metrics(self) -> np.ndarray:
+        out = np.empty((13,) + self.shape, dtype=np.float64)
+        self._check(self.L.ocfd_b200_get_metrics(self.h, _dp(out)), "get_metrics")
+        return out
 
     def set_sweep_impl(self, impl: int):
         self._check(self.L.ocfd_b200_set_sweep_impl(self.h, impl), "set_sweep_impl")

@@ -193,6 +193,136 @@ void oro_set_metrics(oro_state *s, const double *fields13) {
     }
 }
 
+/* d(coordinate)/d(index) along dir for metrics: OCFD_d{x,y,z}0_CD6_kernel
+ * (src/OCFD_Schemes.cu:1236-1304) over the interior, then, when JAC_BOUND of
+ * the direction is non-zero, OCFD_D{x,y,z}0_bound_kernel_{m,p}
+ * (src/OCFD_bound_Scheme.cu:189-349) on the four points at each end, with
+ * each direction's own grouping of the terms. */
+static void jac_d0(oro_state *s, const double *f, double *out, int dir) {
+    size_t st[3] = { 1, (size_t)s->nx2, (size_t)s->nx2 * s->ny2 };
+    long sd = (long)st[dir];
+    double h = dir == 0 ? s->hx : (dir == 1 ? s->hy : s->hz);
+    int n = dir == 0 ? s->nx : (dir == 1 ? s->ny : s->nz);
+    int bound = s->c.jac_bound[dir] != 0;
+#pragma omp parallel for
+    for (int k = 0; k < s->nz; k++)
+        for (int j = 0; j < s->ny; j++)
+            for (int i = 0; i < s->nx; i++) {
+                size_t q = L(s, i + LAP, j + LAP, k + LAP);
+                const double *c = f + q;            /* c[t*sd] = f(X+t) */
+#define F_(t) c[(long)(t) * sd]
+                int X = dir == 0 ? i : (dir == 1 ? j : k);
+                double v = (45.0*(F_(1) - F_(-1)) - 9.0*(F_(2) - F_(-2)) + (F_(3) - F_(-3)))/(60.0*h);
+                if (bound) {
+                    /* lower end: same grouping in x, y, z (points 0..6 of the line) */
+                    if (X == 0) v = (F_(1) - F_(0))/h;
+                    else if (X == 1) v = (F_(1) - F_(-1))*0.5/h;
+                    else if (X == 2) v = (F_(-2) - 8.0*F_(-1) + 8.0*F_(1) - F_(2))/(12.0*h);
+                    else if (X == 3) v = (F_(3) - F_(-3) - 9.0*(F_(2) - F_(-2)) + 45.0*(F_(1) - F_(-1)))/(60.0*h);
+                    /* upper end, t = n-1 */
+                    int u = X - (n - 1);
+                    if (dir != 1) {
+                        if (u == 0) v = (F_(0) - F_(-1))/h;
+                        else if (u == -1) v = (F_(1) - F_(-1))*0.5/h;
+                        else if (u == -2) v = (F_(-2) - 8.0*F_(-1) + 8.0*F_(1) - F_(2))/(12.0*h);
+                        else if (u == -3) v = (F_(3) - F_(-3) - 9.0*(F_(2) - F_(-2)) + 45.0*(F_(1) - F_(-1)))/(60.0*h);
+                    } else {
+                        if (u == 0) v = -(F_(-1) - F_(0))/h;
+                        else if (u == -1) v = -(F_(-1) - F_(1))*0.5/h;
+                        else if (u == -2) v = -(F_(2) - 8.0*F_(1) + 8.0*F_(-1) - F_(-2))/(12.0*h);
+                        else if (u == -3) v = -(F_(-3) - F_(3) - 9.0*(F_(-2) - F_(2)) + 45.0*(F_(-1) - F_(1)))/(60.0*h);
+                    }
+                }
+#undef F_
+                out[I(s, i, j, k)] = v;
+            }
+}
+
+void oro_set_mesh(oro_state *s, const double *xyz3) {
+    /* Init_Jacobian3d (src/OCFD_Comput_Jacobian3d.cu:32-141): every metric
+     * field 1.0 on the LAP box, coordinates into Axx, Ayy, Azz, periodic
+     * exchange of those three, then Comput_Jacobian3d (:221-246). */
+    for (int m = 0; m < 13; m++)
+        for (size_t q = 0; q < s->nlap; q++) s->A[m][q] = 1.0;
+    for (int m = 0; m < 3; m++) {
+        const double *src = xyz3 + (size_t)m * s->nin;
+        for (int k = 0; k < s->nz; k++)
+            for (int j = 0; j < s->ny; j++)
+                for (int i = 0; i < s->nx; i++)
+                    s->A[m][L(s, i + LAP, j + LAP, k + LAP)] = src[I(s, i, j, k)];
+        exchange_xyz(s, s->A[m]);
+    }
+    /* comput_Jac3d (:393-424): xi..zk = d(x,y,z)/d(i,j,k) */
+    double **D = s->grad;   /* scratch: D[3*dir + c] = d coord c / d index dir */
+    for (int dir = 0; dir < 3; dir++)
+        for (int c = 0; c < 3; c++) jac_d0(s, s->A[AXX + c], D[3 * dir + c], dir);
+    /* comput_Jac3d_kernal (:250-391) */
+    int nx = s->nx, ny = s->ny, nz = s->nz;
+#pragma omp parallel for
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i < nx; i++) {
+                size_t c = I(s, i, j, k), q = L(s, i + LAP, j + LAP, k + LAP);
+                double xi1 = D[0][c], yi1 = D[1][c], zi1 = D[2][c];
+                double xj1 = D[3][c], yj1 = D[4][c], zj1 = D[5][c];
+                double xk1 = D[6][c], yk1 = D[7][c], zk1 = D[8][c];
+                double Jac1 = 1.0 / (xi1 * yj1 * zk1 + yi1 * zj1 * xk1 + zi1 * xj1 * yk1
+                                     - zi1 * yj1 * xk1 - yi1 * xj1 * zk1 - xi1 * zj1 * yk1);
+                s->A[AJAC][q] = Jac1;
+                s->A[AKX][q] = (yj1 * zk1 - zj1 * yk1);
+                s->A[AKY][q] = (zj1 * xk1 - xj1 * zk1);
+                s->A[AKZ][q] = (xj1 * yk1 - yj1 * xk1);
+                s->A[AIX][q] = (yk1 * zi1 - zk1 * yi1);
+                s->A[AIY][q] = (zk1 * xi1 - xk1 * zi1);
+                s->A[AIZ][q] = (xk1 * yi1 - yk1 * xi1);
+                s->A[ASX][q] = (yi1 * zj1 - zi1 * yj1);
+                s->A[ASY][q] = (zi1 * xj1 - xi1 * zj1);
+                s->A[ASZ][q] = (xi1 * yj1 - yi1 * xj1);
+            }
+    /* constant extrapolation into the ghost slabs of the 10 computed fields
+     * (x ghosts for interior y,z; y ghosts for interior x,z; z ghosts for
+     * interior x,y), then the periodic exchange overwrites periodic sides */
+    for (int m = AKX; m <= AJAC; m++) {
+        double *A = s->A[m];
+        for (int k = 0; k < nz; k++)
+            for (int j = 0; j < ny; j++)
+                for (int g = 0; g < LAP; g++) {
+                    A[L(s, g, j + LAP, k + LAP)] = A[L(s, LAP, j + LAP, k + LAP)];
+                    A[L(s, nx + LAP + g, j + LAP, k + LAP)] = A[L(s, nx - 1 + LAP, j + LAP, k + LAP)];
+                }
+        for (int k = 0; k < nz; k++)
+            for (int g = 0; g < LAP; g++)
+                for (int i = 0; i < nx; i++) {
+                    A[L(s, i + LAP, g, k + LAP)] = A[L(s, i + LAP, LAP, k + LAP)];
+                    A[L(s, i + LAP, ny + LAP + g, k + LAP)] = A[L(s, i + LAP, ny - 1 + LAP, k + LAP)];
+                }
+        for (int g = 0; g < LAP; g++)
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++) {
+                    A[L(s, i + LAP, j + LAP, g)] = A[L(s, i + LAP, j + LAP, LAP)];
+                    A[L(s, i + LAP, j + LAP, nz + LAP + g)] = A[L(s, i + LAP, j + LAP, nz - 1 + LAP)];
+                }
+        exchange_xyz(s, A);
+    }
+}
+
+int oro_negative_jacobian(const oro_state *s) {
+    /* ana_Jac (src/OCFD_ana.cu:24-48): any Ajac < 0 on the LAP box */
+    for (size_t q = 0; q < s->nlap; q++)
+        if (s->A[AJAC][q] < 0) return 1;
+    return 0;
+}
+
+void oro_get_metrics(const oro_state *s, double *fields13) {
+    for (int m = 0; m < 13; m++) {
+        double *dst = fields13 + (size_t)m * s->nin;
+        for (int k = 0; k < s->nz; k++)
+            for (int j = 0; j < s->ny; j++)
+                for (int i = 0; i < s->nx; i++)
+                    dst[I(s, i, j, k)] = s->A[m][L(s, i + LAP, j + LAP, k + LAP)];
+    }
+}
+
 /* pri_to_cons_kernel (src/commen_kernel.cu:32-66) for one interior cell. */
 static inline void p2c_cell(oro_state *s, int i, int j, int k) {
     size_t q = L(s, i + LAP, j + LAP, k + LAP), n = s->nin, c = I(s, i, j, k);

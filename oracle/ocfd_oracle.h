@@ -58,6 +58,15 @@ void oro_destroy(oro_state *s);
  * (src/OCFD_Comput_Jacobian3d.cu:32-218): 1.0 everywhere, then periodic
  * exchange in the periodic directions. */
 void oro_set_metrics(oro_state *s, const double *fields13);
+/* Mesh coordinates x,y,z, interior [3][nz][ny][nx] (OCFD3d-Mesh.dat): the
+ * metrics are computed as Comput_Jacobian3d does
+ * (src/OCFD_Comput_Jacobian3d.cu:221-424); JAC_BOUND selects the one-sided
+ * derivative closures at both ends of a direction. */
+void oro_set_mesh(oro_state *s, const double *xyz3);
+/* 1 when a Jacobian on the LAP box is negative (ana_Jac, src/OCFD_ana.cu:24-48). */
+int oro_negative_jacobian(const oro_state *s);
+/* The 13 metric fields, interior, in OCFD3d-Jacobi.dat order. */
+void oro_get_metrics(const oro_state *s, double *fields13);
 
 /* Initial primitives d,u,v,w,T, interior [5][nz][ny][nx] (opencfd.dat).
  * Mirrors init() (src/OCFD_init.cu:26-131): ghosts zero, pri_to_cons. */

@@ -58,6 +58,10 @@ def lib():
         L.oro_create.argtypes = [ctypes.POINTER(OroConfig)]
         L.oro_destroy.argtypes = [P]
         L.oro_set_metrics.argtypes = [P, D]
+        L.oro_set_mesh.argtypes = [P, D]
+        L.oro_get_metrics.argtypes = [P, D]
+        L.oro_negative_jacobian.argtypes = [P]
+        L.oro_negative_jacobian.restype = ctypes.c_int
         L.oro_set_primitives.argtypes = [P, D, ctypes.c_int, ctypes.c_double]
         for name in ("oro_prepare", "oro_get_duvwT", "oro_bc", "oro_get_amu",
                      "oro_swap_time_levels"):
@@ -133,8 +137,15 @@ class Oracle:
         self.L = lib()
         self.h = self.L.oro_create(ctypes.byref(self._c))
         self.shape = (cfg.nz, cfg.ny, cfg.nx)
+        # 13 fields: OCFD3d-Jacobi.dat content; 3 fields: OCFD3d-Mesh.dat
+        # coordinates, from which the metrics are computed
         met = np.ascontiguousarray(np.stack([np.asarray(m, np.float64) for m in metrics]))
-        self.L.oro_set_metrics(self.h, _dp(met))
+        if met.shape[0] == 3:
+            self.L.oro_set_mesh(self.h, _dp(met))
+            if self.L.oro_negative_jacobian(self.h):
+                raise ValueError("negative Jacobian (the reference stops here)")
+        else:
+            self.L.oro_set_metrics(self.h, _dp(met))
         pr = np.ascontiguousarray(np.stack([np.asarray(p, np.float64) for p in prims]))
         self.L.oro_set_primitives(self.h, _dp(pr), istep, tt)
         self.L.oro_prepare(self.h)
@@ -187,6 +198,11 @@ class Oracle:
 
     def du(self) -> np.ndarray:
         return self._get5(self.L.oro_get_du)
+
+    def metrics(self) -> np.ndarray:
+        out = np.empty((13,) + self.shape, dtype=np.float64)
+        self.L.oro_get_metrics(self.h, _dp(out))
+        return out
 
     def pressure(self) -> np.ndarray:
         out = np.empty(self.shape, dtype=np.float64)

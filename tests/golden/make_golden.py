@@ -55,6 +55,25 @@ def golden_cases():
         c = cases.random_smooth_case(12, 11, 10, seed=23, scheme_invis=sch, charteric=1, shock=True)
         out.append((f"rnd12x11x10_{sch.lower()}_char", c, 3))
     out.extend(bounded_cases())
+    out.extend(mesh_cases())
+    return out
+
+
+def mesh_cases():
+    """Metrics computed by the solver from mesh coordinates (OCFD3d-Mesh.dat,
+    JAC_BOUND = 1 1 1) on a skewed, stretched grid, x and y closed, z
+    periodic."""
+    out = []
+    c = cases.mesh_case(14, 13, 12, seed=51, scheme_invis="WENO7")
+    out.append(("mesh14x13x12_weno7", c, 3))
+    c = cases.mesh_case(13, 14, 12, seed=52, scheme_invis="SCHEME_HYBRIDAUTO", charteric=1, shock=True,
+                        non_ref=(1, 0, 0, 1, 0, 0))
+    c.cfg.hy_dp_intv = (0.01, 0.2)
+    out.append(("mesh13x14x12_hybrid_char_nonref", c, 3))
+    c = cases.mesh_case(12, 12, 11, seed=53, scheme_invis="UP7", jac_bound=(1, 1, 1),
+                        dif_bound=(1, 1, 1, 1, 0, 0))
+    c.cfg.scheme_vis = "CD8"
+    out.append(("mesh12x12x11_up7_cd8", c, 3))
     return out
 
 

@@ -57,6 +57,11 @@ def small_cases():
         out.append((f"rnd_{sch.lower()}_char", cases.random_smooth_case(12, 11, 10, seed=23, scheme_invis=sch,
                                                                         charteric=1, shock=True)))
     out.extend(bounded_cases())
+    out.append(("mesh_weno7", cases.mesh_case(14, 13, 12, seed=61, scheme_invis="WENO7")))
+    c = cases.mesh_case(13, 14, 12, seed=62, scheme_invis="SCHEME_HYBRIDAUTO", charteric=1, shock=True,
+                        non_ref=(1, 0, 0, 1, 0, 0))
+    c.cfg.hy_dp_intv = (0.01, 0.2)
+    out.append(("mesh_hybrid_char", c))
     return out
 
 
@@ -177,3 +182,26 @@ def test_bounded_sweep_variants(name, case, gpu_lib):
     with pytest.raises(lib.OcfdError) as ei:
         c.step(1)
     assert ei.value.status == -2
+
+
+@pytest.mark.parametrize("iperiodic", [(0, 0, 1), (1, 0, 0), (0, 0, 0)], ids=["z_per", "x_per", "closed"])
+def test_metrics_from_mesh_match_oracle(iperiodic, gpu_lib):
+    """Comput_Jacobian3d on the GPU against the oracle's restatement: the 13
+    metric fields (FP64, tolerance 1e-14 relative per field).  JAC_BOUND is
+    set in every direction: without it a periodic copy of an increasing
+    coordinate makes the Jacobian negative at the seam, where the reference
+    stops."""
+    case = cases.mesh_case(15, 13, 12, seed=63, jac_bound=(1, 1, 1), iperiodic=iperiodic)
+    o = Oracle(case.cfg, case.prims, case.metrics)
+    s = lib.Solver(case.cfg, case.prims, case.metrics)
+    assert not s.uniform_metrics
+    err = rel_l2(s.metrics(), o.metrics())
+    assert np.all(err <= 1e-14), err
+
+
+def test_negative_jacobian_is_rejected(gpu_lib):
+    case = cases.mesh_case(12, 12, 11, seed=64)
+    case.metrics[0] = case.metrics[0][:, :, ::-1].copy()      # mirror x: det < 0
+    with pytest.raises(lib.OcfdError) as ei:
+        lib.Solver(case.cfg, case.prims, case.metrics)
+    assert ei.value.status == -1
