@@ -136,6 +136,20 @@ int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps);
 int ocfd_b200_advance_host(ocfd_b200_ctx *ctx, const double *prim5_in, double *prim5_out,
                            int nsteps);
 
+/* Shock-capturing filter n (0..7): FILTER_NPARA<n+1> = ntime, filter_x,
+ * filter_y, filter_z, ib, ie, jb, je, kb, ke, scheme (2) and FILTER_RPARA<n+1>
+ * = s0, rth, time limit (src/parameters.c:305-325); ranges clamped as
+ * set_para_filtering (src/OCFD_filtering.cu:20-73).  step() then runs
+ * filtering() (:75-183) after every step whose Istep is a multiple of ntime
+ * while tt <= the time limit.  It reads the pressure the hybrid sensor
+ * forms, so it is meaningful with SCHEME_HYBRIDAUTO only (as in the
+ * reference, whose pressure field is otherwise zero). */
+int ocfd_b200_set_filter(ocfd_b200_ctx *ctx, int n, const int npara[11], const double rpara[3]);
+/* filtering() at the context's Istep and tt (src/OCFD_NS_Solver.cu:95). */
+int ocfd_b200_filtering(ocfd_b200_ctx *ctx);
+/* The driver's Istep and tt, which the per-stage calls do not advance. */
+int ocfd_b200_set_time(ocfd_b200_ctx *ctx, int istep, double tt);
+
 /* Per-stage pieces, same semantics as the reference calls of one stage. */
 int ocfd_b200_swap_time_levels(ocfd_b200_ctx *ctx);        /* src/OCFD_NS_Solver.cu:65-73 */
 int ocfd_b200_du_comput(ocfd_b200_ctx *ctx, int krk);      /* src/OCFD_Stream.cu:28-54    */
@@ -196,6 +210,7 @@ void get_duvwT(void);                       /* head/commen_kernel.h:17         *
 void get_Amu(void);                         /* head/commen_kernel.h:20         */
 void OCFD_bc(void);                         /* src/OCFD_boundary.cu:18         */
 void Set_Scheme_HybridAuto(void *stream);   /* head/OCFD_Schemes_hybrid_auto.h:24 (cudaStream_t*) */
+void filtering(double *pf, double *pf_lap, double *pp);   /* src/OCFD_filtering.cu:75 */
 
 #ifdef __cplusplus
 }

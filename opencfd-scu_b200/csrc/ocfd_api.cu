@@ -36,6 +36,7 @@ cudaError_t launch_sweeps2(const Params &p, cudaStream_t st);
 cudaError_t launch_sweeps3(const Params &p, cudaStream_t st);
 cudaError_t launch_mesh_metrics(const Params &p, const int jac_bound[3], double *scratch, cudaStream_t st);
 cudaError_t launch_negative_jacobian(const Params &p, unsigned *flag, cudaStream_t st);
+cudaError_t launch_filter_pass(const Params &p, int dir, const int box[6], double s0, double rth, cudaStream_t st);
 int sweeps3_kernels(const Params &p);
 cudaError_t compute_dirconst(Params &p, DirConst *dev_scratch, cudaStream_t st);
 }  // namespace ocfd
@@ -67,6 +68,12 @@ struct ocfd_b200_ctx {
     double *stage_buf = nullptr;  // 5 interior fields for host transfers
     double *red_buf = nullptr;    // reduction partials + result, then two counters
     unsigned *defer_buf = nullptr;  // three counters (padded to 256 B), then 3 deferred-cell lists
+    double *filter_buf = nullptr;   // pf_lap (5 LAP fields) and the pressure (1 LAP field)
+    // FILTER_NPARA / FILTER_RPARA as set_para_filtering leaves them
+    int nfilter = 0;
+    int fpar[8][11] = {};
+    double frpar[8][3] = {};
+    int fjudge[3] = {0, 0, 0};
     double *pinned = nullptr;     // host staging for advance_host
     size_t pinned_bytes = 0;
     bool have_metrics = false;
@@ -121,7 +128,7 @@ extern "C" const char *ocfd_b200_last_error(const ocfd_b200_ctx *ctx) {
 static void free_all(ocfd_b200_ctx *c) {
     cudaFree(c->prim_buf); cudaFree(c->met_buf); cudaFree(c->cons_buf);
     cudaFree(c->ev_buf); cudaFree(c->flag_buf); cudaFree(c->stage_buf);
-    cudaFree(c->red_buf); cudaFree(c->defer_buf);
+    cudaFree(c->red_buf); cudaFree(c->defer_buf); cudaFree(c->filter_buf);
     if (c->pinned) cudaFreeHost(c->pinned);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -551,6 +558,43 @@ extern "C" int ocfd_b200_swap_time_levels(ocfd_b200_ctx *ctx) {
     return OCFD_OK;
 }
 
+// filtering() (src/OCFD_filtering.cu:75-183) at the context's Istep and tt
+static int run_filters(ocfd_b200_ctx *ctx) {
+    if (!ctx->nfilter) return OCFD_OK;
+    bool any = false;
+    for (int m = 0; m < ctx->nfilter; m++)
+        if (ctx->istep % ctx->fpar[m][0] == 0) any = true;
+    if (!any) return OCFD_OK;
+    const Params &p = ctx->p;
+    {   // periodic exchange of p and pf_lap in the directions any filter uses
+        double *f[6]; int mask[6];
+        const int dm = (ctx->fjudge[0] ? 1 : 0) | (ctx->fjudge[1] ? 2 : 0) | (ctx->fjudge[2] ? 4 : 0);
+        f[0] = p.pfil; mask[0] = dm;
+        for (int m = 0; m < 5; m++) { f[1 + m] = p.flap + (size_t)m * p.lapN; mask[1 + m] = dm; }
+        CK(ocfd::launch_ghost(p, f, mask, 6, ctx->stream), "filter ghost fill");
+        ctx->launches += 1;
+    }
+    for (int m = 0; m < ctx->nfilter; m++) {
+        if (!(ctx->tt <= ctx->frpar[m][2]) || ctx->istep % ctx->fpar[m][0] != 0) continue;
+        const double s0 = ctx->frpar[m][0], rth = ctx->frpar[m][1];
+        int box[6];
+        for (int t = 0; t < 6; t++) box[t] = ctx->fpar[m][4 + t];
+        if (ctx->fpar[m][1] == 1) { CK(ocfd::launch_filter_pass(p, 0, box, s0, rth, ctx->stream), "filter x"); ctx->launches += 1; }
+        if (ctx->fpar[m][2] == 1) { CK(ocfd::launch_filter_pass(p, 1, box, s0, rth, ctx->stream), "filter y"); ctx->launches += 1; }
+        if (ctx->fpar[m][3] == 1) {
+            // filter_z3d_shock launches the y kernel on an (8, 8, 4+2) block:
+            // it filters along y, and its y rows reach only jb + 6*ceil((je-jb)/8)
+            int zb[6];
+            for (int t = 0; t < 6; t++) zb[t] = box[t];
+            const int gy = (box[3] - box[2] + 7) / 8;
+            if (zb[3] > box[2] + 6 * gy + 1) zb[3] = box[2] + 6 * gy + 1;
+            CK(ocfd::launch_filter_pass(p, 1, zb, s0, rth, ctx->stream), "filter z");
+            ctx->launches += 1;
+        }
+    }
+    return OCFD_OK;
+}
+
 extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
     int rc = check_ready(ctx);
     if (rc) return rc;
@@ -561,7 +605,52 @@ extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
             if ((rc = rhs(ctx, krk, krk))) return rc;
         ctx->istep++;
         ctx->tt += ctx->p.dt;
+        if ((rc = run_filters(ctx))) return rc;
     }
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_filtering(ocfd_b200_ctx *ctx) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    return run_filters(ctx);
+}
+
+extern "C" int ocfd_b200_set_time(ocfd_b200_ctx *ctx, int istep, double tt) {
+    if (!ctx) return OCFD_ERR_ARG;
+    ctx->istep = istep;
+    ctx->tt = tt;
+    return OCFD_OK;
+}
+
+// FILTER_NPARA<n+1> / FILTER_RPARA<n+1>, clamped as set_para_filtering does
+// on one rank (src/OCFD_filtering.cu:20-73)
+extern "C" int ocfd_b200_set_filter(ocfd_b200_ctx *ctx, int n, const int npara[11], const double rpara[3]) {
+    if (!ctx || !npara || !rpara) return OCFD_ERR_ARG;
+    if (n < 0 || n >= 8) return fail(ctx, OCFD_ERR_ARG, "filter index must be 0..7");
+    if (npara[0] < 1) return fail(ctx, OCFD_ERR_ARG, "filter step interval must be >= 1");
+    if (npara[10] != 2)
+        return fail(ctx, OCFD_ERR_UNSUPPORTED, "only the shock-capturing filter (scheme 2) is built; "
+                                                "the reference's 9-point filter aborts");
+    Params &p = ctx->p;
+    if (!ctx->filter_buf) {
+        cudaError_t e = cudaMalloc(&ctx->filter_buf, sizeof(double) * 6 * (size_t)p.lapN);
+        if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, OCFD_ERR_NOMEM, "filter buffers"); }
+        CK(cudaMemsetAsync(ctx->filter_buf, 0, sizeof(double) * 6 * (size_t)p.lapN, ctx->stream), "filter init");
+        p.flap = ctx->filter_buf;
+        p.pfil = ctx->filter_buf + 5 * (size_t)p.lapN;
+    }
+    const int nn[3] = { p.nx, p.ny, p.nz };
+    for (int t = 0; t < 11; t++) ctx->fpar[n][t] = npara[t];
+    for (int d = 0; d < 3; d++) {
+        if (npara[1 + d] == 1) ctx->fjudge[d] = 1;
+        if (!p.periodic[d]) {
+            if (ctx->fpar[n][4 + 2 * d] < 6) ctx->fpar[n][4 + 2 * d] = 6;
+            if (ctx->fpar[n][5 + 2 * d] > nn[d] - 5) ctx->fpar[n][5 + 2 * d] = nn[d] - 5;
+        }
+    }
+    for (int t = 0; t < 3; t++) ctx->frpar[n][t] = rpara[t];
+    if (n + 1 > ctx->nfilter) ctx->nfilter = n + 1;
     return OCFD_OK;
 }
 
@@ -749,6 +838,12 @@ extern "C" void Set_Scheme_HybridAuto(void *stream) {
     if (!g_bound) { compat_report(OCFD_ERR_STATE, "Set_Scheme_HybridAuto"); return; }
     cudaError_t e = ocfd::launch_sensor(g_bound->p, g_bound->stream);
     compat_report(e == cudaSuccess ? OCFD_OK : OCFD_ERR_CUDA, "Set_Scheme_HybridAuto");
+}
+// the library keeps pf_lap and p itself; the arguments are the reference's
+// own buffers and are not read
+extern "C" void filtering(double *pf, double *pf_lap, double *pp) {
+    (void)pf; (void)pf_lap; (void)pp;
+    compat_report(g_bound ? ocfd_b200_filtering(g_bound) : OCFD_ERR_STATE, "filtering");
 }
 
 // ---------------------------------------------------------------------------

@@ -57,6 +57,11 @@ struct Params {
     // direction (interior cell indices; capacity N each), and their counts
     unsigned *defer[3];
     unsigned *defer_count;
+    // shock filter (null when no filter is set): U after the stage-3 update
+    // before the face re-projection (5 LAP-box fields) and the pressure
+    // cons_to_pri leaves after the last stage (1 LAP-box field)
+    double *flap;
+    double *pfil;
 };
 
 enum { M_AXX = 0, M_AYY, M_AZZ, M_AKX, M_AKY, M_AKZ, M_AIX, M_AIY, M_AIZ,

@@ -482,10 +482,17 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
             f[m] = t1 * fn + t2 * (p.f[m * N + tid] + p.dt * du[m]);
         }
     }
+    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+    if (krk == 3 && p.flap) {       // pf_lap, OCFD_time_advance_ker3 (src/OCFD_time.cu:78-92)
+#pragma unroll
+        for (int m = 0; m < 5; m++) p.flap[m * p.lapN + o] = f[m];
+    }
     double d1, u1, v1, w1, T2;
     cons_to_prim(p, f, d1, u1, v1, w1, T2);
-    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     p.prim[0][o] = d1; p.prim[1][o] = u1; p.prim[2][o] = v1; p.prim[3][o] = w1; p.prim[4][o] = T2;
+    // cons_to_pri_kernel also leaves the pressure (src/commen_kernel.cu:107),
+    // which the filter after the step reads
+    if (krk == 3 && p.pfil) p.pfil[o] = T2 * d1 / (p.Gamma * p.Ama * p.Ama);
     bool face = (i == 0) || (i == p.nx - 1) || (j == 0) || (j == p.ny - 1) || (k == 0) || (k == p.nz - 1);
     if (face) {
         f[0] = d1;
@@ -557,7 +564,18 @@ __global__ void k_rk_only(Params p, int krk) {
     double fn = p.fn[tid], du = p.du[tid];
     if (krk == 1) p.f[tid] = fn + p.dt * du;
     else if (krk == 2) { double t1 = 3.0 / 4.0, t2 = 1.0 / 4.0; p.f[tid] = t1 * fn + t2 * (p.f[tid] + p.dt * du); }
-    else { double t1 = 1.0 / 3.0, t2 = 2.0 / 3.0; p.f[tid] = t1 * fn + t2 * (p.f[tid] + p.dt * du); }
+    else {
+        double t1 = 1.0 / 3.0, t2 = 2.0 / 3.0;
+        const double v = t1 * fn + t2 * (p.f[tid] + p.dt * du);
+        p.f[tid] = v;
+        if (p.flap) {               // pf_lap
+            const long long m = tid / p.N, c = tid - m * p.N;
+            const int i = (int)(c % p.nx);
+            const long long r = c / p.nx;
+            const int j = (int)(r % p.ny), k = (int)(r / p.ny);
+            p.flap[m * p.lapN + lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP)] = v;
+        }
+    }
 }
 __global__ void k_c2p(Params p) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -566,10 +584,11 @@ __global__ void k_c2p(Params p) {
     int j = (int)(r % p.ny); int k = (int)(r / p.ny);
     const long long N = p.N;
     const double f[5] = {p.f[tid], p.f[N + tid], p.f[2 * N + tid], p.f[3 * N + tid], p.f[4 * N + tid]};
+    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     double d1, u1, v1, w1, T2;
     cons_to_prim(p, f, d1, u1, v1, w1, T2);
-    long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     p.prim[0][o] = d1; p.prim[1][o] = u1; p.prim[2][o] = v1; p.prim[3][o] = w1; p.prim[4][o] = T2;
+    if (p.pfil) p.pfil[o] = T2 * d1 / (p.Gamma * p.Ama * p.Ama);
 }
 __global__ void k_bc_faces(Params p) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;

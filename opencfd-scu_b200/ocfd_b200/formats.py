@@ -70,6 +70,10 @@ class CaseConfig:
     init_stat: int = 1
     ibc: int = 0
     stream: int = 0
+    # FILTER_NPARA<n> / FILTER_RPARA<n> (src/parameters.c:305-325): per filter
+    # ((ntime, filter_x, filter_y, filter_z, ib, ie, jb, je, kb, ke, scheme),
+    #  (s0, rth, time limit)); scheme 2 is the shock-capturing filter
+    filters: Tuple = ()
 
     @property
     def scheme_invis_id(self) -> int:
@@ -137,8 +141,11 @@ def write_config(path: str, cfg: CaseConfig) -> None:
         f"IBC = {cfg.ibc}",
         "BC_NPARA = 0",
         "BC_RPARA = 0",
-        "",
     ]
+    for n, (ip, rp) in enumerate(cfg.filters, start=1):
+        lines.append(f"FILTER_NPARA{n} = {_fmt(tuple(int(v) for v in ip))}")
+        lines.append(f"FILTER_RPARA{n} = {_fmt(tuple(float(v) for v in rp))}")
+    lines.append("")
     with open(path, "w") as fh:
         fh.write("\n".join(lines))
 
@@ -205,6 +212,13 @@ def read_config(path: str) -> CaseConfig:
     cfg.init_stat = int(kv.get("INIT_STAT", "1").split()[0])
     cfg.ibc = int(kv.get("IBC", "0").split()[0])
     cfg.stream = int(kv.get("STREAM", "0").split()[0])
+    filters = []
+    for key in sorted((k for k in kv if k.startswith("FILTER_NPARA")), key=lambda k: int(k[12:] or 0)):
+        rkey = "FILTER_RPARA" + key[12:]
+        ip = tuple(int(x) for x in kv[key].split()[:11])
+        rp = tuple(float(x) for x in kv.get(rkey, "0 0 0").split()[:3])
+        filters.append((ip, rp))
+    cfg.filters = tuple(filters)
     return cfg
 
 

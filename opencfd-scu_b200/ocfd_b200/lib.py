@@ -30,6 +30,7 @@ EXPORTED = (
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
     "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics", "ocfd_b200_set_sweep_impl",
     "ocfd_b200_set_mesh", "ocfd_b200_set_mesh_device", "ocfd_b200_get_metrics",
+    "ocfd_b200_set_filter", "ocfd_b200_filtering", "ocfd_b200_set_time", "filtering",
     "ocfd_b200_set_primitives", "ocfd_b200_set_primitives_device", "ocfd_b200_step",
     "ocfd_b200_advance_host", "ocfd_b200_swap_time_levels", "ocfd_b200_du_comput",
     "ocfd_b200_time_advance", "ocfd_b200_get_duvwT", "ocfd_b200_bc",
@@ -104,6 +105,10 @@ def load(path: Optional[str] = None):
         "ocfd_b200_set_mesh": (ctypes.c_int, [P, D]),
         "ocfd_b200_set_mesh_device": (ctypes.c_int, [P, P]),
         "ocfd_b200_get_metrics": (ctypes.c_int, [P, D]),
+        "ocfd_b200_set_filter": (ctypes.c_int, [P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), D]),
+        "ocfd_b200_filtering": (ctypes.c_int, [P]),
+        "ocfd_b200_set_time": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double]),
+        "filtering": (None, [D, D, D]),
         "ocfd_b200_set_metric_mode": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_uniform_metrics": (ctypes.c_int, [P]),
         "ocfd_b200_set_sweep_impl": (ctypes.c_int, [P, ctypes.c_int]),
@@ -185,6 +190,8 @@ class Solver:
         self.h = h
         if metric_mode:
             self._check(self.L.ocfd_b200_set_metric_mode(self.h, metric_mode), "set_metric_mode")
+        for n, (ip, rp) in enumerate(getattr(cfg, "filters", ()) or ()):
+            self.set_filter(n, ip, rp)
         if metrics is not None:
             self.set_metrics(metrics)
         if prims is not None:
@@ -216,6 +223,11 @@ class Solver:
         if a.shape != (13,) + self.shape:
             raise ValueError(f"metrics shape {a.shape} != {(13,) + self.shape} (or 3 mesh fields)")
         self._check(self.L.ocfd_b200_set_metrics(self.h, _dp(a)), "set_metrics")
+
+    def set_filter(self, n: int, npara, rpara):
+        ia = (ctypes.c_int * 11)(*[int(v) for v in npara])
+        da = (ctypes.c_double * 3)(*[float(v) for v in rpara])
+        self._check(self.L.ocfd_b200_set_filter(self.h, n, ia, da), "set_filter")
 
     def metrics(self) -> np.ndarray:
         out = np.empty((13,) + self.shape, dtype=np.float64)

@@ -52,6 +52,11 @@ struct oro_state {
     int *sch[3];                /* hybrid flags: (nx+1)ny nz, nx(ny+1)nz, nx ny(nz+1) */
     int istep;
     double tt;
+    /* filtering: pf_lap (U after the stage-3 RK update, before the face
+     * re-projection) and the ranges as set_para_filtering leaves them */
+    double *flap;               /* [5][LAP box] */
+    int fpar[8][11];
+    int fjudge[3];
 };
 
 enum { AXX = 0, AYY, AZZ, AKX, AKY, AKZ, AIX, AIY, AIZ, ASX, ASY, ASZ, AJAC };
@@ -103,7 +108,10 @@ oro_state *oro_create(const oro_config *cfg) {
 
     s->d = xcalloc(s->nlap); s->u = xcalloc(s->nlap); s->v = xcalloc(s->nlap);
     s->w = xcalloc(s->nlap); s->T = xcalloc(s->nlap); s->P = xcalloc(s->nlap);
-    s->cc = xcalloc(s->nlap); s->psens = xcalloc(s->nlap);
+    /* one pressure field, as pP_d: Comput_P fills the LAP box at the first
+     * stage of a step (sensor input), cons_to_pri_kernel rewrites the
+     * interior each stage, the filter reads it after the step */
+    s->cc = xcalloc(s->nlap); s->psens = s->P;
     for (int m = 0; m < 13; m++) {
         s->A[m] = xcalloc(s->nlap);
         for (size_t q = 0; q < s->nlap; q++) s->A[m][q] = 1.0;   /* Init_Jacobian3d :36-64 */
@@ -116,12 +124,30 @@ oro_state *oro_create(const oro_config *cfg) {
     s->sch[0] = (int *)calloc((size_t)(s->nx + 1) * s->ny * s->nz, sizeof(int));
     s->sch[1] = (int *)calloc((size_t)s->nx * (s->ny + 1) * s->nz, sizeof(int));
     s->sch[2] = (int *)calloc((size_t)s->nx * s->ny * (s->nz + 1), sizeof(int));
+    /* set_para_filtering (src/OCFD_filtering.cu:20-73) on a single rank:
+     * ranges [ib, ie) etc. (0-based, without LAP), kept 6 cells away from
+     * a non-periodic lower face and 5 from an upper one */
+    s->flap = NULL;
+    if (s->c.nfilter > 8) s->c.nfilter = 8;
+    int nn[3] = { s->nx, s->ny, s->nz };
+    for (int k = 0; k < s->c.nfilter; k++) {
+        for (int t = 0; t < 11; t++) s->fpar[k][t] = s->c.filter_ipara[k][t];
+        for (int d = 0; d < 3; d++) {
+            if (s->fpar[k][1 + d] == 1) s->fjudge[d] = 1;
+            if (s->c.iperiodic[d] != 1) {
+                if (s->fpar[k][4 + 2 * d] < 6) s->fpar[k][4 + 2 * d] = 6;
+                if (s->fpar[k][5 + 2 * d] > nn[d] - 5) s->fpar[k][5 + 2 * d] = nn[d] - 5;
+            }
+        }
+    }
+    if (s->c.nfilter > 0) s->flap = xcalloc(5 * s->nlap);
     return s;
 }
 
 void oro_destroy(oro_state *s) {
     if (!s) return;
-    free(s->d); free(s->u); free(s->v); free(s->w); free(s->T); free(s->P); free(s->cc); free(s->psens);
+    free(s->d); free(s->u); free(s->v); free(s->w); free(s->T); free(s->P); free(s->cc);
+    free(s->flap);
     for (int m = 0; m < 13; m++) free(s->A[m]);
     for (int dir = 0; dir < 3; dir++) { free(s->fp[dir]); free(s->fm[dir]); }
     for (int m = 0; m < 4; m++) { free(s->ev[m]); free(s->vis[m]); }
@@ -1460,6 +1486,91 @@ void oro_time_advance(oro_state *s, int krk) {
         double tmp1 = 1.0/3.0, tmp2 = 2.0/3.0;
 #pragma omp parallel for
         for (long q = 0; q < (long)n5; q++) f[q] = tmp1*fn[q] + tmp2*(f[q] + dt*du[q]);
+        /* OCFD_time_advance_ker3 also writes pf_lap (:78-92) */
+        if (s->flap) {
+            for (int m = 0; m < 5; m++)
+                for (int k = 0; k < s->nz; k++)
+                    for (int j = 0; j < s->ny; j++)
+                        for (int i = 0; i < s->nx; i++)
+                            s->flap[(size_t)m * s->nlap + L(s, i + LAP, j + LAP, k + LAP)] = f[(size_t)m * s->nin + I(s, i, j, k)];
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* shock-capturing filter, src/OCFD_filtering.cu:363-606                     */
+/* ------------------------------------------------------------------------ */
+
+/* sigma of filter_{x,y}3d_shock_kernel at LAP point q along stride sd */
+static double filter_sigma(const double *P, size_t q, long sd, double rth) {
+    double p_m2 = P[q - 2 * sd], p_m1 = P[q - sd], p_00 = P[q], p_p1 = P[q + sd], p_p2 = P[q + 2 * sd];
+    double dp0 = 0.25 * (-p_p1 + 2.0 * p_00 - p_m1);
+    double dp1 = 0.25 * (-p_p2 + 2.0 * p_p1 - p_00);
+    double dp2 = 0.25 * (-p_00 + 2.0 * p_m1 - p_m2);
+    double ri = 0.5 * ((dp0 - dp1) * (dp0 - dp1) + (dp0 - dp2) * (dp0 - dp2)) / (p_00 * p_00) + 1e-16;
+    ri = 1.0 - rth / ri;
+    return 0.5 * (ri + fabs(ri));
+}
+
+/* One pass along dir over cells [b, e-1) along dir and [b, e) across it
+ * (the kernels' coverage); U = pf_lap - filter(pf_lap), written to f.
+ * jcap (>= 0): last covered index + 1 along y, for the z pass that the
+ * reference launches as the y kernel on an (8, 8, 4+2) block (A-3). */
+static void filter_pass(oro_state *s, int dir, const int *r, double s0, double rth, int jcap) {
+    const double c1 = -0.2103830, c2 = 0.0396170;
+    size_t st[3] = { 1, (size_t)s->nx2, (size_t)s->nx2 * s->ny2 };
+    long sd = (long)st[dir];
+    int lo[3] = { r[0], r[2], r[4] }, hi[3] = { r[1], r[3], r[5] };
+    hi[dir] -= 1;
+    if (jcap >= 0 && hi[1] > jcap) hi[1] = jcap;
+#pragma omp parallel for collapse(2)
+    for (int k = lo[2]; k < hi[2]; k++)
+        for (int j = lo[1]; j < hi[1]; j++)
+            for (int i = lo[0]; i < hi[0]; i++) {
+                size_t q = L(s, i + LAP, j + LAP, k + LAP);
+                double hm = filter_sigma(s->psens, q - sd, sd, rth);
+                double h0 = filter_sigma(s->psens, q, sd, rth);
+                double hp = filter_sigma(s->psens, q + sd, sd, rth);
+                double Sc1 = 0.5 * (h0 + hp) * s0;
+                double Sc2 = 0.5 * (h0 + hm) * s0;
+                for (int m = 0; m < 5; m++) {
+                    const double *fl = s->flap + (size_t)m * s->nlap;
+                    s->f[(size_t)m * s->nin + I(s, i, j, k)] = fl[q] - (
+                        Sc1 * (c1 * (fl[q + sd] - fl[q]) + c2 * (fl[q + 2 * sd] - fl[q - sd]))
+                      - Sc2 * (c1 * (fl[q] - fl[q - sd]) + c2 * (fl[q + sd] - fl[q - 2 * sd])));
+                }
+            }
+}
+
+void oro_filtering(oro_state *s) {
+    if (!s->c.nfilter) return;
+    int any = 0;
+    for (int m = 0; m < s->c.nfilter; m++)
+        if (s->istep % s->fpar[m][0] == 0) any = 1;
+    if (!any) return;
+    /* exchange p and the five pf_lap fields in the directions any filter uses */
+    void (*ex[3])(oro_state *, double *) = { exchange_x, exchange_y, exchange_z };
+    for (int d = 0; d < 3; d++) {
+        if (!s->fjudge[d]) continue;
+        ex[d](s, s->psens);
+        for (int m = 0; m < 5; m++) ex[d](s, s->flap + (size_t)m * s->nlap);
+    }
+    for (int m = 0; m < s->c.nfilter; m++) {
+        if (!(s->tt <= s->c.filter_rpara[m][2])) continue;
+        if (s->istep % s->fpar[m][0] != 0) continue;
+        if (s->fpar[m][10] != 2) continue;          /* only the shock filter exists */
+        double s0 = s->c.filter_rpara[m][0], rth = s->c.filter_rpara[m][1];
+        const int *r = &s->fpar[m][4];
+        if (s->fpar[m][1] == 1) filter_pass(s, 0, r, s0, rth, -1);
+        if (s->fpar[m][2] == 1) filter_pass(s, 1, r, s0, rth, -1);
+        if (s->fpar[m][3] == 1) {
+            /* filter_z3d_shock launches the y kernel with blockdim (8, 8, 6)
+             * on the grid for (8, 8, 4): y rows advance by 6 per block, so
+             * only jb + 6*ceil((je-jb)/8) rows are reached */
+            int jb = r[2], je = r[3];
+            int gy = (je - jb + 7) / 8;
+            filter_pass(s, 1, r, s0, rth, jb + 6 * gy);
+        }
     }
 }
 
@@ -1479,6 +1590,7 @@ void oro_step(oro_state *s, int nsteps) {
         }
         s->istep++;
         s->tt += s->c.dt;
+        oro_filtering(s);
     }
 }
 

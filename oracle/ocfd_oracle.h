@@ -45,6 +45,9 @@ typedef struct oro_config {
     int hy_nochar_fixed;       /* CHARTERIC=0 hybrid, components 1-4: 0 = use the
                                   face flag (intent); 1/2/3 = force that flag
                                   (what an uninitialised register yields)       */
+    int nfilter;               /* number of FILTER_NPARA<n> entries (<= 8)      */
+    int filter_ipara[8][11];   /* ntime, fx, fy, fz, ib, ie, jb, je, kb, ke, scheme */
+    double filter_rpara[8][3]; /* s0, rth, time limit                           */
 } oro_config;
 
 typedef struct oro_state oro_state;
@@ -83,8 +86,11 @@ void oro_bc(oro_state *s);                       /* src/OCFD_boundary.cu:18  */
 void oro_get_amu(oro_state *s);                  /* src/commen_kernel.cu:133 */
 void oro_swap_time_levels(oro_state *s);         /* src/OCFD_NS_Solver.cu:63-73 */
 
-/* nsteps full RK3 steps (swap + 3 stages), src/OCFD_NS_Solver.cu:63-89. */
+/* nsteps full RK3 steps (swap + 3 stages, Istep++, filtering),
+ * src/OCFD_NS_Solver.cu:63-95. */
 void oro_step(oro_state *s, int nsteps);
+/* filtering() (src/OCFD_filtering.cu:75-183) at the current Istep / tt. */
+void oro_filtering(oro_state *s);
 
 /* Read-back helpers (interior only). */
 void oro_get_primitives(const oro_state *s, double *prim5);   /* d u v w T  */

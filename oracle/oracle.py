@@ -35,6 +35,9 @@ class OroConfig(ctypes.Structure):
         ("weno_tv_limiter", ctypes.c_double), ("weno_tv_max", ctypes.c_double),
         ("nthreads", ctypes.c_int),
         ("hy_nochar_fixed", ctypes.c_int),
+        ("nfilter", ctypes.c_int),
+        ("filter_ipara", (ctypes.c_int * 11) * 8),
+        ("filter_rpara", (ctypes.c_double * 3) * 8),
     ]
 
 
@@ -116,6 +119,13 @@ def make_config(cfg, nthreads: int = 0, hy_nochar_fixed: int = 3) -> OroConfig:
     c.weno_tv_limiter, c.weno_tv_max = 5.0, 0.2
     c.nthreads = nthreads
     c.hy_nochar_fixed = hy_nochar_fixed
+    filters = list(getattr(cfg, "filters", ()) or ())[:8]
+    c.nfilter = len(filters)
+    for n, (ip, rp) in enumerate(filters):
+        for t in range(11):
+            c.filter_ipara[n][t] = int(ip[t])
+        for t in range(3):
+            c.filter_rpara[n][t] = float(rp[t])
     return c
 
 

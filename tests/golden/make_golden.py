@@ -56,6 +56,36 @@ def golden_cases():
         out.append((f"rnd12x11x10_{sch.lower()}_char", c, 3))
     out.extend(bounded_cases())
     out.extend(mesh_cases())
+    out.extend(filter_cases())
+    return out
+
+
+def filter_cases():
+    """The shock-capturing filter after each step (FILTER_NPARA / FILTER_RPARA,
+    scheme 2) on the hybrid scheme, whose sensor provides the pressure it
+    reads: partial ranges, the z pass that filters along y (A-3), a closed
+    direction (ranges kept 6/5 cells from the faces), two filters with
+    different intervals and a time limit."""
+    out = []
+
+    def hyb(nx, ny, nz, seed, **kw):
+        c = cases.random_smooth_case(nx, ny, nz, seed=seed, scheme_invis="SCHEME_HYBRIDAUTO", charteric=1,
+                                     shock=True, **kw)
+        c.cfg.hy_dp_intv = (0.01, 0.2)
+        return c
+    # z pass without the y pass: the y ghosts are not exchanged then, so the
+    # y range keeps every read inside the box (rows 3..18 of 22); the z pass
+    # reaches rows 3..14 only
+    c = hyb(18, 22, 13, 71)
+    c.cfg.filters = (((1, 1, 0, 1, 0, 18, 3, 19, 0, 13, 2), (1.0, 1e-5, 10.0)),)
+    out.append(("fil18x22x13_hybrid_x_zquirk", c, 3))
+    c = hyb(19, 14, 13, 72, iperiodic=(0, 1, 1), dif_bound=(1, 1, 0, 0, 0, 0))
+    c.cfg.filters = (((1, 1, 1, 1, 0, 19, 0, 14, 0, 13, 2), (0.8, 1e-5, 10.0)),)
+    out.append(("fil19x14x13_hybrid_xyz_bounded", c, 3))
+    c = hyb(17, 18, 13, 73)
+    c.cfg.filters = (((2, 1, 0, 0, 0, 17, 0, 18, 0, 13, 2), (1.0, 1e-5, 10.0)),
+                     ((1, 0, 1, 0, 3, 12, 2, 16, 1, 12, 2), (0.7, 2e-5, 0.003)))
+    out.append(("fil17x18x13_hybrid_two_filters", c, 3))
     return out
 
 

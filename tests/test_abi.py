@@ -17,7 +17,7 @@ def _declared_symbols():
     names = set(re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", text))
     return {n for n in names if n.startswith("ocfd_b200_") or n in
             ("du_comput", "OCFD_time_advance", "get_duvwT", "get_Amu", "OCFD_bc",
-             "Set_Scheme_HybridAuto")}
+             "Set_Scheme_HybridAuto", "filtering")}
 
 
 def test_header_and_binding_agree():

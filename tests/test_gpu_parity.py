@@ -62,6 +62,12 @@ def small_cases():
                         non_ref=(1, 0, 0, 1, 0, 0))
     c.cfg.hy_dp_intv = (0.01, 0.2)
     out.append(("mesh_hybrid_char", c))
+    c = cases.random_smooth_case(17, 18, 13, seed=65, scheme_invis="SCHEME_HYBRIDAUTO", charteric=1, shock=True,
+                                 iperiodic=(1, 0, 1), dif_bound=(0, 0, 1, 1, 0, 0))
+    c.cfg.hy_dp_intv = (0.01, 0.2)
+    c.cfg.filters = (((1, 1, 1, 1, 2, 15, 0, 18, 0, 13, 2), (0.9, 1e-5, 10.0)),
+                     ((2, 0, 0, 1, 0, 17, 0, 18, 3, 11, 2), (0.5, 2e-5, 10.0)))
+    out.append(("filter_hybrid_char", c))
     return out
 
 
