@@ -136,6 +136,17 @@ int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps);
 int ocfd_b200_advance_host(ocfd_b200_ctx *ctx, const double *prim5_in, double *prim5_out,
                            int nsteps);
 
+/* Boundary-condition family IBC with BC_NPARA / BC_RPARA (bc_parameter,
+ * src/OCFD_boundary_init.c:50-93).  0: none; 108: compression corner
+ * (src/OCFD_boundary_compression_conner.cu:122-180) with npara = MZMAX, MTMAX,
+ * INLET_BOUNDARY, IFLAG_WALL_NOT_NORMAL and rpara = TW, EPSL, X_DIST_BEGIN,
+ * X_DIST_END, BETA, X_WALL_BEGIN, X_UP_BOUNDARY_BEGIN, SLZ; inlet4 is the
+ * flow1d-inlet.dat profile [4][ny] (d,u,v,T), needed when INLET_BOUNDARY = 1.
+ * Call after the metrics (the wall and top coordinates are read from them)
+ * and before set_primitives; MZMAX > 0 (random phases) is not built. */
+int ocfd_b200_set_bc(ocfd_b200_ctx *ctx, int ibc, const int *npara, int nnpara, const double *rpara,
+                     int nrpara, const double *inlet4);
+
 /* Shock-capturing filter n (0..7): FILTER_NPARA<n+1> = ntime, filter_x,
  * filter_y, filter_z, ib, ie, jb, je, kb, ke, scheme (2) and FILTER_RPARA<n+1>
  * = s0, rth, time limit (src/parameters.c:305-325); ranges clamped as

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 namespace ocfd {
 cudaError_t launch_sensor(const Params &p, cudaStream_t st);
@@ -37,6 +38,7 @@ cudaError_t launch_sweeps3(const Params &p, cudaStream_t st);
 cudaError_t launch_mesh_metrics(const Params &p, const int jac_bound[3], double *scratch, cudaStream_t st);
 cudaError_t launch_negative_jacobian(const Params &p, unsigned *flag, cudaStream_t st);
 cudaError_t launch_filter_pass(const Params &p, int dir, const int box[6], double s0, double rth, cudaStream_t st);
+cudaError_t launch_bc108(const Params &p, double ht, cudaStream_t st);
 int sweeps3_kernels(const Params &p);
 cudaError_t compute_dirconst(Params &p, DirConst *dev_scratch, cudaStream_t st);
 }  // namespace ocfd
@@ -74,6 +76,11 @@ struct ocfd_b200_ctx {
     int fpar[8][11] = {};
     double frpar[8][3] = {};
     int fjudge[3] = {0, 0, 0};
+    // IBC 108: device profile/shape arrays and the wall-blowing time law
+    double *bc_buf = nullptr;
+    double bc_beta = 0.0;
+    int bc_mtmax = 0;
+    double bc_TM[64] = {};
     double *pinned = nullptr;     // host staging for advance_host
     size_t pinned_bytes = 0;
     bool have_metrics = false;
@@ -128,7 +135,7 @@ extern "C" const char *ocfd_b200_last_error(const ocfd_b200_ctx *ctx) {
 static void free_all(ocfd_b200_ctx *c) {
     cudaFree(c->prim_buf); cudaFree(c->met_buf); cudaFree(c->cons_buf);
     cudaFree(c->ev_buf); cudaFree(c->flag_buf); cudaFree(c->stage_buf);
-    cudaFree(c->red_buf); cudaFree(c->defer_buf); cudaFree(c->filter_buf);
+    cudaFree(c->red_buf); cudaFree(c->defer_buf); cudaFree(c->filter_buf); cudaFree(c->bc_buf);
     if (c->pinned) cudaFreeHost(c->pinned);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -328,6 +335,22 @@ struct TimerScope {
 // One stage's RHS.  fused_rk = 0: du_comput semantics (du complete on
 // return).  fused_rk = KRK: the viscous divergence kernel also applies the
 // RK stage, cons->prim and the face re-projection (step() path).
+// the boundary-condition family's values on the primitives
+// (bc_user_Compression_conner, src/OCFD_boundary_compression_conner.cu:122-180)
+static int apply_bc(ocfd_b200_ctx *ctx) {
+    if (ctx->p.ibc != 108) return OCFD_OK;
+    double ht = 0.;
+    if (ctx->bc_beta > 0.) {
+        for (int m = 0; m < ctx->bc_mtmax && m < 64; m++)
+            ht = ht + ctx->bc_TM[m] * sin((m + 1) * ctx->bc_beta * ctx->tt);
+    } else {
+        ht = 1.;
+    }
+    CK(ocfd::launch_bc108(ctx->p, ht, ctx->stream), "boundary conditions");
+    ctx->launches += 3;
+    return OCFD_OK;
+}
+
 static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
     const Params &p = ctx->p;
     if (p.scheme_invis == 310 && krk == 1) {
@@ -353,6 +376,12 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
         TimerScope ts(ctx, T_VIS);
         CK(ocfd::launch_viscous(p, fused_rk, ctx->stream), "viscous");
         ctx->launches += 3;
+    }
+    if (fused_rk && p.ibc) {        // OCFD_bc: boundary values, then the faces
+        int rc = apply_bc(ctx);
+        if (rc) return rc;
+        CK(ocfd::launch_bc_faces(p, ctx->stream), "face re-projection");
+        ctx->launches += 1;
     }
     return OCFD_OK;
 }
@@ -530,10 +559,17 @@ static int set_prims_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKind 
     if (rc) return rc;
     CK(ocfd::launch_p2c(p, p.f, ctx->stream), "pri_to_cons");
     ctx->launches += 1;
-    // NS_solver_real pre-loop: exchange, OCFD_bc (re-projects the faces of f
-    // from the same primitives: no change), get_Amu (formed on the fly)
+    // NS_solver_real pre-loop: exchange, OCFD_bc (the boundary family's
+    // values, then the faces of f re-projected: without a family no change),
+    // get_Amu (formed on the fly)
     rc = ghost_prims(ctx);
     if (rc) return rc;
+    ctx->tt = tt;
+    if (p.ibc) {
+        if ((rc = apply_bc(ctx))) return rc;
+        CK(ocfd::launch_bc_faces(p, ctx->stream), "face re-projection");
+        ctx->launches += 1;
+    }
     CK(cudaStreamSynchronize(ctx->stream), "set_primitives");
     ctx->istep = istep;
     ctx->tt = tt;
@@ -623,6 +659,83 @@ extern "C" int ocfd_b200_set_time(ocfd_b200_ctx *ctx, int istep, double tt) {
     return OCFD_OK;
 }
 
+// IBC and BC_NPARA / BC_RPARA (bc_parameter, src/OCFD_boundary_init.c:50-93)
+// with the set-up of bc_user_Compression_conner_init (:376-438)
+extern "C" int ocfd_b200_set_bc(ocfd_b200_ctx *ctx, int ibc, const int *npara, int nnpara, const double *rpara,
+                                int nrpara, const double *inlet4) {
+    if (!ctx) return OCFD_ERR_ARG;
+    Params &p = ctx->p;
+    if (ibc == 0) { p.ibc = 0; return OCFD_OK; }
+    if (ibc != 108)
+        return fail(ctx, OCFD_ERR_UNSUPPORTED, "IBC " + std::to_string(ibc) + " is not built (0 or 108)");
+    if (!npara || !rpara || nnpara < 4 || nrpara < 8)
+        return fail(ctx, OCFD_ERR_ARG, "IBC 108 needs 4 BC_NPARA and 8 BC_RPARA values");
+    if (!ctx->have_metrics) return fail(ctx, OCFD_ERR_STATE, "set the metrics or mesh before the boundary conditions");
+    const int MZ = npara[0], MT = npara[1], inlet_file = npara[2], not_normal = npara[3];
+    if (MZ > 0)
+        return fail(ctx, OCFD_ERR_UNSUPPORTED, "MZMAX > 0 draws random spanwise phases (rand()); use MZMAX <= 0");
+    if (MT > 64) return fail(ctx, OCFD_ERR_ARG, "MTMAX must be <= 64");
+    if (inlet_file == 1 && !inlet4) return fail(ctx, OCFD_ERR_ARG, "INLET_BOUNDARY = 1 needs the inflow profile");
+    const double TW = rpara[0], EPSL = rpara[1], DB = rpara[2], DE = rpara[3], BETA = rpara[4];
+    const double XUP = rpara[6], SL = rpara[7];
+    const double PI = 3.14159265358979323846;
+    // wall and top coordinates from the x and z metric records
+    const size_t inB = sizeof(double) * (size_t)p.N;
+    std::string err;
+    double *hx = (double *)malloc(inB), *hz = (double *)malloc(inB);
+    if (!hx || !hz) { free(hx); free(hz); return fail(ctx, OCFD_ERR_NOMEM, "host buffers for the boundary set-up"); }
+    cudaError_t e = ocfd::launch_gather(p, p.met[0], ctx->stage_buf, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hx, ctx->stage_buf, inB, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = ocfd::launch_gather(p, p.met[2], ctx->stage_buf, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hz, ctx->stage_buf, inB, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) { free(hx); free(hz); return cuda_fail(ctx, e, "boundary set-up read-back"); }
+    const int nx = p.nx, ny = p.ny, nz = p.nz;
+    std::vector<double> host((size_t)4 * ny + nx + nz);
+    double *ub1 = host.data(), *fx = ub1 + 4 * ny, *gz = fx + nx;
+    for (int j = 0; j < ny; j++) {
+        if (inlet_file == 1) for (int c = 0; c < 4; c++) ub1[c * ny + j] = inlet4[c * ny + j];
+        else { ub1[j] = 1.; ub1[ny + j] = 1.; ub1[2 * ny + j] = 0.; ub1[3 * ny + j] = 1.; }
+    }
+    int x_begin = 0;
+    for (int i = 0; i < nx; i++) {
+        if (hx[i + (size_t)nx * (ny - 1)] <= XUP) x_begin = i;         // top row, first z plane
+        const double xa = hx[i];                                        // wall row, first z plane
+        if (xa >= DB && xa <= DE) {
+            const double seta = 10. * PI * (xa - DB) / (DB - DE);
+            fx[i] = 4. / sqrt(27.) * sin(seta) * (1. - cos(seta));
+        } else {
+            fx[i] = 0.;
+        }
+    }
+    for (int k = 0; k < nz; k++) {
+        const double za = hz[(size_t)nx * ny * k];                      // x = 0, y = 0
+        gz[k] = MZ == 0 ? 1. : sin(-2. * PI * MZ * (za / SL));
+    }
+    free(hx); free(hz);
+    double Ttmp = 0.;
+    for (int k = 0; k < MT; k++) {
+        ctx->bc_TM[0] = 1.;
+        if (k > 0) ctx->bc_TM[k] = ctx->bc_TM[k - 1] / 1.25;
+        Ttmp = Ttmp + ctx->bc_TM[k];
+    }
+    for (int k = 0; k < MT; k++) ctx->bc_TM[k] = ctx->bc_TM[k] / Ttmp;
+    if (!ctx->bc_buf) {
+        e = cudaMalloc(&ctx->bc_buf, sizeof(double) * host.size());
+        if (e != cudaSuccess) { cudaGetLastError(); return fail(ctx, OCFD_ERR_NOMEM, "boundary arrays"); }
+    }
+    CK(cudaMemcpyAsync(ctx->bc_buf, host.data(), sizeof(double) * host.size(), cudaMemcpyHostToDevice, ctx->stream),
+       "boundary arrays");
+    CK(cudaStreamSynchronize(ctx->stream), "set_bc");
+    p.bc_ub1 = ctx->bc_buf; p.bc_fx = ctx->bc_buf + 4 * ny; p.bc_gz = p.bc_fx + nx;
+    p.bc_xbegin = x_begin;
+    p.bc_wall_mode = not_normal != 0 ? 0 : (TW > 0 ? 1 : 2);
+    p.bc_tw = TW; p.bc_epsl = EPSL;
+    ctx->bc_beta = BETA; ctx->bc_mtmax = MT;
+    p.ibc = 108;
+    return OCFD_OK;
+}
+
 // FILTER_NPARA<n+1> / FILTER_RPARA<n+1>, clamped as set_para_filtering does
 // on one rank (src/OCFD_filtering.cu:20-73)
 extern "C" int ocfd_b200_set_filter(ocfd_b200_ctx *ctx, int n, const int npara[11], const double rpara[3]) {
@@ -681,6 +794,7 @@ extern "C" int ocfd_b200_get_duvwT(ocfd_b200_ctx *ctx) {
 extern "C" int ocfd_b200_bc(ocfd_b200_ctx *ctx) {
     int rc = check_ready(ctx);
     if (rc) return rc;
+    if ((rc = apply_bc(ctx))) return rc;
     CK(ocfd::launch_bc_faces(ctx->p, ctx->stream), "face re-projection");
     ctx->launches += 1;
     return OCFD_OK;

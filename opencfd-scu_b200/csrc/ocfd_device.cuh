@@ -62,6 +62,14 @@ struct Params {
     // cons_to_pri leaves after the last stage (1 LAP-box field)
     double *flap;
     double *pfil;
+    // boundary-condition family (IBC; 0 none, 108 compression corner): the
+    // inflow profile [4][ny] (d,u,v,T), wall blowing shapes fx [nx], gz [nz],
+    // first x of the upper inflow row, wall treatment (0 none, 1 TW > 0,
+    // 2 TW <= 0), wall temperature and blowing amplitude
+    int ibc;
+    const double *bc_ub1, *bc_fx, *bc_gz;
+    int bc_xbegin, bc_wall_mode;
+    double bc_tw, bc_epsl;
 };
 
 enum { M_AXX = 0, M_AYY, M_AZZ, M_AKX, M_AKY, M_AKZ, M_AIX, M_AIY, M_AIZ,

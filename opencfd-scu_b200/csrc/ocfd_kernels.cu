@@ -493,8 +493,10 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
     // cons_to_pri_kernel also leaves the pressure (src/commen_kernel.cu:107),
     // which the filter after the step reads
     if (krk == 3 && p.pfil) p.pfil[o] = T2 * d1 / (p.Gamma * p.Ama * p.Ama);
+    // with a boundary-condition family the faces are re-projected after it
+    // sets the boundary values (k_bc_faces)
     bool face = (i == 0) || (i == p.nx - 1) || (j == 0) || (j == p.ny - 1) || (k == 0) || (k == p.nz - 1);
-    if (face) {
+    if (face && !p.ibc) {
         f[0] = d1;
         f[1] = u1 * d1;
         f[2] = v1 * d1;

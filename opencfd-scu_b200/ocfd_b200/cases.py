@@ -16,7 +16,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
-from typing import List, Tuple
+from typing import Optional, List, Tuple
 
 import numpy as np
 
@@ -27,8 +27,9 @@ from .formats import CaseConfig
 class Case:
     cfg: CaseConfig
     prims: List[np.ndarray]       # d,u,v,w,T each (nz,ny,nx)
-    metrics: List[np.ndarray]     # 13 fields each (nz,ny,nx)
+    metrics: List[np.ndarray]     # 13 metric fields, or 3 mesh coordinate fields, each (nz,ny,nx)
     description: str = ""
+    inlet: Optional[np.ndarray] = None   # IBC 108 inflow profile [4][ny] (d,u,v,T), flow1d-inlet.dat
 
     @property
     def shape(self) -> Tuple[int, int, int]:
@@ -228,3 +229,75 @@ def mesh_case(nx: int, ny: int, nz: int, seed: int = 7, scheme_invis: str = "WEN
     cfg.jac_bound = tuple(jac_bound)
     return Case(cfg, base.prims, [x, y, z],
                 f"mesh {nx}x{ny}x{nz} seed={seed} skew={skew} scheme={scheme_invis}")
+
+
+
+def ramp_case(nx: int = 512, ny: int = 128, nz: int = 64, angle_deg: float = 24.0, ama: float = 2.9,
+              re: float = 5000.0, tw: float = 2.5, seed: int = 2024, fluct: float = 0.02,
+              scheme_invis: str = "SCHEME_HYBRIDAUTO", charteric: int = 1, cfl: float = 0.3,
+              filters=(((1, 1, 1, 0, 0, 100000, 0, 100000, 0, 100000, 2), (1.0, 1e-5, 1e9)),),
+              epsl: float = 0.0, beta: float = 0.0, mtmax: int = 0) -> Case:
+    """24-degree compression ramp (the compression-corner family, IBC 108).
+
+    Mesh (OCFD3d-Mesh.dat, metrics computed by the solver): x in [0, Lx]
+    with the corner at 0.5 Lx, the wall following the ramp, wall-normal
+    tanh stretching with a first cell of 0.01 delta up to Ly, periodic span
+    Lz.  Inflow: a 1/7-power boundary layer of thickness delta = 1 at an
+    isothermal wall (T_w = tw, linear T(u), uniform pressure), written as the
+    flow1d-inlet.dat profile; the initial field is that profile everywhere
+    plus seeded relative fluctuations of size ``fluct``.  x and y are closed
+    (DIF_BOUND = 1, JAC_BOUND = 1), z periodic; hybrid scheme with the shock
+    filter every step; dt from the CFL number at t = 0."""
+    rng = np.random.default_rng(seed)
+    Lx, Ly, Lz = 40.0, 15.0, 8.0
+    xc = 0.5 * Lx
+    t = math.tan(math.radians(angle_deg))
+    xs = np.linspace(0.0, Lx, nx)
+    yw = np.where(xs > xc, (xs - xc) * t, 0.0)
+    eta = np.linspace(0.0, 1.0, ny)
+    # tanh stretching: y(eta) = H (1 - tanh(b (1-eta)) / tanh(b)), first cell 0.01
+    b = 1.0
+    for _ in range(60):
+        h1 = Ly * (1.0 - math.tanh(b * (1.0 - eta[1])) / math.tanh(b))
+        b *= (h1 / 0.01) ** 0.25
+    st = 1.0 - np.tanh(b * (1.0 - eta)) / math.tanh(b)
+    zs = np.arange(nz) * (Lz / nz)
+    Z, Y, X = np.meshgrid(zs, st, xs, indexing="ij")
+    ywall = np.broadcast_to(yw[None, None, :], X.shape)
+    x = X.copy()
+    y = ywall + (Ly - ywall) * Y
+    z = Z.copy()
+    # inflow profile from the wall distance at x = 0
+    dist = y[0, :, 0]
+    # profile wall temperature: tw, or the recovery temperature for an
+    # adiabatic wall (tw <= 0 selects the adiabatic boundary condition)
+    tpw = tw if tw > 0 else 1.0 + 0.89 * 0.2 * ama * ama
+    u_in = np.clip(dist / 1.0, 0.0, 1.0) ** (1.0 / 7.0)
+    T_in = tpw - (tpw - 1.0) * u_in
+    d_in = 1.0 / T_in
+    inlet = np.stack([d_in, u_in, np.zeros(ny), T_in])
+    # initial field: the profile by wall distance, plus fluctuations
+    dwall = y - ywall
+    uu = np.clip(dwall, 0.0, 1.0) ** (1.0 / 7.0)
+    TT = tpw - (tpw - 1.0) * uu
+    dd = 1.0 / TT
+    noise = lambda: fluct * rng.standard_normal(X.shape)
+    d = dd * (1.0 + noise())
+    u = uu * (1.0 + noise())
+    v = 0.01 * noise()
+    w = 0.01 * noise()
+    T = TT * (1.0 + noise())
+    c0 = math.sqrt(tpw) / ama
+    dx = Lx / (nx - 1)
+    dt = cfl * min(dx, 0.01) / (1.0 + c0)
+    cfg = CaseConfig(nx=nx, ny=ny, nz=nz, iperiodic=(0, 0, 1), jac_bound=(1, 1, 1),
+                     dif_bound=(1, 1, 1, 1, 0, 0), non_ref=(0, 0, 0, 0, 0, 0),
+                     scheme_invis=scheme_invis, scheme_vis="CD6", charteric=charteric,
+                     hy_dp_intv=(0.01, 0.2), re=re, ama=ama, gamma=1.4, pr=0.72, epsl_sw=0.0, dt=dt,
+                     ibc=108, bc_npara=(0, mtmax, 1, 0),
+                     bc_rpara=(tw, epsl, 0.25 * Lx, 0.4 * Lx, beta, 0.0, 0.8 * Lx, Lz))
+    # the filter ranges are clamped to the box by the solver
+    cfg.filters = tuple(((ip[0], ip[1], ip[2], ip[3], 0, nx, 0, ny, 0, nz, ip[10]), rp) for ip, rp in filters)
+    return Case(cfg, [d, u, v, w, T], [x, y, z],
+                f"compression ramp {nx}x{ny}x{nz} angle={angle_deg} Ma={ama} Re={re} Tw={tw} seed={seed}",
+                inlet=inlet)

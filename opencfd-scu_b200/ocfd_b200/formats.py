@@ -74,6 +74,11 @@ class CaseConfig:
     # ((ntime, filter_x, filter_y, filter_z, ib, ie, jb, je, kb, ke, scheme),
     #  (s0, rth, time limit)); scheme 2 is the shock-capturing filter
     filters: Tuple = ()
+    # BC_NPARA / BC_RPARA of the boundary family IBC (src/parameters.c:290-298);
+    # IBC 108: (MZMAX, MTMAX, INLET_BOUNDARY, IFLAG_WALL_NOT_NORMAL) and
+    # (TW, EPSL, X_DIST_BEGIN, X_DIST_END, BETA, X_WALL_BEGIN, X_UP_BOUNDARY_BEGIN, SLZ)
+    bc_npara: Tuple = ()
+    bc_rpara: Tuple = ()
 
     @property
     def scheme_invis_id(self) -> int:
@@ -139,8 +144,8 @@ def write_config(path: str, cfg: CaseConfig) -> None:
         f"KSTEP_SAVE = {cfg.kstep_save}",
         f"INIT_STAT = {cfg.init_stat}",
         f"IBC = {cfg.ibc}",
-        "BC_NPARA = 0",
-        "BC_RPARA = 0",
+        f"BC_NPARA = {_fmt(tuple(int(v) for v in cfg.bc_npara)) if cfg.bc_npara else 0}",
+        f"BC_RPARA = {_fmt(tuple(float(v) for v in cfg.bc_rpara)) if cfg.bc_rpara else 0}",
     ]
     for n, (ip, rp) in enumerate(cfg.filters, start=1):
         lines.append(f"FILTER_NPARA{n} = {_fmt(tuple(int(v) for v in ip))}")
@@ -212,6 +217,9 @@ def read_config(path: str) -> CaseConfig:
     cfg.init_stat = int(kv.get("INIT_STAT", "1").split()[0])
     cfg.ibc = int(kv.get("IBC", "0").split()[0])
     cfg.stream = int(kv.get("STREAM", "0").split()[0])
+    if "BC_NPARA" in kv and cfg.ibc:
+        cfg.bc_npara = tuple(int(x) for x in kv["BC_NPARA"].split())
+        cfg.bc_rpara = tuple(float(x) for x in kv.get("BC_RPARA", "").split())
     filters = []
     for key in sorted((k for k in kv if k.startswith("FILTER_NPARA")), key=lambda k: int(k[12:] or 0)):
         rkey = "FILTER_RPARA" + key[12:]
@@ -299,3 +307,27 @@ def read_metric_file(path: str, shape: Tuple[int, int, int], count: int = 13) ->
         data = fh.read()
     fields, _ = _read_blocks(memoryview(data), 0, shape, count, path)
     return fields
+
+
+# --------------------------------------------------------------------------
+# flow1d-inlet.dat (IBC 108 inlet profile, src/OCFD_boundary_init.c:386-394)
+# --------------------------------------------------------------------------
+
+def write_inlet_file(path: str, profile: np.ndarray, y: Optional[np.ndarray] = None) -> None:
+    """One header line, then NY rows ``y d u v T``; profile is [4][ny] (d,u,v,T)."""
+    profile = np.asarray(profile, dtype=np.float64)
+    ny = profile.shape[1]
+    yy = np.arange(ny, dtype=np.float64) if y is None else np.asarray(y, dtype=np.float64)
+    with open(path, "w") as fh:
+        fh.write("variables = y d u v T\n")
+        for j in range(ny):
+            fh.write("%.17e %.17e %.17e %.17e %.17e\n" % (yy[j], profile[0, j], profile[1, j],
+                                                         profile[2, j], profile[3, j]))
+
+
+def read_inlet_file(path: str, ny: int) -> np.ndarray:
+    with open(path) as fh:
+        fh.readline()
+        rows = [[float(x) for x in fh.readline().split()[:5]] for _ in range(ny)]
+    a = np.array(rows, dtype=np.float64)
+    return np.ascontiguousarray(a[:, 1:5].T)

@@ -30,7 +30,7 @@ EXPORTED = (
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
     "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics", "ocfd_b200_set_sweep_impl",
     "ocfd_b200_set_mesh", "ocfd_b200_set_mesh_device", "ocfd_b200_get_metrics",
-    "ocfd_b200_set_filter", "ocfd_b200_filtering", "ocfd_b200_set_time", "filtering",
+    "ocfd_b200_set_filter", "ocfd_b200_filtering", "ocfd_b200_set_time", "filtering", "ocfd_b200_set_bc",
     "ocfd_b200_set_primitives", "ocfd_b200_set_primitives_device", "ocfd_b200_step",
     "ocfd_b200_advance_host", "ocfd_b200_swap_time_levels", "ocfd_b200_du_comput",
     "ocfd_b200_time_advance", "ocfd_b200_get_duvwT", "ocfd_b200_bc",
@@ -108,6 +108,8 @@ def load(path: Optional[str] = None):
         "ocfd_b200_set_filter": (ctypes.c_int, [P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), D]),
         "ocfd_b200_filtering": (ctypes.c_int, [P]),
         "ocfd_b200_set_time": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double]),
+        "ocfd_b200_set_bc": (ctypes.c_int, [P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int, D,
+                                            ctypes.c_int, D]),
         "filtering": (None, [D, D, D]),
         "ocfd_b200_set_metric_mode": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_uniform_metrics": (ctypes.c_int, [P]),
@@ -178,7 +180,7 @@ class Solver:
 
     def __init__(self, cfg: CaseConfig, prims: Optional[Sequence[np.ndarray]] = None,
                  metrics: Optional[Sequence[np.ndarray]] = None, device: int = 0,
-                 istep: int = 0, tt: float = 0.0, metric_mode: int = 0):
+                 istep: int = 0, tt: float = 0.0, metric_mode: int = 0, inlet=None):
         self.L = load()
         self.cfg = cfg
         self.shape = (cfg.nz, cfg.ny, cfg.nx)
@@ -194,6 +196,8 @@ class Solver:
             self.set_filter(n, ip, rp)
         if metrics is not None:
             self.set_metrics(metrics)
+            if getattr(cfg, "ibc", 0):
+                self.set_bc(cfg.ibc, cfg.bc_npara, cfg.bc_rpara, inlet)
         if prims is not None:
             self.set_primitives(prims, istep, tt)
 
@@ -223,6 +227,15 @@ class Solver:
         if a.shape != (13,) + self.shape:
             raise ValueError(f"metrics shape {a.shape} != {(13,) + self.shape} (or 3 mesh fields)")
         self._check(self.L.ocfd_b200_set_metrics(self.h, _dp(a)), "set_metrics")
+
+    def set_bc(self, ibc: int, npara, rpara, inlet=None):
+        ia = (ctypes.c_int * max(1, len(npara)))(*[int(v) for v in npara])
+        da = (ctypes.c_double * max(1, len(rpara)))(*[float(v) for v in rpara])
+        ip = None
+        if inlet is not None:
+            self._inlet = np.ascontiguousarray(np.asarray(inlet, np.float64))
+            ip = _dp(self._inlet)
+        self._check(self.L.ocfd_b200_set_bc(self.h, int(ibc), ia, len(npara), da, len(rpara), ip), "set_bc")
 
     def set_filter(self, n: int, npara, rpara):
         ia = (ctypes.c_int * 11)(*[int(v) for v in npara])

@@ -57,6 +57,11 @@ struct oro_state {
     double *flap;               /* [5][LAP box] */
     int fpar[8][11];
     int fjudge[3];
+    /* IBC 108 (bc_user_Compression_conner_init, src/OCFD_boundary_init.c:376-438) */
+    int bc_ready, x_begin;
+    double *ub1;                /* [4][ny] d u v T */
+    double *bfx, *bgz;          /* [nx], [nz] blowing shapes */
+    double TM[64];
 };
 
 enum { AXX = 0, AYY, AZZ, AKX, AKY, AKZ, AIX, AIY, AIZ, ASX, ASY, ASZ, AJAC };
@@ -141,13 +146,118 @@ oro_state *oro_create(const oro_config *cfg) {
         }
     }
     if (s->c.nfilter > 0) s->flap = xcalloc(5 * s->nlap);
+    s->bc_ready = 0;
+    s->ub1 = xcalloc(4 * (size_t)s->ny);
+    for (int j = 0; j < s->ny; j++) { s->ub1[j] = 1.0; s->ub1[s->ny + j] = 1.0; s->ub1[2 * s->ny + j] = 0.0; s->ub1[3 * s->ny + j] = 1.0; }
+    s->bfx = xcalloc(s->nx); s->bgz = xcalloc(s->nz);
     return s;
+}
+
+void oro_set_inlet(oro_state *s, const double *ub1) {
+    memcpy(s->ub1, ub1, 4 * (size_t)s->ny * sizeof(double));
+}
+
+/* x_begin, the blowing shapes fx (x) and gz (z) and the frequency weights TM,
+ * from the wall and top coordinates (get_xs_blow_suction_multiwave,
+ * get_fait_multifrequancy, src/OCFD_boundary_init.c:376-521).  MZMAX > 0
+ * draws random phases with rand() and is not restated. */
+static void bc108_init(oro_state *s) {
+    const double PI = 3.14159265358979323846;
+    const double *Axx = s->A[AXX], *Azz = s->A[AZZ];
+    double DB = s->c.bc_rpara[2], DE = s->c.bc_rpara[3], SL = s->c.bc_rpara[7], XUP = s->c.bc_rpara[6];
+    int MZ = s->c.bc_npara[0], MT = s->c.bc_npara[1];
+    s->x_begin = 0;
+    for (int i = 0; i < s->nx; i++)
+        if (Axx[L(s, i + LAP, s->ny + LAP - 1, LAP)] <= XUP) s->x_begin = i;
+    for (int i = 0; i < s->nx; i++) {
+        double xa = Axx[L(s, i + LAP, LAP, LAP)];
+        if (xa >= DB && xa <= DE) {
+            double seta = 10. * PI * (xa - DB)/(DB - DE);
+            s->bfx[i] = 4. / sqrt(27.) * sin(seta) * (1. - cos(seta));
+        } else {
+            s->bfx[i] = 0.;
+        }
+    }
+    for (int k = 0; k < s->nz; k++) {
+        double za = Azz[L(s, LAP, LAP, k + LAP)];
+        double seta = za / SL;
+        if (MZ == 0) s->bgz[k] = 1.;
+        else s->bgz[k] = sin(-2. * PI * MZ * seta);      /* MZ < 0 */
+    }
+    double Ttmp = 0.;
+    for (int k = 0; k < MT && k < 64; k++) {
+        s->TM[0] = 1.;
+        if (k > 0) s->TM[k] = s->TM[k - 1] / 1.25;
+        Ttmp = Ttmp + s->TM[k];
+    }
+    for (int k = 0; k < MT && k < 64; k++) s->TM[k] = s->TM[k] / Ttmp;
+    s->bc_ready = 1;
+}
+
+/* bc_user_Compression_conner (src/OCFD_boundary_compression_conner.cu:122-180) */
+static void bc108(oro_state *s) {
+    if (!s->bc_ready) bc108_init(s);
+    int nx = s->nx, ny = s->ny, nz = s->nz;
+    const double *ub1 = s->ub1;
+    /* inlet, i = 1: the ghost columns and the first column take the profile */
+    for (int k = 0; k < nz; k++)
+        for (int j = 0; j < ny; j++)
+            for (int i = 0; i <= LAP; i++) {
+                size_t q = L(s, i, j + LAP, k + LAP);
+                s->d[q] = ub1[j]; s->u[q] = ub1[ny + j]; s->v[q] = ub1[2 * ny + j];
+                s->w[q] = 0.; s->T[q] = ub1[3 * ny + j];
+            }
+    /* upper boundary from x_begin on */
+    for (int k = 0; k < nz; k++)
+        for (int i = s->x_begin; i < nx; i++) {
+            size_t q = L(s, i + LAP, ny + LAP - 1, k + LAP);
+            s->d[q] = ub1[ny - 1]; s->u[q] = ub1[ny + ny - 1]; s->v[q] = ub1[2 * ny + ny - 1];
+            s->w[q] = 0.; s->T[q] = ub1[3 * ny + ny - 1];
+        }
+    double BETA = s->c.bc_rpara[4], EPSL = s->c.bc_rpara[1], TW = s->c.bc_rpara[0];
+    double ht = 0.;
+    if (BETA > 0.) {
+        for (int m = 0; m < s->c.bc_npara[1] && m < 64; m++) ht = ht + s->TM[m] * sin((m + 1)*BETA*s->tt);
+    } else {
+        ht = 1.;
+    }
+    /* wall, j = 1: no slip with blowing, then the wall temperature */
+    for (int k = 0; k < nz; k++)
+        for (int i = 0; i < nx; i++) {
+            size_t q = L(s, i + LAP, LAP, k + LAP);
+            s->u[q] = 0.;
+            s->v[q] = EPSL * s->bfx[i] * s->bgz[k] * ht;
+            s->w[q] = 0.;
+        }
+    if (s->c.bc_npara[3] != 0) return;           /* "non-normal wall is not supported" */
+    size_t sy = (size_t)s->nx2;
+    for (int k = 0; k < nz; k++)
+        for (int i = 0; i < nx; i++) {
+            size_t q = L(s, i + LAP, LAP, k + LAP);
+            double pw;
+            if (TW > 0) {
+                pw = (18. * s->d[q + sy] * s->T[q + sy] - 9. * s->d[q + 2 * sy] * s->T[q + 2 * sy]
+                      + 2. * s->d[q + 3 * sy] * s->T[q + 3 * sy]) / 11.;
+                s->T[q] = TW;
+                s->d[q] = pw / s->T[q];
+                for (int g = 0; g < LAP; g++) {
+                    size_t qg = L(s, i + LAP, g, k + LAP), qm = L(s, i + LAP, 2 * LAP - g, k + LAP);
+                    s->d[qg] = s->d[qm]; s->u[qg] = -s->u[qm]; s->v[qg] = -s->v[qm];
+                    s->w[qg] = -s->w[qm]; s->T[qg] = s->T[qm];
+                }
+            } else {
+                s->T[q] = (18. * s->T[q + sy] - 9. * s->T[q + 2 * sy] + 2. * s->T[q + 3 * sy]) / 11.;
+                pw = (18. * s->d[q + sy] * s->T[q + sy] - 9. * s->d[q + 2 * sy] * s->T[q + 2 * sy]
+                      + 2. * s->d[q + 3 * sy] * s->T[q + 3 * sy]) / 11.;
+                s->d[q] = pw / s->T[q];
+            }
+        }
 }
 
 void oro_destroy(oro_state *s) {
     if (!s) return;
     free(s->d); free(s->u); free(s->v); free(s->w); free(s->T); free(s->P); free(s->cc);
-    free(s->flap);
+    free(s->flap); free(s->ub1); free(s->bfx); free(s->bgz);
     for (int m = 0; m < 13; m++) free(s->A[m]);
     for (int dir = 0; dir < 3; dir++) { free(s->fp[dir]); free(s->fm[dir]); }
     for (int m = 0; m < 4; m++) { free(s->ev[m]); free(s->vis[m]); }
@@ -418,8 +528,10 @@ void oro_get_duvwT(oro_state *s) {
             }
 }
 
-/* OCFD_bc face re-projection, src/OCFD_boundary.cu:40-91 (IBC unset). */
+/* OCFD_bc (src/OCFD_boundary.cu:18-92): the IBC 108 boundary values, then
+ * the face re-projection of all six faces. */
 void oro_bc(oro_state *s) {
+    if (s->c.ibc == 108) bc108(s);
     int nx = s->nx, ny = s->ny, nz = s->nz;
     for (int k = 0; k < nz; k++) for (int j = 0; j < ny; j++) { p2c_cell(s, 0, j, k); p2c_cell(s, nx - 1, j, k); }
     for (int k = 0; k < nz; k++) for (int i = 0; i < nx; i++) { p2c_cell(s, i, 0, k); p2c_cell(s, i, ny - 1, k); }

@@ -45,6 +45,10 @@ typedef struct oro_config {
     int hy_nochar_fixed;       /* CHARTERIC=0 hybrid, components 1-4: 0 = use the
                                   face flag (intent); 1/2/3 = force that flag
                                   (what an uninitialised register yields)       */
+    int ibc;                   /* IBC: 0 none, 108 compression corner           */
+    int bc_npara[4];           /* 108: MZMAX MTMAX INLET_BOUNDARY IFLAG_WALL_NOT_NORMAL */
+    double bc_rpara[8];        /* 108: TW EPSL X_DIST_BEGIN X_DIST_END BETA
+                                  X_WALL_BEGIN X_UP_BOUNDARY_BEGIN SLZ          */
     int nfilter;               /* number of FILTER_NPARA<n> entries (<= 8)      */
     int filter_ipara[8][11];   /* ntime, fx, fy, fz, ib, ie, jb, je, kb, ke, scheme */
     double filter_rpara[8][3]; /* s0, rth, time limit                           */
@@ -74,6 +78,10 @@ void oro_get_metrics(const oro_state *s, double *fields13);
 /* Initial primitives d,u,v,w,T, interior [5][nz][ny][nx] (opencfd.dat).
  * Mirrors init() (src/OCFD_init.cu:26-131): ghosts zero, pri_to_cons. */
 void oro_set_primitives(oro_state *s, const double *prim5, int istep, double tt);
+
+/* Inlet profile of IBC 108 (flow1d-inlet.dat columns d,u,v,T), [4][ny];
+ * without it (INLET_BOUNDARY = 0) the profile is d=u=T=1, v=0. */
+void oro_set_inlet(oro_state *s, const double *ub1);
 
 /* Pre-loop of NS_solver_real (src/OCFD_NS_Solver.cu:45-53). */
 void oro_prepare(oro_state *s);

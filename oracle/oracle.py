@@ -35,6 +35,9 @@ class OroConfig(ctypes.Structure):
         ("weno_tv_limiter", ctypes.c_double), ("weno_tv_max", ctypes.c_double),
         ("nthreads", ctypes.c_int),
         ("hy_nochar_fixed", ctypes.c_int),
+        ("ibc", ctypes.c_int),
+        ("bc_npara", ctypes.c_int * 4),
+        ("bc_rpara", ctypes.c_double * 8),
         ("nfilter", ctypes.c_int),
         ("filter_ipara", (ctypes.c_int * 11) * 8),
         ("filter_rpara", (ctypes.c_double * 3) * 8),
@@ -62,6 +65,7 @@ def lib():
         L.oro_destroy.argtypes = [P]
         L.oro_set_metrics.argtypes = [P, D]
         L.oro_set_mesh.argtypes = [P, D]
+        L.oro_set_inlet.argtypes = [P, D]
         L.oro_get_metrics.argtypes = [P, D]
         L.oro_negative_jacobian.argtypes = [P]
         L.oro_negative_jacobian.restype = ctypes.c_int
@@ -119,6 +123,11 @@ def make_config(cfg, nthreads: int = 0, hy_nochar_fixed: int = 3) -> OroConfig:
     c.weno_tv_limiter, c.weno_tv_max = 5.0, 0.2
     c.nthreads = nthreads
     c.hy_nochar_fixed = hy_nochar_fixed
+    c.ibc = int(getattr(cfg, "ibc", 0))
+    for t, v in enumerate(list(getattr(cfg, "bc_npara", ()) or ())[:4]):
+        c.bc_npara[t] = int(v)
+    for t, v in enumerate(list(getattr(cfg, "bc_rpara", ()) or ())[:8]):
+        c.bc_rpara[t] = float(v)
     filters = list(getattr(cfg, "filters", ()) or ())[:8]
     c.nfilter = len(filters)
     for n, (ip, rp) in enumerate(filters):
@@ -139,7 +148,8 @@ class Oracle:
     0 gives the face flag to every component."""
 
     def __init__(self, cfg, prims: Sequence[np.ndarray], metrics: Sequence[np.ndarray],
-                 nthreads: int = 0, istep: int = 0, tt: float = 0.0, hy_nochar_fixed: int = 3):
+                 nthreads: int = 0, istep: int = 0, tt: float = 0.0, hy_nochar_fixed: int = 3,
+                 inlet=None):
         if cfg.hy_style != 2 and cfg.scheme_invis_id == 310:
             raise NotImplementedError("oracle covers HY_STYLE=2 only")
         self.cfg = cfg
@@ -156,6 +166,9 @@ class Oracle:
                 raise ValueError("negative Jacobian (the reference stops here)")
         else:
             self.L.oro_set_metrics(self.h, _dp(met))
+        if inlet is not None:           # IBC 108 profile [4][ny]
+            ub = np.ascontiguousarray(np.asarray(inlet, np.float64))
+            self.L.oro_set_inlet(self.h, _dp(ub))
         pr = np.ascontiguousarray(np.stack([np.asarray(p, np.float64) for p in prims]))
         self.L.oro_set_primitives(self.h, _dp(pr), istep, tt)
         self.L.oro_prepare(self.h)

@@ -49,6 +49,9 @@ def _write_inputs(case, workdir: str) -> None:
     # the reference turns into metrics when OCFD3d-Jacobi.dat is absent
     name = "OCFD3d-Mesh.dat" if len(case.metrics) == 3 else "OCFD3d-Jacobi.dat"
     formats.write_metric_file(os.path.join(workdir, name), case.metrics)
+    inlet = getattr(case, "inlet", None)
+    if inlet is not None:
+        formats.write_inlet_file(os.path.join(workdir, "flow1d-inlet.dat"), inlet)
 
 
 def run_and_read(case, nsteps: int, timeout: float = 900.0):

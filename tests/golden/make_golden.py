@@ -57,6 +57,25 @@ def golden_cases():
     out.extend(bounded_cases())
     out.extend(mesh_cases())
     out.extend(filter_cases())
+    out.extend(ramp_cases())
+    return out
+
+
+def ramp_cases():
+    """The compression-corner boundary family (IBC 108) on a small ramp mesh:
+    isothermal wall with the inflow profile file, hybrid scheme and filter;
+    adiabatic wall with time-dependent wall blowing; the default profile."""
+    out = []
+    c = cases.ramp_case(32, 20, 8, seed=91)
+    out.append(("ramp32x20x8_bc108_tw_filter", c, 3))
+    c = cases.ramp_case(30, 18, 8, seed=92, tw=-1.0, epsl=0.05, beta=40.0, mtmax=3,
+                        scheme_invis="WENO7", charteric=0, filters=())
+    c.cfg.bc_rpara = (-1.0, 0.05, 4.0, 30.0, 40.0, 0.0, 30.0, 8.0)
+    out.append(("ramp30x18x8_bc108_adiabatic_blowing", c, 3))
+    c = cases.ramp_case(28, 18, 8, seed=93, filters=())
+    c.cfg.bc_npara = (0, 0, 0, 0)            # INLET_BOUNDARY 0: d = u = T = 1, v = 0
+    c.inlet = None
+    out.append(("ramp28x18x8_bc108_default_inlet", c, 3))
     return out
 
 
@@ -156,8 +175,9 @@ def main(argv=None):
             runs.append(out)
         same = bool(np.array_equal(runs[0], runs[1]))
         c = case.cfg
+        extra = {} if case.inlet is None else {"inlet": np.asarray(case.inlet)}
         np.savez_compressed(
-            os.path.join(args.out, name + ".npz"),
+            os.path.join(args.out, name + ".npz"), **extra,
             prims_in=np.stack(case.prims), metrics=np.stack(case.metrics),
             out_run0=runs[0], out_run1=runs[1], nsteps=nsteps, istep=istep, tt=tt,
             config=json.dumps({k: (list(v) if isinstance(v, tuple) else v)

@@ -68,6 +68,10 @@ def small_cases():
     c.cfg.filters = (((1, 1, 1, 1, 2, 15, 0, 18, 0, 13, 2), (0.9, 1e-5, 10.0)),
                      ((2, 0, 0, 1, 0, 17, 0, 18, 3, 11, 2), (0.5, 2e-5, 10.0)))
     out.append(("filter_hybrid_char", c))
+    out.append(("ramp_bc108", cases.ramp_case(30, 18, 8, seed=66)))
+    c = cases.ramp_case(28, 18, 8, seed=67, tw=-1.0, epsl=0.05, beta=40.0, mtmax=3, filters=())
+    c.cfg.bc_rpara = (-1.0, 0.05, 4.0, 30.0, 40.0, 0.0, 30.0, 8.0)
+    out.append(("ramp_bc108_adiabatic_blowing", c))
     return out
 
 
@@ -98,8 +102,8 @@ CASES = small_cases()
 
 @pytest.mark.parametrize("name,case", CASES, ids=[n for n, _ in CASES])
 def test_rhs_matches_oracle(name, case, gpu_lib):
-    o = Oracle(case.cfg, case.prims, case.metrics)
-    s = lib.Solver(case.cfg, case.prims, case.metrics)
+    o = Oracle(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+    s = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
     o.swap(); s.swap()
     o.du_comput(1)
     s.du_comput(1)
@@ -113,8 +117,8 @@ def test_rhs_matches_oracle(name, case, gpu_lib):
 @pytest.mark.parametrize("name,case", CASES, ids=[n for n, _ in CASES])
 def test_steps_match_oracle(name, case, gpu_lib):
     nsteps = 3
-    o = Oracle(case.cfg, case.prims, case.metrics)
-    s = lib.Solver(case.cfg, case.prims, case.metrics)
+    o = Oracle(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+    s = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
     o.step(nsteps)
     s.step(nsteps)
     ep = rel_l2(s.primitives(), o.primitives())
@@ -163,7 +167,8 @@ def _golden_case(path):
 def test_matches_reference_golden(path, gpu_lib):
     z, cfg = _golden_case(path)
     nsteps = int(z["nsteps"])
-    s = lib.Solver(cfg, list(z["prims_in"]), list(z["metrics"]))
+    inlet = z["inlet"] if "inlet" in z.files else None
+    s = lib.Solver(cfg, list(z["prims_in"]), list(z["metrics"]), inlet=inlet)
     s.step(nsteps)
     got = s.primitives()
     ref = z["out_run0"]
@@ -211,3 +216,23 @@ def test_negative_jacobian_is_rejected(gpu_lib):
     with pytest.raises(lib.OcfdError) as ei:
         lib.Solver(case.cfg, case.prims, case.metrics)
     assert ei.value.status == -1
+
+
+def test_per_stage_api_equals_step_with_bc_and_filter(gpu_lib):
+    """The compat sequence (du_comput, time_advance, get_duvwT, OCFD_bc,
+    filtering) against step(), with IBC 108 and the shock filter."""
+    case = cases.ramp_case(26, 16, 8, seed=68)
+    a = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+    b = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+    a.step(2)
+    for n in range(2):
+        b.swap()
+        for krk in (1, 2, 3):
+            b.du_comput(krk)
+            b.time_advance(krk)
+            b.get_duvwT()
+            b.bc()
+        b.L.ocfd_b200_set_time(b.h, n + 1, (n + 1) * case.cfg.dt)
+        assert b.L.ocfd_b200_filtering(b.h) == 0
+    assert np.array_equal(a.primitives(), b.primitives())
+    assert np.array_equal(a.conserved(), b.conserved())

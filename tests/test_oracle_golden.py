@@ -34,7 +34,8 @@ def test_golden_fixtures_present():
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
 def test_oracle_matches_reference(path):
     z, cfg = load(path)
-    o = Oracle(cfg, list(z["prims_in"]), list(z["metrics"]))
+    inlet = z["inlet"] if "inlet" in z.files else None
+    o = Oracle(cfg, list(z["prims_in"]), list(z["metrics"]), inlet=inlet)
     o.step(int(z["nsteps"]))
     got = o.primitives()
     ref = z["out_run0"]
