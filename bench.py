@@ -105,24 +105,51 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
-def make_case(n: int):
+# The three plain-FP64 workloads (BASELINE configurations):
+#   iso  decaying isotropic turbulence n^3 (default 256^3), hybrid UP7/WENO7/WENO5
+#        with the Jameson sensor and characteristic projection, CD6, periodic;
+#   tgv  Taylor-Green vortex n^3 (64^3), WENO7 + CD6, Mach 0.1, Re 1600;
+#   ramp 24-degree compression ramp 512x128x64 (scaled by n/128 in y), metrics
+#        computed from the mesh, IBC 108 walls and inflow, hybrid + shock filter.
+WORKLOADS = {
+    "iso": "isotropic turbulence {nx}^3, hybrid UP7/WENO7/WENO5 (Jameson sensor) + characteristic "
+           "projection, CD6 viscous, SSP-RK3, plain FP64",
+    "tgv": "Taylor-Green vortex {nx}^3, WENO7 + CD6 viscous, SSP-RK3, plain FP64",
+    "ramp": "24-degree compression ramp {nx}x{ny}x{nz}, Mach 2.9, Re 5000, Tw 2.5, metrics from the mesh "
+            "(FP64), IBC 108, hybrid + characteristic + shock filter, CD6, SSP-RK3, plain FP64",
+}
+
+
+def make_case(workload: str, n: int):
     from ocfd_b200 import cases
+    if workload == "tgv":
+        return cases.taylor_green(n, seed=1234)
+    if workload == "ramp":
+        return cases.ramp_case(4 * n, n, n // 2, seed=2024)
     return cases.isotropic_turbulence(n, seed=2024, charteric=1)
 
 
-def cpu_baseline(n_sample: int = 64, steps: int = 1):
+def default_n(workload: str) -> int:
+    return {"iso": 256, "tgv": 64, "ramp": 128}[workload]
+
+
+def cells_of(case) -> int:
+    return case.cfg.nx * case.cfg.ny * case.cfg.nz
+
+
+def cpu_baseline(workload: str, n_sample: int, steps: int = 1):
     """The OpenMP FP64 oracle timed on this host on a bounded sample."""
     from oracle.oracle import Oracle
-    c = make_case(n_sample)
+    c = make_case(workload, n_sample)
     cores = os.cpu_count() or 1
-    o = Oracle(c.cfg, c.prims, c.metrics, nthreads=cores)
+    o = Oracle(c.cfg, c.prims, c.metrics, nthreads=cores, inlet=c.inlet)
     o.step(1)                                   # warm-up
     t0 = time.perf_counter()
     o.step(steps)
     dt = time.perf_counter() - t0
-    v = n_sample ** 3 * 3 * steps / dt / 1e9
+    v = cells_of(c) * 3 * steps / dt / 1e9
     return {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
-            "sample": f"{steps} RK3 step(s) of the same case at {n_sample}^3 "
+            "sample": f"{steps} RK3 step(s) of the same case at {c.cfg.nx}x{c.cfg.ny}x{c.cfg.nz} "
                       f"(OpenMP FP64 oracle, {cores} threads, {dt:.2f} s)"}
 
 
@@ -149,11 +176,12 @@ def run_ours(args, rank, world, dist):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     n = args.n
-    case = make_case(n)
-    solver = lib.Solver(case.cfg, case.prims, case.metrics, device=dev)
+    case = make_case(args.workload, n)
+    solver = lib.Solver(case.cfg, case.prims, case.metrics, device=dev, inlet=case.inlet)
     stream = torch.cuda.Stream(device=dev)
     solver.set_stream(stream.cuda_stream)
-    cells = n ** 3
+    cells = cells_of(case)
+    nx, ny, nz = case.cfg.nx, case.cfg.ny, case.cfg.nz
 
     # warm-up
     solver.step(args.warmup)
@@ -191,7 +219,7 @@ def run_ours(args, rank, world, dist):
 
     # end to end through the C ABI with host buffers (pinned), one RK3 step
     # per call: H2D of the primitives, the step, D2H of the primitives
-    shape = (5, n, n, n)
+    shape = (5, nz, ny, nx)
     hin = torch.empty(shape, dtype=torch.float64).pin_memory()
     hout = torch.empty(shape, dtype=torch.float64).pin_memory()
     a_in = hin.numpy()
@@ -215,26 +243,32 @@ def run_ours(args, rank, world, dist):
     fam_ms = {k: v[0] / max(v[1], 1) for k, v in fam.items() if v[1] > 0}
     dom = max(fam, key=lambda k: fam[k][0])
     dom_ms_per_stage = fam[dom][0] / 3.0                  # one step = 3 stages
-    dom_bytes = DOM_BYTES.get(dom, B_ALG) * cells
+    uniform = solver.uniform_metrics
+    dom_table = DOM_BYTES if uniform else DOM_BYTES_FIELDS
+    b_alg = B_ALG if uniform else B_ALG_FIELDS
+    dom_bytes = dom_table.get(dom, b_alg) * cells
     achieved = dom_bytes / (dom_ms_per_stage / 1e3) / 1e9
     stage_ms = ms_max / args.steps / 3.0
+    state_gb = 8 * cells * (15 + 35 * (nx + 8) * (ny + 8) * (nz + 8) / cells) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"isotropic turbulence {n}^3, hybrid UP7/WENO7/WENO5 (Jameson "
-                               f"sensor) + characteristic projection, CD6 viscous, SSP-RK3, plain FP64",
-                   "grid": [n, n, n], "stages_per_step": 3, "scheme": "SCHEME_HYBRIDAUTO style 2, CHARTERIC=1",
-                   "seed": 2024, "l2": "inputs larger than L2 (state ~8 GB/GPU)",
+        "config": {"workload": WORKLOADS[args.workload].format(nx=nx, ny=ny, nz=nz),
+                   "grid": [nx, ny, nz], "stages_per_step": 3,
+                   "scheme": f"SCHEME_INVIS {case.cfg.scheme_invis}, CHARTERIC={case.cfg.charteric}",
+                   "seed": 2024 if args.workload != "tgv" else 1234,
+                   "l2": f"inputs larger than L2 (state ~{state_gb:.1f} GB/GPU)" if state_gb > 0.5
+                         else f"state ~{state_gb:.2f} GB/GPU, partly L2-resident",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": (TRAFFIC_PER_CELL[dom] * cells if dom in TRAFFIC_PER_CELL else None),
+                     "traffic": (TRAFFIC_PER_CELL[dom] * cells if (uniform and dom in TRAFFIC_PER_CELL) else None),
                      "traffic_source": TRAFFIC_SOURCE,
-                     "algorithmic_bytes_per_cell": DOM_BYTES.get(dom, B_ALG),
+                     "algorithmic_bytes_per_cell": dom_table.get(dom, b_alg),
                      "launch_ms": dom_ms_per_stage},
-        "stage_roofline": {"bytes_per_cell_stage": B_ALG, "achieved_gbs": B_ALG * cells / (stage_ms / 1e3) / 1e9,
-                           "frac": B_ALG * cells / (stage_ms / 1e3) / 1e9 / hbm},
+        "stage_roofline": {"bytes_per_cell_stage": b_alg, "achieved_gbs": b_alg * cells / (stage_ms / 1e3) / 1e9,
+                           "frac": b_alg * cells / (stage_ms / 1e3) / 1e9 / hbm},
         "kernel_ms_per_stage": {k: fam[k][0] / 3.0 for k in fam},
         "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                 "steps": e2e_steps, "api": "ocfd_b200_advance_host"},
@@ -263,6 +297,18 @@ DOM_BYTES = {
 # for one stage's launches of each family, from one ncu capture of the same
 # kernels at 160^3 (profiles/stage_kernels_iso160.txt); the traffic scales with
 # the cells processed, so the bench line reports it times the cells of a launch.
+# Grids whose metrics are fields (the ramp): the sweeps also read the
+# direction's 3 metrics at every split point and Ajac per cell (+4 words per
+# direction), k_vis_ev reads 9 metrics and Ajac, k_vis_div Ajac (+11 words);
+# the stage-level bound adds the 10 metric fields (SURVEY's B_alg = 200 B).
+DOM_BYTES_FIELDS = {
+    "inviscid_sweeps": (40 + 12) * 8.0,
+    "viscous_rk_update": (53 + 11) * 8.0,
+    "ghost_fill": 0.0,
+    "sensor": 19.0,
+}
+B_ALG_FIELDS = 200.0
+
 TRAFFIC_PER_CELL = {
     "inviscid_sweeps": 307.8,       # 3 sweeps + 3 fix-ups
     "viscous_rk_update": 377.6,     # k_vis_ev + k_vis_div (Ev ghost fill not captured)
@@ -277,22 +323,23 @@ def run_reference(args, rank, world):
     from oracle import ref_runner
     n = args.n
     if not ref_runner.available():
-        c = cpu_baseline(64, 1)
+        c = cpu_baseline(args.workload, max(8, n // 4), 1)
         return {"impl": "reference", "metric": METRIC, "value": c["value"], "unit": METRIC,
                 "n_gpus": world, "steps": 1, "warmup": 1, "higher_is_better": True,
                 "note": "reference build missing; CPU oracle port timed instead",
                 "cpu_baseline": c, "e2e": {"value": c["value"], "unit": METRIC,
                                             "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    case = make_case(n)
+    case = make_case(args.workload, n)
     ref_steps = max(1, min(args.steps, args.ref_steps))
     secs, out = ref_runner.time_steps(case, args.warmup, ref_steps)
-    v = n ** 3 * 3 * ref_steps / secs / 1e9
+    v = cells_of(case) * 3 * ref_steps / secs / 1e9
+    nx, ny, nz = case.cfg.nx, case.cfg.ny, case.cfg.nz
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": 1,
             "steps": ref_steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / ref_steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"isotropic turbulence {n}^3, hybrid + characteristic, CD6, SSP-RK3, FP64",
-                       "grid": [n, n, n], "build": "reference sources, nvcc -O3 sm_100a, single-rank MPI shim",
+            "config": {"workload": WORKLOADS[args.workload].format(nx=nx, ny=ny, nz=nz),
+                       "grid": [nx, ny, nz], "build": "reference sources, nvcc -O3 sm_100a, single-rank MPI shim",
                        "timing": "reference's own MPI_Wtime interval print"},
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": 1, "kind": "reference",
                              "sample": f"{ref_steps} steps of the reference CUDA build on 1 B200, "
@@ -306,7 +353,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--n", type=int, default=256, help="grid points per direction")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="iso")
+    ap.add_argument("--n", type=int, default=0,
+                    help="grid size (iso, tgv: n^3; ramp: 4n x n x n/2); 0 = the configuration's own")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--ref-steps", type=int, default=4)
     ap.add_argument("--cpu-sample", type=int, default=64)
@@ -314,6 +363,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.n <= 0:
+        args.n = default_n(args.workload)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -331,7 +382,8 @@ def main():
     else:
         line = run_ours(args, rank, world, dist)
         if line is not None and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(args.cpu_sample, 1)
+            sample = {"iso": args.cpu_sample, "tgv": args.cpu_sample, "ramp": args.cpu_sample // 2}[args.workload]
+            line["cpu_baseline"] = cpu_baseline(args.workload, sample, 1)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

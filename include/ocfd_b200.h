@@ -95,15 +95,23 @@ int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode);
 int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx);
 /* Inviscid sweep kernel variant: 4 (default) no block barriers: each warp
  * walks its own lines (one x row, or 8 y or z lines) through a ring of
- * split values in shared memory; for UP7 and the hybrid scheme the loop
- * makes no calls and the cells next to non-UP7 faces are finished by a
- * second kernel with the same arithmetic; 5 the same walk with every face
- * through one in-loop dispatch; 2 one thread per (face, sign) in tiles
+ * split values in shared memory.  For UP7 the loop makes no calls and the
+ * cells at bounded line ends are finished by a second kernel with the same
+ * arithmetic; for WENO7 and the characteristic hybrid scheme every face,
+ * closure and line-end rule is formed in the walk (variant 6), except that a
+ * hybrid direction whose sensor pass marked almost every face UP7 takes the
+ * UP7 walk with its few other cells deferred (the choice is read back once
+ * per step, after the sensor); 5 the walk with every face through one
+ * in-loop dispatch; 6 the in-line walk alone (characteristic hybrid scheme
+ * and WENO7 only); 2 one thread per (face, sign) in tiles
  * with the five characteristic fields in registers, register budget for 4
  * blocks per SM; 3 the same with a budget for 3 blocks; 1 one thread per
  * (face, sign, field).  All agree to the parity bound (WENO weights
  * amplify the different multiply-add contractions). */
 int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl);
+/* Bit d set: direction d currently takes the walk that forms every face in
+ * line (variant 4 after the last sensor pass, or variant 6). */
+int ocfd_b200_sweep_walks(const ocfd_b200_ctx *ctx);
 int ocfd_b200_set_metrics_device(ocfd_b200_ctx *ctx, const double *metrics13_dev);
 /* Mesh coordinates x,y,z, 3 interior fields (host or device memory), from
  * which the 13 metric fields are computed on the GPU.  Replaces the

@@ -35,6 +35,11 @@ cudaError_t launch_mean(const Params &p, int which, double *scratch, unsigned lo
 int reduce_scratch_doubles();
 cudaError_t launch_sweeps2(const Params &p, cudaStream_t st);
 cudaError_t launch_sweeps3(const Params &p, cudaStream_t st);
+cudaError_t launch_sweeps4(const Params &p, cudaStream_t st);
+bool sweeps4_supported(const Params &p);
+cudaError_t launch_sweep4_dir(const Params &p, int dir, cudaStream_t st);
+cudaError_t launch_sweep3_dir(const Params &p, int dir, cudaStream_t st);
+bool sweeps3_defers(const Params &p);
 cudaError_t launch_mesh_metrics(const Params &p, const int jac_bound[3], double *scratch, cudaStream_t st);
 cudaError_t launch_negative_jacobian(const Params &p, unsigned *flag, cudaStream_t st);
 cudaError_t launch_filter_pass(const Params &p, int dir, const int box[6], double s0, double rth, cudaStream_t st);
@@ -83,6 +88,12 @@ struct ocfd_b200_ctx {
     double bc_TM[64] = {};
     double *pinned = nullptr;     // host staging for advance_host
     size_t pinned_bytes = 0;
+    // hybrid scheme, variant 4: per direction, 1 = the walk that forms every
+    // face in line, 0 = the UP7 walk with deferred cells; chosen after each
+    // sensor pass from its count of non-UP7 faces
+    unsigned *h_flag_count = nullptr;   // pinned
+    int walk4[3] = {1, 1, 1};
+    double walk4_threshold = 0.002;     // deferred cells per cell above which the inline walk is used
     bool have_metrics = false;
     int metric_mode = 0;          // 0 auto-detect uniform grids, 1 always read the fields
     bool have_state = false;
@@ -137,6 +148,7 @@ static void free_all(ocfd_b200_ctx *c) {
     cudaFree(c->ev_buf); cudaFree(c->flag_buf); cudaFree(c->stage_buf);
     cudaFree(c->red_buf); cudaFree(c->defer_buf); cudaFree(c->filter_buf); cudaFree(c->bc_buf);
     if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->h_flag_count) cudaFreeHost(c->h_flag_count);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
@@ -248,6 +260,9 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     p.flag[2] = p.flag[1] + (size_t)p.nx * (p.ny + 1) * p.nz;
     p.defer_count = ctx->defer_buf;
     for (int d = 0; d < 3; d++) p.defer[d] = ctx->defer_buf ? ctx->defer_buf + 64 + (size_t)d * N : nullptr;
+    p.flag_count = nullptr;
+    if (ctx->defer_buf && cudaHostAlloc((void **)&ctx->h_flag_count, 64, cudaHostAllocDefault) == cudaSuccess)
+        p.flag_count = ctx->defer_buf + 8;
 
     if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreate(&ctx->ev[0])) != cudaSuccess || (e = cudaEventCreate(&ctx->ev[1])) != cudaSuccess) {
@@ -351,12 +366,52 @@ static int apply_bc(ocfd_b200_ctx *ctx) {
     return OCFD_OK;
 }
 
+// Which walk each direction takes under variant 4 for the hybrid scheme.
+// The UP7 walk leaves the two cells beside every non-UP7 face, and the ~10
+// cells at each bounded end of a line, to a per-cell fix-up kernel that
+// costs about as much as 80 cells of the walk; above a small fraction of
+// such cells the walk that forms every face in line is faster.
+static bool walk4_wanted(const ocfd_b200_ctx *ctx, int d, unsigned nonup7) {
+    const Params &p = ctx->p;
+    const long long nf = (long long)(p.nx + (d == 0)) * (p.ny + (d == 1)) * (p.nz + (d == 2));
+    const int n = d == 0 ? p.nx : (d == 1 ? p.ny : p.nz);
+    const bool ends = p.bnd_lo[d] || p.bnd_hi[d] || p.nonref_lo[d] == 1 || p.nonref_hi[d] == 1;
+    const double deferred = 2.0 * (double)nonup7 / (double)nf + (ends ? 10.0 / n : 0.0);
+    return deferred > ctx->walk4_threshold;
+}
+
+static int sweeps_auto(ocfd_b200_ctx *ctx) {
+    const Params &p = ctx->p;
+    const bool hyb = p.scheme_invis == 310;
+    int w[3];
+    for (int d = 0; d < 3; d++) w[d] = hyb ? ctx->walk4[d] : 1;
+    if ((!w[0] || !w[1] || !w[2]) && ocfd::sweeps3_defers(p))
+        CK(cudaMemsetAsync(p.defer_count, 0, 3 * sizeof(unsigned), ctx->stream), "deferred counters");
+    for (int d = 0; d < 3; d++) {
+        if (w[d]) {
+            CK(ocfd::launch_sweep4_dir(p, d, ctx->stream), "inviscid sweeps");
+            ctx->launches += 1;
+        } else {
+            CK(ocfd::launch_sweep3_dir(p, d, ctx->stream), "inviscid sweeps");
+            ctx->launches += ocfd::sweeps3_defers(p) ? 2 : 1;
+        }
+    }
+    return OCFD_OK;
+}
+
 static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
     const Params &p = ctx->p;
     if (p.scheme_invis == 310 && krk == 1) {
         TimerScope ts(ctx, T_SENSOR);
         CK(ocfd::launch_sensor(p, ctx->stream), "sensor");
         ctx->launches += 1;
+        if (p.sweep_impl == 4 && ocfd::sweeps4_supported(p) && p.flag_count) {
+            // the choice follows this pass's flags: one small read-back per step
+            CK(cudaMemcpyAsync(ctx->h_flag_count, p.flag_count, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                               ctx->stream), "flag counts");
+            CK(cudaStreamSynchronize(ctx->stream), "flag counts");
+            for (int d = 0; d < 3; d++) ctx->walk4[d] = walk4_wanted(ctx, d, ctx->h_flag_count[d]);
+        }
     }
     {
         TimerScope ts(ctx, T_GHOST);
@@ -367,10 +422,18 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
         TimerScope ts(ctx, T_SWEEP);
         if (p.has_bnd && p.sweep_impl < 4)
             return fail(ctx, OCFD_ERR_UNSUPPORTED, "sweep variants 1-3 have no boundary closures (use 4 or 5)");
-        if (p.sweep_impl == 1)      CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
+        if (p.sweep_impl == 6 && !ocfd::sweeps4_supported(p))
+            return fail(ctx, OCFD_ERR_UNSUPPORTED, "sweep variant 6 covers the characteristic hybrid scheme and WENO7");
+        if (p.sweep_impl == 4 && ocfd::sweeps4_supported(p)) {
+            int rc = sweeps_auto(ctx);
+            if (rc) return rc;
+        }
+        else if (p.sweep_impl == 1) CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
+        else if (p.sweep_impl == 6) CK(ocfd::launch_sweeps4(p, ctx->stream), "inviscid sweeps");
         else if (p.sweep_impl >= 4) CK(ocfd::launch_sweeps3(p, ctx->stream), "inviscid sweeps");
         else                        CK(ocfd::launch_sweeps2(p, ctx->stream), "inviscid sweeps");
-        ctx->launches += p.sweep_impl >= 4 ? ocfd::sweeps3_kernels(p) : 3;
+        if (!(p.sweep_impl == 4 && ocfd::sweeps4_supported(p)))
+            ctx->launches += p.sweep_impl == 6 ? 3 : (p.sweep_impl >= 4 ? ocfd::sweeps3_kernels(p) : 3);
     }
     {
         TimerScope ts(ctx, T_VIS);
@@ -458,8 +521,17 @@ extern "C" int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode) {
 }
 extern "C" int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx) { return ctx ? ctx->p.uniform_metrics : 0; }
 
+extern "C" int ocfd_b200_sweep_walks(const ocfd_b200_ctx *ctx) {
+    if (!ctx) return OCFD_ERR_ARG;
+    const Params &p = ctx->p;
+    if (p.sweep_impl == 6) return 7;
+    if (p.sweep_impl != 4 || !ocfd::sweeps4_supported(p)) return 0;
+    if (p.scheme_invis != 310) return 7;
+    return ctx->walk4[0] | (ctx->walk4[1] << 1) | (ctx->walk4[2] << 2);
+}
+
 extern "C" int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl) {
-    if (!ctx || impl < 1 || impl > 5) return OCFD_ERR_ARG;
+    if (!ctx || impl < 1 || impl > 6) return OCFD_ERR_ARG;
     ctx->p.sweep_impl = impl;
     return OCFD_OK;
 }

@@ -57,6 +57,7 @@ struct Params {
     // direction (interior cell indices; capacity N each), and their counts
     unsigned *defer[3];
     unsigned *defer_count;
+    unsigned *flag_count;          // faces per direction whose hybrid flag is not 1 (sensor), or null
     // shock filter (null when no filter is set): U after the stage-3 update
     // before the face re-projection (5 LAP-box fields) and the pressure
     // cons_to_pri leaves after the last stage (1 LAP-box field)

@@ -59,6 +59,14 @@ __global__ void k_sensor(Params p) {
     if (dp0 > p.dp1) kp += 1;
     if (dp0 > p.dp2) kp += 1;
     p.flag[dir][q] = (int8_t)kp;
+    if (p.flag_count) {            // one atomic per warp and direction
+        const unsigned act = __activemask();
+        const int lane = threadIdx.x & 31;
+        for (int d = 0; d < 3; d++) {
+            const unsigned m = __ballot_sync(act, dir == d && kp != 1);
+            if (m && lane == __ffs(act) - 1) atomicAdd(p.flag_count + d, (unsigned)__popc(m));
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -673,6 +681,10 @@ static cudaError_t launch_sweep(const Params &p, cudaStream_t st) {
 cudaError_t launch_sensor(const Params &p, cudaStream_t st) {
     long long n = (long long)(p.nx + 1) * p.ny * p.nz + (long long)p.nx * (p.ny + 1) * p.nz
                 + (long long)p.nx * p.ny * (p.nz + 1);
+    if (p.flag_count) {
+        cudaError_t e = cudaMemsetAsync(p.flag_count, 0, 3 * sizeof(unsigned), st);
+        if (e != cudaSuccess) return e;
+    }
     k_sensor<<<blocks_for(n, 256), 256, 0, st>>>(p);
     return cudaGetLastError();
 }

@@ -195,6 +195,59 @@ def test_bounded_sweep_variants(name, case, gpu_lib):
     assert ei.value.status == -2
 
 
+def _walk4_supported(cfg):
+    return (cfg.scheme_invis == "SCHEME_HYBRIDAUTO" and cfg.charteric) or \
+           (cfg.scheme_invis == "WENO7" and not cfg.charteric)
+
+
+@pytest.mark.parametrize("name,case", CASES, ids=[n for n, _ in CASES])
+def test_inline_walk_matches_dispatch(name, case, gpu_lib):
+    """Variant 6 forms every face of the characteristic hybrid scheme and of
+    WENO7 inside the walk (closures and first/last-cell rules included);
+    variant 5 sends them through the out-of-line face routine.  Same
+    arithmetic, so the same state after two steps to the last bits; any other
+    scheme is refused."""
+    a = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+    a.set_sweep_impl(6)
+    if not _walk4_supported(case.cfg):
+        with pytest.raises(lib.OcfdError) as ei:
+            a.step(1)
+        assert ei.value.status == -2
+        return
+    b = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+    b.set_sweep_impl(5)
+    a.step(2)
+    b.step(2)
+    assert np.all(rel_l2(a.primitives(), b.primitives()) <= 1e-14), name
+
+
+def test_walk_choice_follows_sensor(gpu_lib):
+    """Variant 4 picks a walk per direction after each sensor pass: the UP7
+    walk where (almost) every face is UP7, the in-line walk where many are
+    not; WENO7 always takes the in-line walk.  Either way the state matches
+    the in-loop dispatch."""
+    smooth = cases.isotropic_turbulence(16, seed=9, charteric=1)
+    s = lib.Solver(smooth.cfg, smooth.prims, smooth.metrics)
+    s.step(1)
+    nonup7 = [int(np.count_nonzero(f != 1)) for f in s.flags()]
+    walks = s.sweep_walks()
+    for d in range(3):
+        assert ((walks >> d) & 1) == (2 * nonup7[d] / s.flags()[d].size > 0.002), (d, nonup7, walks)
+    shock = cases.random_smooth_case(13, 17, 11, seed=4, scheme_invis="SCHEME_HYBRIDAUTO", charteric=1,
+                                     shock=True, curvilinear=True)
+    s = lib.Solver(shock.cfg, shock.prims, shock.metrics)
+    s.step(2)
+    assert s.sweep_walks() == 7
+    b = lib.Solver(shock.cfg, shock.prims, shock.metrics)
+    b.set_sweep_impl(5)
+    b.step(2)
+    assert np.all(rel_l2(s.primitives(), b.primitives()) <= 1e-14)
+    tgv = cases.taylor_green(16, seed=3)
+    s = lib.Solver(tgv.cfg, tgv.prims, tgv.metrics)
+    s.step(1)
+    assert s.sweep_walks() == 7
+
+
 @pytest.mark.parametrize("iperiodic", [(0, 0, 1), (1, 0, 0), (0, 0, 0)], ids=["z_per", "x_per", "closed"])
 def test_metrics_from_mesh_match_oracle(iperiodic, gpu_lib):
     """Comput_Jacobian3d on the GPU against the oracle's restatement: the 13
