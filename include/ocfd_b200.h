@@ -109,6 +109,17 @@ int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx);
  * (face, sign, field).  All agree to the parity bound (WENO weights
  * amplify the different multiply-add contractions). */
 int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl);
+/* Arithmetic form of the stencils.  0 (default): FP64 throughout, the
+ * reference's own arithmetic.  1, the precision form: the Steger-Warming
+ * split, characteristic projection, reconstruction, sensor and viscous
+ * stencils run in FP32 on FP32 copies of the primitives, with the stage
+ * RHS and the viscous fluxes stored in FP32; the conserved state, the RK3
+ * update, cons->prim, the grid metrics and the reductions stay FP64.
+ * Covers the characteristic hybrid scheme and WENO7 without a
+ * boundary-condition family or filter (OCFD_ERR_UNSUPPORTED otherwise);
+ * whole steps only (ocfd_b200_step).  Switching back recomputes the FP64
+ * primitives from the conserved state. */
+int ocfd_b200_set_precision(ocfd_b200_ctx *ctx, int form);
 /* Bit d set: direction d currently takes the walk that forms every face in
  * line (variant 4 after the last sensor pass, or variant 6). */
 int ocfd_b200_sweep_walks(const ocfd_b200_ctx *ctx);

@@ -20,6 +20,8 @@
 namespace ocfd {
 cudaError_t launch_sensor(const Params &p, cudaStream_t st);
 cudaError_t launch_ghost(const Params &p, double *const *fields, const int *dirmask, int nf, cudaStream_t st);
+cudaError_t launch_ghost32(const Params &p, float *const *fields, const int *dirmask, int nf, cudaStream_t st);
+cudaError_t launch_prims_to_fp32(const Params &p, cudaStream_t st);
 cudaError_t launch_sweeps(const Params &p, cudaStream_t st);
 cudaError_t launch_viscous(const Params &p, int krk, cudaStream_t st);
 cudaError_t launch_rk(const Params &p, int krk, cudaStream_t st);
@@ -92,6 +94,11 @@ struct ocfd_b200_ctx {
     // face in line, 0 = the UP7 walk with deferred cells; chosen after each
     // sensor pass from its count of non-UP7 faces
     unsigned *h_flag_count = nullptr;   // pinned
+    // precision form: FP32 primitives (5 LAP fields), stage RHS (5 interior
+    // fields) and viscous fluxes (12 LAP fields); the FP64 primitives are
+    // brought up to date from the conserved state before they are read
+    float *prec_buf = nullptr;
+    bool prims64_stale = false;
     int walk4[3] = {1, 1, 1};
     double walk4_threshold = 0.002;     // deferred cells per cell above which the inline walk is used
     bool have_metrics = false;
@@ -149,6 +156,7 @@ static void free_all(ocfd_b200_ctx *c) {
     cudaFree(c->red_buf); cudaFree(c->defer_buf); cudaFree(c->filter_buf); cudaFree(c->bc_buf);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->h_flag_count) cudaFreeHost(c->h_flag_count);
+    cudaFree(c->prec_buf);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
@@ -312,11 +320,33 @@ extern "C" int ocfd_b200_synchronize(ocfd_b200_ctx *ctx) {
 // internal helpers
 // ---------------------------------------------------------------------------
 
-static int ghost_prims(ocfd_b200_ctx *ctx) {
+static int ghost_prims64(ocfd_b200_ctx *ctx) {
     double *f[5]; int mask[5];
     for (int m = 0; m < 5; m++) { f[m] = ctx->p.prim[m]; mask[m] = 7; }
     CK(ocfd::launch_ghost(ctx->p, f, mask, 5, ctx->stream), "ghost fill");
     ctx->launches += 1;
+    return OCFD_OK;
+}
+
+// the primitives the stencils read: FP64, or FP32 in the precision form
+static int ghost_prims(ocfd_b200_ctx *ctx) {
+    if (!ctx->p.mixed) return ghost_prims64(ctx);
+    float *f[5]; int mask[5];
+    for (int m = 0; m < 5; m++) { f[m] = ctx->p.prim32[m]; mask[m] = 7; }
+    CK(ocfd::launch_ghost32(ctx->p, f, mask, 5, ctx->stream), "ghost fill");
+    ctx->launches += 1;
+    return OCFD_OK;
+}
+
+// precision form: FP64 primitives (interior and ghosts) from the FP64
+// conserved state, before anything reads them
+static int refresh_prims64(ocfd_b200_ctx *ctx) {
+    if (!ctx->prims64_stale) return OCFD_OK;
+    CK(ocfd::launch_c2p(ctx->p, ctx->stream), "cons_to_pri");
+    ctx->launches += 1;
+    int rc = ghost_prims64(ctx);
+    if (rc) return rc;
+    ctx->prims64_stale = false;
     return OCFD_OK;
 }
 
@@ -384,7 +414,7 @@ static int sweeps_auto(ocfd_b200_ctx *ctx) {
     const Params &p = ctx->p;
     const bool hyb = p.scheme_invis == 310;
     int w[3];
-    for (int d = 0; d < 3; d++) w[d] = hyb ? ctx->walk4[d] : 1;
+    for (int d = 0; d < 3; d++) w[d] = (hyb && !p.mixed) ? ctx->walk4[d] : 1;
     if ((!w[0] || !w[1] || !w[2]) && ocfd::sweeps3_defers(p))
         CK(cudaMemsetAsync(p.defer_count, 0, 3 * sizeof(unsigned), ctx->stream), "deferred counters");
     for (int d = 0; d < 3; d++) {
@@ -405,7 +435,7 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
         TimerScope ts(ctx, T_SENSOR);
         CK(ocfd::launch_sensor(p, ctx->stream), "sensor");
         ctx->launches += 1;
-        if (p.sweep_impl == 4 && ocfd::sweeps4_supported(p) && p.flag_count) {
+        if (p.sweep_impl == 4 && !p.mixed && ocfd::sweeps4_supported(p) && p.flag_count) {
             // the choice follows this pass's flags: one small read-back per step
             CK(cudaMemcpyAsync(ctx->h_flag_count, p.flag_count, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost,
                                ctx->stream), "flag counts");
@@ -424,7 +454,7 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
             return fail(ctx, OCFD_ERR_UNSUPPORTED, "sweep variants 1-3 have no boundary closures (use 4 or 5)");
         if (p.sweep_impl == 6 && !ocfd::sweeps4_supported(p))
             return fail(ctx, OCFD_ERR_UNSUPPORTED, "sweep variant 6 covers the characteristic hybrid scheme and WENO7");
-        if (p.sweep_impl == 4 && ocfd::sweeps4_supported(p)) {
+        if (p.mixed || (p.sweep_impl == 4 && ocfd::sweeps4_supported(p))) {
             int rc = sweeps_auto(ctx);
             if (rc) return rc;
         }
@@ -432,7 +462,7 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
         else if (p.sweep_impl == 6) CK(ocfd::launch_sweeps4(p, ctx->stream), "inviscid sweeps");
         else if (p.sweep_impl >= 4) CK(ocfd::launch_sweeps3(p, ctx->stream), "inviscid sweeps");
         else                        CK(ocfd::launch_sweeps2(p, ctx->stream), "inviscid sweeps");
-        if (!(p.sweep_impl == 4 && ocfd::sweeps4_supported(p)))
+        if (!(p.mixed || (p.sweep_impl == 4 && ocfd::sweeps4_supported(p))))
             ctx->launches += p.sweep_impl == 6 ? 3 : (p.sweep_impl >= 4 ? ocfd::sweeps3_kernels(p) : 3);
     }
     {
@@ -520,6 +550,40 @@ extern "C" int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode) {
     return OCFD_OK;
 }
 extern "C" int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx) { return ctx ? ctx->p.uniform_metrics : 0; }
+
+extern "C" int ocfd_b200_set_precision(ocfd_b200_ctx *ctx, int form) {
+    if (!ctx || form < 0 || form > 1) return OCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    Params &p = ctx->p;
+    if (form == 0) {
+        if (!p.mixed) return OCFD_OK;
+        if (int rc = refresh_prims64(ctx)) return rc;
+        p.mixed = 0;
+        CK(cudaStreamSynchronize(ctx->stream), "set_precision");
+        return OCFD_OK;
+    }
+    if (p.mixed) return OCFD_OK;
+    if (!ocfd::sweeps4_supported(p))
+        return fail(ctx, OCFD_ERR_UNSUPPORTED, "the precision form covers the characteristic hybrid scheme and WENO7");
+    if (p.ibc || ctx->nfilter)
+        return fail(ctx, OCFD_ERR_UNSUPPORTED, "the precision form has no boundary-condition family or filter");
+    if (!ctx->prec_buf) {
+        const size_t n = 17 * (size_t)p.lapN + 5 * (size_t)p.N;
+        cudaError_t e = cudaMalloc((void **)&ctx->prec_buf, n * sizeof(float));
+        if (e != cudaSuccess) { ctx->prec_buf = nullptr; return cuda_fail(ctx, e, "precision-form buffers"); }
+        CK(cudaMemsetAsync(ctx->prec_buf, 0, n * sizeof(float), ctx->stream), "memset");
+    }
+    for (int m = 0; m < 5; m++) p.prim32[m] = ctx->prec_buf + (size_t)m * p.lapN;
+    p.ev32 = ctx->prec_buf + 5 * (size_t)p.lapN;
+    p.du32 = ctx->prec_buf + 17 * (size_t)p.lapN;
+    p.mixed = 1;
+    if (ctx->have_state) {
+        CK(ocfd::launch_prims_to_fp32(p, ctx->stream), "FP32 primitives");
+        ctx->launches += 1;
+    }
+    CK(cudaStreamSynchronize(ctx->stream), "set_precision");
+    return OCFD_OK;
+}
 
 extern "C" int ocfd_b200_sweep_walks(const ocfd_b200_ctx *ctx) {
     if (!ctx) return OCFD_ERR_ARG;
@@ -634,7 +698,7 @@ static int set_prims_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKind 
     // NS_solver_real pre-loop: exchange, OCFD_bc (the boundary family's
     // values, then the faces of f re-projected: without a family no change),
     // get_Amu (formed on the fly)
-    rc = ghost_prims(ctx);
+    rc = ghost_prims64(ctx);
     if (rc) return rc;
     ctx->tt = tt;
     if (p.ibc) {
@@ -642,6 +706,11 @@ static int set_prims_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKind 
         CK(ocfd::launch_bc_faces(p, ctx->stream), "face re-projection");
         ctx->launches += 1;
     }
+    if (p.mixed) {
+        CK(ocfd::launch_prims_to_fp32(p, ctx->stream), "FP32 primitives");
+        ctx->launches += 1;
+    }
+    ctx->prims64_stale = false;
     CK(cudaStreamSynchronize(ctx->stream), "set_primitives");
     ctx->istep = istep;
     ctx->tt = tt;
@@ -707,6 +776,9 @@ extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
     int rc = check_ready(ctx);
     if (rc) return rc;
     if (nsteps < 0) return fail(ctx, OCFD_ERR_ARG, "nsteps < 0");
+    if (ctx->p.mixed && (ctx->p.ibc || ctx->nfilter))
+        return fail(ctx, OCFD_ERR_UNSUPPORTED, "the precision form has no boundary-condition family or filter");
+    if (ctx->p.mixed && nsteps > 0) ctx->prims64_stale = true;
     for (int n = 0; n < nsteps; n++) {
         ocfd_b200_swap_time_levels(ctx);
         for (int krk = 1; krk <= 3; krk++)
@@ -842,6 +914,7 @@ extern "C" int ocfd_b200_set_filter(ocfd_b200_ctx *ctx, int n, const int npara[1
 extern "C" int ocfd_b200_du_comput(ocfd_b200_ctx *ctx, int krk) {
     int rc = check_ready(ctx);
     if (rc) return rc;
+    if (ctx->p.mixed) return fail(ctx, OCFD_ERR_UNSUPPORTED, "the precision form runs whole steps only");
     if (krk < 1 || krk > 3) return fail(ctx, OCFD_ERR_ARG, "KRK must be 1..3");
     return rhs(ctx, krk, 0);
 }
@@ -849,6 +922,7 @@ extern "C" int ocfd_b200_du_comput(ocfd_b200_ctx *ctx, int krk) {
 extern "C" int ocfd_b200_time_advance(ocfd_b200_ctx *ctx, int krk) {
     int rc = check_ready(ctx);
     if (rc) return rc;
+    if (ctx->p.mixed) return fail(ctx, OCFD_ERR_UNSUPPORTED, "the precision form runs whole steps only");
     if (krk < 1 || krk > 3) return fail(ctx, OCFD_ERR_ARG, "KRK must be 1..3");
     CK(ocfd::launch_rk_only(ctx->p, krk, ctx->stream), "time advance");
     ctx->launches += 1;
@@ -858,6 +932,7 @@ extern "C" int ocfd_b200_time_advance(ocfd_b200_ctx *ctx, int krk) {
 extern "C" int ocfd_b200_get_duvwT(ocfd_b200_ctx *ctx) {
     int rc = check_ready(ctx);
     if (rc) return rc;
+    if (ctx->p.mixed) return fail(ctx, OCFD_ERR_UNSUPPORTED, "the precision form runs whole steps only");
     CK(ocfd::launch_c2p(ctx->p, ctx->stream), "cons_to_pri");
     ctx->launches += 1;
     return OCFD_OK;
@@ -866,6 +941,7 @@ extern "C" int ocfd_b200_get_duvwT(ocfd_b200_ctx *ctx) {
 extern "C" int ocfd_b200_bc(ocfd_b200_ctx *ctx) {
     int rc = check_ready(ctx);
     if (rc) return rc;
+    if (ctx->p.mixed) return fail(ctx, OCFD_ERR_UNSUPPORTED, "the precision form runs whole steps only");
     if ((rc = apply_bc(ctx))) return rc;
     CK(ocfd::launch_bc_faces(ctx->p, ctx->stream), "face re-projection");
     ctx->launches += 1;
@@ -879,6 +955,7 @@ extern "C" int ocfd_b200_bc(ocfd_b200_ctx *ctx) {
 extern "C" int ocfd_b200_get_primitives_device(ocfd_b200_ctx *ctx, double *out) {
     if (!ctx || !out) return OCFD_ERR_ARG;
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (int rc = refresh_prims64(ctx)) return rc;
     for (int m = 0; m < 5; m++) {
         CK(ocfd::launch_gather(ctx->p, ctx->p.prim[m], out + (size_t)m * ctx->p.N, ctx->stream), "gather");
         ctx->launches += 1;
@@ -890,6 +967,7 @@ extern "C" int ocfd_b200_get_primitives_device(ocfd_b200_ctx *ctx, double *out) 
 extern "C" int ocfd_b200_get_primitives(ocfd_b200_ctx *ctx, double *out) {
     if (!ctx || !out) return OCFD_ERR_ARG;
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (int rc = refresh_prims64(ctx)) return rc;
     for (int m = 0; m < 5; m++) {
         CK(ocfd::launch_gather(ctx->p, ctx->p.prim[m], ctx->stage_buf + (size_t)m * ctx->p.N, ctx->stream), "gather");
         ctx->launches += 1;
@@ -912,6 +990,7 @@ extern "C" int ocfd_b200_get_conserved(ocfd_b200_ctx *ctx, double *out) {
     return ctx ? get_interior5(ctx, ctx->p.f, out, "get_conserved") : OCFD_ERR_ARG;
 }
 extern "C" int ocfd_b200_get_du(ocfd_b200_ctx *ctx, double *out) {
+    if (ctx && ctx->p.mixed) return fail(ctx, OCFD_ERR_UNSUPPORTED, "the precision form keeps du in FP32");
     return ctx ? get_interior5(ctx, ctx->p.du, out, "get_du") : OCFD_ERR_ARG;
 }
 
@@ -931,6 +1010,7 @@ extern "C" int ocfd_b200_get_flags(ocfd_b200_ctx *ctx, int8_t *fx, int8_t *fy, i
 extern "C" int ocfd_b200_ana_residual(ocfd_b200_ctx *ctx, int which, double *mean) {
     int rc = check_ready(ctx);
     if (rc) return rc;
+    if ((rc = refresh_prims64(ctx))) return rc;
     if (!mean || which < 0 || which > 1) return fail(ctx, OCFD_ERR_ARG, "which must be 0 (E) or 1 (T)");
     CK(ocfd::launch_mean(ctx->p, which, ctx->red_buf, nullptr, ctx->stream), "reduction");
     ctx->launches += 2;
@@ -945,6 +1025,7 @@ extern "C" int ocfd_b200_ana_residual(ocfd_b200_ctx *ctx, int which, double *mea
 extern "C" int ocfd_b200_check_state(ocfd_b200_ctx *ctx, long long *n_nan, long long *n_neg_t, double *mean_t) {
     int rc = check_ready(ctx);
     if (rc) return rc;
+    if ((rc = refresh_prims64(ctx))) return rc;
     int nd = ocfd::reduce_scratch_doubles();
     unsigned long long *counts = reinterpret_cast<unsigned long long *>(ctx->red_buf + nd);
     CK(ocfd::launch_mean(ctx->p, 1, ctx->red_buf, counts, ctx->stream), "state check");

@@ -43,6 +43,13 @@ struct Params {
     int has_bnd;
     // state
     double *prim[5];        // d u v w T on the LAP box
+    // precision form (mixed = 1): the primitives the stencils read, the stage
+    // RHS and the viscous fluxes in FP32; the conserved state, the RK
+    // update and cons->prim stay FP64 (null when the form is off)
+    int mixed;
+    float *prim32[5];
+    float *du32;
+    float *ev32;
     const double *met[13];  // Axx Ayy Azz Akx Aky Akz Aix Aiy Aiz Asx Asy Asz Ajac (LAP box)
     double *f, *fn, *du;    // [5][nz][ny][nx]
     double *ev;             // [12] LAP-box fields: Ev1..4 of x, then y, then z

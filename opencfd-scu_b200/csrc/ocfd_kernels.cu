@@ -15,7 +15,7 @@
 // characteristic field, so the 5x5 projection of the 8-point stencil is a
 // 5-term dot product per thread; phase C forms du of each tile cell from
 // the two neighbouring face fluxes (no atomics).
-#include "ocfd_device.cuh"
+#include "ocfd_fp32.cuh"
 
 #include <cuda_runtime.h>
 
@@ -27,6 +27,7 @@ namespace ocfd {
 // belongs to cell q-1; P = p00*d*T is formed on the fly from the LAP-box d,T
 // as they stand before this stage's ghost fill.
 // ---------------------------------------------------------------------------
+template <typename R>
 __global__ void k_sensor(Params p) {
     long long nfx = (long long)(p.nx + 1) * p.ny * p.nz;
     long long nfy = (long long)p.nx * (p.ny + 1) * p.nz;
@@ -44,20 +45,20 @@ __global__ void k_sensor(Params p) {
     int j = (int)(r % ey);
     int k = (int)(r / ey);
     int ci = i + OCFD_LAP - (dir == 0), cj = j + OCFD_LAP - (dir == 1), ck = k + OCFD_LAP - (dir == 2);
-    const double *d = p.prim[0], *T = p.prim[4];
+    const R *d = prim_r<R>(p, 0), *T = prim_r<R>(p, 4);
     long long c = lap_index(p, ci, cj, ck);
-    const double p00 = p.p00;
+    const R p00 = (R)p.p00;
     auto P = [&](long long o) { return p00 * d[o] * T[o]; };
-    double P0 = P(c);
-    double Pm = P(c - 1), Pp = P(c + 1);
-    double dp0 = fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
+    R P0 = P(c);
+    R Pm = P(c - 1), Pp = P(c + 1);
+    R dp0 = fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
     Pm = P(c - p.ys); Pp = P(c + p.ys);
     dp0 += fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
     Pm = P(c - p.zs); Pp = P(c + p.zs);
     dp0 += fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
     int kp = 1;
-    if (dp0 > p.dp1) kp += 1;
-    if (dp0 > p.dp2) kp += 1;
+    if (dp0 > (R)p.dp1) kp += 1;
+    if (dp0 > (R)p.dp2) kp += 1;
     p.flag[dir][q] = (int8_t)kp;
     if (p.flag_count) {            // one atomic per warp and direction
         const unsigned act = __activemask();
@@ -76,9 +77,10 @@ __global__ void k_sensor(Params p) {
 // read only interior cells, so one launch fills all of them.
 // fields: list of base pointers; dirmask selects directions per field.
 // ---------------------------------------------------------------------------
-struct GhostList { double *f[12]; int dirmask[12]; int n; };
+template <typename T> struct GhostList { T *f[12]; int dirmask[12]; int n; };
 
-__global__ void k_ghost(Params p, GhostList g) {
+template <typename T>
+__global__ void k_ghost(Params p, GhostList<T> g) {
     const int L = OCFD_LAP;
     long long sx = 2LL * L * p.ny * p.nz, sy = 2LL * L * p.nx * p.nz, sz = 2LL * L * p.nx * p.ny;
     long long per = sx + sy + sz;
@@ -86,7 +88,7 @@ __global__ void k_ghost(Params p, GhostList g) {
     if (tid >= per * g.n) return;
     int fi = (int)(tid / per);
     long long q = tid - (long long)fi * per;
-    double *f = g.f[fi];
+    T *f = g.f[fi];
     int mask = g.dirmask[fi];
     if (q < sx) {
         if (!(mask & 1) || !p.periodic[0]) return;
@@ -347,8 +349,9 @@ k_sweep(Params p) {
 // first derivative of a LAP field along stride s at o (OCFD_d?0 with CD6 or
 // CD8, src/OCFD_Schemes.cu:96-156; put_d0_kernel divides by h)
 // (the division by h is the corrected product with RN(1/h), div_const)
-__device__ __forceinline__ double d0(const double *f, long long o, long long s, double h, double ih, bool c8) {
-    double t;
+template <typename R>
+__device__ __forceinline__ R d0(const R *f, long long o, long long s, R h, R ih, bool c8) {
+    R t;
     if (c8) t = cd8(f[o - 4 * s], f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s], f[o + 4 * s]);
     else    t = cd6(f[o - 3 * s], f[o - 2 * s], f[o - s], f[o + s], f[o + 2 * s], f[o + 3 * s]);
     return div_const(t, h, ih);
@@ -358,25 +361,26 @@ __device__ __forceinline__ double d0(const double *f, long long o, long long s, 
 // closed (DIF_BOUND = 1): the one-sided and lower-order formulas of
 // OCFD_D0bound_scheme_kernel (src/OCFD_bound_Scheme.cu:79-186) on the four
 // points next to a closed face, the lower face first as in its case 7/8/9.
-__device__ __forceinline__ double d0b(const double *f, long long o, long long s, double h, double ih, bool c8,
-                                      int X, int n, bool lo, bool hi) {
+template <typename R>
+__device__ __forceinline__ R d0b(const R *f, long long o, long long s, R h, R ih, bool c8,
+                                 int X, int n, bool lo, bool hi) {
     if (lo && X <= 3) {
-        double t;
+        R t;
         if (X == 0)      t = (f[o + s] - f[o]);
-        else if (X == 1) t = (f[o + s] - f[o - s]) * 0.5;
-        else if (X == 2) t = (f[o - 2 * s] - 8.0 * f[o - s] + 8.0 * f[o + s] - f[o + 2 * s]) / 12.0;
-        else             t = (f[o + 3 * s] - f[o - 3 * s] - 9.0 * (f[o + 2 * s] - f[o - 2 * s])
-                             + 45.0 * (f[o + s] - f[o - s])) / 60.0;
+        else if (X == 1) t = (f[o + s] - f[o - s]) * (R)0.5;
+        else if (X == 2) t = (f[o - 2 * s] - (R)8.0 * f[o - s] + (R)8.0 * f[o + s] - f[o + 2 * s]) / (R)12.0;
+        else             t = (f[o + 3 * s] - f[o - 3 * s] - (R)9.0 * (f[o + 2 * s] - f[o - 2 * s])
+                             + (R)45.0 * (f[o + s] - f[o - s])) / (R)60.0;
         return div_const(t, h, ih);
     }
     if (hi && X >= n - 4) {
-        double t;
+        R t;
         const int q = X - n;
         if (q == -1)      t = (f[o] - f[o - s]);
-        else if (q == -2) t = (f[o + s] - f[o - s]) * 0.5;
-        else if (q == -3) t = (f[o - 2 * s] - 8.0 * f[o - s] + 8.0 * f[o + s] - f[o + 2 * s]) / 12.0;
-        else              t = (f[o + 3 * s] - f[o - 3 * s] - 9.0 * (f[o + 2 * s] - f[o - 2 * s])
-                              + 45.0 * (f[o + s] - f[o - s])) / 60.0;
+        else if (q == -2) t = (f[o + s] - f[o - s]) * (R)0.5;
+        else if (q == -3) t = (f[o - 2 * s] - (R)8.0 * f[o - s] + (R)8.0 * f[o + s] - f[o + 2 * s]) / (R)12.0;
+        else              t = (f[o + 3 * s] - f[o - 3 * s] - (R)9.0 * (f[o + 2 * s] - f[o - 2 * s])
+                              + (R)45.0 * (f[o + s] - f[o - s])) / (R)60.0;
         return div_const(t, h, ih);
     }
     return d0(f, o, s, h, ih, c8);
@@ -399,7 +403,7 @@ __device__ __forceinline__ void cons_to_prim(const Params &p, const double f[5],
 // and temperature derivatives (du_viscous_Jacobian3d_init :58-77) are formed
 // here from the LAP-box primitives instead of being stored; the stress and
 // heat flux do not depend on the direction, so they are formed once per cell.
-template <bool UNI>
+template <bool UNI, typename R>
 __global__ void __launch_bounds__(256, 5) k_vis_ev(Params p) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= p.N) return;
@@ -407,62 +411,64 @@ __global__ void __launch_bounds__(256, 5) k_vis_ev(Params p) {
     int j = (int)(r % p.ny); int k = (int)(r / p.ny);
     long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     const bool c8 = p.scheme_vis == 204;
-    double Akx = metric<UNI>(p, M_AKX, o), Aix = metric<UNI>(p, M_AIX, o), Asx = metric<UNI>(p, M_ASX, o);
-    double Aky = metric<UNI>(p, M_AKY, o), Aiy = metric<UNI>(p, M_AIY, o), Asy = metric<UNI>(p, M_ASY, o);
-    double Akz = metric<UNI>(p, M_AKZ, o), Aiz = metric<UNI>(p, M_AIZ, o), Asz = metric<UNI>(p, M_ASZ, o);
-    double Tc = p.prim[4][o];
-    double Amu = p.amu_C0 * sqrt(Tc * Tc * Tc) / (p.Tsb + Tc);      // get_Amu_kernal
-    const double *U = p.prim[1], *V = p.prim[2], *W = p.prim[3], *TT = p.prim[4];
-    const double ihx = p.inv_h[0], ihy = p.inv_h[1], ihz = p.inv_h[2];
-    double uk, ui, us, vk, vi, vs, wk, wi, ws, Tk, Ti, Ts;
+    R Akx = (R)metric<UNI>(p, M_AKX, o), Aix = (R)metric<UNI>(p, M_AIX, o), Asx = (R)metric<UNI>(p, M_ASX, o);
+    R Aky = (R)metric<UNI>(p, M_AKY, o), Aiy = (R)metric<UNI>(p, M_AIY, o), Asy = (R)metric<UNI>(p, M_ASY, o);
+    R Akz = (R)metric<UNI>(p, M_AKZ, o), Aiz = (R)metric<UNI>(p, M_AIZ, o), Asz = (R)metric<UNI>(p, M_ASZ, o);
+    const R *U = prim_r<R>(p, 1), *V = prim_r<R>(p, 2), *W = prim_r<R>(p, 3), *TT = prim_r<R>(p, 4);
+    R Tc = TT[o];
+    R Amu = (R)p.amu_C0 * sqrt_r(Tc * Tc * Tc) / ((R)p.Tsb + Tc);      // get_Amu_kernal
+    const R ihx = (R)p.inv_h[0], ihy = (R)p.inv_h[1], ihz = (R)p.inv_h[2];
+    const R hx = (R)p.hx, hy = (R)p.hy, hz = (R)p.hz;
+    R uk, ui, us, vk, vi, vs, wk, wi, ws, Tk, Ti, Ts;
     if (!p.has_bnd) {
-        uk = d0(U, o, 1, p.hx, ihx, c8); ui = d0(U, o, p.ys, p.hy, ihy, c8); us = d0(U, o, p.zs, p.hz, ihz, c8);
-        vk = d0(V, o, 1, p.hx, ihx, c8); vi = d0(V, o, p.ys, p.hy, ihy, c8); vs = d0(V, o, p.zs, p.hz, ihz, c8);
-        wk = d0(W, o, 1, p.hx, ihx, c8); wi = d0(W, o, p.ys, p.hy, ihy, c8); ws = d0(W, o, p.zs, p.hz, ihz, c8);
-        Tk = d0(TT, o, 1, p.hx, ihx, c8); Ti = d0(TT, o, p.ys, p.hy, ihy, c8); Ts = d0(TT, o, p.zs, p.hz, ihz, c8);
+        uk = d0(U, o, 1, hx, ihx, c8); ui = d0(U, o, p.ys, hy, ihy, c8); us = d0(U, o, p.zs, hz, ihz, c8);
+        vk = d0(V, o, 1, hx, ihx, c8); vi = d0(V, o, p.ys, hy, ihy, c8); vs = d0(V, o, p.zs, hz, ihz, c8);
+        wk = d0(W, o, 1, hx, ihx, c8); wi = d0(W, o, p.ys, hy, ihy, c8); ws = d0(W, o, p.zs, hz, ihz, c8);
+        Tk = d0(TT, o, 1, hx, ihx, c8); Ti = d0(TT, o, p.ys, hy, ihy, c8); Ts = d0(TT, o, p.zs, hz, ihz, c8);
     } else {
-        const bool lx = p.bnd_lo[0], hx = p.bnd_hi[0], ly = p.bnd_lo[1], hy = p.bnd_hi[1];
-        const bool lz = p.bnd_lo[2], hz = p.bnd_hi[2];
-        uk = d0b(U, o, 1, p.hx, ihx, c8, i, p.nx, lx, hx); ui = d0b(U, o, p.ys, p.hy, ihy, c8, j, p.ny, ly, hy);
-        us = d0b(U, o, p.zs, p.hz, ihz, c8, k, p.nz, lz, hz);
-        vk = d0b(V, o, 1, p.hx, ihx, c8, i, p.nx, lx, hx); vi = d0b(V, o, p.ys, p.hy, ihy, c8, j, p.ny, ly, hy);
-        vs = d0b(V, o, p.zs, p.hz, ihz, c8, k, p.nz, lz, hz);
-        wk = d0b(W, o, 1, p.hx, ihx, c8, i, p.nx, lx, hx); wi = d0b(W, o, p.ys, p.hy, ihy, c8, j, p.ny, ly, hy);
-        ws = d0b(W, o, p.zs, p.hz, ihz, c8, k, p.nz, lz, hz);
-        Tk = d0b(TT, o, 1, p.hx, ihx, c8, i, p.nx, lx, hx); Ti = d0b(TT, o, p.ys, p.hy, ihy, c8, j, p.ny, ly, hy);
-        Ts = d0b(TT, o, p.zs, p.hz, ihz, c8, k, p.nz, lz, hz);
+        const bool bxl = p.bnd_lo[0], bxh = p.bnd_hi[0], byl = p.bnd_lo[1], byh = p.bnd_hi[1];
+        const bool bzl = p.bnd_lo[2], bzh = p.bnd_hi[2];
+        uk = d0b(U, o, 1, hx, ihx, c8, i, p.nx, bxl, bxh); ui = d0b(U, o, p.ys, hy, ihy, c8, j, p.ny, byl, byh);
+        us = d0b(U, o, p.zs, hz, ihz, c8, k, p.nz, bzl, bzh);
+        vk = d0b(V, o, 1, hx, ihx, c8, i, p.nx, bxl, bxh); vi = d0b(V, o, p.ys, hy, ihy, c8, j, p.ny, byl, byh);
+        vs = d0b(V, o, p.zs, hz, ihz, c8, k, p.nz, bzl, bzh);
+        wk = d0b(W, o, 1, hx, ihx, c8, i, p.nx, bxl, bxh); wi = d0b(W, o, p.ys, hy, ihy, c8, j, p.ny, byl, byh);
+        ws = d0b(W, o, p.zs, hz, ihz, c8, k, p.nz, bzl, bzh);
+        Tk = d0b(TT, o, 1, hx, ihx, c8, i, p.nx, bxl, bxh); Ti = d0b(TT, o, p.ys, hy, ihy, c8, j, p.ny, byl, byh);
+        Ts = d0b(TT, o, p.zs, hz, ihz, c8, k, p.nz, bzl, bzh);
     }
-    double ux = uk*Akx + ui*Aix + us*Asx;
-    double vx = vk*Akx + vi*Aix + vs*Asx;
-    double wx = wk*Akx + wi*Aix + ws*Asx;
-    double uy = uk*Aky + ui*Aiy + us*Asy;
-    double vy = vk*Aky + vi*Aiy + vs*Asy;
-    double wy = wk*Aky + wi*Aiy + ws*Asy;
-    double uz = uk*Akz + ui*Aiz + us*Asz;
-    double vz = vk*Akz + vi*Aiz + vs*Asz;
-    double wz = wk*Akz + wi*Aiz + ws*Asz;
-    double div = ux + vy + wz;
-    double s11 = (2.0*ux - 2.0/3.0*div) * Amu;
-    double s22 = (2.0*vy - 2.0/3.0*div) * Amu;
-    double s33 = (2.0*wz - 2.0/3.0*div) * Amu;
-    double s12 = (uy + vx) * Amu;
-    double s13 = (uz + wx) * Amu;
-    double s23 = (vz + wy) * Amu;
-    double uu = p.prim[1][o], vv = p.prim[2][o], ww = p.prim[3][o];
-    double Amuk = Amu * p.vis_c;
-    double Tx = Tk*Akx + Ti*Aix + Ts*Asx;
-    double Ty = Tk*Aky + Ti*Aiy + Ts*Asy;
-    double Tz = Tk*Akz + Ti*Aiz + Ts*Asz;
-    double E1 = uu*s11 + vv*s12 + ww*s13 + Amuk*Tx;
-    double E2 = uu*s12 + vv*s22 + ww*s23 + Amuk*Ty;
-    double E3 = uu*s13 + vv*s23 + ww*s33 + Amuk*Tz;
-    double Aj1 = metric<UNI>(p, M_AJAC, o);
+    R ux = uk*Akx + ui*Aix + us*Asx;
+    R vx = vk*Akx + vi*Aix + vs*Asx;
+    R wx = wk*Akx + wi*Aix + ws*Asx;
+    R uy = uk*Aky + ui*Aiy + us*Asy;
+    R vy = vk*Aky + vi*Aiy + vs*Asy;
+    R wy = wk*Aky + wi*Aiy + ws*Asy;
+    R uz = uk*Akz + ui*Aiz + us*Asz;
+    R vz = vk*Akz + vi*Aiz + vs*Asz;
+    R wz = wk*Akz + wi*Aiz + ws*Asz;
+    R div = ux + vy + wz;
+    R s11 = ((R)2.0*ux - (R)(2.0/3.0)*div) * Amu;
+    R s22 = ((R)2.0*vy - (R)(2.0/3.0)*div) * Amu;
+    R s33 = ((R)2.0*wz - (R)(2.0/3.0)*div) * Amu;
+    R s12 = (uy + vx) * Amu;
+    R s13 = (uz + wx) * Amu;
+    R s23 = (vz + wy) * Amu;
+    R uu = U[o], vv = V[o], ww = W[o];
+    R Amuk = Amu * (R)p.vis_c;
+    R Tx = Tk*Akx + Ti*Aix + Ts*Asx;
+    R Ty = Tk*Aky + Ti*Aiy + Ts*Asy;
+    R Tz = Tk*Akz + Ti*Aiz + Ts*Asz;
+    R E1 = uu*s11 + vv*s12 + ww*s13 + Amuk*Tx;
+    R E2 = uu*s12 + vv*s22 + ww*s23 + Amuk*Ty;
+    R E3 = uu*s13 + vv*s23 + ww*s33 + Amuk*Tz;
+    R Aj1 = (R)metric<UNI>(p, M_AJAC, o);
+    R *const evb = ev_r<R>(p);
 #pragma unroll
     for (int dd = 0; dd < 3; dd++) {
-        double akx = metric<UNI>(p, M_AKX + 3 * dd, o) * Aj1;
-        double aky = metric<UNI>(p, M_AKX + 3 * dd + 1, o) * Aj1;
-        double akz = metric<UNI>(p, M_AKX + 3 * dd + 2, o) * Aj1;
-        double *ev = p.ev + (long long)(4 * dd) * p.lapN;
+        R akx = (R)metric<UNI>(p, M_AKX + 3 * dd, o) * Aj1;
+        R aky = (R)metric<UNI>(p, M_AKX + 3 * dd + 1, o) * Aj1;
+        R akz = (R)metric<UNI>(p, M_AKX + 3 * dd + 2, o) * Aj1;
+        R *ev = evb + (long long)(4 * dd) * p.lapN;
         ev[o]              = (akx*s11 + aky*s12 + akz*s13);
         ev[p.lapN + o]     = (akx*s12 + aky*s22 + akz*s23);
         ev[2 * p.lapN + o] = (akx*s13 + aky*s23 + akz*s33);
@@ -497,7 +503,12 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
     }
     double d1, u1, v1, w1, T2;
     cons_to_prim(p, f, d1, u1, v1, w1, T2);
-    p.prim[0][o] = d1; p.prim[1][o] = u1; p.prim[2][o] = v1; p.prim[3][o] = w1; p.prim[4][o] = T2;
+    if (p.mixed) {      // the stencils of the precision form read FP32 primitives
+        p.prim32[0][o] = (float)d1; p.prim32[1][o] = (float)u1; p.prim32[2][o] = (float)v1;
+        p.prim32[3][o] = (float)w1; p.prim32[4][o] = (float)T2;
+    } else {
+        p.prim[0][o] = d1; p.prim[1][o] = u1; p.prim[2][o] = v1; p.prim[3][o] = w1; p.prim[4][o] = T2;
+    }
     // cons_to_pri_kernel also leaves the pressure (src/commen_kernel.cu:107),
     // which the filter after the step reads
     if (krk == 3 && p.pfil) p.pfil[o] = T2 * d1 / (p.Gamma * p.Ama * p.Ama);
@@ -519,7 +530,7 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
 // (du_viscous_Jacobian3d_{x,y,z}_final + YF_Pe_XF, src/commen_kernel.cu:158-169).
 // RK = true: the stage's du is complete here, so the RK update, cons->prim
 // and the face re-projection follow in the same thread and du is not stored.
-template <bool UNI, bool RK>
+template <bool UNI, bool RK, typename R>
 __global__ void __launch_bounds__(256, 5) k_vis_div(Params p, int krk) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= p.N) return;
@@ -527,30 +538,36 @@ __global__ void __launch_bounds__(256, 5) k_vis_div(Params p, int krk) {
     int j = (int)(r % p.ny); int k = (int)(r / p.ny);
     long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     const long long st[3] = { 1LL, p.ys, p.zs };
-    const double hh[3] = { p.hx, p.hy, p.hz };
+    const R hh[3] = { (R)p.hx, (R)p.hy, (R)p.hz };
+    const R ihh[3] = { (R)p.inv_h[0], (R)p.inv_h[1], (R)p.inv_h[2] };
     const bool c8 = p.scheme_vis == 204;
-    double ajac = metric<UNI>(p, M_AJAC, o);
-    double acc[5];
+    const R ajac = (R)metric<UNI>(p, M_AJAC, o);
+    R *const du = du_r<R>(p);
+    const R *const evb = ev_r<R>(p);
+    R acc[5];
 #pragma unroll
-    for (int m = 0; m < 5; m++) acc[m] = (RK || m > 0) ? p.du[m * p.N + tid] : 0.0;
+    for (int m = 0; m < 5; m++) acc[m] = (RK || m > 0) ? du[m * p.N + tid] : (R)0.0;
 #pragma unroll
     for (int dd = 0; dd < 3; dd++) {
 #pragma unroll
         for (int m = 0; m < 4; m++) {
-            const double *f = p.ev + (long long)(4 * dd + m) * p.lapN;
+            const R *f = evb + (long long)(4 * dd + m) * p.lapN;
             if (!p.has_bnd) {
-                acc[m + 1] += ajac * d0(f, o, st[dd], hh[dd], p.inv_h[dd], c8);
+                acc[m + 1] += ajac * d0(f, o, st[dd], hh[dd], ihh[dd], c8);
             } else {
                 const int X = dd == 0 ? i : (dd == 1 ? j : k), n = dd == 0 ? p.nx : (dd == 1 ? p.ny : p.nz);
-                acc[m + 1] += ajac * d0b(f, o, st[dd], hh[dd], p.inv_h[dd], c8, X, n, p.bnd_lo[dd], p.bnd_hi[dd]);
+                acc[m + 1] += ajac * d0b(f, o, st[dd], hh[dd], ihh[dd], c8, X, n, p.bnd_lo[dd], p.bnd_hi[dd]);
             }
         }
     }
     if (RK) {
-        rk_cell(p, krk, tid, i, j, k, acc);
+        double a64[5];
+#pragma unroll
+        for (int m = 0; m < 5; m++) a64[m] = (double)acc[m];
+        rk_cell(p, krk, tid, i, j, k, a64);
     } else {
 #pragma unroll
-        for (int m = 0; m < 4; m++) p.du[(m + 1) * p.N + tid] = acc[m + 1];
+        for (int m = 0; m < 4; m++) du[(m + 1) * p.N + tid] = acc[m + 1];
     }
 }
 
@@ -562,7 +579,7 @@ __global__ void k_rk_update(Params p, int krk) {
     int j = (int)(r % p.ny); int k = (int)(r / p.ny);
     double du[5];
 #pragma unroll
-    for (int m = 0; m < 5; m++) du[m] = p.du[m * p.N + tid];
+    for (int m = 0; m < 5; m++) du[m] = p.mixed ? (double)p.du32[m * p.N + tid] : p.du[m * p.N + tid];
     rk_cell(p, krk, tid, i, j, k, du);
 }
 
@@ -648,6 +665,15 @@ __global__ void k_gather_interior(Params p, const double *src_lap, double *dst) 
     int j = (int)(r % p.ny); int k = (int)(r / p.ny);
     dst[tid] = src_lap[lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP)];
 }
+// the FP32 primitives of the precision form from the FP64 ones (whole LAP box)
+__global__ void k_prims_to_fp32(Params p) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= 5 * p.lapN) return;
+    const int m = (int)(tid / p.lapN);
+    const long long q = tid - (long long)m * p.lapN;
+    p.prim32[m][q] = (float)p.prim[m][q];
+}
+
 __global__ void k_fill(double *f, long long n, double v) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid < n) f[tid] = v;
@@ -685,17 +711,25 @@ cudaError_t launch_sensor(const Params &p, cudaStream_t st) {
         cudaError_t e = cudaMemsetAsync(p.flag_count, 0, 3 * sizeof(unsigned), st);
         if (e != cudaSuccess) return e;
     }
-    k_sensor<<<blocks_for(n, 256), 256, 0, st>>>(p);
+    if (p.mixed) k_sensor<float><<<blocks_for(n, 256), 256, 0, st>>>(p);
+    else         k_sensor<double><<<blocks_for(n, 256), 256, 0, st>>>(p);
     return cudaGetLastError();
 }
 
-cudaError_t launch_ghost(const Params &p, double *const *fields, const int *dirmask, int nf, cudaStream_t st) {
-    GhostList g;
+template <typename T>
+static cudaError_t launch_ghost_t(const Params &p, T *const *fields, const int *dirmask, int nf, cudaStream_t st) {
+    GhostList<T> g;
     g.n = nf;
     for (int i = 0; i < nf; i++) { g.f[i] = fields[i]; g.dirmask[i] = dirmask[i]; }
     long long per = 2LL * OCFD_LAP * ((long long)p.ny * p.nz + (long long)p.nx * p.nz + (long long)p.nx * p.ny);
-    k_ghost<<<blocks_for(per * nf, 256), 256, 0, st>>>(p, g);
+    k_ghost<T><<<blocks_for(per * nf, 256), 256, 0, st>>>(p, g);
     return cudaGetLastError();
+}
+cudaError_t launch_ghost(const Params &p, double *const *fields, const int *dirmask, int nf, cudaStream_t st) {
+    return launch_ghost_t<double>(p, fields, dirmask, nf, st);
+}
+cudaError_t launch_ghost32(const Params &p, float *const *fields, const int *dirmask, int nf, cudaStream_t st) {
+    return launch_ghost_t<float>(p, fields, dirmask, nf, st);
 }
 
 template <bool UNI>
@@ -709,26 +743,33 @@ cudaError_t launch_sweeps(const Params &p, cudaStream_t st) {
     return p.uniform_metrics ? launch_sweeps_t<true>(p, st) : launch_sweeps_t<false>(p, st);
 }
 
-// krk = 0: viscous terms into du; krk = 1..3: viscous terms, then the RK
-// stage update in the same kernel (du is not written)
-cudaError_t launch_viscous(const Params &p, int krk, cudaStream_t st) {
+template <typename R>
+static cudaError_t launch_viscous_t(const Params &p, int krk, cudaStream_t st) {
     unsigned nb = blocks_for(p.N, 256);
-    if (p.uniform_metrics) k_vis_ev<true><<<nb, 256, 0, st>>>(p);
-    else                   k_vis_ev<false><<<nb, 256, 0, st>>>(p);
-    double *evf[12]; int mask[12];
+    if (p.uniform_metrics) k_vis_ev<true, R><<<nb, 256, 0, st>>>(p);
+    else                   k_vis_ev<false, R><<<nb, 256, 0, st>>>(p);
+    R *evf[12]; int mask[12];
+    R *evb = sizeof(R) == 8 ? (R *)p.ev : (R *)p.ev32;
     for (int dd = 0; dd < 3; dd++)
-        for (int m = 0; m < 4; m++) { evf[4 * dd + m] = p.ev + (long long)(4 * dd + m) * p.lapN; mask[4 * dd + m] = 1 << dd; }
+        for (int m = 0; m < 4; m++) { evf[4 * dd + m] = evb + (long long)(4 * dd + m) * p.lapN; mask[4 * dd + m] = 1 << dd; }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if ((e = launch_ghost(p, evf, mask, 12, st)) != cudaSuccess) return e;
+    if ((e = launch_ghost_t<R>(p, evf, mask, 12, st)) != cudaSuccess) return e;
     if (krk == 0) {
-        if (p.uniform_metrics) k_vis_div<true, false><<<nb, 256, 0, st>>>(p, 0);
-        else                   k_vis_div<false, false><<<nb, 256, 0, st>>>(p, 0);
+        if (p.uniform_metrics) k_vis_div<true, false, R><<<nb, 256, 0, st>>>(p, 0);
+        else                   k_vis_div<false, false, R><<<nb, 256, 0, st>>>(p, 0);
     } else {
-        if (p.uniform_metrics) k_vis_div<true, true><<<nb, 256, 0, st>>>(p, krk);
-        else                   k_vis_div<false, true><<<nb, 256, 0, st>>>(p, krk);
+        if (p.uniform_metrics) k_vis_div<true, true, R><<<nb, 256, 0, st>>>(p, krk);
+        else                   k_vis_div<false, true, R><<<nb, 256, 0, st>>>(p, krk);
     }
     return cudaGetLastError();
+}
+
+// krk = 0: viscous terms into du; krk = 1..3: viscous terms, then the RK
+// stage update in the same kernel (du is not written).  FP32 stencils in
+// the precision form.
+cudaError_t launch_viscous(const Params &p, int krk, cudaStream_t st) {
+    return p.mixed ? launch_viscous_t<float>(p, krk, st) : launch_viscous_t<double>(p, krk, st);
 }
 
 cudaError_t launch_rk(const Params &p, int krk, cudaStream_t st) {
@@ -760,6 +801,11 @@ cudaError_t launch_rk_only(const Params &p, int krk, cudaStream_t st) {
     k_rk_only<<<blocks_for(5 * p.N, 256), 256, 0, st>>>(p, krk);
     return cudaGetLastError();
 }
+cudaError_t launch_prims_to_fp32(const Params &p, cudaStream_t st) {
+    k_prims_to_fp32<<<blocks_for(5 * p.lapN, 256), 256, 0, st>>>(p);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_c2p(const Params &p, cudaStream_t st) {
     k_c2p<<<blocks_for(p.N, 256), 256, 0, st>>>(p);
     return cudaGetLastError();

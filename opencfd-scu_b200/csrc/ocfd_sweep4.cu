@@ -28,8 +28,8 @@ using namespace walk;
 enum { K_HYBC = 0, K_W7 = 1 };
 
 // ring value sv of point Q of line col
-template <int RING, int LC>
-__device__ __forceinline__ double rv(const double *ring, int col, int sv, int Q) {
+template <int RING, int LC, typename R>
+__device__ __forceinline__ R rv(const R *ring, int col, int sv, int Q) {
     return ring[(sv * RING + (Q & (RING - 1))) * LC + col];
 }
 
@@ -38,25 +38,25 @@ __device__ __forceinline__ double rv(const double *ring, int col, int sv, int Q)
 // reconstruction (or the boundary closure) and the back-projection, with
 // the operations and order of face_generic.  Point F-3+k is stencil entry k;
 // sign 0 uses entries 0..6, sign 1 entries 1..7.
-template <int S, int RING, int LC>
-__device__ __forceinline__ void char_sign(const double *ring, int col, int F, int n, bool w7, bool near,
-                                          bool lo, bool hi, const double (&rec)[FP_N], double (&out)[10]) {
+template <int S, int RING, int LC, typename R>
+__device__ __forceinline__ void char_sign(const R *ring, int col, int F, int n, bool w7, bool near,
+                                          bool lo, bool hi, const R (&rec)[FP_N], R (&out)[10]) {
     constexpr int K0 = S, K1 = S + 6;
-    double fv[5][8];
+    R fv[5][8];
 #pragma unroll
     for (int m = 0; m < 5; m++)
 #pragma unroll
         for (int k = 0; k < 8; k++)
-            fv[m][k] = (k >= K0 && k <= K1) ? rv<RING, LC>(ring, col, S * 5 + m, F - 3 + k) : 0.0;
-    double o5[5];
+            fv[m][k] = (k >= K0 && k <= K1) ? rv<RING, LC>(ring, col, S * 5 + m, F - 3 + k) : (R)0.0;
+    R o5[5];
 #pragma unroll
     for (int c = 0; c < 5; c++) {
-        double Lr[5], vals[8], Rc[5];
+        R Lr[5], vals[8], Rc[5];
         L_row(rec, 1, c, Lr);
 #pragma unroll
         for (int k = 0; k < 8; k++)
-            vals[k] = (k >= K0 && k <= K1) ? dot5(Lr, fv[0][k], fv[1][k], fv[2][k], fv[3][k], fv[4][k]) : 0.0;
-        double res;
+            vals[k] = (k >= K0 && k <= K1) ? dot5(Lr, fv[0][k], fv[1][k], fv[2][k], fv[3][k], fv[4][k]) : (R)0.0;
+        R res;
         if (!(near && closure(S, lo, hi, S ? 4 : 3, S ? 3 : 4, F, n, vals, res)))
             res = w7 ? (S ? weno7_m(vals) : weno7_p(vals)) : (S ? weno5_m(vals) : weno5_p(vals));
         R_col(rec, 1, c, Rc);
@@ -75,15 +75,15 @@ __device__ __forceinline__ void char_sign(const double *ring, int col, int F, in
 // A face on the flux components with a boundary closure in reach: W7 picks
 // WENO7, else UP7; (KA, KB) are the closure extents of the reference kernel
 // of each sign.
-template <int RING, int LC, bool W7>
-__device__ __forceinline__ void comp_face_closure(const double *ring, int col, int F, int n, bool lo, bool hi,
-                                               int KA0, int KB0, int KA1, int KB1, double *out) {
+template <int RING, int LC, bool W7, typename R>
+__device__ __forceinline__ void comp_face_closure(const R *ring, int col, int F, int n, bool lo, bool hi,
+                                                  int KA0, int KB0, int KA1, int KB1, R *out) {
     for (int sv = 0; sv < 10; sv++) {
         const int sign = sv >= 5;
-        double vals[8];
+        R vals[8];
 #pragma unroll
         for (int k = 0; k < 8; k++) vals[k] = rv<RING, LC>(ring, col, sv, F - 3 + k);
-        double r;
+        R r;
         if (!closure(sign, lo, hi, sign ? KA1 : KA0, sign ? KB1 : KB0, F, n, vals, r)) {
             if (W7) r = sign ? weno7_m(vals) : weno7_p(vals);
             else    r = sign ? up7_m_q(vals) : up7_p_q(vals);
@@ -92,14 +92,14 @@ __device__ __forceinline__ void comp_face_closure(const double *ring, int col, i
     }
 }
 
-template <int RING, int LC>
-__device__ __forceinline__ void face_w7(const double *ring, int col, int F, double (&out)[10]) {
+template <int RING, int LC, typename R>
+__device__ __forceinline__ void face_w7(const R *ring, int col, int F, R (&out)[10]) {
 #pragma unroll
     for (int sv = 0; sv < 10; sv++) {
-        double vals[8];
+        R vals[8];
 #pragma unroll
         for (int k = 0; k < 8; k++)
-            vals[k] = (sv < 5 ? k < 7 : k > 0) ? rv<RING, LC>(ring, col, sv, F - 3 + k) : 0.0;
+            vals[k] = (sv < 5 ? k < 7 : k > 0) ? rv<RING, LC>(ring, col, sv, F - 3 + k) : (R)0.0;
         out[sv] = sv < 5 ? weno7_p(vals) : weno7_m(vals);
     }
 }
@@ -107,13 +107,13 @@ __device__ __forceinline__ void face_w7(const double *ring, int col, int F, doub
 // Flux of face F+1/2 (both signs, all fields) of one lane's line.  Every
 // path is in line: a call here, even on the rare closure faces alone,
 // makes the walk keep its loop state in local memory around it.
-template <int KIND, int RING, int LC, bool UNI>
-__device__ __forceinline__ void face4(const Params &p, int dir, const double *ring, int col, int F, int n,
+template <int KIND, int RING, int LC, bool UNI, typename R>
+__device__ __forceinline__ void face4(const Params &p, int dir, const R *ring, int col, int F, int n,
                                       int hflag, long long o0, long long sd, bool lo, bool hi,
-                                      double (&out)[10]) {
+                                      R (&out)[10]) {
     const bool near = (lo && F <= 3) || (hi && F >= n - 5);
     if (near && (KIND == K_W7 || hflag == 1)) {
-        double tmp[10];
+        R tmp[10];
         if (KIND == K_W7) comp_face_closure<RING, LC, true>(ring, col, F, n, lo, hi, 3, 3, 3, 3, tmp);
         else              comp_face_closure<RING, LC, false>(ring, col, F, n, lo, hi, 3, 4, 4, 3, tmp);
 #pragma unroll
@@ -122,7 +122,7 @@ __device__ __forceinline__ void face4(const Params &p, int dir, const double *ri
     }
     if (KIND == K_W7) { face_w7<RING, LC>(ring, col, F, out); return; }
     if (hflag == 1) { face_up7<RING, LC>(ring, col, F, out); return; }
-    double rec[FP_N];
+    R rec[FP_N];
     face_record<UNI>(p, dir, o0, o0 + sd, rec);
     char_sign<0, RING, LC>(ring, col, F, n, hflag == 2, near, lo, hi, rec, out);
     char_sign<1, RING, LC>(ring, col, F, n, hflag == 2, near, lo, hi, rec, out);
@@ -133,28 +133,28 @@ __device__ __forceinline__ void face4(const Params &p, int dir, const double *ri
 // OCFD_bound_character_kernel_{p,m}, src/OCFD_flux_charteric.cu:16-319):
 // a non-reflecting face adds nothing, the characteristic kernels take a
 // first-order flux difference from the split values at X-1 .. X+2.
-template <int DIR, int KIND, int RING, int LC>
-__device__ __forceinline__ void du_rule_cell(const Params &p, const double *ring, int col, int X, int n,
-                                             double *__restrict__ du, long long ci, double aj, double h,
-                                             double ih, const double (&cur)[10], const double (&prv)[10]) {
+template <int DIR, int KIND, int RING, int LC, typename R, typename D>
+__device__ __forceinline__ void du_rule_cell(const Params &p, const R *ring, int col, int X, int n,
+                                             D *__restrict__ du, long long ci, R aj, R h,
+                                             R ih, const R (&cur)[10], const R (&prv)[10]) {
     constexpr bool char_kernel = KIND == K_HYBC;
     const bool lo = p.bnd_lo[DIR], hi = p.bnd_hi[DIR];
     const bool only_lo = lo && !hi, only_hi = hi && !lo;     // flag 1..6, not 7..9
     const bool first = X == 0, last = X == n - 1;
     const long long N = p.N;
     for (int m = 0; m < 5; m++) {
-        double acc = DIR == 0 ? 0.0 : du[m * N + ci];
+        R acc = DIR == 0 ? (R)0.0 : (R)du[m * N + ci];
         if (!char_kernel ? (first && p.nonref_lo[DIR] == 1) : (only_lo && p.nonref_lo[DIR] == 1 && first)) {
-            acc += 0.0;
+            acc += (R)0.0;
         } else if (char_kernel && ((only_lo && first) || (only_hi && last))) {
-            double tmp;
+            R tmp;
             if (first) {
                 tmp = rv<RING, LC>(ring, col, m, X + 1) - rv<RING, LC>(ring, col, m, X);
             } else {
-                const double f0 = rv<RING, LC>(ring, col, m, X), f1 = rv<RING, LC>(ring, col, m, X - 1);
-                const double f2 = rv<RING, LC>(ring, col, m, X - 2);
-                const double tr = f0 + 0.5 * minmod2(f0 - f1, f0 - f1);
-                const double tl = f1 + 0.5 * minmod2(f0 - f1, f1 - f2);
+                const R f0 = rv<RING, LC>(ring, col, m, X), f1 = rv<RING, LC>(ring, col, m, X - 1);
+                const R f2 = rv<RING, LC>(ring, col, m, X - 2);
+                const R tr = f0 + (R)0.5 * minmod2(f0 - f1, f0 - f1);
+                const R tl = f1 + (R)0.5 * minmod2(f0 - f1, f1 - f2);
                 tmp = tr - tl;
             }
             acc += div_const(-aj * tmp, h, ih);
@@ -164,14 +164,14 @@ __device__ __forceinline__ void du_rule_cell(const Params &p, const double *ring
         // the reference's y kernel tests flag 3 for its lower face, so that
         // first-order flux never applies on y
         if (!char_kernel ? (last && p.nonref_hi[DIR] == 1) : (only_hi && p.nonref_hi[DIR] == 1 && last)) {
-            acc += 0.0;
+            acc += (R)0.0;
         } else if (char_kernel && ((DIR != 1 && only_lo && first) || (only_hi && last))) {
-            double tmp;
+            R tmp;
             if (first) {
-                const double f0 = rv<RING, LC>(ring, col, 5 + m, X), f1 = rv<RING, LC>(ring, col, 5 + m, X + 1);
-                const double f2 = rv<RING, LC>(ring, col, 5 + m, X + 2);
-                const double tr = f1 - 0.5 * minmod2(f2 - f1, f1 - f0);
-                const double tl = f0 - 0.5 * minmod2(f1 - f0, f1 - f0);
+                const R f0 = rv<RING, LC>(ring, col, 5 + m, X), f1 = rv<RING, LC>(ring, col, 5 + m, X + 1);
+                const R f2 = rv<RING, LC>(ring, col, 5 + m, X + 2);
+                const R tr = f1 - (R)0.5 * minmod2(f2 - f1, f1 - f0);
+                const R tl = f0 - (R)0.5 * minmod2(f1 - f0, f1 - f0);
                 tmp = tr - tl;
             } else {
                 tmp = rv<RING, LC>(ring, col, 5 + m, X) - rv<RING, LC>(ring, col, 5 + m, X - 1);
@@ -180,31 +180,34 @@ __device__ __forceinline__ void du_rule_cell(const Params &p, const double *ring
         } else {
             acc += div_const(-aj * (cur[5 + m] - prv[5 + m]), h, ih);
         }
-        du[m * N + ci] = acc;
+        du[m * N + ci] = (D)acc;
     }
 }
 
+// MINB: resident blocks per SM the register budget is fitted to; 3 (168
+// registers, a few spills) runs faster than 2 (no spills) on the
+// characteristic faces.
 // The walk: a warp covers LC lines and LY = 32 / LC consecutive cells of
 // each, LY cells per pass.  Per pass every lane splits one new point into
 // the ring, forms the flux of the face on the right of its cell into the
 // face buffer (FR = 2 LY slots per line, so a pass never overwrites a face
 // that the previous pass's lanes still read), then adds its cell's du with
 // the face on its left from the buffer.
-template <int DIR, bool UNI, bool EPS0, int KIND>
-__global__ void __launch_bounds__(32 * SW, 3) k_sweep4(const __grid_constant__ Params p, int seg_len) {
+template <int DIR, bool UNI, bool EPS0, int KIND, int MINB, typename R>
+__global__ void __launch_bounds__(32 * SW, MINB) k_sweep4(const __grid_constant__ Params p, int seg_len) {
     constexpr int LC = Shape<DIR>::LC, LY = 32 / LC, RING = Shape<DIR>::RING, FR = 2 * LY;
     // the next pass's points overwrite slots this pass reads unless the
     // ring spans both windows
     constexpr bool SYNC2 = 2 * LY + 6 >= RING;
-    extern __shared__ double smem4[];          // per warp: ring, then face buffer
+    extern __shared__ __align__(16) unsigned char smem4[];   // per warp: ring, then face buffer
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int col = lane % LC, ly = lane / LC;
     const long long grp = (long long)blockIdx.x * SW + wid;     // line group of this warp
     const int ngx = (p.nx + LC - 1) / LC;
     const long long ngroups = DIR == 0 ? (long long)p.ny * p.nz : (long long)ngx * (DIR == 1 ? p.nz : p.ny);
     if (grp >= ngroups) return;                                 // the whole warp
-    double *ring = smem4 + (size_t)wid * 10 * (RING + FR) * LC;
-    double *fbuf = ring + 10 * RING * LC;
+    R *ring = reinterpret_cast<R *>(smem4) + (size_t)wid * 10 * (RING + FR) * LC;
+    R *fbuf = ring + 10 * RING * LC;
     const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
     const int y0 = blockIdx.y * seg_len;
     const int y1 = min(n, y0 + seg_len);
@@ -234,15 +237,15 @@ __global__ void __launch_bounds__(32 * SW, 3) k_sweep4(const __grid_constant__ P
             fl = p.flag[2] + (long long)xs + (long long)p.nx * c3; fst = (long long)p.nx * p.ny;
         }
     }
-    double *__restrict__ du = p.du;
+    R *__restrict__ du = du_r<R>(p);
     const long long N = p.N;
     const bool lo = p.bnd_lo[DIR], hi = p.bnd_hi[DIR];
-    const double h = DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz), ih = p.inv_h[DIR];
+    const R h = (R)(DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz)), ih = (R)p.inv_h[DIR];
 
     // points y0-4 .. y0+3 and the face left of cell y0
     for (int r = ly; r < 8; r += LY) {
         if (colok) {
-            double q5[5];
+            R q5[5];
             const long long o = base + (long long)(y0 - 4 + r) * sd;
             load5(p, o, q5);
             ring_put<DIR, RING, LC, UNI, EPS0>(p, ring, col, y0 - 4 + r, o, q5);
@@ -251,7 +254,7 @@ __global__ void __launch_bounds__(32 * SW, 3) k_sweep4(const __grid_constant__ P
     __syncwarp();
     if (ly == 0 && colok) {
         const int hf = KIND == K_HYBC ? (int)fl[(long long)y0 * fst] : 2;
-        double cur[10];
+        R cur[10];
         face4<KIND, RING, LC, UNI>(p, DIR, ring, col, y0 - 1, n, hf, base + (long long)(y0 - 1) * sd, sd, lo, hi, cur);
 #pragma unroll
         for (int sv = 0; sv < 10; sv++) fbuf[(sv * FR + ((y0 - 1) & (FR - 1))) * LC + col] = cur[sv];
@@ -262,14 +265,14 @@ __global__ void __launch_bounds__(32 * SW, 3) k_sweep4(const __grid_constant__ P
         const int F = Y0 + ly;
         const bool valid = colok && F < y1;
         if (colok && P <= y1 + 3) {
-            double q5[5];
+            R q5[5];
             const long long o = base + (long long)P * sd;
             load5(p, o, q5);
             ring_put<DIR, RING, LC, UNI, EPS0>(p, ring, col, P, o, q5);
         }
         const int hflag = (KIND == K_HYBC && valid) ? (int)fl[(long long)(F + 1) * fst] : 2;
         __syncwarp();
-        double cur[10];
+        R cur[10];
         if (valid) {
             face4<KIND, RING, LC, UNI>(p, DIR, ring, col, F, n, hflag, base + (long long)F * sd, sd, lo, hi, cur);
 #pragma unroll
@@ -277,15 +280,15 @@ __global__ void __launch_bounds__(32 * SW, 3) k_sweep4(const __grid_constant__ P
         }
         __syncwarp();
         if (valid) {
-            double prv[10];
+            R prv[10];
 #pragma unroll
             for (int sv = 0; sv < 10; sv++) prv[sv] = fbuf[(sv * FR + ((F - 1) & (FR - 1))) * LC + col];
             const long long ci = cb + (long long)F * cst;
-            const double aj = metric<UNI>(p, M_AJAC, base + (long long)F * sd);
+            const R aj = (R)metric<UNI>(p, M_AJAC, base + (long long)F * sd);
             if (p.has_bnd && rule_cell(p, DIR, F, n)) {
                 du_rule_cell<DIR, KIND, RING, LC>(p, ring, col, F, n, du, ci, aj, h, ih, cur, prv);
             } else {
-                double old[5];
+                R old[5];
                 if (DIR != 0) {
 #pragma unroll
                     for (int m = 0; m < 5; m++) old[m] = du[m * N + ci];
@@ -298,7 +301,7 @@ __global__ void __launch_bounds__(32 * SW, 3) k_sweep4(const __grid_constant__ P
     }
 }
 
-template <int DIR, bool UNI, bool EPS0, int KIND>
+template <int DIR, bool UNI, bool EPS0, int KIND, int MINB, typename R>
 cudaError_t launch_dir4(const Params &p, cudaStream_t st) {
     constexpr int LC = Shape<DIR>::LC, LY = 32 / LC;
     const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
@@ -306,7 +309,7 @@ cudaError_t launch_dir4(const Params &p, cudaStream_t st) {
     const long long groups = DIR == 0 ? (long long)p.ny * p.nz : ngx * (DIR == 1 ? p.nz : p.ny);
     // split lines into segments when there are fewer than about four waves
     // of warps; a segment re-splits 8 points and re-forms one face
-    const long long want = 4LL * 148 * 3 * SW;
+    const long long want = 4LL * 148 * MINB * SW;
     long long nseg = (want + groups - 1) / groups;
     long long maxseg = n / (4 * LY) > 0 ? n / (4 * LY) : 1;
     if (nseg > maxseg) nseg = maxseg;
@@ -315,43 +318,38 @@ cudaError_t launch_dir4(const Params &p, cudaStream_t st) {
     seg_len = (seg_len + LY - 1) / LY * LY;
     nseg = (n + seg_len - 1) / seg_len;
     dim3 grid((unsigned)((groups + SW - 1) / SW), (unsigned)nseg);
-    constexpr int smem = SW * 10 * (Shape<DIR>::RING + 2 * LY) * LC * (int)sizeof(double);
+    constexpr int smem = SW * 10 * (Shape<DIR>::RING + 2 * LY) * LC * (int)sizeof(R);
     static bool attr_set = false;             // above the 48 KB default
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_sweep4<DIR, UNI, EPS0, KIND>,
+        cudaError_t e = cudaFuncSetAttribute(k_sweep4<DIR, UNI, EPS0, KIND, MINB, R>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    k_sweep4<DIR, UNI, EPS0, KIND><<<grid, 32 * SW, smem, st>>>(p, seg_len);
+    k_sweep4<DIR, UNI, EPS0, KIND, MINB, R><<<grid, 32 * SW, smem, st>>>(p, seg_len);
     return cudaGetLastError();
 }
 
-template <bool UNI, bool EPS0, int KIND>
+// FP64: register budget for 3 blocks per SM; FP32 (the precision form): 4
+template <bool UNI, bool EPS0, int KIND, typename R>
 cudaError_t dir4k(const Params &p, int dir, cudaStream_t st) {
-    if (dir == 0) return launch_dir4<0, UNI, EPS0, KIND>(p, st);
-    if (dir == 1) return launch_dir4<1, UNI, EPS0, KIND>(p, st);
-    return launch_dir4<2, UNI, EPS0, KIND>(p, st);
+    constexpr int MINB = sizeof(R) == 8 ? 3 : 4;
+    if (dir == 0) return launch_dir4<0, UNI, EPS0, KIND, MINB, R>(p, st);
+    if (dir == 1) return launch_dir4<1, UNI, EPS0, KIND, MINB, R>(p, st);
+    return launch_dir4<2, UNI, EPS0, KIND, MINB, R>(p, st);
 }
 
-template <bool UNI, bool EPS0, int KIND>
-cudaError_t launch4m(const Params &p, cudaStream_t st) {
-    cudaError_t e;
-    if ((e = dir4k<UNI, EPS0, KIND>(p, 0, st)) != cudaSuccess) return e;
-    if ((e = dir4k<UNI, EPS0, KIND>(p, 1, st)) != cudaSuccess) return e;
-    return dir4k<UNI, EPS0, KIND>(p, 2, st);
-}
-
-template <bool UNI, bool EPS0>
-cudaError_t launch4(const Params &p, cudaStream_t st) {
-    if (p.scheme_invis == 310 && p.charteric) return launch4m<UNI, EPS0, K_HYBC>(p, st);
-    return launch4m<UNI, EPS0, K_W7>(p, st);
-}
-
-template <bool UNI, bool EPS0>
+template <bool UNI, bool EPS0, typename R>
 cudaError_t dir4(const Params &p, int dir, cudaStream_t st) {
-    if (p.scheme_invis == 310 && p.charteric) return dir4k<UNI, EPS0, K_HYBC>(p, dir, st);
-    return dir4k<UNI, EPS0, K_W7>(p, dir, st);
+    if (p.scheme_invis == 310 && p.charteric) return dir4k<UNI, EPS0, K_HYBC, R>(p, dir, st);
+    return dir4k<UNI, EPS0, K_W7, R>(p, dir, st);
+}
+
+template <typename R>
+cudaError_t dir4r(const Params &p, int dir, cudaStream_t st) {
+    if (p.uniform_metrics)
+        return p.epsl_sw == 0.0 ? dir4<true, true, R>(p, dir, st) : dir4<true, false, R>(p, dir, st);
+    return dir4<false, false, R>(p, dir, st);
 }
 
 }  // namespace
@@ -362,19 +360,17 @@ bool sweeps4_supported(const Params &p) {
     return (p.scheme_invis == 310 && p.charteric) || (p.scheme_invis == 303 && !p.charteric);
 }
 
-// one direction of the walk (one kernel)
+// one direction of the walk (one kernel); FP32 in the precision form
 cudaError_t launch_sweep4_dir(const Params &p, int dir, cudaStream_t st) {
     if (!sweeps4_supported(p)) return cudaErrorNotSupported;
-    if (p.uniform_metrics)
-        return p.epsl_sw == 0.0 ? dir4<true, true>(p, dir, st) : dir4<true, false>(p, dir, st);
-    return dir4<false, false>(p, dir, st);
+    return p.mixed ? dir4r<float>(p, dir, st) : dir4r<double>(p, dir, st);
 }
 
 cudaError_t launch_sweeps4(const Params &p, cudaStream_t st) {
-    if (!sweeps4_supported(p)) return cudaErrorNotSupported;
-    if (p.uniform_metrics)
-        return p.epsl_sw == 0.0 ? launch4<true, true>(p, st) : launch4<true, false>(p, st);
-    return launch4<false, false>(p, st);
+    cudaError_t e;
+    for (int d = 0; d < 3; d++)
+        if ((e = launch_sweep4_dir(p, d, st)) != cudaSuccess) return e;
+    return cudaSuccess;
 }
 
 }  // namespace ocfd

@@ -3,7 +3,7 @@
 // shared memory, the face record, the UP7 face, the boundary tests and the
 // du update of one cell.
 #pragma once
-#include "ocfd_face.cuh"
+#include "ocfd_fp32.cuh"
 
 namespace ocfd {
 namespace walk {
@@ -18,48 +18,49 @@ struct Win {
     __device__ __forceinline__ double at(int sv, int k) const { return b[((s0 + k) & mask) * ks + sv * vs]; }
 };
 
-// Steger-Warming split of LAP point o along direction DIR into fp/fm
-template <int DIR, bool UNI, bool EPS0>
-__device__ __forceinline__ void split_point(const Params &p, long long o, double d, double u, double v,
-                                            double w, double T, double *fp, double *fm) {
-    double cc = div_const(sqrt(T), p.Ama, p.inv_Ama);
+// Steger-Warming split of LAP point o along direction DIR into fp/fm, in
+// the precision R of the primitives given
+template <int DIR, bool UNI, bool EPS0, typename R>
+__device__ __forceinline__ void split_point(const Params &p, long long o, R d, R u, R v,
+                                            R w, R T, R *fp, R *fm) {
+    R cc = div_const(sqrt_r(T), (R)p.Ama, (R)p.inv_Ama);
     if constexpr (UNI) {
         const DirConst &dc = p.dc[DIR];
-        sw_split_pre<EPS0>(d * p.tmp0, u, v, w, cc, dc.A[0], dc.A[1], dc.A[2], dc.ss,
-                           dc.An[0], dc.An[1], dc.An[2], p, fp, fm);
+        sw_split_pre<EPS0>(d * (R)p.tmp0, u, v, w, cc, (R)dc.A[0], (R)dc.A[1], (R)dc.A[2], (R)dc.ss,
+                           (R)dc.An[0], (R)dc.An[1], (R)dc.An[2], p, fp, fm);
     } else {
         const int mA = M_AKX + 3 * DIR;
-        sw_split(d * p.tmp0, u, v, w, cc, p.met[mA][o], p.met[mA + 1][o], p.met[mA + 2][o], p.Gamma,
-                 p.epsl_sw, p.split_C1, p.split_C3, fp, fm);
+        sw_split(d * (R)p.tmp0, u, v, w, cc, (R)p.met[mA][o], (R)p.met[mA + 1][o], (R)p.met[mA + 2][o],
+                 (R)p.Gamma, (R)p.epsl_sw, (R)p.split_C1, (R)p.split_C3, fp, fm);
     }
 }
 
 // characteristic face record between LAP cells o0 and o1 (get_para_charteric_*,
 // src/OCFD_flux_charteric.cu:330-418)
-template <bool UNI>
-__device__ __forceinline__ void face_record(const Params &p, int dir, long long o0, long long o1, double *rec) {
-    const double *u = p.prim[1], *v = p.prim[2], *w = p.prim[3], *T = p.prim[4];
-    double c0v = div_const(sqrt(T[o0]), p.Ama, p.inv_Ama);
-    double c1v = div_const(sqrt(T[o1]), p.Ama, p.inv_Ama);
-    double u1 = (u[o0] + u[o1]) * 0.5, v1 = (v[o0] + v[o1]) * 0.5, w1 = (w[o0] + w[o1]) * 0.5;
-    double c1 = (c0v + c1v) * 0.5;
+template <bool UNI, typename R>
+__device__ __forceinline__ void face_record(const Params &p, int dir, long long o0, long long o1, R *rec) {
+    const R *u = prim_r<R>(p, 1), *v = prim_r<R>(p, 2), *w = prim_r<R>(p, 3), *T = prim_r<R>(p, 4);
+    R c0v = div_const(sqrt_r(T[o0]), (R)p.Ama, (R)p.inv_Ama);
+    R c1v = div_const(sqrt_r(T[o1]), (R)p.Ama, (R)p.inv_Ama);
+    R u1 = (u[o0] + u[o1]) * (R)0.5, v1 = (v[o0] + v[o1]) * (R)0.5, w1 = (w[o0] + w[o1]) * (R)0.5;
+    R c1 = (c0v + c1v) * (R)0.5;
     if (UNI) {
         const DirConst &dc = p.dc[dir];
-        double KK = (p.Gamma - 1.0) / (c1 * c1);
+        R KK = ((R)p.Gamma - (R)1.0) / (c1 * c1);
         rec[FU] = u1; rec[FV] = v1; rec[FW] = w1; rec[FC] = c1; rec[FKK] = KK;
-        rec[FX1] = 1.0 / (2.0 * c1);
-        double v2 = (u1 * u1 + v1 * v1 + w1 * w1) * 0.5;
+        rec[FX1] = (R)1.0 / ((R)2.0 * c1);
+        R v2 = (u1 * u1 + v1 * v1 + w1 * w1) * (R)0.5;
         rec[FV2] = v2;
-        rec[FUN] = u1 * dc.n[0] + v1 * dc.n[1] + w1 * dc.n[2];
-        rec[FH] = v2 + 1.0 / KK;
-        rec[FN1] = dc.n[0]; rec[FN2] = dc.n[1]; rec[FN3] = dc.n[2];
-        rec[FL1] = dc.l[0]; rec[FL2] = dc.l[1]; rec[FL3] = dc.l[2];
-        rec[FM1] = dc.m[0]; rec[FM2] = dc.m[1]; rec[FM3] = dc.m[2];
+        rec[FUN] = u1 * (R)dc.n[0] + v1 * (R)dc.n[1] + w1 * (R)dc.n[2];
+        rec[FH] = v2 + (R)1.0 / KK;
+        rec[FN1] = (R)dc.n[0]; rec[FN2] = (R)dc.n[1]; rec[FN3] = (R)dc.n[2];
+        rec[FL1] = (R)dc.l[0]; rec[FL2] = (R)dc.l[1]; rec[FL3] = (R)dc.l[2];
+        rec[FM1] = (R)dc.m[0]; rec[FM2] = (R)dc.m[1]; rec[FM3] = (R)dc.m[2];
     } else {
         const int mA = M_AKX + 3 * dir;
-        make_record(u1, v1, w1, c1, (p.met[mA][o0] + p.met[mA][o1]) * 0.5,
-                    (p.met[mA + 1][o0] + p.met[mA + 1][o1]) * 0.5,
-                    (p.met[mA + 2][o0] + p.met[mA + 2][o1]) * 0.5, p, rec, 1);
+        make_record(u1, v1, w1, c1, (R)((p.met[mA][o0] + p.met[mA][o1]) * 0.5),
+                    (R)((p.met[mA + 1][o0] + p.met[mA + 1][o1]) * 0.5),
+                    (R)((p.met[mA + 2][o0] + p.met[mA + 2][o1]) * 0.5), p, rec, 1);
     }
 }
 
@@ -152,16 +153,16 @@ __device__ __forceinline__ bool up7_face(const Params &p, int hflag) {
 
 // du of one cell from the face fluxes on its right (cur) and left (prv):
 // x+ then x- for every field, as the reference's single-writer order
-template <bool FIRST>
-__device__ __forceinline__ void add_du(double *__restrict__ du, long long N, long long ci, double aj,
-                                       double h, double ih, const double *cur, const double *prv,
-                                       const double *old) {
+// (R: precision of the fluxes and of du; D: the storage of du)
+template <bool FIRST, typename R, typename D>
+__device__ __forceinline__ void add_du(D *__restrict__ du, long long N, long long ci, R aj,
+                                       R h, R ih, const R *cur, const R *prv, const D *old) {
 #pragma unroll
     for (int m = 0; m < 5; m++) {
-        double acc = FIRST ? 0.0 : old[m];
+        R acc = FIRST ? (R)0.0 : (R)old[m];
         acc += div_const(-aj * (cur[m] - prv[m]), h, ih);
         acc += div_const(-aj * (cur[5 + m] - prv[5 + m]), h, ih);
-        du[m * N + ci] = acc;
+        du[m * N + ci] = (D)acc;
     }
 }
 
@@ -183,11 +184,11 @@ template <> struct Shape<1> { static constexpr int LC = 8, RING = 16; };
 template <> struct Shape<2> { static constexpr int LC = 8, RING = 16; };
 
 // UP7 flux of face F+1/2 (both signs, all fields) from the ring
-template <int RING, int LC>
-__device__ __forceinline__ void face_up7(const double *ring, int col, int F, double (&out)[10]) {
+template <int RING, int LC, typename R>
+__device__ __forceinline__ void face_up7(const R *ring, int col, int F, R (&out)[10]) {
 #pragma unroll
     for (int sv = 0; sv < 10; sv++) {
-        double vals[8];
+        R vals[8];
 #pragma unroll
         for (int t = 0; t < 8; t++) vals[t] = ring[(sv * RING + ((F - 3 + t) & (RING - 1))) * LC + col];
         out[sv] = sv < 5 ? up7_p_q(vals) : up7_m_q(vals);
@@ -196,10 +197,10 @@ __device__ __forceinline__ void face_up7(const double *ring, int col, int F, dou
 
 
 // split of one point (primitives q5, LAP offset o) into ring slot P
-template <int DIR, int RING, int LC, bool UNI, bool EPS0>
-__device__ __forceinline__ void ring_put(const Params &p, double *ring, int col, int P, long long o,
-                                         const double (&q5)[5]) {
-    double fp[5], fm[5];
+template <int DIR, int RING, int LC, bool UNI, bool EPS0, typename R>
+__device__ __forceinline__ void ring_put(const Params &p, R *ring, int col, int P, long long o,
+                                         const R (&q5)[5]) {
+    R fp[5], fm[5];
     split_point<DIR, UNI, EPS0>(p, o, q5[0], q5[1], q5[2], q5[3], q5[4], fp, fm);
     const int q = P & (RING - 1);
 #pragma unroll
@@ -209,9 +210,10 @@ __device__ __forceinline__ void ring_put(const Params &p, double *ring, int col,
     }
 }
 
-__device__ __forceinline__ void load5(const Params &p, long long o, double (&q5)[5]) {
+template <typename R>
+__device__ __forceinline__ void load5(const Params &p, long long o, R (&q5)[5]) {
 #pragma unroll
-    for (int m = 0; m < 5; m++) q5[m] = __ldg(p.prim[m] + o);
+    for (int m = 0; m < 5; m++) q5[m] = __ldg(prim_r<R>(p, m) + o);
 }
 
 }  // namespace walk

@@ -29,7 +29,7 @@ EXPORTED = (
     "ocfd_b200_create", "ocfd_b200_destroy", "ocfd_b200_set_stream", "ocfd_b200_get_stream",
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
     "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics", "ocfd_b200_set_sweep_impl",
-    "ocfd_b200_sweep_walks",
+    "ocfd_b200_sweep_walks", "ocfd_b200_set_precision",
     "ocfd_b200_set_mesh", "ocfd_b200_set_mesh_device", "ocfd_b200_get_metrics",
     "ocfd_b200_set_filter", "ocfd_b200_filtering", "ocfd_b200_set_time", "filtering", "ocfd_b200_set_bc",
     "ocfd_b200_set_primitives", "ocfd_b200_set_primitives_device", "ocfd_b200_step",
@@ -116,6 +116,7 @@ def load(path: Optional[str] = None):
         "ocfd_b200_uniform_metrics": (ctypes.c_int, [P]),
         "ocfd_b200_set_sweep_impl": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_sweep_walks": (ctypes.c_int, [P]),
+        "ocfd_b200_set_precision": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_set_primitives": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_double]),
         "ocfd_b200_set_primitives_device": (ctypes.c_int, [P, P, ctypes.c_int, ctypes.c_double]),
         "ocfd_b200_step": (ctypes.c_int, [P, ctypes.c_int]),
@@ -251,6 +252,10 @@ class Solver:
 
     def set_sweep_impl(self, impl: int):
         self._check(self.L.ocfd_b200_set_sweep_impl(self.h, impl), "set_sweep_impl")
+
+    def set_precision(self, form: int):
+        """0: FP64 throughout; 1: FP32 stencils with FP64 RK3 accumulation."""
+        self._check(self.L.ocfd_b200_set_precision(self.h, form), "set_precision")
 
     def sweep_walks(self) -> int:
         """Bit d set: direction d takes the walk that forms every face in line."""
