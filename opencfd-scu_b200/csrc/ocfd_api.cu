@@ -414,7 +414,7 @@ static int sweeps_auto(ocfd_b200_ctx *ctx) {
     const Params &p = ctx->p;
     const bool hyb = p.scheme_invis == 310;
     int w[3];
-    for (int d = 0; d < 3; d++) w[d] = (hyb && !p.mixed) ? ctx->walk4[d] : 1;
+    for (int d = 0; d < 3; d++) w[d] = (hyb && p.sweep_impl != 6) ? ctx->walk4[d] : 1;
     if ((!w[0] || !w[1] || !w[2]) && ocfd::sweeps3_defers(p))
         CK(cudaMemsetAsync(p.defer_count, 0, 3 * sizeof(unsigned), ctx->stream), "deferred counters");
     for (int d = 0; d < 3; d++) {
@@ -435,7 +435,7 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
         TimerScope ts(ctx, T_SENSOR);
         CK(ocfd::launch_sensor(p, ctx->stream), "sensor");
         ctx->launches += 1;
-        if (p.sweep_impl == 4 && !p.mixed && ocfd::sweeps4_supported(p) && p.flag_count) {
+        if ((p.sweep_impl == 4 || p.mixed) && ocfd::sweeps4_supported(p) && p.flag_count) {
             // the choice follows this pass's flags: one small read-back per step
             CK(cudaMemcpyAsync(ctx->h_flag_count, p.flag_count, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost,
                                ctx->stream), "flag counts");

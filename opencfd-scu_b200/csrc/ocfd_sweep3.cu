@@ -15,6 +15,8 @@
 
 namespace ocfd {
 
+cudaError_t launch_sweep4_fix(const Params &p, int dir, cudaStream_t st);
+
 namespace {
 
 using namespace walk;
@@ -42,20 +44,21 @@ __device__ __forceinline__ void face_flux(const Params &p, int dir, const double
 // its live values in registers.
 // MINB: resident blocks per SM the register budget is fitted to (5: 96
 // registers; 4: 128).
-template <int DIR, bool UNI, bool EPS0, int MINB, bool FAST>
+template <int DIR, bool UNI, bool EPS0, int MINB, bool FAST, typename R = double>
 __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant__ Params p, int seg_len) {
     constexpr int LC = Shape<DIR>::LC, LY = 32 / LC, RING = Shape<DIR>::RING;
     // the next pass's points overwrite slots this pass reads unless the
     // ring spans both windows
     constexpr bool SYNC2 = 2 * LY + 6 >= RING;
-    __shared__ double ring_all[SW][10 * RING * LC];
+    static_assert(FAST || sizeof(R) == 8, "the in-loop dispatch is FP64 only");
+    __shared__ R ring_all[SW][10 * RING * LC];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int col = lane % LC, ly = lane / LC;
     const long long grp = (long long)blockIdx.x * SW + wid;     // line group of this warp
     const int ngx = (p.nx + LC - 1) / LC;
     const long long ngroups = DIR == 0 ? (long long)p.ny * p.nz : (long long)ngx * (DIR == 1 ? p.nz : p.ny);
     if (grp >= ngroups) return;                                 // the whole warp
-    double *ring = ring_all[wid];
+    R *ring = ring_all[wid];
     const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
     const int y0 = blockIdx.y * seg_len;
     const int y1 = min(n, y0 + seg_len);
@@ -85,24 +88,24 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
             fl = p.flag[2] + (long long)xs + (long long)p.nx * c3; fst = (long long)p.nx * p.ny;
         }
     }
-    double *__restrict__ du = p.du;
+    R *__restrict__ du = du_r<R>(p);
     const long long N = p.N;
     const bool hybrid = p.scheme_invis == 310;
-    const double h = DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz), ih = p.inv_h[DIR];
+    const R h = (R)(DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz)), ih = (R)p.inv_h[DIR];
 
     // points y0-4 .. y0+3 and the face left of cell y0
     for (int r = ly; r < 8; r += LY) {
         if (colok) {
-            double q5[5];
+            R q5[5];
             const long long o = base + (long long)(y0 - 4 + r) * sd;
             load5(p, o, q5);
             ring_put<DIR, RING, LC, UNI, EPS0>(p, ring, col, y0 - 4 + r, o, q5);
         }
     }
     __syncwarp();
-    double carry[10], cur[10];
+    R carry[10], cur[10];
 #pragma unroll
-    for (int m = 0; m < 10; m++) cur[m] = 0.0;
+    for (int m = 0; m < 10; m++) cur[m] = (R)0.0;
     int slow = 0, carry_slow = 0;
     if (ly == 0 && colok) {
         const int hf = hybrid ? (int)fl[(long long)y0 * fst] : 2;
@@ -110,7 +113,8 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
             slow = !up7_face(p, hf) || near_closure(p, DIR, y0 - 1, n);
             if (!slow) face_up7<RING, LC>(ring, col, y0 - 1, cur);
         } else {
-            face_flux<RING, LC, UNI>(p, DIR, ring, col, y0 - 1, n, hf, base + (long long)(y0 - 1) * sd, sd, cur);
+            if constexpr (sizeof(R) == 8)
+                face_flux<RING, LC, UNI>(p, DIR, ring, col, y0 - 1, n, hf, base + (long long)(y0 - 1) * sd, sd, cur);
         }
     }
 #pragma unroll
@@ -119,7 +123,7 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
 
     // the primitives of this lane's next point and the flag of its next
     // face are loaded one pass ahead
-    double nq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    R nq[5] = {(R)0.0, (R)0.0, (R)0.0, (R)0.0, (R)0.0};
     int nflag = 2;
     if (colok && y0 + 4 + ly <= y1 + 3) load5(p, base + (long long)(y0 + 4 + ly) * sd, nq);
     if (hybrid && colok && y0 + ly < y1) nflag = fl[(long long)(y0 + ly + 1) * fst];
@@ -134,7 +138,7 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
         if (hybrid && colok && F + LY < y1) nflag = fl[(long long)(F + LY + 1) * fst];
         __syncwarp();
         const long long ci = cb + (long long)F * cst;
-        double old[5];
+        R old[5];
         if (DIR != 0 && valid) {
 #pragma unroll
             for (int m = 0; m < 5; m++) old[m] = du[m * N + ci];
@@ -143,12 +147,13 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
             slow = valid && (!up7_face(p, hflag) || near_closure(p, DIR, F, n));
             if (valid && !slow) face_up7<RING, LC>(ring, col, F, cur);
         } else {
-            if (valid) face_flux<RING, LC, UNI>(p, DIR, ring, col, F, n, hflag, base + (long long)F * sd, sd, cur);
+            if constexpr (sizeof(R) == 8)
+                if (valid) face_flux<RING, LC, UNI>(p, DIR, ring, col, F, n, hflag, base + (long long)F * sd, sd, cur);
         }
-        double prv[10];
+        R prv[10];
 #pragma unroll
         for (int m = 0; m < 10; m++) {
-            double t = __shfl_up_sync(FULL, cur[m], LC);
+            R t = __shfl_up_sync(FULL, cur[m], LC);
             prv[m] = ly == 0 ? carry[m] : t;
             carry[m] = __shfl_sync(FULL, cur[m], (LY - 1) * LC + col);
         }
@@ -172,7 +177,7 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
             }
         }
         if (valid && !defer) {
-            double aj = metric<UNI>(p, M_AJAC, base + (long long)F * sd);
+            R aj = (R)metric<UNI>(p, M_AJAC, base + (long long)F * sd);
             if (DIR == 0) add_du<true>(du, N, ci, aj, h, ih, cur, prv, old);
             else          add_du<false>(du, N, ci, aj, h, ih, cur, prv, old);
         }
@@ -284,7 +289,7 @@ __global__ void __launch_bounds__(128) k_sweep3_fix(const __grid_constant__ Para
     }
 }
 
-template <int DIR, bool UNI, bool EPS0, int MINB, bool FAST>
+template <int DIR, bool UNI, bool EPS0, int MINB, bool FAST, typename R = double>
 cudaError_t launch_dir(const Params &p, cudaStream_t st) {
     constexpr int LC = Shape<DIR>::LC, LY = 32 / LC;
     const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
@@ -301,9 +306,11 @@ cudaError_t launch_dir(const Params &p, cudaStream_t st) {
     seg_len = (seg_len + LY - 1) / LY * LY;
     nseg = (n + seg_len - 1) / seg_len;
     dim3 grid((unsigned)((groups + SW - 1) / SW), (unsigned)nseg);
-    k_sweep3<DIR, UNI, EPS0, MINB, FAST><<<grid, 32 * SW, 0, st>>>(p, seg_len);
+    k_sweep3<DIR, UNI, EPS0, MINB, FAST, R><<<grid, 32 * SW, 0, st>>>(p, seg_len);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !(FAST || p.has_bnd)) return e;
+    // FP32: the fix-up of the precision form (ocfd_sweep4.cu)
+    if (sizeof(R) == 4) return launch_sweep4_fix(p, DIR, st);
     // the deferred-cell count is only known on the device: a fixed grid
     // that strides over it (usually a few thousand cells, often none)
     k_sweep3_fix<DIR, UNI, EPS0><<<2 * 148, 128, 0, st>>>(p);
@@ -346,6 +353,12 @@ namespace {
 template <bool UNI, bool EPS0>
 cudaError_t dir3(const Params &p, int dir, cudaStream_t st) {
     if (p.has_bnd && !p.defer[0]) return cudaErrorNotSupported;
+    if (p.mixed) {              // precision form: the call-free walk in FP32
+        if (!use_fast(p) || p.scheme_invis != 310) return cudaErrorNotSupported;
+        if (dir == 0) return launch_dir<0, UNI, EPS0, 6, true, float>(p, st);
+        if (dir == 1) return launch_dir<1, UNI, EPS0, 6, true, float>(p, st);
+        return launch_dir<2, UNI, EPS0, 6, true, float>(p, st);
+    }
     if (use_fast(p)) {
         if (dir == 0) return launch_dir<0, UNI, EPS0, 4, true>(p, st);
         if (dir == 1) return launch_dir<1, UNI, EPS0, 4, true>(p, st);

@@ -301,6 +301,59 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep4(const __grid_constant_
     }
 }
 
+// Cells the call-free UP7 walk left (precision form): each thread takes one
+// cell, splits the 9 points X-4 .. X+4 of its line into a private 16-slot
+// ring, forms faces X-1/2 and X+1/2 with the walk's own face routine and
+// adds the cell's du in the same order.
+template <int DIR, bool UNI, bool EPS0, int KIND, typename R>
+__global__ void __launch_bounds__(128) k_sweep4_fix(const __grid_constant__ Params p) {
+    const unsigned cnt = p.defer_count[DIR];
+    const long long sd = DIR == 0 ? 1LL : (DIR == 1 ? p.ys : p.zs);
+    const R h = (R)(DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz)), ih = (R)p.inv_h[DIR];
+    const bool lo = p.bnd_lo[DIR], hi = p.bnd_hi[DIR];
+    const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
+    R *__restrict__ du = du_r<R>(p);
+    const long long N = p.N;
+    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
+        const long long ci = p.defer[DIR][e];
+        const int i = (int)(ci % p.nx);
+        const long long r = ci / p.nx;
+        const int j = (int)(r % p.ny), k = (int)(r / p.ny);
+        const int X = DIR == 0 ? i : (DIR == 1 ? j : k);
+        const long long oX = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+        R win[10 * 16];
+        for (int t = -4; t <= 4; t++) {
+            R q5[5];
+            const long long o = oX + (long long)t * sd;
+            load5(p, o, q5);
+            ring_put<DIR, 16, 1, UNI, EPS0>(p, win, 0, X + t, o, q5);
+        }
+        // flag of face F+1/2 is entry F+1 of the direction's flag array
+        auto flag_at = [&](int e1) -> int {
+            if (KIND != K_HYBC) return 2;
+            long long q = DIR == 0 ? (long long)e1 + (long long)(p.nx + 1) * ((long long)j + (long long)p.ny * k)
+                        : DIR == 1 ? (long long)i + (long long)p.nx * ((long long)e1 + (long long)(p.ny + 1) * k)
+                                   : (long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * e1);
+            return p.flag[DIR][q];
+        };
+        R prv[10], cur[10];
+        face4<KIND, 16, 1, UNI>(p, DIR, win, 0, X - 1, n, flag_at(X), oX - sd, sd, lo, hi, prv);
+        face4<KIND, 16, 1, UNI>(p, DIR, win, 0, X, n, flag_at(X + 1), oX, sd, lo, hi, cur);
+        const R aj = (R)metric<UNI>(p, M_AJAC, oX);
+        if (p.has_bnd && rule_cell(p, DIR, X, n)) {
+            du_rule_cell<DIR, KIND, 16, 1>(p, win, 0, X, n, du, ci, aj, h, ih, cur, prv);
+        } else {
+            R old[5];
+            if (DIR != 0) {
+#pragma unroll
+                for (int m = 0; m < 5; m++) old[m] = du[m * N + ci];
+            }
+            if (DIR == 0) add_du<true>(du, N, ci, aj, h, ih, cur, prv, old);
+            else          add_du<false>(du, N, ci, aj, h, ih, cur, prv, old);
+        }
+    }
+}
+
 template <int DIR, bool UNI, bool EPS0, int KIND, int MINB, typename R>
 cudaError_t launch_dir4(const Params &p, cudaStream_t st) {
     constexpr int LC = Shape<DIR>::LC, LY = 32 / LC;
@@ -358,6 +411,18 @@ cudaError_t dir4r(const Params &p, int dir, cudaStream_t st) {
 // projection, WENO7 on the flux components
 bool sweeps4_supported(const Params &p) {
     return (p.scheme_invis == 310 && p.charteric) || (p.scheme_invis == 303 && !p.charteric);
+}
+
+// fix-up of the cells the FP32 call-free UP7 walk deferred in direction dir
+cudaError_t launch_sweep4_fix(const Params &p, int dir, cudaStream_t st) {
+    if (!(p.scheme_invis == 310 && p.charteric)) return cudaErrorNotSupported;
+    const bool u = p.uniform_metrics, e0 = p.epsl_sw == 0.0;
+#define OCFD_FIX4(D, U, E) k_sweep4_fix<D, U, E, K_HYBC, float><<<2 * 148, 128, 0, st>>>(p)
+    if (dir == 0)      { if (u && e0) OCFD_FIX4(0, true, true); else if (u) OCFD_FIX4(0, true, false); else OCFD_FIX4(0, false, false); }
+    else if (dir == 1) { if (u && e0) OCFD_FIX4(1, true, true); else if (u) OCFD_FIX4(1, true, false); else OCFD_FIX4(1, false, false); }
+    else               { if (u && e0) OCFD_FIX4(2, true, true); else if (u) OCFD_FIX4(2, true, false); else OCFD_FIX4(2, false, false); }
+#undef OCFD_FIX4
+    return cudaGetLastError();
 }
 
 // one direction of the walk (one kernel); FP32 in the precision form
