@@ -120,6 +120,38 @@ int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl);
  * whole steps only (ocfd_b200_step).  Switching back recomputes the FP64
  * primitives from the conserved state. */
 int ocfd_b200_set_precision(ocfd_b200_ctx *ctx, int form);
+/* Learned scheme switch (hybrid scheme).  A 14 -> 32 -> 32 -> 1 ReLU network
+ * over normalised pressure and density differences on the sensor's 7-point
+ * stencil takes the place of the plain sensor's choice
+ * (Comput_Scheme_point_Jameson, src/OCFD_Schemes_hybrid_auto.cu:611-703) and
+ * writes the same flag arrays: a cell whose confidence max(s, 1 - s),
+ * s = sigmoid(output), reaches `confidence` gets flag 1 (s < 1/2) or the
+ * larger of 2 and the plain flag (s >= 1/2); any other cell keeps the plain
+ * flag.  Inference: BF16 tensor-core products, FP32 accumulation.  The
+ * parameter vector (ocfd_b200_mlp_nparam() floats) is mu[14] sigma[14]
+ * W1[32][14] b1[32] W2[32][32] b2[32] W3[32] b3, features standardised as
+ * (f - mu) / sigma.  params = NULL switches back to the plain sensor. */
+int ocfd_b200_mlp_nparam(void);
+int ocfd_b200_set_switch(ocfd_b200_ctx *ctx, const float *params, int nparam, double confidence);
+/* Cells decided by the network, cells left to the plain flag, and network
+ * flags that differ from the plain flag, summed over sensor passes since
+ * the last ocfd_b200_set_switch. */
+int ocfd_b200_switch_stats(ocfd_b200_ctx *ctx, long long counts[3]);
+/* Features (count x 14, FP32) and labels (1 where the plain flag is 2 or
+ * 3) of interior cells first .. first+count-1 (x fastest) of the current
+ * state, into host arrays: the training data of the switch. */
+int ocfd_b200_switch_features(ocfd_b200_ctx *ctx, long long first, long long count, float *feat, float *label);
+/* Stand-alone network kernels on the current device (host arrays in and
+ * out): logits of n feature rows through the tensor-core path; the FP32
+ * gradient (network part, from W1 on) and loss of the summed binary
+ * cross-entropy over n rows with positives weighted pos_w; Adam training
+ * over shuffled mini-batches (params in/out, mean loss per epoch out). */
+const char *ocfd_b200_mlp_last_error(void);
+int ocfd_b200_mlp_infer(const float *params, const float *feat, long long n, float *logit);
+int ocfd_b200_mlp_grad(const float *params, const float *feat, const float *label, long long n, float pos_w,
+                       float *grad, double *loss);
+int ocfd_b200_mlp_train(float *params, const float *feat, const float *label, long long n, int epochs, int batch,
+                        float lr, float pos_w, unsigned long long seed, double *epoch_loss);
 /* Bit d set: direction d currently takes the walk that forms every face in
  * line (variant 4 after the last sensor pass, or variant 6). */
 int ocfd_b200_sweep_walks(const ocfd_b200_ctx *ctx);

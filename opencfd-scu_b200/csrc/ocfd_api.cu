@@ -48,6 +48,18 @@ cudaError_t launch_filter_pass(const Params &p, int dir, const int box[6], doubl
 cudaError_t launch_bc108(const Params &p, double ht, cudaStream_t st);
 int sweeps3_kernels(const Params &p);
 cudaError_t compute_dirconst(Params &p, DirConst *dev_scratch, cudaStream_t st);
+int mlp_nparam();
+int mlp_nnet();
+int mlp_grad_blocks(long long n);
+cudaError_t launch_switch_features(const Params &p, long long first, long long count, float *feat, float *label,
+                                   cudaStream_t st);
+cudaError_t launch_switch_infer(const Params &p, const float *w, float conf_logit, unsigned long long *stats,
+                                cudaStream_t st);
+cudaError_t launch_mlp_infer(const float *w, const float *feat, long long n, float *logit, cudaStream_t st);
+cudaError_t launch_mlp_grad(const float *w, const float *feat, const float *label, const int *idx, long long n,
+                            float pos_w, float *part, float *lpart, float *grad, double *loss, cudaStream_t st);
+cudaError_t launch_mlp_adam(float *w, const float *grad, float *m1, float *m2, float scale, float lr, int t,
+                            cudaStream_t st);
 }  // namespace ocfd
 
 using ocfd::Params;
@@ -99,6 +111,12 @@ struct ocfd_b200_ctx {
     // brought up to date from the conserved state before they are read
     float *prec_buf = nullptr;
     bool prims64_stale = false;
+    // learned scheme switch: parameter vector on the device, the confidence
+    // threshold as a logit, decision counters
+    float *sw_w = nullptr;
+    unsigned long long *sw_stats = nullptr;
+    bool sw_on = false;
+    float sw_conf_logit = 0.0f;
     int walk4[3] = {1, 1, 1};
     double walk4_threshold = 0.002;     // deferred cells per cell above which the inline walk is used
     bool have_metrics = false;
@@ -157,6 +175,8 @@ static void free_all(ocfd_b200_ctx *c) {
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->h_flag_count) cudaFreeHost(c->h_flag_count);
     cudaFree(c->prec_buf);
+    cudaFree(c->sw_w);
+    cudaFree(c->sw_stats);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
@@ -433,7 +453,9 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
     const Params &p = ctx->p;
     if (p.scheme_invis == 310 && krk == 1) {
         TimerScope ts(ctx, T_SENSOR);
-        CK(ocfd::launch_sensor(p, ctx->stream), "sensor");
+        if (ctx->sw_on) CK(ocfd::launch_switch_infer(p, ctx->sw_w, ctx->sw_conf_logit, ctx->sw_stats, ctx->stream),
+                           "learned switch");
+        else            CK(ocfd::launch_sensor(p, ctx->stream), "sensor");
         ctx->launches += 1;
         if ((p.sweep_impl == 4 || p.mixed) && ocfd::sweeps4_supported(p) && p.flag_count) {
             // the choice follows this pass's flags: one small read-back per step
@@ -582,6 +604,176 @@ extern "C" int ocfd_b200_set_precision(ocfd_b200_ctx *ctx, int form) {
         ctx->launches += 1;
     }
     CK(cudaStreamSynchronize(ctx->stream), "set_precision");
+    return OCFD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// learned scheme switch
+// ---------------------------------------------------------------------------
+extern "C" int ocfd_b200_mlp_nparam(void) { return ocfd::mlp_nparam(); }
+
+extern "C" int ocfd_b200_set_switch(ocfd_b200_ctx *ctx, const float *params, int nparam, double confidence) {
+    if (!ctx) return OCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (!params) { ctx->sw_on = false; return OCFD_OK; }
+    if (nparam != ocfd::mlp_nparam() || !(confidence > 0.5 && confidence < 1.0))
+        return fail(ctx, OCFD_ERR_ARG, "switch: parameter count or confidence (0.5, 1) wrong");
+    for (int i = 0; i < 14; i++)
+        if (!(params[14 + i] > 0.0f)) return fail(ctx, OCFD_ERR_ARG, "switch: feature scales must be > 0");
+    if (!ctx->sw_w) {
+        CK(cudaMalloc((void **)&ctx->sw_w, sizeof(float) * nparam), "switch parameters");
+        CK(cudaMalloc((void **)&ctx->sw_stats, 4 * sizeof(unsigned long long)), "switch counters");
+    }
+    CK(cudaMemcpyAsync(ctx->sw_w, params, sizeof(float) * nparam, cudaMemcpyHostToDevice, ctx->stream),
+       "switch parameters");
+    CK(cudaMemsetAsync(ctx->sw_stats, 0, 4 * sizeof(unsigned long long), ctx->stream), "switch counters");
+    CK(cudaStreamSynchronize(ctx->stream), "set_switch");
+    ctx->sw_conf_logit = (float)log(confidence / (1.0 - confidence));
+    ctx->sw_on = true;
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_switch_stats(ocfd_b200_ctx *ctx, long long counts[3]) {
+    if (!ctx || !counts) return OCFD_ERR_ARG;
+    unsigned long long h[4] = {0, 0, 0, 0};
+    if (ctx->sw_stats) {
+        CK(cudaMemcpyAsync(h, ctx->sw_stats, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "switch counters");
+        CK(cudaStreamSynchronize(ctx->stream), "switch counters");
+    }
+    for (int i = 0; i < 3; i++) counts[i] = (long long)h[i];
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_switch_features(ocfd_b200_ctx *ctx, long long first, long long count, float *feat,
+                                         float *label) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (!feat || !label || first < 0 || count < 0 || first + count > ctx->p.N)
+        return fail(ctx, OCFD_ERR_ARG, "switch_features: range outside the interior");
+    if (count == 0) return OCFD_OK;
+    if ((rc = refresh_prims64(ctx))) return rc;
+    float *buf = nullptr;
+    CK(cudaMalloc((void **)&buf, sizeof(float) * 15 * (size_t)count), "feature buffer");
+    cudaError_t e = ocfd::launch_switch_features(ctx->p, first, count, buf, buf + 14 * (size_t)count, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(feat, buf, sizeof(float) * 14 * (size_t)count, cudaMemcpyDeviceToHost,
+                                              ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(label, buf + 14 * (size_t)count, sizeof(float) * (size_t)count,
+                                              cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(buf);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "switch_features");
+    ctx->launches += 1;
+    return OCFD_OK;
+}
+
+// stand-alone network entry points (no solver context; current device)
+namespace {
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() { if (p) cudaFree(p); }
+    cudaError_t alloc(size_t b) { return cudaMalloc(&p, b); }
+    template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+thread_local std::string g_mlp_err;
+int mlp_fail(cudaError_t e, const char *where) {
+    g_mlp_err = std::string(where) + ": " + cudaGetErrorString(e);
+    return OCFD_ERR_CUDA;
+}
+#define MCK(call, where) do { cudaError_t e_ = (call); if (e_ != cudaSuccess) return mlp_fail(e_, where); } while (0)
+}  // namespace
+
+extern "C" const char *ocfd_b200_mlp_last_error(void) { return g_mlp_err.c_str(); }
+
+extern "C" int ocfd_b200_mlp_infer(const float *params, const float *feat, long long n, float *logit) {
+    if (!params || !feat || !logit || n < 0) return OCFD_ERR_ARG;
+    if (n == 0) return OCFD_OK;
+    const int np = ocfd::mlp_nparam();
+    DevBuf w, f, z;
+    MCK(w.alloc(sizeof(float) * np), "alloc");
+    MCK(f.alloc(sizeof(float) * 14 * (size_t)n), "alloc");
+    MCK(z.alloc(sizeof(float) * (size_t)n), "alloc");
+    MCK(cudaMemcpy(w.p, params, sizeof(float) * np, cudaMemcpyHostToDevice), "copy");
+    MCK(cudaMemcpy(f.p, feat, sizeof(float) * 14 * (size_t)n, cudaMemcpyHostToDevice), "copy");
+    MCK(ocfd::launch_mlp_infer(w.as<float>(), f.as<float>(), n, z.as<float>(), 0), "mlp_infer");
+    MCK(cudaMemcpy(logit, z.p, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost), "copy");
+    return OCFD_OK;
+}
+
+// gradient of the summed loss over rows 0..n-1 (network part of the
+// parameter vector, from W1 on) and the summed loss
+extern "C" int ocfd_b200_mlp_grad(const float *params, const float *feat, const float *label, long long n,
+                                  float pos_w, float *grad, double *loss) {
+    if (!params || !feat || !label || !grad || !loss || n <= 0) return OCFD_ERR_ARG;
+    const int np = ocfd::mlp_nparam(), nn = ocfd::mlp_nnet(), nb = ocfd::mlp_grad_blocks(n);
+    DevBuf w, f, y, part, lpart, g, l;
+    MCK(w.alloc(sizeof(float) * np), "alloc");
+    MCK(f.alloc(sizeof(float) * 14 * (size_t)n), "alloc");
+    MCK(y.alloc(sizeof(float) * (size_t)n), "alloc");
+    MCK(part.alloc(sizeof(float) * (size_t)nb * nn), "alloc");
+    MCK(lpart.alloc(sizeof(float) * (size_t)nb), "alloc");
+    MCK(g.alloc(sizeof(float) * nn), "alloc");
+    MCK(l.alloc(sizeof(double)), "alloc");
+    MCK(cudaMemcpy(w.p, params, sizeof(float) * np, cudaMemcpyHostToDevice), "copy");
+    MCK(cudaMemcpy(f.p, feat, sizeof(float) * 14 * (size_t)n, cudaMemcpyHostToDevice), "copy");
+    MCK(cudaMemcpy(y.p, label, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice), "copy");
+    MCK(cudaMemset(l.p, 0, sizeof(double)), "memset");
+    MCK(ocfd::launch_mlp_grad(w.as<float>(), f.as<float>(), y.as<float>(), nullptr, n, pos_w, part.as<float>(),
+                              lpart.as<float>(), g.as<float>(), l.as<double>(), 0), "mlp_grad");
+    MCK(cudaMemcpy(grad, g.p, sizeof(float) * nn, cudaMemcpyDeviceToHost), "copy");
+    MCK(cudaMemcpy(loss, l.p, sizeof(double), cudaMemcpyDeviceToHost), "copy");
+    return OCFD_OK;
+}
+
+// Adam over shuffled mini-batches of mean loss; params (in/out) is the
+// full parameter vector (mu and sigma are kept); epoch_loss[e] = mean loss
+// of epoch e
+extern "C" int ocfd_b200_mlp_train(float *params, const float *feat, const float *label, long long n, int epochs,
+                                   int batch, float lr, float pos_w, unsigned long long seed, double *epoch_loss) {
+    if (!params || !feat || !label || n <= 0 || epochs < 0 || batch <= 0 || n > 0x7fffffffLL) return OCFD_ERR_ARG;
+    const int np = ocfd::mlp_nparam(), nn = ocfd::mlp_nnet(), nbmax = ocfd::mlp_grad_blocks(batch);
+    DevBuf w, f, y, part, lpart, g, l, m1, m2, perm;
+    MCK(w.alloc(sizeof(float) * np), "alloc");
+    MCK(f.alloc(sizeof(float) * 14 * (size_t)n), "alloc");
+    MCK(y.alloc(sizeof(float) * (size_t)n), "alloc");
+    MCK(part.alloc(sizeof(float) * (size_t)nbmax * nn), "alloc");
+    MCK(lpart.alloc(sizeof(float) * (size_t)nbmax), "alloc");
+    MCK(g.alloc(sizeof(float) * nn), "alloc");
+    MCK(l.alloc(sizeof(double)), "alloc");
+    MCK(m1.alloc(sizeof(float) * nn), "alloc");
+    MCK(m2.alloc(sizeof(float) * nn), "alloc");
+    MCK(perm.alloc(sizeof(int) * (size_t)n), "alloc");
+    MCK(cudaMemcpy(w.p, params, sizeof(float) * np, cudaMemcpyHostToDevice), "copy");
+    MCK(cudaMemcpy(f.p, feat, sizeof(float) * 14 * (size_t)n, cudaMemcpyHostToDevice), "copy");
+    MCK(cudaMemcpy(y.p, label, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice), "copy");
+    MCK(cudaMemset(m1.p, 0, sizeof(float) * nn), "memset");
+    MCK(cudaMemset(m2.p, 0, sizeof(float) * nn), "memset");
+    std::vector<int> order((size_t)n);
+    for (long long i = 0; i < n; i++) order[(size_t)i] = (int)i;
+    unsigned long long state = seed ? seed : 0x9E3779B97F4A7C15ULL;
+    auto next = [&state]() {           // splitmix64
+        unsigned long long z = (state += 0x9E3779B97F4A7C15ULL);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        return z ^ (z >> 31);
+    };
+    int t = 0;
+    for (int ep = 0; ep < epochs; ep++) {
+        for (long long i = n - 1; i > 0; i--) std::swap(order[(size_t)i], order[(size_t)(next() % (unsigned long long)(i + 1))]);
+        MCK(cudaMemcpy(perm.p, order.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice), "copy");
+        MCK(cudaMemset(l.p, 0, sizeof(double)), "memset");
+        for (long long b0 = 0; b0 < n; b0 += batch) {
+            const long long nb = std::min<long long>(batch, n - b0);
+            MCK(ocfd::launch_mlp_grad(w.as<float>(), f.as<float>(), y.as<float>(), perm.as<int>() + b0, nb, pos_w,
+                                      part.as<float>(), lpart.as<float>(), g.as<float>(), l.as<double>(), 0),
+                "mlp_grad");
+            MCK(ocfd::launch_mlp_adam(w.as<float>(), g.as<float>(), m1.as<float>(), m2.as<float>(),
+                                      1.0f / (float)nb, lr, ++t, 0), "mlp_adam");
+        }
+        double ls = 0.0;
+        MCK(cudaMemcpy(&ls, l.p, sizeof(double), cudaMemcpyDeviceToHost), "copy");
+        if (epoch_loss) epoch_loss[ep] = ls / (double)n;
+    }
+    MCK(cudaMemcpy(params, w.p, sizeof(float) * np, cudaMemcpyDeviceToHost), "copy");
     return OCFD_OK;
 }
 

@@ -30,6 +30,8 @@ EXPORTED = (
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
     "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics", "ocfd_b200_set_sweep_impl",
     "ocfd_b200_sweep_walks", "ocfd_b200_set_precision",
+    "ocfd_b200_mlp_nparam", "ocfd_b200_set_switch", "ocfd_b200_switch_stats", "ocfd_b200_switch_features",
+    "ocfd_b200_mlp_last_error", "ocfd_b200_mlp_infer", "ocfd_b200_mlp_grad", "ocfd_b200_mlp_train",
     "ocfd_b200_set_mesh", "ocfd_b200_set_mesh_device", "ocfd_b200_get_metrics",
     "ocfd_b200_set_filter", "ocfd_b200_filtering", "ocfd_b200_set_time", "filtering", "ocfd_b200_set_bc",
     "ocfd_b200_set_primitives", "ocfd_b200_set_primitives_device", "ocfd_b200_step",
@@ -92,6 +94,7 @@ def load(path: Optional[str] = None):
     P = ctypes.c_void_p
     D = ctypes.POINTER(ctypes.c_double)
     I8 = ctypes.POINTER(ctypes.c_int8)
+    F = ctypes.POINTER(ctypes.c_float)
     sig = {
         "ocfd_b200_abi_version": (ctypes.c_int, []),
         "ocfd_b200_status_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -117,6 +120,15 @@ def load(path: Optional[str] = None):
         "ocfd_b200_set_sweep_impl": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_sweep_walks": (ctypes.c_int, [P]),
         "ocfd_b200_set_precision": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_mlp_nparam": (ctypes.c_int, []),
+        "ocfd_b200_set_switch": (ctypes.c_int, [P, F, ctypes.c_int, ctypes.c_double]),
+        "ocfd_b200_switch_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_longlong)]),
+        "ocfd_b200_switch_features": (ctypes.c_int, [P, ctypes.c_longlong, ctypes.c_longlong, F, F]),
+        "ocfd_b200_mlp_last_error": (ctypes.c_char_p, []),
+        "ocfd_b200_mlp_infer": (ctypes.c_int, [F, F, ctypes.c_longlong, F]),
+        "ocfd_b200_mlp_grad": (ctypes.c_int, [F, F, F, ctypes.c_longlong, ctypes.c_float, F, D]),
+        "ocfd_b200_mlp_train": (ctypes.c_int, [F, F, F, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_float, ctypes.c_float, ctypes.c_ulonglong, D]),
         "ocfd_b200_set_primitives": (ctypes.c_int, [P, D, ctypes.c_int, ctypes.c_double]),
         "ocfd_b200_set_primitives_device": (ctypes.c_int, [P, P, ctypes.c_int, ctypes.c_double]),
         "ocfd_b200_step": (ctypes.c_int, [P, ctypes.c_int]),
@@ -158,6 +170,54 @@ def load(path: Optional[str] = None):
 
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _mlp_check(rc: int, what: str):
+    if rc != 0:
+        L = load()
+        raise OcfdError(rc, f"{what}: {L.ocfd_b200_status_string(rc).decode()} "
+                            f"({L.ocfd_b200_mlp_last_error().decode()})")
+
+
+def mlp_nparam() -> int:
+    return int(load().ocfd_b200_mlp_nparam())
+
+
+def mlp_infer(params: np.ndarray, feat: np.ndarray) -> np.ndarray:
+    """Logits of feature rows (n x 14) through the tensor-core network."""
+    w = np.ascontiguousarray(params, np.float32)
+    f = np.ascontiguousarray(feat, np.float32)
+    out = np.empty(f.shape[0], np.float32)
+    _mlp_check(load().ocfd_b200_mlp_infer(_fp(w), _fp(f), f.shape[0], _fp(out)), "mlp_infer")
+    return out
+
+
+def mlp_grad(params: np.ndarray, feat: np.ndarray, label: np.ndarray, pos_w: float = 1.0):
+    """(gradient of the summed loss w.r.t. the network parameters, summed loss)."""
+    w = np.ascontiguousarray(params, np.float32)
+    f = np.ascontiguousarray(feat, np.float32)
+    y = np.ascontiguousarray(label, np.float32)
+    g = np.empty(w.size - 28, np.float32)
+    loss = ctypes.c_double()
+    _mlp_check(load().ocfd_b200_mlp_grad(_fp(w), _fp(f), _fp(y), f.shape[0], pos_w, _fp(g), ctypes.byref(loss)),
+               "mlp_grad")
+    return g, loss.value
+
+
+def mlp_train(params: np.ndarray, feat: np.ndarray, label: np.ndarray, epochs: int, batch: int = 16384,
+              lr: float = 1e-3, pos_w: float = 1.0, seed: int = 1):
+    """Adam on the GPU; returns (trained parameter vector, mean loss per epoch)."""
+    w = np.array(params, np.float32)
+    f = np.ascontiguousarray(feat, np.float32)
+    y = np.ascontiguousarray(label, np.float32)
+    hist = np.zeros(max(epochs, 1), np.float64)
+    _mlp_check(load().ocfd_b200_mlp_train(_fp(w), _fp(f), _fp(y), f.shape[0], epochs, batch, lr, pos_w, seed,
+                                          _dp(hist)), "mlp_train")
+    return w, hist[:epochs]
 
 
 def make_config(cfg: CaseConfig, device: int = 0) -> Config:
@@ -256,6 +316,29 @@ class Solver:
     def set_precision(self, form: int):
         """0: FP64 throughout; 1: FP32 stencils with FP64 RK3 accumulation."""
         self._check(self.L.ocfd_b200_set_precision(self.h, form), "set_precision")
+
+    def set_switch(self, params: Optional[np.ndarray], confidence: float = 0.9):
+        """Learned scheme switch with the plain sensor below `confidence`; None: plain."""
+        if params is None:
+            self._check(self.L.ocfd_b200_set_switch(self.h, None, 0, 0.0), "set_switch")
+            return
+        self._switch_w = np.ascontiguousarray(params, np.float32)
+        self._check(self.L.ocfd_b200_set_switch(self.h, _fp(self._switch_w), self._switch_w.size, confidence),
+                    "set_switch")
+
+    def switch_stats(self) -> Tuple[int, int, int]:
+        c = (ctypes.c_longlong * 3)()
+        self._check(self.L.ocfd_b200_switch_stats(self.h, c), "switch_stats")
+        return int(c[0]), int(c[1]), int(c[2])
+
+    def switch_features(self, first: int = 0, count: Optional[int] = None):
+        """(features count x 14, labels count) of interior cells first.. (x fastest)."""
+        n = self.cfg.nx * self.cfg.ny * self.cfg.nz
+        count = n - first if count is None else count
+        f = np.empty((count, 14), np.float32)
+        y = np.empty(count, np.float32)
+        self._check(self.L.ocfd_b200_switch_features(self.h, first, count, _fp(f), _fp(y)), "switch_features")
+        return f, y
 
     def sweep_walks(self) -> int:
         """Bit d set: direction d takes the walk that forms every face in line."""
