@@ -117,33 +117,65 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], 
                  : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// x: this lane's 14 standardised features; sbuf: 32 x 16 bf16 (one warp's
-// staging) plus 32 floats for the logits
-__device__ __forceinline__ float warp_mlp(const float *__restrict__ w, const float (&x)[MLP_IN],
-                                          __nv_bfloat16 *sA, float *sL) {
+// one lane's share of the network for the tensor-core products: B operands
+// of layer 1 (n-tiles 0..3) and layer 2 (n-tiles 0..3, k-steps 0..1) as
+// BF16 pairs, and the biases / output weights of its accumulator columns
+struct MlpFrag {
+    unsigned w1[4][2], w2[4][2][2];
+    float b1[4][2], b2[4][2], w3[4][2], b3;
+};
+
+__device__ __forceinline__ void load_frags(const float *__restrict__ w, MlpFrag &fr) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int m = 0; m < 16; m++) sA[lane * 16 + m] = __float2bfloat16_rn(m < MLP_IN ? x[m] : 0.0f);
-    __syncwarp();
-    // layer 1: Z1 (32 x 32) = X (32 x 16) W1^T + b1; B[k][n] = W1[n][k]
-    float z1[2][4][4];
 #pragma unroll
     for (int nt = 0; nt < 4; nt++) {
         const int n = nt * 8 + g;
         const float *W1 = w + OFF_W1 + n * MLP_IN;
-        const unsigned b0 = pack_bf16(W1[2 * t], W1[2 * t + 1]);
-        const unsigned b1 = 2 * t + 8 < MLP_IN ? pack_bf16(W1[2 * t + 8], W1[2 * t + 9]) : 0u;
-        const float bl = w[OFF_B1 + nt * 8 + 2 * t], bh = w[OFF_B1 + nt * 8 + 2 * t + 1];
+        fr.w1[nt][0] = pack_bf16(W1[2 * t], W1[2 * t + 1]);
+        fr.w1[nt][1] = 2 * t + 8 < MLP_IN ? pack_bf16(W1[2 * t + 8], W1[2 * t + 9]) : 0u;
+        const float *W2 = w + OFF_W2 + n * MLP_H;
 #pragma unroll
-        for (int mt = 0; mt < 2; mt++) {
-            const __nv_bfloat16 *row0 = sA + (mt * 16 + g) * 16, *row1 = sA + (mt * 16 + g + 8) * 16;
-            unsigned a[4];
-            a[0] = *reinterpret_cast<const unsigned *>(row0 + 2 * t);
-            a[1] = *reinterpret_cast<const unsigned *>(row1 + 2 * t);
-            a[2] = *reinterpret_cast<const unsigned *>(row0 + 2 * t + 8);
-            a[3] = *reinterpret_cast<const unsigned *>(row1 + 2 * t + 8);
-            z1[mt][nt][0] = bl; z1[mt][nt][1] = bh; z1[mt][nt][2] = bl; z1[mt][nt][3] = bh;
-            mma_bf16(z1[mt][nt], a, b0, b1);
+        for (int kk = 0; kk < 2; kk++) {
+            fr.w2[nt][kk][0] = pack_bf16(W2[kk * 16 + 2 * t], W2[kk * 16 + 2 * t + 1]);
+            fr.w2[nt][kk][1] = pack_bf16(W2[kk * 16 + 2 * t + 8], W2[kk * 16 + 2 * t + 9]);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            fr.b1[nt][h] = w[OFF_B1 + nt * 8 + 2 * t + h];
+            fr.b2[nt][h] = w[OFF_B2 + nt * 8 + 2 * t + h];
+            fr.w3[nt][h] = w[OFF_W3 + nt * 8 + 2 * t + h];
+        }
+    }
+    fr.b3 = w[OFF_B3];
+}
+
+// x: this lane's 14 standardised features; sA: 32 x 16 bf16 (one warp's
+// staging), sL: 32 floats; returns this lane's logit
+__device__ __forceinline__ float warp_mlp(const MlpFrag &fr, const float (&x)[MLP_IN],
+                                          __nv_bfloat16 *sA, float *sL) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    __syncwarp();                       // the previous tile's reads of sA / sL are done
+#pragma unroll
+    for (int m = 0; m < 16; m += 2) {
+        const unsigned v = pack_bf16(m < MLP_IN ? x[m] : 0.0f, m + 1 < MLP_IN ? x[m + 1] : 0.0f);
+        *reinterpret_cast<unsigned *>(sA + lane * 16 + m) = v;
+    }
+    __syncwarp();
+    // layer 1: Z1 (32 x 32) = X (32 x 16) W1^T + b1; B[k][n] = W1[n][k]
+    float z1[2][4][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+        const __nv_bfloat16 *row0 = sA + (mt * 16 + g) * 16, *row1 = sA + (mt * 16 + g + 8) * 16;
+        unsigned a[4];
+        a[0] = *reinterpret_cast<const unsigned *>(row0 + 2 * t);
+        a[1] = *reinterpret_cast<const unsigned *>(row1 + 2 * t);
+        a[2] = *reinterpret_cast<const unsigned *>(row0 + 2 * t + 8);
+        a[3] = *reinterpret_cast<const unsigned *>(row1 + 2 * t + 8);
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            z1[mt][nt][0] = fr.b1[nt][0]; z1[mt][nt][1] = fr.b1[nt][1];
+            z1[mt][nt][2] = fr.b1[nt][0]; z1[mt][nt][3] = fr.b1[nt][1];
+            mma_bf16(z1[mt][nt], a, fr.w1[nt][0], fr.w1[nt][1]);
         }
     }
     // ReLU; the accumulator tiles of n-tiles 2kk and 2kk+1 are the A operand
@@ -163,23 +195,13 @@ __device__ __forceinline__ float warp_mlp(const float *__restrict__ w, const flo
     float part[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};     // [m-tile][row g / g+8]
 #pragma unroll
     for (int nt = 0; nt < 4; nt++) {
-        const int n = nt * 8 + g;
-        const float *W2 = w + OFF_W2 + n * MLP_H;
-        unsigned b[2][2];
-#pragma unroll
-        for (int kk = 0; kk < 2; kk++) {
-            b[kk][0] = pack_bf16(W2[kk * 16 + 2 * t], W2[kk * 16 + 2 * t + 1]);
-            b[kk][1] = pack_bf16(W2[kk * 16 + 2 * t + 8], W2[kk * 16 + 2 * t + 9]);
-        }
-        const float bl = w[OFF_B2 + nt * 8 + 2 * t], bh = w[OFF_B2 + nt * 8 + 2 * t + 1];
-        const float wl = w[OFF_W3 + nt * 8 + 2 * t], wh = w[OFF_W3 + nt * 8 + 2 * t + 1];
 #pragma unroll
         for (int mt = 0; mt < 2; mt++) {
-            float z[4] = {bl, bh, bl, bh};
-            mma_bf16(z, a2[mt][0], b[0][0], b[0][1]);
-            mma_bf16(z, a2[mt][1], b[1][0], b[1][1]);
-            part[mt][0] += fmaxf(z[0], 0.0f) * wl + fmaxf(z[1], 0.0f) * wh;
-            part[mt][1] += fmaxf(z[2], 0.0f) * wl + fmaxf(z[3], 0.0f) * wh;
+            float z[4] = {fr.b2[nt][0], fr.b2[nt][1], fr.b2[nt][0], fr.b2[nt][1]};
+            mma_bf16(z, a2[mt][0], fr.w2[nt][0][0], fr.w2[nt][0][1]);
+            mma_bf16(z, a2[mt][1], fr.w2[nt][1][0], fr.w2[nt][1][1]);
+            part[mt][0] += fmaxf(z[0], 0.0f) * fr.w3[nt][0] + fmaxf(z[1], 0.0f) * fr.w3[nt][1];
+            part[mt][1] += fmaxf(z[2], 0.0f) * fr.w3[nt][0] + fmaxf(z[3], 0.0f) * fr.w3[nt][1];
         }
     }
 #pragma unroll
@@ -192,29 +214,41 @@ __device__ __forceinline__ float warp_mlp(const float *__restrict__ w, const flo
             if (t == 0) sL[mt * 16 + h * 8 + g] = v;
         }
     __syncwarp();
-    const float logit = sL[lane] + w[OFF_B3];
-    __syncwarp();
-    return logit;
+    return sL[lane] + fr.b3;
 }
 
-__device__ __forceinline__ void standardise(const float *__restrict__ w, const float (&f)[MLP_IN], float (&x)[MLP_IN]) {
+__device__ __forceinline__ void standardise(const float *mu, const float *sg, const float (&f)[MLP_IN],
+                                            float (&x)[MLP_IN]) {
 #pragma unroll
-    for (int m = 0; m < MLP_IN; m++) x[m] = (f[m] - w[OFF_MU + m]) / w[OFF_SG + m];
+    for (int m = 0; m < MLP_IN; m++) x[m] = (f[m] - mu[m]) / sg[m];
 }
 
-// logits of n raw feature rows (the network alone, for checks)
+// the block's copy of the standardisation constants
+__device__ __forceinline__ void load_standard(const float *__restrict__ w, float *sMu, float *sSg) {
+    if (threadIdx.x < MLP_IN) { sMu[threadIdx.x] = w[OFF_MU + threadIdx.x]; sSg[threadIdx.x] = w[OFF_SG + threadIdx.x]; }
+    __syncthreads();
+}
+
+// logits of n raw feature rows (the network alone, for checks); each warp
+// loads its weight fragments once and walks 32-row tiles
 __global__ void __launch_bounds__(128) k_mlp_infer(const float *__restrict__ w, const float *__restrict__ feat,
                                                    long long n, float *logit) {
     __shared__ __align__(16) __nv_bfloat16 sA[4][32 * 16];
-    __shared__ float sL[4][32];
-    const int wid = threadIdx.x >> 5;
-    const long long row = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    float f[MLP_IN], x[MLP_IN];
+    __shared__ float sL[4][32], sMu[MLP_IN], sSg[MLP_IN];
+    load_standard(w, sMu, sSg);
+    MlpFrag fr;
+    load_frags(w, fr);
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long ntile = (n + 31) / 32, nw = (long long)gridDim.x * 4;
+    for (long long tile = (long long)blockIdx.x * 4 + wid; tile < ntile; tile += nw) {
+        const long long row = tile * 32 + lane;
+        float f[MLP_IN], x[MLP_IN];
 #pragma unroll
-    for (int m = 0; m < MLP_IN; m++) f[m] = row < n ? feat[row * MLP_IN + m] : 0.0f;
-    standardise(w, f, x);
-    const float z = warp_mlp(w, x, sA[wid], sL[wid]);
-    if (row < n) logit[row] = z;
+        for (int m = 0; m < MLP_IN; m++) f[m] = row < n ? feat[row * MLP_IN + m] : 0.0f;
+        standardise(sMu, sSg, f, x);
+        const float z = warp_mlp(fr, x, sA[wid], sL[wid]);
+        if (row < n) logit[row] = z;
+    }
 }
 
 // The learned switch over the extended box: cell (i, j, k), each of -1 ..
@@ -227,50 +261,57 @@ template <typename R>
 __global__ void __launch_bounds__(128) k_switch_infer(Params p, const float *__restrict__ w, float conf_logit,
                                                       unsigned long long *stats) {
     __shared__ __align__(16) __nv_bfloat16 sA[4][32 * 16];
-    __shared__ float sL[4][32];
+    __shared__ float sL[4][32], sMu[MLP_IN], sSg[MLP_IN];
+    load_standard(w, sMu, sSg);
+    MlpFrag fr;
+    load_frags(w, fr);
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long ex = p.nx + 1, ey = p.ny + 1, ez = p.nz + 1;
-    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = tid < ex * ey * ez;
-    int i = 0, j = 0, k = 0;
-    float f[MLP_IN] = {};
-    R dp = (R)0;
-    if (live) {
-        i = (int)(tid % ex) - 1;
-        const long long r = tid / ex;
-        j = (int)(r % ey) - 1; k = (int)(r / ey) - 1;
-        const long long om[3] = {-1LL, -p.ys, -p.zs}, op[3] = {1LL, p.ys, p.zs};
-        switch_features<R>(p, lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP), om, op, f, dp);
-    }
-    float x[MLP_IN];
-    standardise(w, f, x);
-    const float z = warp_mlp(w, x, sA[wid], sL[wid]);
-    if (!live) return;
-    const int plain = plain_flag(p, dp);
-    const bool sure = fabsf(z) >= conf_logit;
-    const int kp = sure ? (z >= 0.0f ? max(2, plain) : 1) : plain;
-    const bool inx = j >= 0 && k >= 0, iny = i >= 0 && k >= 0, inz = i >= 0 && j >= 0;
-    if (inx) p.flag[0][(long long)(i + 1) + ex * ((long long)j + (long long)p.ny * k)] = (int8_t)kp;
-    if (iny) p.flag[1][(long long)i + (long long)p.nx * ((long long)(j + 1) + ey * k)] = (int8_t)kp;
-    if (inz) p.flag[2][(long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * (k + 1))] = (int8_t)kp;
-    const unsigned act = __activemask();
-    if (p.flag_count) {          // faces per direction whose flag is not 1
-        const bool non1 = kp != 1;
-        const unsigned mx = __ballot_sync(act, non1 && inx), my = __ballot_sync(act, non1 && iny),
-                       mz = __ballot_sync(act, non1 && inz);
-        if (lane == __ffs(act) - 1) {
-            if (mx) atomicAdd(p.flag_count + 0, (unsigned)__popc(mx));
-            if (my) atomicAdd(p.flag_count + 1, (unsigned)__popc(my));
-            if (mz) atomicAdd(p.flag_count + 2, (unsigned)__popc(mz));
+    const long long ex = p.nx + 1, ey = p.ny + 1, ez = p.nz + 1, total = ex * ey * ez;
+    const long long ntile = (total + 31) / 32, nw = (long long)gridDim.x * 4;
+    const long long om[3] = {-1LL, -p.ys, -p.zs}, op[3] = {1LL, p.ys, p.zs};
+    unsigned long long n_sure = 0, n_unsure = 0, n_differ = 0;
+    for (long long tile = (long long)blockIdx.x * 4 + wid; tile < ntile; tile += nw) {
+        const long long tid = tile * 32 + lane;
+        const bool live = tid < total;
+        int i = 0, j = 0, k = 0;
+        float f[MLP_IN] = {};
+        R dp = (R)0;
+        if (live) {
+            i = (int)(tid % ex) - 1;
+            const long long r = tid / ex;
+            j = (int)(r % ey) - 1; k = (int)(r / ey) - 1;
+            switch_features<R>(p, lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP), om, op, f, dp);
+        }
+        float x[MLP_IN];
+        standardise(sMu, sSg, f, x);
+        const float z = warp_mlp(fr, x, sA[wid], sL[wid]);
+        const int plain = plain_flag(p, dp);
+        const bool sure = fabsf(z) >= conf_logit;
+        const int kp = sure ? (z >= 0.0f ? max(2, plain) : 1) : plain;
+        const bool inx = live && j >= 0 && k >= 0, iny = live && i >= 0 && k >= 0, inz = live && i >= 0 && j >= 0;
+        if (inx) p.flag[0][(long long)(i + 1) + ex * ((long long)j + (long long)p.ny * k)] = (int8_t)kp;
+        if (iny) p.flag[1][(long long)i + (long long)p.nx * ((long long)(j + 1) + ey * k)] = (int8_t)kp;
+        if (inz) p.flag[2][(long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * (k + 1))] = (int8_t)kp;
+        if (p.flag_count) {          // faces per direction whose flag is not 1
+            const bool non1 = kp != 1;
+            const unsigned mx = __ballot_sync(0xffffffffu, non1 && inx), my = __ballot_sync(0xffffffffu, non1 && iny),
+                           mz = __ballot_sync(0xffffffffu, non1 && inz);
+            if (lane == 0) {
+                if (mx) atomicAdd(p.flag_count + 0, (unsigned)__popc(mx));
+                if (my) atomicAdd(p.flag_count + 1, (unsigned)__popc(my));
+                if (mz) atomicAdd(p.flag_count + 2, (unsigned)__popc(mz));
+            }
+        }
+        if (stats) {
+            const unsigned ms = __ballot_sync(0xffffffffu, live && sure), mu = __ballot_sync(0xffffffffu, live && !sure),
+                           md = __ballot_sync(0xffffffffu, live && sure && kp != plain);
+            n_sure += __popc(ms); n_unsure += __popc(mu); n_differ += __popc(md);
         }
     }
-    if (stats) {
-        const unsigned ms = __ballot_sync(act, sure), md = __ballot_sync(act, sure && kp != plain);
-        if (lane == __ffs(act) - 1) {
-            atomicAdd(stats + 0, (unsigned long long)__popc(ms));
-            atomicAdd(stats + 1, (unsigned long long)__popc(act & ~ms));
-            atomicAdd(stats + 2, (unsigned long long)__popc(md));
-        }
+    if (stats && lane == 0 && (n_sure | n_unsure | n_differ)) {
+        atomicAdd(stats + 0, n_sure);
+        atomicAdd(stats + 1, n_unsure);
+        atomicAdd(stats + 2, n_differ);
     }
 }
 
@@ -407,15 +448,18 @@ cudaError_t launch_switch_infer(const Params &p, const float *w, float conf_logi
         cudaError_t e = cudaMemsetAsync(p.flag_count, 0, 3 * sizeof(unsigned), st);
         if (e != cudaSuccess) return e;
     }
+    // persistent warps: a few resident blocks per SM, each warp over many tiles
     const long long n = (long long)(p.nx + 1) * (p.ny + 1) * (p.nz + 1);
-    const unsigned nb = (unsigned)((n + 127) / 128);
+    const long long need = (n + 127) / 128;
+    const unsigned nb = (unsigned)(need < 148 * 4 ? need : 148 * 4);
     if (p.mixed) k_switch_infer<float><<<nb, 128, 0, st>>>(p, w, conf_logit, stats);
     else         k_switch_infer<double><<<nb, 128, 0, st>>>(p, w, conf_logit, stats);
     return cudaGetLastError();
 }
 
 cudaError_t launch_mlp_infer(const float *w, const float *feat, long long n, float *logit, cudaStream_t st) {
-    k_mlp_infer<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, feat, n, logit);
+    const long long need = (n + 127) / 128;
+    k_mlp_infer<<<(unsigned)(need < 148 * 8 ? need : 148 * 8), 128, 0, st>>>(w, feat, n, logit);
     return cudaGetLastError();
 }
 
