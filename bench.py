@@ -137,16 +137,24 @@ def cells_of(case) -> int:
     return case.cfg.nx * case.cfg.ny * case.cfg.nz
 
 
-def cpu_baseline(workload: str, n_sample: int, steps: int = 1):
-    """The OpenMP FP64 oracle timed on this host on a bounded sample."""
+def cpu_baseline(workload: str, n_sample: int, steps: int = 0, budget_s: float = 12.0):
+    """The OpenMP FP64 oracle timed on this host on a bounded sample: whole
+    RK3 steps of the case at a reduced size until about budget_s seconds of
+    CPU work have run (or exactly `steps` steps when given)."""
     from oracle.oracle import Oracle
     c = make_case(workload, n_sample)
     cores = os.cpu_count() or 1
     o = Oracle(c.cfg, c.prims, c.metrics, nthreads=cores, inlet=c.inlet)
     o.step(1)                                   # warm-up
     t0 = time.perf_counter()
-    o.step(steps)
-    dt = time.perf_counter() - t0
+    done = 0
+    while True:
+        o.step(1)
+        done += 1
+        dt = time.perf_counter() - t0
+        if (steps and done >= steps) or (not steps and dt >= budget_s) or done >= 10000:
+            break
+    steps = done
     v = cells_of(c) * 3 * steps / dt / 1e9
     return {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
             "sample": f"{steps} RK3 step(s) of the same case at {c.cfg.nx}x{c.cfg.ny}x{c.cfg.nz} "
@@ -178,6 +186,11 @@ def run_ours(args, rank, world, dist):
     n = args.n
     case = make_case(args.workload, n)
     solver = lib.Solver(case.cfg, case.prims, case.metrics, device=dev, inlet=case.inlet)
+    if args.form != "fp64":             # precision form (and the learned switch)
+        solver.set_precision(1)
+    if args.form == "fp32-learned":
+        from ocfd_b200 import learned
+        solver.set_switch(learned.load_model(SWITCH_MODEL), 0.9)
     stream = torch.cuda.Stream(device=dev)
     solver.set_stream(stream.cuda_stream)
     cells = cells_of(case)
@@ -245,6 +258,8 @@ def run_ours(args, rank, world, dist):
     dom_ms_per_stage = fam[dom][0] / 3.0                  # one step = 3 stages
     uniform = solver.uniform_metrics
     dom_table = DOM_BYTES if uniform else DOM_BYTES_FIELDS
+    if args.form != "fp64":
+        dom_table = DOM_BYTES_FP32
     b_alg = B_ALG if uniform else B_ALG_FIELDS
     dom_bytes = dom_table.get(dom, b_alg) * cells
     achieved = dom_bytes / (dom_ms_per_stage / 1e3) / 1e9
@@ -253,9 +268,11 @@ def run_ours(args, rank, world, dist):
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.form == "fp64" else "f32 stencils / f64 RK3 accumulation",
+        "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload].format(nx=nx, ny=ny, nz=nz),
-                   "grid": [nx, ny, nz], "stages_per_step": 3,
+                   "grid": [nx, ny, nz], "stages_per_step": 3, "form": args.form,
                    "scheme": f"SCHEME_INVIS {case.cfg.scheme_invis}, CHARTERIC={case.cfg.charteric}",
                    "seed": 2024 if args.workload != "tgv" else 1234,
                    "l2": f"inputs larger than L2 (state ~{state_gb:.1f} GB/GPU)" if state_gb > 0.5
@@ -263,7 +280,8 @@ def run_ours(args, rank, world, dist):
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": (TRAFFIC_PER_CELL[dom] * cells if (uniform and dom in TRAFFIC_PER_CELL) else None),
+                     "traffic": (TRAFFIC_PER_CELL[dom] * cells
+                                 if (uniform and args.form == "fp64" and dom in TRAFFIC_PER_CELL) else None),
                      "traffic_source": TRAFFIC_SOURCE,
                      "algorithmic_bytes_per_cell": dom_table.get(dom, b_alg),
                      "launch_ms": dom_ms_per_stage},
@@ -309,6 +327,22 @@ DOM_BYTES_FIELDS = {
 }
 B_ALG_FIELDS = 200.0
 
+# The precision form (uniform grids): FP32 primitives, du and Ev, FP64 f, fn:
+#   inviscid_sweeps: 40 FP32 words                                 -> 160 B
+#   viscous_rk_update: u,v,w,T in, 12 Ev out and in, du in (FP32, 33 words),
+#                    fn, f in and f out (FP64, 15 words), d,u,v,w,T out (FP32)
+#                                                                  -> 272 B
+#   sensor / learned switch: d,T in (FP32), three int8 flags out   -> 11 B
+DOM_BYTES_FP32 = {
+    "inviscid_sweeps": 160.0,
+    "viscous_rk_update": 272.0,
+    "ghost_fill": 0.0,
+    "sensor": 11.0,
+}
+
+SWITCH_MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "opencfd-scu_b200", "ocfd_b200", "data",
+                            "switch_c1c3.npz")
+
 TRAFFIC_PER_CELL = {
     "inviscid_sweeps": 307.8,       # 3 sweeps + 3 fix-ups
     "viscous_rk_update": 377.6,     # k_vis_ev + k_vis_div (Ev ghost fill not captured)
@@ -323,7 +357,7 @@ def run_reference(args, rank, world):
     from oracle import ref_runner
     n = args.n
     if not ref_runner.available():
-        c = cpu_baseline(args.workload, max(8, n // 4), 1)
+        c = cpu_baseline(args.workload, max(8, n // 4))
         return {"impl": "reference", "metric": METRIC, "value": c["value"], "unit": METRIC,
                 "n_gpus": world, "steps": 1, "warmup": 1, "higher_is_better": True,
                 "note": "reference build missing; CPU oracle port timed instead",
@@ -354,11 +388,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="iso")
+    ap.add_argument("--form", choices=("fp64", "fp32", "fp32-learned"), default="fp64",
+                    help="fp64: the plain path; fp32: FP32 stencils with FP64 RK3 accumulation; "
+                         "fp32-learned: that with the learned scheme switch")
     ap.add_argument("--n", type=int, default=0,
                     help="grid size (iso, tgv: n^3; ramp: 4n x n x n/2); 0 = the configuration's own")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--ref-steps", type=int, default=4)
-    ap.add_argument("--cpu-sample", type=int, default=64)
+    ap.add_argument("--cpu-sample", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -383,7 +420,7 @@ def main():
         line = run_ours(args, rank, world, dist)
         if line is not None and not args.no_cpu_baseline:
             sample = {"iso": args.cpu_sample, "tgv": args.cpu_sample, "ramp": args.cpu_sample // 2}[args.workload]
-            line["cpu_baseline"] = cpu_baseline(args.workload, sample, 1)
+            line["cpu_baseline"] = cpu_baseline(args.workload, sample)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
