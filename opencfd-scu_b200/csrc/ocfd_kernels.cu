@@ -25,47 +25,50 @@ namespace ocfd {
 // hybrid sensor, style 2: Comput_P + Comput_Scheme_point_{x,y,z}_Jameson
 // (src/OCFD_Schemes_hybrid_auto.cu:48-68, :611-703).  Flag q along DIR
 // belongs to cell q-1; P = p00*d*T is formed on the fly from the LAP-box d,T
-// as they stand before this stage's ghost fill.
+// as they stand before this stage's ghost fill.  The three arrays' entries
+// of one cell share its value, so one thread per cell of the extended box
+// (-1 .. n-1 in each direction) forms it once and writes the entries the
+// cell owns: entry i+1 of the x array (j, k interior), j+1 of the y array,
+// k+1 of the z array.
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void k_sensor(Params p) {
-    long long nfx = (long long)(p.nx + 1) * p.ny * p.nz;
-    long long nfy = (long long)p.nx * (p.ny + 1) * p.nz;
-    long long nfz = (long long)p.nx * p.ny * (p.nz + 1);
-    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int dir;
-    long long q;
-    if (tid < nfx) { dir = 0; q = tid; }
-    else if (tid < nfx + nfy) { dir = 1; q = tid - nfx; }
-    else if (tid < nfx + nfy + nfz) { dir = 2; q = tid - nfx - nfy; }
-    else return;
-    int ex = p.nx + (dir == 0), ey = p.ny + (dir == 1);
-    int i = (int)(q % ex);
-    long long r = q / ex;
-    int j = (int)(r % ey);
-    int k = (int)(r / ey);
-    int ci = i + OCFD_LAP - (dir == 0), cj = j + OCFD_LAP - (dir == 1), ck = k + OCFD_LAP - (dir == 2);
-    const R *d = prim_r<R>(p, 0), *T = prim_r<R>(p, 4);
-    long long c = lap_index(p, ci, cj, ck);
-    const R p00 = (R)p.p00;
-    auto P = [&](long long o) { return p00 * d[o] * T[o]; };
-    R P0 = P(c);
-    R Pm = P(c - 1), Pp = P(c + 1);
-    R dp0 = fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
-    Pm = P(c - p.ys); Pp = P(c + p.ys);
-    dp0 += fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
-    Pm = P(c - p.zs); Pp = P(c + p.zs);
-    dp0 += fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
+    const long long ex = p.nx + 1, ey = p.ny + 1, ez = p.nz + 1;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= ex * ey * ez) return;
+    const int i = (int)(tid % ex) - 1;
+    const long long r = tid / ex;
+    const int j = (int)(r % ey) - 1, k = (int)(r / ey) - 1;
+    const bool inx = j >= 0 && k >= 0, iny = i >= 0 && k >= 0, inz = i >= 0 && j >= 0;
     int kp = 1;
-    if (dp0 > (R)p.dp1) kp += 1;
-    if (dp0 > (R)p.dp2) kp += 1;
-    p.flag[dir][q] = (int8_t)kp;
-    if (p.flag_count) {            // one atomic per warp and direction
+    if (inx || iny || inz) {
+        const R *d = prim_r<R>(p, 0), *T = prim_r<R>(p, 4);
+        const long long c = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+        const R p00 = (R)p.p00;
+        auto P = [&](long long o) { return p00 * d[o] * T[o]; };
+        R P0 = P(c);
+        R Pm = P(c - 1), Pp = P(c + 1);
+        R dp0 = fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
+        Pm = P(c - p.ys); Pp = P(c + p.ys);
+        dp0 += fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
+        Pm = P(c - p.zs); Pp = P(c + p.zs);
+        dp0 += fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
+        if (dp0 > (R)p.dp1) kp += 1;
+        if (dp0 > (R)p.dp2) kp += 1;
+        if (inx) p.flag[0][(long long)(i + 1) + ex * ((long long)j + (long long)p.ny * k)] = (int8_t)kp;
+        if (iny) p.flag[1][(long long)i + (long long)p.nx * ((long long)(j + 1) + ey * k)] = (int8_t)kp;
+        if (inz) p.flag[2][(long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * (k + 1))] = (int8_t)kp;
+    }
+    if (p.flag_count) {            // faces per direction whose flag is not 1
         const unsigned act = __activemask();
         const int lane = threadIdx.x & 31;
-        for (int d = 0; d < 3; d++) {
-            const unsigned m = __ballot_sync(act, dir == d && kp != 1);
-            if (m && lane == __ffs(act) - 1) atomicAdd(p.flag_count + d, (unsigned)__popc(m));
+        const bool non1 = kp != 1;
+        const unsigned mx = __ballot_sync(act, non1 && inx), my = __ballot_sync(act, non1 && iny),
+                       mz = __ballot_sync(act, non1 && inz);
+        if (lane == __ffs(act) - 1) {
+            if (mx) atomicAdd(p.flag_count + 0, (unsigned)__popc(mx));
+            if (my) atomicAdd(p.flag_count + 1, (unsigned)__popc(my));
+            if (mz) atomicAdd(p.flag_count + 2, (unsigned)__popc(mz));
         }
     }
 }
@@ -399,16 +402,29 @@ __device__ __forceinline__ void cons_to_prim(const Params &p, const double f[5],
     T2 = div_const(f[4] - 0.5 * d1 * (u1 * u1 + v1 * v1 + w1 * w1), dcv, 1.0 / dcv);
 }
 
+// Cell of a thread of the viscous kernels: a block of 256 threads covers a
+// 32 x 8 tile of one z plane (grid: x tiles * y tiles, nz), so most y
+// neighbours of its cells are loaded by the same block and meet in L1.
+constexpr int VT_X = 32, VT_Y = 8;
+__device__ __forceinline__ bool tile_cell(const Params &p, int &i, int &j, int &k, long long &tid) {
+    const int ntx = (p.nx + VT_X - 1) / VT_X;
+    i = (int)(blockIdx.x % ntx) * VT_X + (int)(threadIdx.x % VT_X);
+    j = (int)(blockIdx.x / ntx) * VT_Y + (int)(threadIdx.x / VT_X);
+    k = (int)blockIdx.y;
+    if (i >= p.nx || j >= p.ny) return false;
+    tid = in_index(p, i, j, k);
+    return true;
+}
+
 // Ev1..4 of all three directions (vis_flux_ker :178-236).  The 12 velocity
 // and temperature derivatives (du_viscous_Jacobian3d_init :58-77) are formed
 // here from the LAP-box primitives instead of being stored; the stress and
 // heat flux do not depend on the direction, so they are formed once per cell.
 template <bool UNI, typename R>
 __global__ void __launch_bounds__(256, 5) k_vis_ev(Params p) {
-    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= p.N) return;
-    int i = (int)(tid % p.nx); long long r = tid / p.nx;
-    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    int i, j, k;
+    long long tid;
+    if (!tile_cell(p, i, j, k, tid)) return;
     long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     const bool c8 = p.scheme_vis == 204;
     R Akx = (R)metric<UNI>(p, M_AKX, o), Aix = (R)metric<UNI>(p, M_AIX, o), Asx = (R)metric<UNI>(p, M_ASX, o);
@@ -532,10 +548,9 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
 // and the face re-projection follow in the same thread and du is not stored.
 template <bool UNI, bool RK, typename R>
 __global__ void __launch_bounds__(256, 5) k_vis_div(Params p, int krk) {
-    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= p.N) return;
-    int i = (int)(tid % p.nx); long long r = tid / p.nx;
-    int j = (int)(r % p.ny); int k = (int)(r / p.ny);
+    int i, j, k;
+    long long tid;
+    if (!tile_cell(p, i, j, k, tid)) return;
     long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     const long long st[3] = { 1LL, p.ys, p.zs };
     const R hh[3] = { (R)p.hx, (R)p.hy, (R)p.hz };
@@ -705,8 +720,7 @@ static cudaError_t launch_sweep(const Params &p, cudaStream_t st) {
 }
 
 cudaError_t launch_sensor(const Params &p, cudaStream_t st) {
-    long long n = (long long)(p.nx + 1) * p.ny * p.nz + (long long)p.nx * (p.ny + 1) * p.nz
-                + (long long)p.nx * p.ny * (p.nz + 1);
+    const long long n = (long long)(p.nx + 1) * (p.ny + 1) * (p.nz + 1);
     if (p.flag_count) {
         cudaError_t e = cudaMemsetAsync(p.flag_count, 0, 3 * sizeof(unsigned), st);
         if (e != cudaSuccess) return e;
@@ -745,7 +759,7 @@ cudaError_t launch_sweeps(const Params &p, cudaStream_t st) {
 
 template <typename R>
 static cudaError_t launch_viscous_t(const Params &p, int krk, cudaStream_t st) {
-    unsigned nb = blocks_for(p.N, 256);
+    const dim3 nb((unsigned)(((p.nx + VT_X - 1) / VT_X) * ((p.ny + VT_Y - 1) / VT_Y)), (unsigned)p.nz);
     if (p.uniform_metrics) k_vis_ev<true, R><<<nb, 256, 0, st>>>(p);
     else                   k_vis_ev<false, R><<<nb, 256, 0, st>>>(p);
     R *evf[12]; int mask[12];
