@@ -57,9 +57,9 @@ __device__ __forceinline__ void switch_features(const Params &p, long long c, co
         f[a] = (float)t;
         f[3 + a] = (float)((Pp - Pm) / den);
         const R Dm = d[c + om[a]], Dp = d[c + op[a]];
-        const R dd = Dm + 2*D0 + Dp;
-        f[6 + a] = (float)(fabs(-Dm + 2*D0 - Dp) / dd);
-        f[9 + a] = (float)((Dp - Dm) / dd);
+        const R rdd = (R)1 / (Dm + 2*D0 + Dp);
+        f[6 + a] = (float)(fabs(-Dm + 2*D0 - Dp) * rdd);
+        f[9 + a] = (float)((Dp - Dm) * rdd);
     }
     f[12] = f[0] + f[1] + f[2];
     f[13] = f[6] + f[7] + f[8];
@@ -217,15 +217,16 @@ __device__ __forceinline__ float warp_mlp(const MlpFrag &fr, const float (&x)[ML
     return sL[lane] + fr.b3;
 }
 
-__device__ __forceinline__ void standardise(const float *mu, const float *sg, const float (&f)[MLP_IN],
+// (f - mu) / sigma, as a product with the block's reciprocals of sigma
+__device__ __forceinline__ void standardise(const float *mu, const float *isg, const float (&f)[MLP_IN],
                                             float (&x)[MLP_IN]) {
 #pragma unroll
-    for (int m = 0; m < MLP_IN; m++) x[m] = (f[m] - mu[m]) / sg[m];
+    for (int m = 0; m < MLP_IN; m++) x[m] = (f[m] - mu[m]) * isg[m];
 }
 
-// the block's copy of the standardisation constants
-__device__ __forceinline__ void load_standard(const float *__restrict__ w, float *sMu, float *sSg) {
-    if (threadIdx.x < MLP_IN) { sMu[threadIdx.x] = w[OFF_MU + threadIdx.x]; sSg[threadIdx.x] = w[OFF_SG + threadIdx.x]; }
+// the block's copy of the standardisation constants (mu, 1 / sigma)
+__device__ __forceinline__ void load_standard(const float *__restrict__ w, float *sMu, float *sIsg) {
+    if (threadIdx.x < MLP_IN) { sMu[threadIdx.x] = w[OFF_MU + threadIdx.x]; sIsg[threadIdx.x] = 1.0f / w[OFF_SG + threadIdx.x]; }
     __syncthreads();
 }
 
@@ -234,8 +235,8 @@ __device__ __forceinline__ void load_standard(const float *__restrict__ w, float
 __global__ void __launch_bounds__(128) k_mlp_infer(const float *__restrict__ w, const float *__restrict__ feat,
                                                    long long n, float *logit) {
     __shared__ __align__(16) __nv_bfloat16 sA[4][32 * 16];
-    __shared__ float sL[4][32], sMu[MLP_IN], sSg[MLP_IN];
-    load_standard(w, sMu, sSg);
+    __shared__ float sL[4][32], sMu[MLP_IN], sIsg[MLP_IN];
+    load_standard(w, sMu, sIsg);
     MlpFrag fr;
     load_frags(w, fr);
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -245,7 +246,7 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const float *__restrict__ w, 
         float f[MLP_IN], x[MLP_IN];
 #pragma unroll
         for (int m = 0; m < MLP_IN; m++) f[m] = row < n ? feat[row * MLP_IN + m] : 0.0f;
-        standardise(sMu, sSg, f, x);
+        standardise(sMu, sIsg, f, x);
         const float z = warp_mlp(fr, x, sA[wid], sL[wid]);
         if (row < n) logit[row] = z;
     }
@@ -261,8 +262,8 @@ template <typename R>
 __global__ void __launch_bounds__(128) k_switch_infer(Params p, const float *__restrict__ w, float conf_logit,
                                                       unsigned long long *stats) {
     __shared__ __align__(16) __nv_bfloat16 sA[4][32 * 16];
-    __shared__ float sL[4][32], sMu[MLP_IN], sSg[MLP_IN];
-    load_standard(w, sMu, sSg);
+    __shared__ float sL[4][32], sMu[MLP_IN], sIsg[MLP_IN];
+    load_standard(w, sMu, sIsg);
     MlpFrag fr;
     load_frags(w, fr);
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(128) k_switch_infer(Params p, const float *__r
             switch_features<R>(p, lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP), om, op, f, dp);
         }
         float x[MLP_IN];
-        standardise(sMu, sSg, f, x);
+        standardise(sMu, sIsg, f, x);
         const float z = warp_mlp(fr, x, sA[wid], sL[wid]);
         const int plain = plain_flag(p, dp);
         const bool sure = fabsf(z) >= conf_logit;
