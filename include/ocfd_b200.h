@@ -120,6 +120,11 @@ int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl);
  * whole steps only (ocfd_b200_step).  Switching back recomputes the FP64
  * primitives from the conserved state. */
 int ocfd_b200_set_precision(ocfd_b200_ctx *ctx, int form);
+/* HybridAuto_scheme_Proportion (src/OCFD_Schemes_hybrid_auto.cu:745-829):
+ * frac[3*d + t], the share of direction d's flag entries that are 1 (t=0),
+ * 2 (t=1) or any other value (t=2), for the flags the last sensor pass
+ * wrote. */
+int ocfd_b200_scheme_proportion(ocfd_b200_ctx *ctx, double frac[9]);
 /* Learned scheme switch (hybrid scheme).  A 14 -> 32 -> 32 -> 1 ReLU network
  * over normalised pressure and density differences on the sensor's 7-point
  * stencil takes the place of the plain sensor's choice

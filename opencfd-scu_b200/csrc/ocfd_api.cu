@@ -22,6 +22,7 @@ cudaError_t launch_sensor(const Params &p, cudaStream_t st);
 cudaError_t launch_ghost(const Params &p, double *const *fields, const int *dirmask, int nf, cudaStream_t st);
 cudaError_t launch_ghost32(const Params &p, float *const *fields, const int *dirmask, int nf, cudaStream_t st);
 cudaError_t launch_prims_to_fp32(const Params &p, cudaStream_t st);
+cudaError_t launch_flag_hist(const Params &p, unsigned long long *counts, cudaStream_t st);
 cudaError_t launch_sweeps(const Params &p, cudaStream_t st);
 cudaError_t launch_viscous(const Params &p, int krk, cudaStream_t st);
 cudaError_t launch_rk(const Params &p, int krk, cudaStream_t st);
@@ -87,7 +88,7 @@ struct ocfd_b200_ctx {
     double *ev_buf = nullptr;     // 12 LAP fields
     int8_t *flag_buf = nullptr;
     double *stage_buf = nullptr;  // 5 interior fields for host transfers
-    double *red_buf = nullptr;    // reduction partials + result, then two counters
+    double *red_buf = nullptr;    // reduction partials + result, then 16 words of counters
     unsigned *defer_buf = nullptr;  // three counters (padded to 256 B), then 3 deferred-cell lists
     double *filter_buf = nullptr;   // pf_lap (5 LAP fields) and the pressure (1 LAP field)
     // FILTER_NPARA / FILTER_RPARA as set_para_filtering leaves them
@@ -270,7 +271,7 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
         (rc = alloc((void **)&ctx->ev_buf, 12 * lapB, "viscous fluxes")) ||
         (rc = alloc((void **)&ctx->flag_buf, flagN, "flags")) ||
         (rc = alloc((void **)&ctx->stage_buf, 5 * inB, "staging")) ||
-        (rc = alloc((void **)&ctx->red_buf, sizeof(double) * (ocfd::reduce_scratch_doubles() + 2), "reduction")) ||
+        (rc = alloc((void **)&ctx->red_buf, sizeof(double) * (ocfd::reduce_scratch_doubles() + 16), "reduction")) ||
         // deferred-cell lists of the call-free sweep (cell indices fit 32 bits)
         (N < (1LL << 32) && (rc = alloc((void **)&ctx->defer_buf, sizeof(unsigned) * (64 + 3 * (size_t)N),
                                         "deferred cells")))) {
@@ -1231,6 +1232,26 @@ extern "C" int ocfd_b200_check_state(ocfd_b200_ctx *ctx, long long *n_nan, long 
     if (n_nan) *n_nan = (long long)c[0];
     if (n_neg_t) *n_neg_t = (long long)c[1];
     if (mean_t) *mean_t = host[0];
+    return OCFD_OK;
+}
+
+// HybridAuto_scheme_Proportion (src/OCFD_Schemes_hybrid_auto.cu:745-829):
+// frac[3 * dir + t] = share of direction dir's flag entries of type t (flag
+// 1, flag 2, any other value), as the reference prints them
+extern "C" int ocfd_b200_scheme_proportion(ocfd_b200_ctx *ctx, double frac[9]) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (!frac) return fail(ctx, OCFD_ERR_ARG, "frac is null");
+    const Params &p = ctx->p;
+    unsigned long long *counts = reinterpret_cast<unsigned long long *>(ctx->red_buf + ocfd::reduce_scratch_doubles());
+    CK(ocfd::launch_flag_hist(p, counts, ctx->stream), "scheme proportion");
+    ctx->launches += 1;
+    unsigned long long h[9];
+    CK(cudaMemcpyAsync(h, counts, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "scheme proportion");
+    CK(cudaStreamSynchronize(ctx->stream), "scheme proportion");
+    const double n[3] = {(double)(p.nx + 1) * p.ny * p.nz, (double)p.nx * (p.ny + 1) * p.nz,
+                         (double)p.nx * p.ny * (p.nz + 1)};
+    for (int i = 0; i < 9; i++) frac[i] = (double)h[i] / n[i / 3];
     return OCFD_OK;
 }
 

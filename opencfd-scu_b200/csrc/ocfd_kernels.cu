@@ -421,7 +421,7 @@ __device__ __forceinline__ bool tile_cell(const Params &p, int &i, int &j, int &
 // here from the LAP-box primitives instead of being stored; the stress and
 // heat flux do not depend on the direction, so they are formed once per cell.
 template <bool UNI, typename R>
-__global__ void __launch_bounds__(256, 5) k_vis_ev(Params p) {
+__global__ void __launch_bounds__(256, sizeof(R) == 8 ? 5 : 6) k_vis_ev(Params p) {
     int i, j, k;
     long long tid;
     if (!tile_cell(p, i, j, k, tid)) return;
@@ -547,7 +547,7 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
 // RK = true: the stage's du is complete here, so the RK update, cons->prim
 // and the face re-projection follow in the same thread and du is not stored.
 template <bool UNI, bool RK, typename R>
-__global__ void __launch_bounds__(256, 5) k_vis_div(Params p, int krk) {
+__global__ void __launch_bounds__(256, 6) k_vis_div(Params p, int krk) {
     int i, j, k;
     long long tid;
     if (!tile_cell(p, i, j, k, tid)) return;
@@ -689,6 +689,28 @@ __global__ void k_prims_to_fp32(Params p) {
     p.prim32[m][q] = (float)p.prim[m][q];
 }
 
+// HybridAuto_scheme_Proportion (src/OCFD_Schemes_hybrid_auto.cu:745-829):
+// per direction, the entries of the flag array equal to 1, equal to 2, and
+// any other value; counts[3 * dir + type]
+__global__ void k_flag_hist(Params p, unsigned long long *counts) {
+    const long long nfx = (long long)(p.nx + 1) * p.ny * p.nz, nfy = (long long)p.nx * (p.ny + 1) * p.nz,
+                    nfz = (long long)p.nx * p.ny * (p.nz + 1);
+    unsigned long long c[9] = {};
+    const long long tot = nfx + nfy + nfz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const int d = t < nfx ? 0 : (t < nfx + nfy ? 1 : 2);
+        const long long q = d == 0 ? t : (d == 1 ? t - nfx : t - nfx - nfy);
+        const int f = p.flag[d][q];
+        c[3 * d + (f == 1 ? 0 : (f == 2 ? 1 : 2))] += 1;
+    }
+#pragma unroll
+    for (int i = 0; i < 9; i++) {
+        unsigned long long v = c[i];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(counts + i, v);
+    }
+}
+
 __global__ void k_fill(double *f, long long n, double v) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid < n) f[tid] = v;
@@ -815,6 +837,13 @@ cudaError_t launch_rk_only(const Params &p, int krk, cudaStream_t st) {
     k_rk_only<<<blocks_for(5 * p.N, 256), 256, 0, st>>>(p, krk);
     return cudaGetLastError();
 }
+cudaError_t launch_flag_hist(const Params &p, unsigned long long *counts, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(counts, 0, 9 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    k_flag_hist<<<4 * 148, 256, 0, st>>>(p, counts);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_prims_to_fp32(const Params &p, cudaStream_t st) {
     k_prims_to_fp32<<<blocks_for(5 * p.lapN, 256), 256, 0, st>>>(p);
     return cudaGetLastError();

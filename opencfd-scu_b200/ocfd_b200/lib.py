@@ -30,7 +30,7 @@ EXPORTED = (
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
     "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics", "ocfd_b200_set_sweep_impl",
     "ocfd_b200_sweep_walks", "ocfd_b200_set_precision",
-    "ocfd_b200_mlp_nparam", "ocfd_b200_set_switch", "ocfd_b200_switch_stats", "ocfd_b200_switch_features",
+    "ocfd_b200_scheme_proportion", "ocfd_b200_mlp_nparam", "ocfd_b200_set_switch", "ocfd_b200_switch_stats", "ocfd_b200_switch_features",
     "ocfd_b200_mlp_last_error", "ocfd_b200_mlp_infer", "ocfd_b200_mlp_grad", "ocfd_b200_mlp_train",
     "ocfd_b200_set_mesh", "ocfd_b200_set_mesh_device", "ocfd_b200_get_metrics",
     "ocfd_b200_set_filter", "ocfd_b200_filtering", "ocfd_b200_set_time", "filtering", "ocfd_b200_set_bc",
@@ -120,6 +120,7 @@ def load(path: Optional[str] = None):
         "ocfd_b200_set_sweep_impl": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_sweep_walks": (ctypes.c_int, [P]),
         "ocfd_b200_set_precision": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_scheme_proportion": (ctypes.c_int, [P, D]),
         "ocfd_b200_mlp_nparam": (ctypes.c_int, []),
         "ocfd_b200_set_switch": (ctypes.c_int, [P, F, ctypes.c_int, ctypes.c_double]),
         "ocfd_b200_switch_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_longlong)]),
@@ -339,6 +340,12 @@ class Solver:
         y = np.empty(count, np.float32)
         self._check(self.L.ocfd_b200_switch_features(self.h, first, count, _fp(f), _fp(y)), "switch_features")
         return f, y
+
+    def scheme_proportion(self) -> np.ndarray:
+        """[direction][type]: share of each flag array's entries that are 1, 2, other."""
+        out = np.zeros(9)
+        self._check(self.L.ocfd_b200_scheme_proportion(self.h, _dp(out)), "scheme_proportion")
+        return out.reshape(3, 3)
 
     def sweep_walks(self) -> int:
         """Bit d set: direction d takes the walk that forms every face in line."""

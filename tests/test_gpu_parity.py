@@ -248,6 +248,20 @@ def test_walk_choice_follows_sensor(gpu_lib):
     assert s.sweep_walks() == 7
 
 
+def test_scheme_proportion(gpu_lib):
+    """HybridAuto_scheme_Proportion: the shares of flags 1, 2 and other per
+    direction, against counts of the flag arrays read back."""
+    c = cases.random_smooth_case(13, 17, 11, seed=4, scheme_invis="SCHEME_HYBRIDAUTO", charteric=1,
+                                 shock=True, curvilinear=True)
+    s = lib.Solver(c.cfg, c.prims, c.metrics)
+    s.step(1)
+    got = s.scheme_proportion()
+    for d, f in enumerate(s.flags()):
+        want = [np.mean(f == 1), np.mean(f == 2), np.mean((f != 1) & (f != 2))]
+        assert np.allclose(got[d], want, rtol=0, atol=1e-15), (d, got[d], want)
+    assert np.allclose(got.sum(1), 1.0)
+
+
 @pytest.mark.parametrize("iperiodic", [(0, 0, 1), (1, 0, 0), (0, 0, 0)], ids=["z_per", "x_per", "closed"])
 def test_metrics_from_mesh_match_oracle(iperiodic, gpu_lib):
     """Comput_Jacobian3d on the GPU against the oracle's restatement: the 13
