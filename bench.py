@@ -313,7 +313,7 @@ DOM_BYTES = {
 
 # Measured DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell
 # for one stage's launches of each family, from one ncu capture of the same
-# kernels at 160^3 (profiles/stage_kernels_iso160.txt); the traffic scales with
+# kernels at 160^3 (profiles/stage_traffic_iso160.txt); the traffic scales with
 # the cells processed, so the bench line reports it times the cells of a launch.
 # Grids whose metrics are fields (the ramp): the sweeps also read the
 # direction's 3 metrics at every split point and Ajac per cell (+4 words per
@@ -344,10 +344,10 @@ SWITCH_MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "opencfd
                             "switch_c1c3.npz")
 
 TRAFFIC_PER_CELL = {
-    "inviscid_sweeps": 307.8,       # 3 sweeps + 3 fix-ups
-    "viscous_rk_update": 377.6,     # k_vis_ev + k_vis_div (Ev ghost fill not captured)
+    "inviscid_sweeps": 304.6,       # 3 sweeps + 3 fix-ups
+    "viscous_rk_update": 385.6,     # k_vis_ev + k_vis_div (Ev ghost fill not captured)
 }
-TRAFFIC_SOURCE = "ncu capture at 160^3 scaled by cells (profiles/stage_kernels_iso160.txt)"
+TRAFFIC_SOURCE = "ncu capture at 160^3 scaled by cells (profiles/stage_traffic_iso160.txt)"
 
 
 def run_reference(args, rank, world):
