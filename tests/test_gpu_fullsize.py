@@ -179,3 +179,17 @@ def test_c4_ramp_500_steps_within_reference_sensitivity(ramp500):
     err = rel_l2(s.primitives(), ref)
     assert np.all(spread > 1e-9), spread          # the sensitivity is real
     assert np.all(err <= 2.0 * spread), (err, spread)
+
+
+def test_c3_precision_form_256_50_steps(iso256):
+    """C3: the precision form on the C2 input against the FP64 path after 50
+    steps (measured 8e-8 .. 1.6e-7 relative L2 on the conserved variables;
+    bound 1e-6)."""
+    case, _, _ = iso256
+    a = lib.Solver(case.cfg, case.prims, case.metrics)
+    b = lib.Solver(case.cfg, case.prims, case.metrics)
+    b.set_precision(1)
+    a.step(50)
+    b.step(50)
+    err = rel_l2(b.conserved(), a.conserved())
+    assert np.all(err <= 1e-6) and np.all(err > 0), err
