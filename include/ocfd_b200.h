@@ -224,6 +224,28 @@ int ocfd_b200_time_advance(ocfd_b200_ctx *ctx, int krk);   /* src/OCFD_time.cu:9
 int ocfd_b200_get_duvwT(ocfd_b200_ctx *ctx);               /* src/commen_kernel.cu:111-118 */
 int ocfd_b200_bc(ocfd_b200_ctx *ctx);                      /* src/OCFD_boundary.cu:18-92  */
 
+/* ---- the grid split in z across GPUs (one z slab per process) --------- */
+/* Replaces the reference's z decomposition (part3d with NPX0 = NPY0 = 1,
+ * src/OCFD_mpi.c:120-190) and its z halo exchange
+ * (exchange_boundary_z_packed_dev, src/OCFD_mpi_dev.cu:271-310, host-staged
+ * MPI_Sendrecv there): the ghost planes of each slab come from its
+ * neighbours' interior planes over NCCL, device to device, wherever the
+ * single-GPU path wraps z.  The context's nz is the slab's plane count.
+ * ocfd_b200_slab_unique_id: one rank makes the id (NCCL's unique id) and
+ * hands it to the others (e.g. over torch.distributed).
+ * ocfd_b200_set_slab: call on every rank, right after create and before the
+ * filters, metrics and state (collective: it returns once all nranks have
+ * joined); rank_lo / rank_hi are the ranks holding the planes below / above
+ * (ID_ZM1 / ID_ZP1, src/OCFD_mpi.c:183-189), z_offset this slab's first
+ * global plane (k_offset).  Requires IPERIODIC z = 1 and at least 4 planes
+ * per slab.  ana_residual, check_state and scheme_proportion then return
+ * whole-grid values on every rank; the per-step walk choice uses the whole
+ * grid's flag counts.  OCFD_ERR_UNSUPPORTED when NCCL cannot be loaded. */
+#define OCFD_SLAB_ID_BYTES 128
+int ocfd_b200_slab_unique_id(unsigned char id[OCFD_SLAB_ID_BYTES]);
+int ocfd_b200_set_slab(ocfd_b200_ctx *ctx, int nranks, int rank, int rank_lo, int rank_hi, int z_offset,
+                       int nz_global, const unsigned char id[OCFD_SLAB_ID_BYTES]);
+
 /* Read-back (synchronous). */
 int ocfd_b200_get_primitives(ocfd_b200_ctx *ctx, double *prim5);
 int ocfd_b200_get_primitives_device(ocfd_b200_ctx *ctx, double *prim5_dev);

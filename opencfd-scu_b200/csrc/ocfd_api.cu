@@ -24,7 +24,9 @@ cudaError_t launch_ghost32(const Params &p, float *const *fields, const int *dir
 cudaError_t launch_prims_to_fp32(const Params &p, cudaStream_t st);
 cudaError_t launch_flag_hist(const Params &p, unsigned long long *counts, cudaStream_t st);
 cudaError_t launch_sweeps(const Params &p, cudaStream_t st);
-cudaError_t launch_viscous(const Params &p, int krk, cudaStream_t st);
+cudaError_t launch_vis_ev(const Params &p, cudaStream_t st);
+cudaError_t launch_vis_div(const Params &p, int krk, cudaStream_t st);
+void ev_ghost_fields(const Params &p, void *fields[12], int dirmask[12]);
 cudaError_t launch_rk(const Params &p, int krk, cudaStream_t st);
 cudaError_t launch_rk_only(const Params &p, int krk, cudaStream_t st);
 cudaError_t launch_c2p(const Params &p, cudaStream_t st);
@@ -33,8 +35,17 @@ cudaError_t launch_p2c(const Params &p, double *out, cudaStream_t st);
 cudaError_t launch_scatter(const Params &p, const double *src, double *dst_lap, cudaStream_t st);
 cudaError_t launch_gather(const Params &p, const double *src_lap, double *dst, cudaStream_t st);
 cudaError_t launch_fill(double *f, long long n, double v, cudaStream_t st);
-cudaError_t launch_mean(const Params &p, int which, double *scratch, unsigned long long *counts,
+cudaError_t launch_mean(const Params &p, int which, double *scratch, unsigned long long *counts, double ncell,
                         cudaStream_t st);
+struct Slab;
+int slab_unique_id(unsigned char id[128], std::string &err);
+Slab *slab_create(const Params &p, int nranks, int rank, int lo, int hi, const unsigned char id[128],
+                  std::string &err);
+void slab_destroy(Slab *s);
+int slab_exchange(Slab *s, const Params &p, double *const *f, int nf, cudaStream_t st, std::string &err);
+int slab_exchange32(Slab *s, const Params &p, float *const *f, int nf, cudaStream_t st, std::string &err);
+int slab_allreduce(Slab *s, void *buf, size_t count, int type, cudaStream_t st, std::string &err);
+int slab_launches_per_exchange();
 int reduce_scratch_doubles();
 cudaError_t launch_sweeps2(const Params &p, cudaStream_t st);
 cudaError_t launch_sweeps3(const Params &p, cudaStream_t st);
@@ -120,6 +131,11 @@ struct ocfd_b200_ctx {
     float sw_conf_logit = 0.0f;
     int walk4[3] = {1, 1, 1};
     double walk4_threshold = 0.002;     // deferred cells per cell above which the inline walk is used
+    // the grid split in z across GPUs: this rank's slab starts at global
+    // plane z_offset of nz_global; ghost planes in z come from the
+    // neighbouring slabs (null: one GPU holds the grid)
+    ocfd::Slab *slab = nullptr;
+    int z_offset = 0, nz_global = 0, slab_count = 1;
     bool have_metrics = false;
     int metric_mode = 0;          // 0 auto-detect uniform grids, 1 always read the fields
     bool have_state = false;
@@ -133,6 +149,11 @@ struct ocfd_b200_ctx {
     long long t_n[OCFD_TIMER_COUNT] = {0};
     std::string err;
 };
+
+// interior cells of the whole grid
+static double global_cells(const ocfd_b200_ctx *c) {
+    return c->slab ? (double)c->p.nx * c->p.ny * c->nz_global : (double)c->p.N;
+}
 
 static int fail(ocfd_b200_ctx *c, int code, const std::string &msg) {
     if (c) c->err = msg; else g_create_error = msg;
@@ -178,6 +199,8 @@ static void free_all(ocfd_b200_ctx *c) {
     cudaFree(c->prec_buf);
     cudaFree(c->sw_w);
     cudaFree(c->sw_stats);
+    ocfd::slab_destroy(c->slab);
+    c->slab = nullptr;
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
@@ -244,6 +267,7 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     p.inv_h[0] = 1.0 / p.hx; p.inv_h[1] = 1.0 / p.hy; p.inv_h[2] = 1.0 / p.hz;
     p.inv_Ama = 1.0 / Ma;
     for (int d = 0; d < 3; d++) p.periodic[d] = cfg->iperiodic[d];
+    p.zface_lo = p.zface_hi = 1;
     p.has_bnd = 0;
     for (int d = 0; d < 3; d++) {
         p.bnd_lo[d] = cfg->dif_bound[2 * d] == 1;
@@ -341,12 +365,55 @@ extern "C" int ocfd_b200_synchronize(ocfd_b200_ctx *ctx) {
 // internal helpers
 // ---------------------------------------------------------------------------
 
+static cudaError_t ghost_launch(const Params &p, double *const *f, const int *mask, int n, cudaStream_t st) {
+    return ocfd::launch_ghost(p, f, mask, n, st);
+}
+static cudaError_t ghost_launch(const Params &p, float *const *f, const int *mask, int n, cudaStream_t st) {
+    return ocfd::launch_ghost32(p, f, mask, n, st);
+}
+static int slab_exchange(ocfd_b200_ctx *ctx, double *const *f, int n, std::string &err) {
+    return ocfd::slab_exchange(ctx->slab, ctx->p, f, n, ctx->stream, err);
+}
+static int slab_exchange(ocfd_b200_ctx *ctx, float *const *f, int n, std::string &err) {
+    return ocfd::slab_exchange32(ctx->slab, ctx->p, f, n, ctx->stream, err);
+}
+
+// Ghost fill of LAP-box fields, mask bit d for direction d: the periodic
+// wrap on one GPU; with the grid split in z, the x and y wraps here and the
+// z ghost planes from the neighbouring slabs (the reference's
+// exchange_boundary_{x,y,z}_packed_dev order, src/OCFD_mpi_dev.cu:186-310)
+template <typename T>
+static int fill_ghosts(ocfd_b200_ctx *ctx, T *const *f, const int *mask, int n, const char *what) {
+    if (!ctx->slab) {
+        CK(ghost_launch(ctx->p, f, mask, n, ctx->stream), what);
+        ctx->launches += 1;
+        return OCFD_OK;
+    }
+    int mxy[16];
+    T *fz[16];
+    int nz = 0;
+    bool xy = false;
+    for (int m = 0; m < n; m++) {
+        mxy[m] = mask[m] & 3;
+        xy = xy || mxy[m];
+        if (mask[m] & 4) fz[nz++] = f[m];
+    }
+    if (xy) {
+        CK(ghost_launch(ctx->p, f, mxy, n, ctx->stream), what);
+        ctx->launches += 1;
+    }
+    if (nz) {
+        std::string err;
+        if (slab_exchange(ctx, fz, nz, err)) return fail(ctx, OCFD_ERR_CUDA, std::string(what) + ": " + err);
+        ctx->launches += ocfd::slab_launches_per_exchange();
+    }
+    return OCFD_OK;
+}
+
 static int ghost_prims64(ocfd_b200_ctx *ctx) {
     double *f[5]; int mask[5];
     for (int m = 0; m < 5; m++) { f[m] = ctx->p.prim[m]; mask[m] = 7; }
-    CK(ocfd::launch_ghost(ctx->p, f, mask, 5, ctx->stream), "ghost fill");
-    ctx->launches += 1;
-    return OCFD_OK;
+    return fill_ghosts(ctx, f, mask, 5, "ghost fill");
 }
 
 // the primitives the stencils read: FP64, or FP32 in the precision form
@@ -354,9 +421,7 @@ static int ghost_prims(ocfd_b200_ctx *ctx) {
     if (!ctx->p.mixed) return ghost_prims64(ctx);
     float *f[5]; int mask[5];
     for (int m = 0; m < 5; m++) { f[m] = ctx->p.prim32[m]; mask[m] = 7; }
-    CK(ocfd::launch_ghost32(ctx->p, f, mask, 5, ctx->stream), "ghost fill");
-    ctx->launches += 1;
-    return OCFD_OK;
+    return fill_ghosts(ctx, f, mask, 5, "ghost fill");
 }
 
 // precision form: FP64 primitives (interior and ghosts) from the FP64
@@ -374,11 +439,10 @@ static int refresh_prims64(ocfd_b200_ctx *ctx) {
 static int ghost_metrics(ocfd_b200_ctx *ctx) {
     double *f[12]; int mask[12];
     for (int m = 0; m < 12; m++) { f[m] = const_cast<double *>(ctx->p.met[m]); mask[m] = 7; }
-    CK(ocfd::launch_ghost(ctx->p, f, mask, 12, ctx->stream), "metric ghost fill");
+    int rc = fill_ghosts(ctx, f, mask, 12, "metric ghost fill");
+    if (rc) return rc;
     double *fj[1] = { const_cast<double *>(ctx->p.met[12]) }; int mj[1] = { 7 };
-    CK(ocfd::launch_ghost(ctx->p, fj, mj, 1, ctx->stream), "metric ghost fill");
-    ctx->launches += 2;
-    return OCFD_OK;
+    return fill_ghosts(ctx, fj, mj, 1, "metric ghost fill");
 }
 
 struct TimerScope {
@@ -424,7 +488,10 @@ static int apply_bc(ocfd_b200_ctx *ctx) {
 // such cells the walk that forms every face in line is faster.
 static bool walk4_wanted(const ocfd_b200_ctx *ctx, int d, unsigned nonup7) {
     const Params &p = ctx->p;
-    const long long nf = (long long)(p.nx + (d == 0)) * (p.ny + (d == 1)) * (p.nz + (d == 2));
+    // flag entries the count covers (with the grid split in z, the counts are
+    // summed over the slabs, each with its own nz + 1 entries in z)
+    const long long nzc = ctx->slab ? (long long)ctx->nz_global + (d == 2) * (ctx->slab_count - 1) : p.nz;
+    const long long nf = (long long)(p.nx + (d == 0)) * (p.ny + (d == 1)) * (nzc + (d == 2));
     const int n = d == 0 ? p.nx : (d == 1 ? p.ny : p.nz);
     const bool ends = p.bnd_lo[d] || p.bnd_hi[d] || p.nonref_lo[d] == 1 || p.nonref_hi[d] == 1;
     const double deferred = 2.0 * (double)nonup7 / (double)nf + (ends ? 10.0 / n : 0.0);
@@ -460,6 +527,11 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
         ctx->launches += 1;
         if ((p.sweep_impl == 4 || p.mixed) && ocfd::sweeps4_supported(p) && p.flag_count) {
             // the choice follows this pass's flags: one small read-back per step
+            if (ctx->slab) {        // every slab takes the same walk: counts of the whole grid
+                std::string err;
+                if (ocfd::slab_allreduce(ctx->slab, p.flag_count, 3, 2, ctx->stream, err))
+                    return fail(ctx, OCFD_ERR_CUDA, err);
+            }
             CK(cudaMemcpyAsync(ctx->h_flag_count, p.flag_count, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost,
                                ctx->stream), "flag counts");
             CK(cudaStreamSynchronize(ctx->stream), "flag counts");
@@ -490,8 +562,14 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
     }
     {
         TimerScope ts(ctx, T_VIS);
-        CK(ocfd::launch_viscous(p, fused_rk, ctx->stream), "viscous");
-        ctx->launches += 3;
+        CK(ocfd::launch_vis_ev(p, ctx->stream), "viscous fluxes");
+        void *evf[12]; int mask[12];
+        ocfd::ev_ghost_fields(p, evf, mask);
+        int rc = p.mixed ? fill_ghosts(ctx, reinterpret_cast<float *const *>(evf), mask, 12, "Ev ghost fill")
+                         : fill_ghosts(ctx, reinterpret_cast<double *const *>(evf), mask, 12, "Ev ghost fill");
+        if (rc) return rc;
+        CK(ocfd::launch_vis_div(p, fused_rk, ctx->stream), "viscous divergence");
+        ctx->launches += 2;
     }
     if (fused_rk && p.ibc) {        // OCFD_bc: boundary values, then the faces
         int rc = apply_bc(ctx);
@@ -573,6 +651,48 @@ extern "C" int ocfd_b200_set_metric_mode(ocfd_b200_ctx *ctx, int mode) {
     return OCFD_OK;
 }
 extern "C" int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx) { return ctx ? ctx->p.uniform_metrics : 0; }
+
+// ---------------------------------------------------------------------------
+// the grid split in z across GPUs (part3d with NPX0 = NPY0 = 1,
+// src/OCFD_mpi.c:120-190)
+// ---------------------------------------------------------------------------
+extern "C" int ocfd_b200_slab_unique_id(unsigned char id[OCFD_SLAB_ID_BYTES]) {
+    if (!id) return fail(nullptr, OCFD_ERR_ARG, "id is null");
+    std::string err;
+    if (ocfd::slab_unique_id(id, err)) return fail(nullptr, OCFD_ERR_UNSUPPORTED, err);
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_set_slab(ocfd_b200_ctx *ctx, int nranks, int rank, int rank_lo, int rank_hi, int z_offset,
+                                  int nz_global, const unsigned char id[OCFD_SLAB_ID_BYTES]) {
+    if (!ctx || !id) return OCFD_ERR_ARG;
+    Params &p = ctx->p;
+    if (ctx->slab) return fail(ctx, OCFD_ERR_STATE, "the slab is already set");
+    if (ctx->have_metrics || ctx->have_state || ctx->nfilter)
+        return fail(ctx, OCFD_ERR_STATE, "set the slab before the filters, metrics and state");
+    if (nranks < 1 || rank < 0 || rank >= nranks || rank_lo < 0 || rank_lo >= nranks || rank_hi < 0 ||
+        rank_hi >= nranks)
+        return fail(ctx, OCFD_ERR_ARG, "rank, neighbour ranks and rank count out of range");
+    if (!p.periodic[2])
+        return fail(ctx, OCFD_ERR_UNSUPPORTED, "the z split needs a periodic z direction (IPERIODIC z = 1)");
+    if (p.nz < OCFD_LAP) return fail(ctx, OCFD_ERR_ARG, "a slab needs at least 4 z planes");
+    if (z_offset < 0 || nz_global < p.nz || z_offset + p.nz > nz_global)
+        return fail(ctx, OCFD_ERR_ARG, "slab planes outside the grid");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    std::string err;
+    ctx->slab = ocfd::slab_create(p, nranks, rank, rank_lo, rank_hi, id, err);
+    if (!ctx->slab) return fail(ctx, OCFD_ERR_CUDA, err);
+    ctx->z_offset = z_offset;
+    ctx->nz_global = nz_global;
+    ctx->slab_count = nranks;
+    // hz = 1/(NZ_GLOBAL - 1) (src/OCFD_init.cu:29-31); OCFD_bc re-projects
+    // only the faces of the whole grid (src/OCFD_boundary.cu:78-95)
+    p.hz = 1.0 / (nz_global - 1.0);
+    p.inv_h[2] = 1.0 / p.hz;
+    p.zface_lo = z_offset == 0;
+    p.zface_hi = z_offset + p.nz == nz_global;
+    return OCFD_OK;
+}
 
 extern "C" int ocfd_b200_set_precision(ocfd_b200_ctx *ctx, int form) {
     if (!ctx || form < 0 || form > 1) return OCFD_ERR_ARG;
@@ -817,8 +937,8 @@ static int set_mesh_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKind k
     {   // periodic exchange of the coordinates
         double *f[3]; int mask[3];
         for (int m = 0; m < 3; m++) { f[m] = const_cast<double *>(p.met[m]); mask[m] = 7; }
-        CK(ocfd::launch_ghost(p, f, mask, 3, ctx->stream), "mesh ghost fill");
-        ctx->launches += 1;
+        int rc = fill_ghosts(ctx, f, mask, 3, "mesh ghost fill");
+        if (rc) return rc;
     }
     // the Ev scratch (12 LAP fields) holds the nine coordinate derivatives
     CK(ocfd::launch_mesh_metrics(p, ctx->cfg.jac_bound, ctx->ev_buf, ctx->stream), "metrics from mesh");
@@ -826,8 +946,8 @@ static int set_mesh_impl(ocfd_b200_ctx *ctx, const double *src, cudaMemcpyKind k
     {   // periodic exchange of the ten computed fields
         double *f[10]; int mask[10];
         for (int m = 0; m < 10; m++) { f[m] = const_cast<double *>(p.met[ocfd::M_AKX + m]); mask[m] = 7; }
-        CK(ocfd::launch_ghost(p, f, mask, 10, ctx->stream), "metric ghost fill");
-        ctx->launches += 1;
+        int rc = fill_ghosts(ctx, f, mask, 10, "metric ghost fill");
+        if (rc) return rc;
     }
     unsigned *flag = reinterpret_cast<unsigned *>(ctx->red_buf);
     CK(ocfd::launch_negative_jacobian(p, flag, ctx->stream), "Jacobian check");
@@ -941,8 +1061,8 @@ static int run_filters(ocfd_b200_ctx *ctx) {
         const int dm = (ctx->fjudge[0] ? 1 : 0) | (ctx->fjudge[1] ? 2 : 0) | (ctx->fjudge[2] ? 4 : 0);
         f[0] = p.pfil; mask[0] = dm;
         for (int m = 0; m < 5; m++) { f[1 + m] = p.flap + (size_t)m * p.lapN; mask[1 + m] = dm; }
-        CK(ocfd::launch_ghost(p, f, mask, 6, ctx->stream), "filter ghost fill");
-        ctx->launches += 1;
+        int rc = fill_ghosts(ctx, f, mask, 6, "filter ghost fill");
+        if (rc) return rc;
     }
     for (int m = 0; m < ctx->nfilter; m++) {
         if (!(ctx->tt <= ctx->frpar[m][2]) || ctx->istep % ctx->fpar[m][0] != 0) continue;
@@ -1091,13 +1211,31 @@ extern "C" int ocfd_b200_set_filter(ocfd_b200_ctx *ctx, int n, const int npara[1
         p.pfil = ctx->filter_buf + 5 * (size_t)p.lapN;
     }
     const int nn[3] = { p.nx, p.ny, p.nz };
+    int kb = npara[8], ke = npara[9];
+    if (ctx->slab) {
+        // set_para_filtering (src/OCFD_filtering.cu:56-61) on this slab:
+        // k ranges are global; a slab that holds none of the range would
+        // filter rows of another slab's local numbering there, so such a
+        // range is refused
+        const int k0 = ctx->z_offset, k1 = ctx->z_offset + p.nz;
+        if (kb >= k1 || ke <= k0)
+            return fail(ctx, OCFD_ERR_UNSUPPORTED, "with the grid split in z, a filter's k range must reach every slab");
+        kb = kb < k0 ? 0 : kb - k0;
+        ke = ke >= k1 ? p.nz : ke - k0;
+    }
     for (int t = 0; t < 11; t++) ctx->fpar[n][t] = npara[t];
+    ctx->fpar[n][8] = kb;
+    ctx->fpar[n][9] = ke;
     for (int d = 0; d < 3; d++) {
         if (npara[1 + d] == 1) ctx->fjudge[d] = 1;
         if (!p.periodic[d]) {
             if (ctx->fpar[n][4 + 2 * d] < 6) ctx->fpar[n][4 + 2 * d] = 6;
             if (ctx->fpar[n][5 + 2 * d] > nn[d] - 5) ctx->fpar[n][5 + 2 * d] = nn[d] - 5;
         }
+        // a range past the grid (e.g. 0 .. 100000 for "everything") ends at
+        // the grid, so no pass reaches beyond the fields
+        if (ctx->fpar[n][4 + 2 * d] < 0) ctx->fpar[n][4 + 2 * d] = 0;
+        if (ctx->fpar[n][5 + 2 * d] > nn[d]) ctx->fpar[n][5 + 2 * d] = nn[d];
     }
     for (int t = 0; t < 3; t++) ctx->frpar[n][t] = rpara[t];
     if (n + 1 > ctx->nfilter) ctx->nfilter = n + 1;
@@ -1205,8 +1343,13 @@ extern "C" int ocfd_b200_ana_residual(ocfd_b200_ctx *ctx, int which, double *mea
     if (rc) return rc;
     if ((rc = refresh_prims64(ctx))) return rc;
     if (!mean || which < 0 || which > 1) return fail(ctx, OCFD_ERR_ARG, "which must be 0 (E) or 1 (T)");
-    CK(ocfd::launch_mean(ctx->p, which, ctx->red_buf, nullptr, ctx->stream), "reduction");
+    CK(ocfd::launch_mean(ctx->p, which, ctx->red_buf, nullptr, global_cells(ctx), ctx->stream), "reduction");
     ctx->launches += 2;
+    if (ctx->slab) {
+        std::string err;
+        if (ocfd::slab_allreduce(ctx->slab, ctx->red_buf + ocfd::reduce_scratch_doubles() - 1, 1, 0, ctx->stream, err))
+            return fail(ctx, OCFD_ERR_CUDA, err);
+    }
     CK(cudaMemcpyAsync(mean, ctx->red_buf + ocfd::reduce_scratch_doubles() - 1, sizeof(double),
                        cudaMemcpyDeviceToHost, ctx->stream), "reduction read-back");
     CK(cudaStreamSynchronize(ctx->stream), "reduction");
@@ -1221,8 +1364,14 @@ extern "C" int ocfd_b200_check_state(ocfd_b200_ctx *ctx, long long *n_nan, long 
     if ((rc = refresh_prims64(ctx))) return rc;
     int nd = ocfd::reduce_scratch_doubles();
     unsigned long long *counts = reinterpret_cast<unsigned long long *>(ctx->red_buf + nd);
-    CK(ocfd::launch_mean(ctx->p, 1, ctx->red_buf, counts, ctx->stream), "state check");
+    CK(ocfd::launch_mean(ctx->p, 1, ctx->red_buf, counts, global_cells(ctx), ctx->stream), "state check");
     ctx->launches += 2;
+    if (ctx->slab) {
+        std::string err;
+        if (ocfd::slab_allreduce(ctx->slab, ctx->red_buf + nd - 1, 1, 0, ctx->stream, err) ||
+            ocfd::slab_allreduce(ctx->slab, counts, 2, 1, ctx->stream, err))
+            return fail(ctx, OCFD_ERR_CUDA, err);
+    }
     double host[3];
     CK(cudaMemcpyAsync(host, ctx->red_buf + nd - 1, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
        "state check read-back");
@@ -1246,11 +1395,16 @@ extern "C" int ocfd_b200_scheme_proportion(ocfd_b200_ctx *ctx, double frac[9]) {
     unsigned long long *counts = reinterpret_cast<unsigned long long *>(ctx->red_buf + ocfd::reduce_scratch_doubles());
     CK(ocfd::launch_flag_hist(p, counts, ctx->stream), "scheme proportion");
     ctx->launches += 1;
+    if (ctx->slab) {
+        std::string err;
+        if (ocfd::slab_allreduce(ctx->slab, counts, 9, 1, ctx->stream, err)) return fail(ctx, OCFD_ERR_CUDA, err);
+    }
     unsigned long long h[9];
     CK(cudaMemcpyAsync(h, counts, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "scheme proportion");
     CK(cudaStreamSynchronize(ctx->stream), "scheme proportion");
-    const double n[3] = {(double)(p.nx + 1) * p.ny * p.nz, (double)p.nx * (p.ny + 1) * p.nz,
-                         (double)p.nx * p.ny * (p.nz + 1)};
+    const double nzg = ctx->slab ? ctx->nz_global : p.nz;      // the whole grid's flag entries
+    const double n[3] = {(double)(p.nx + 1) * p.ny * nzg, (double)p.nx * (p.ny + 1) * nzg,
+                         (double)p.nx * p.ny * (nzg + (ctx->slab ? ctx->slab_count : 1))};
     for (int i = 0; i < 9; i++) frac[i] = (double)h[i] / n[i / 3];
     return OCFD_OK;
 }

@@ -35,6 +35,9 @@ struct Params {
     int scheme_invis, scheme_vis, charteric;
     int nochar_comp_flag;   // flag of components 1-4, non-characteristic hybrid (0 = face flag)
     int periodic[3];
+    // whether the local z faces k = 0 / k = nz-1 are faces of the whole grid
+    // (1 on one GPU; with the grid split in z, only on the first / last slab)
+    int zface_lo, zface_hi;
     // faces of each direction: boundary closures where DIF_BOUND is 1
     // (OCFD_bound, src/OCFD_bound_Scheme.cu:436-469) and the NON_REFLETION
     // value (OCFD_bound_non_ref, :352-433); has_bnd: any of them is set

@@ -530,7 +530,8 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
     if (krk == 3 && p.pfil) p.pfil[o] = T2 * d1 / (p.Gamma * p.Ama * p.Ama);
     // with a boundary-condition family the faces are re-projected after it
     // sets the boundary values (k_bc_faces)
-    bool face = (i == 0) || (i == p.nx - 1) || (j == 0) || (j == p.ny - 1) || (k == 0) || (k == p.nz - 1);
+    bool face = (i == 0) || (i == p.nx - 1) || (j == 0) || (j == p.ny - 1) || (k == 0 && p.zface_lo) ||
+                (k == p.nz - 1 && p.zface_hi);
     if (face && !p.ibc) {
         f[0] = d1;
         f[1] = u1 * d1;
@@ -637,7 +638,8 @@ __global__ void k_bc_faces(Params p) {
     if (tid >= p.N) return;
     int i = (int)(tid % p.nx); long long r = tid / p.nx;
     int j = (int)(r % p.ny); int k = (int)(r / p.ny);
-    bool face = (i == 0) || (i == p.nx - 1) || (j == 0) || (j == p.ny - 1) || (k == 0) || (k == p.nz - 1);
+    bool face = (i == 0) || (i == p.nx - 1) || (j == 0) || (j == p.ny - 1) || (k == 0 && p.zface_lo) ||
+                (k == p.nz - 1 && p.zface_hi);
     if (!face) return;
     long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     double d = p.prim[0][o], u = p.prim[1][o], v = p.prim[2][o], w = p.prim[3][o], T = p.prim[4][o];
@@ -780,17 +782,16 @@ cudaError_t launch_sweeps(const Params &p, cudaStream_t st) {
 }
 
 template <typename R>
-static cudaError_t launch_viscous_t(const Params &p, int krk, cudaStream_t st) {
+static cudaError_t launch_vis_ev_t(const Params &p, cudaStream_t st) {
     const dim3 nb((unsigned)(((p.nx + VT_X - 1) / VT_X) * ((p.ny + VT_Y - 1) / VT_Y)), (unsigned)p.nz);
     if (p.uniform_metrics) k_vis_ev<true, R><<<nb, 256, 0, st>>>(p);
     else                   k_vis_ev<false, R><<<nb, 256, 0, st>>>(p);
-    R *evf[12]; int mask[12];
-    R *evb = sizeof(R) == 8 ? (R *)p.ev : (R *)p.ev32;
-    for (int dd = 0; dd < 3; dd++)
-        for (int m = 0; m < 4; m++) { evf[4 * dd + m] = evb + (long long)(4 * dd + m) * p.lapN; mask[4 * dd + m] = 1 << dd; }
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    if ((e = launch_ghost_t<R>(p, evf, mask, 12, st)) != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t launch_vis_div_t(const Params &p, int krk, cudaStream_t st) {
+    const dim3 nb((unsigned)(((p.nx + VT_X - 1) / VT_X) * ((p.ny + VT_Y - 1) / VT_Y)), (unsigned)p.nz);
     if (krk == 0) {
         if (p.uniform_metrics) k_vis_div<true, false, R><<<nb, 256, 0, st>>>(p, 0);
         else                   k_vis_div<false, false, R><<<nb, 256, 0, st>>>(p, 0);
@@ -801,11 +802,30 @@ static cudaError_t launch_viscous_t(const Params &p, int krk, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-// krk = 0: viscous terms into du; krk = 1..3: viscous terms, then the RK
-// stage update in the same kernel (du is not written).  FP32 stencils in
-// the precision form.
-cudaError_t launch_viscous(const Params &p, int krk, cudaStream_t st) {
-    return p.mixed ? launch_viscous_t<float>(p, krk, st) : launch_viscous_t<double>(p, krk, st);
+// The viscous part in two launches with the Ev ghost exchange between them:
+// k_vis_ev forms the 12 Ev fields (4 per direction) on the interior; the
+// caller fills the ghosts of each direction's four (ev_ghost_fields); then
+// k_vis_div.  krk = 0: viscous terms into du; krk = 1..3: viscous terms,
+// then the RK stage update in the same kernel (du is not written).  FP32
+// stencils in the precision form.
+cudaError_t launch_vis_ev(const Params &p, cudaStream_t st) {
+    return p.mixed ? launch_vis_ev_t<float>(p, st) : launch_vis_ev_t<double>(p, st);
+}
+
+cudaError_t launch_vis_div(const Params &p, int krk, cudaStream_t st) {
+    return p.mixed ? launch_vis_div_t<float>(p, krk, st) : launch_vis_div_t<double>(p, krk, st);
+}
+
+// base pointers of the 12 Ev fields (FP64, or FP32 in the precision form)
+// and the direction each needs ghosts in (bit d for direction d)
+void ev_ghost_fields(const Params &p, void *fields[12], int dirmask[12]) {
+    char *evb = p.mixed ? (char *)p.ev32 : (char *)p.ev;
+    const size_t es = p.mixed ? sizeof(float) : sizeof(double);
+    for (int dd = 0; dd < 3; dd++)
+        for (int m = 0; m < 4; m++) {
+            fields[4 * dd + m] = evb + (size_t)(4 * dd + m) * (size_t)p.lapN * es;
+            dirmask[4 * dd + m] = 1 << dd;
+        }
 }
 
 cudaError_t launch_rk(const Params &p, int krk, cudaStream_t st) {
@@ -925,14 +945,17 @@ __global__ void __launch_bounds__(RED_THREADS) k_reduce_final(const double *part
 }
 
 // scratch: RED_BLOCKS + 1 doubles and two counters
-cudaError_t launch_mean(const Params &p, int which, double *scratch, unsigned long long *counts,
+// ncell: the divisor (the cells of the whole grid; with the grid split in z
+// each slab divides its sum by the whole grid's count and the slabs' results
+// are summed)
+cudaError_t launch_mean(const Params &p, int which, double *scratch, unsigned long long *counts, double ncell,
                         cudaStream_t st) {
     if (counts) {
         cudaError_t e = cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), st);
         if (e != cudaSuccess) return e;
     }
     k_reduce_partial<<<RED_BLOCKS, RED_THREADS, 0, st>>>(p, which, scratch, counts);
-    k_reduce_final<<<1, RED_THREADS, 0, st>>>(scratch, RED_BLOCKS, (double)p.N, scratch + RED_BLOCKS);
+    k_reduce_final<<<1, RED_THREADS, 0, st>>>(scratch, RED_BLOCKS, ncell, scratch + RED_BLOCKS);
     return cudaGetLastError();
 }
 int reduce_scratch_doubles() { return RED_BLOCKS + 1; }

@@ -32,11 +32,16 @@ __global__ void k_jac_d0(Params p, const double *__restrict__ f, double *__restr
     const double *c = f + lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     auto F = [&](int t) { return c[(long long)t * s]; };
     double v = (45.0 * (F(1) - F(-1)) - 9.0 * (F(2) - F(-2)) + (F(3) - F(-3))) / (60.0 * h);
-    if (bound) {
+    // CHECK_Z (src/OCFD_bound_Scheme.cu:64-72): with the grid split in z,
+    // the z closures belong to the first and last slab only
+    const bool lo_side = DIR != 2 || p.zface_lo, hi_side = DIR != 2 || p.zface_hi;
+    if (bound && lo_side) {
         if (X == 0)      v = (F(1) - F(0)) / h;
         else if (X == 1) v = (F(1) - F(-1)) * 0.5 / h;
         else if (X == 2) v = (F(-2) - 8.0 * F(-1) + 8.0 * F(1) - F(2)) / (12.0 * h);
         else if (X == 3) v = (F(3) - F(-3) - 9.0 * (F(2) - F(-2)) + 45.0 * (F(1) - F(-1))) / (60.0 * h);
+    }
+    if (bound && hi_side) {
         const int u = X - (n - 1);
         if (DIR != 1) {
             if (u == 0)       v = (F(0) - F(-1)) / h;

@@ -29,7 +29,7 @@ EXPORTED = (
     "ocfd_b200_create", "ocfd_b200_destroy", "ocfd_b200_set_stream", "ocfd_b200_get_stream",
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
     "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics", "ocfd_b200_set_sweep_impl",
-    "ocfd_b200_sweep_walks", "ocfd_b200_set_precision",
+    "ocfd_b200_sweep_walks", "ocfd_b200_set_precision", "ocfd_b200_slab_unique_id", "ocfd_b200_set_slab",
     "ocfd_b200_scheme_proportion", "ocfd_b200_mlp_nparam", "ocfd_b200_set_switch", "ocfd_b200_switch_stats", "ocfd_b200_switch_features",
     "ocfd_b200_mlp_last_error", "ocfd_b200_mlp_infer", "ocfd_b200_mlp_grad", "ocfd_b200_mlp_train",
     "ocfd_b200_set_mesh", "ocfd_b200_set_mesh_device", "ocfd_b200_get_metrics",
@@ -120,6 +120,9 @@ def load(path: Optional[str] = None):
         "ocfd_b200_set_sweep_impl": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_sweep_walks": (ctypes.c_int, [P]),
         "ocfd_b200_set_precision": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_slab_unique_id": (ctypes.c_int, [ctypes.c_char_p]),
+        "ocfd_b200_set_slab": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_int, ctypes.c_char_p]),
         "ocfd_b200_scheme_proportion": (ctypes.c_int, [P, D]),
         "ocfd_b200_mlp_nparam": (ctypes.c_int, []),
         "ocfd_b200_set_switch": (ctypes.c_int, [P, F, ctypes.c_int, ctypes.c_double]),
@@ -221,6 +224,20 @@ def mlp_train(params: np.ndarray, feat: np.ndarray, label: np.ndarray, epochs: i
     return w, hist[:epochs]
 
 
+SLAB_ID_BYTES = 128
+
+
+def slab_unique_id() -> bytes:
+    """The communicator id one rank makes for a z-split run (NCCL's unique
+    id, 128 bytes) and hands to the others."""
+    L = load()
+    buf = ctypes.create_string_buffer(SLAB_ID_BYTES)
+    rc = L.ocfd_b200_slab_unique_id(buf)
+    if rc != OCFD_OK:
+        raise OcfdError(rc, "ocfd_b200_slab_unique_id", (L.ocfd_b200_last_error(None) or b"").decode())
+    return buf.raw
+
+
 def make_config(cfg: CaseConfig, device: int = 0) -> Config:
     c = Config()
     c.nx, c.ny, c.nz = cfg.nx, cfg.ny, cfg.nz
@@ -244,7 +261,7 @@ class Solver:
 
     def __init__(self, cfg: CaseConfig, prims: Optional[Sequence[np.ndarray]] = None,
                  metrics: Optional[Sequence[np.ndarray]] = None, device: int = 0,
-                 istep: int = 0, tt: float = 0.0, metric_mode: int = 0, inlet=None):
+                 istep: int = 0, tt: float = 0.0, metric_mode: int = 0, inlet=None, slab=None):
         self.L = load()
         self.cfg = cfg
         self.shape = (cfg.nz, cfg.ny, cfg.nx)
@@ -254,6 +271,10 @@ class Solver:
         if rc != OCFD_OK:
             raise OcfdError(rc, "ocfd_b200_create", (self.L.ocfd_b200_last_error(None) or b"").decode())
         self.h = h
+        self.slab = slab
+        if slab is not None:        # slabs.SlabSpec: before the filters, metrics and state
+            self._check(self.L.ocfd_b200_set_slab(self.h, slab.nranks, slab.rank, slab.rank_lo, slab.rank_hi,
+                                                  slab.z_offset, slab.nz_global, slab.comm_id), "set_slab")
         if metric_mode:
             self._check(self.L.ocfd_b200_set_metric_mode(self.h, metric_mode), "set_metric_mode")
         for n, (ip, rp) in enumerate(getattr(cfg, "filters", ()) or ()):
