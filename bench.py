@@ -14,6 +14,12 @@ Metric: Gcell-RK-stage/s = cells x 3 x steps / seconds / 1e9.
 With N > 1 (torchrun) every rank runs an independent replica of the same
 grid on its own GPU (the path has no exchange step on one grid per GPU);
 value = all ranks' cell-stages / max-over-ranks time ("scaling": "weak").
+With --decomp z the N ranks instead hold the z slabs of one grid of
+n x n x (n N) cells (each slab the n^3 case, so the whole grid is that case
+repeated N times in z and stays periodic); the slabs swap ghost planes over
+NCCL inside every ghost fill ("scaling": "weak", per-GPU work fixed).  On one
+GPU, --decomp z runs a single slab whose neighbour is itself, which times the
+exchange path against the periodic wrap.
 """
 from __future__ import annotations
 
@@ -185,7 +191,14 @@ def run_ours(args, rank, world, dist):
     torch.cuda.set_device(dev)
     n = args.n
     case = make_case(args.workload, n)
-    solver = lib.Solver(case.cfg, case.prims, case.metrics, device=dev, inlet=case.inlet)
+    slab = None
+    if args.decomp == "z":
+        from ocfd_b200 import slabs
+        if args.workload == "ramp" and world > 1:
+            raise SystemExit("--decomp z repeats the case in z; the ramp's mesh coordinates would not follow")
+        cid = slabs.share_id(group=None) if dist else lib.slab_unique_id()
+        slab = slabs.slab_spec(rank, world, case.cfg.nz * world, cid)
+    solver = lib.Solver(case.cfg, case.prims, case.metrics, device=dev, inlet=case.inlet, slab=slab)
     if args.form != "fp64":             # precision form (and the learned switch)
         solver.set_precision(1)
     if args.form == "fp32-learned":
@@ -277,7 +290,8 @@ def run_ours(args, rank, world, dist):
                    "seed": 2024 if args.workload != "tgv" else 1234,
                    "l2": f"inputs larger than L2 (state ~{state_gb:.1f} GB/GPU)" if state_gb > 0.5
                          else f"state ~{state_gb:.2f} GB/GPU, partly L2-resident",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": (f"z slabs x{world} (grid {nx}x{ny}x{nz * world}, ghost planes over NCCL)"
+                                   if args.decomp == "z" else f"replicas x{world}")},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": (TRAFFIC_PER_CELL[dom] * cells
@@ -393,6 +407,8 @@ def main():
                          "fp32-learned: that with the learned scheme switch")
     ap.add_argument("--n", type=int, default=0,
                     help="grid size (iso, tgv: n^3; ramp: 4n x n x n/2); 0 = the configuration's own")
+    ap.add_argument("--decomp", choices=("replicas", "z"), default="replicas",
+                    help="N > 1: independent replicas, or the z slabs of one grid (ghost planes over NCCL)")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--ref-steps", type=int, default=4)
     ap.add_argument("--cpu-sample", type=int, default=96)

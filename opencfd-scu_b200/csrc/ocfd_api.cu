@@ -25,7 +25,7 @@ cudaError_t launch_prims_to_fp32(const Params &p, cudaStream_t st);
 cudaError_t launch_flag_hist(const Params &p, unsigned long long *counts, cudaStream_t st);
 cudaError_t launch_sweeps(const Params &p, cudaStream_t st);
 cudaError_t launch_vis_ev(const Params &p, cudaStream_t st);
-cudaError_t launch_vis_div(const Params &p, int krk, cudaStream_t st);
+cudaError_t launch_vis_div(const Params &p, int krk, int k0, int k1, cudaStream_t st);
 void ev_ghost_fields(const Params &p, void *fields[12], int dirmask[12]);
 cudaError_t launch_rk(const Params &p, int krk, cudaStream_t st);
 cudaError_t launch_rk_only(const Params &p, int krk, cudaStream_t st);
@@ -136,6 +136,11 @@ struct ocfd_b200_ctx {
     // neighbouring slabs (null: one GPU holds the grid)
     ocfd::Slab *slab = nullptr;
     int z_offset = 0, nz_global = 0, slab_count = 1;
+    // the primitives' z exchange runs on its own stream while the x and y
+    // sweeps (which read no z ghosts) run; the z sweep waits for it
+    cudaStream_t xstream = nullptr;
+    cudaEvent_t xev[2] = {nullptr, nullptr};
+    bool x_pending = false;
     bool have_metrics = false;
     int metric_mode = 0;          // 0 auto-detect uniform grids, 1 always read the fields
     bool have_state = false;
@@ -199,8 +204,11 @@ static void free_all(ocfd_b200_ctx *c) {
     cudaFree(c->prec_buf);
     cudaFree(c->sw_w);
     cudaFree(c->sw_stats);
+    if (c->xstream) cudaStreamSynchronize(c->xstream);
     ocfd::slab_destroy(c->slab);
     c->slab = nullptr;
+    for (auto &e : c->xev) if (e) cudaEventDestroy(e);
+    if (c->xstream) cudaStreamDestroy(c->xstream);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
@@ -371,19 +379,30 @@ static cudaError_t ghost_launch(const Params &p, double *const *f, const int *ma
 static cudaError_t ghost_launch(const Params &p, float *const *f, const int *mask, int n, cudaStream_t st) {
     return ocfd::launch_ghost32(p, f, mask, n, st);
 }
-static int slab_exchange(ocfd_b200_ctx *ctx, double *const *f, int n, std::string &err) {
-    return ocfd::slab_exchange(ctx->slab, ctx->p, f, n, ctx->stream, err);
+static int slab_exchange(ocfd_b200_ctx *ctx, double *const *f, int n, cudaStream_t st, std::string &err) {
+    return ocfd::slab_exchange(ctx->slab, ctx->p, f, n, st, err);
 }
-static int slab_exchange(ocfd_b200_ctx *ctx, float *const *f, int n, std::string &err) {
-    return ocfd::slab_exchange32(ctx->slab, ctx->p, f, n, ctx->stream, err);
+static int slab_exchange(ocfd_b200_ctx *ctx, float *const *f, int n, cudaStream_t st, std::string &err) {
+    return ocfd::slab_exchange32(ctx->slab, ctx->p, f, n, st, err);
+}
+
+// the solver stream waits for a z exchange left running on its own stream
+static int join_z(ocfd_b200_ctx *ctx) {
+    if (!ctx->x_pending) return OCFD_OK;
+    ctx->x_pending = false;
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->xev[1], 0), "z exchange join");
+    return OCFD_OK;
 }
 
 // Ghost fill of LAP-box fields, mask bit d for direction d: the periodic
 // wrap on one GPU; with the grid split in z, the x and y wraps here and the
 // z ghost planes from the neighbouring slabs (the reference's
 // exchange_boundary_{x,y,z}_packed_dev order, src/OCFD_mpi_dev.cu:186-310)
+// defer_z: the z exchange runs on the exchange stream; join_z before
+// anything reads the z ghosts
 template <typename T>
-static int fill_ghosts(ocfd_b200_ctx *ctx, T *const *f, const int *mask, int n, const char *what) {
+static int fill_ghosts(ocfd_b200_ctx *ctx, T *const *f, const int *mask, int n, const char *what,
+                       bool defer_z = false) {
     if (!ctx->slab) {
         CK(ghost_launch(ctx->p, f, mask, n, ctx->stream), what);
         ctx->launches += 1;
@@ -404,8 +423,20 @@ static int fill_ghosts(ocfd_b200_ctx *ctx, T *const *f, const int *mask, int n, 
     }
     if (nz) {
         std::string err;
-        if (slab_exchange(ctx, fz, nz, err)) return fail(ctx, OCFD_ERR_CUDA, std::string(what) + ": " + err);
+        cudaStream_t st = ctx->stream;
+        if (defer_z && ctx->xstream) {
+            int rc = join_z(ctx);
+            if (rc) return rc;
+            CK(cudaEventRecord(ctx->xev[0], ctx->stream), "z exchange fork");
+            CK(cudaStreamWaitEvent(ctx->xstream, ctx->xev[0], 0), "z exchange fork");
+            st = ctx->xstream;
+        }
+        if (slab_exchange(ctx, fz, nz, st, err)) return fail(ctx, OCFD_ERR_CUDA, std::string(what) + ": " + err);
         ctx->launches += ocfd::slab_launches_per_exchange();
+        if (st != ctx->stream) {
+            CK(cudaEventRecord(ctx->xev[1], st), "z exchange done");
+            ctx->x_pending = true;
+        }
     }
     return OCFD_OK;
 }
@@ -417,11 +448,15 @@ static int ghost_prims64(ocfd_b200_ctx *ctx) {
 }
 
 // the primitives the stencils read: FP64, or FP32 in the precision form
-static int ghost_prims(ocfd_b200_ctx *ctx) {
-    if (!ctx->p.mixed) return ghost_prims64(ctx);
+static int ghost_prims(ocfd_b200_ctx *ctx, bool defer_z = false) {
+    if (!ctx->p.mixed) {
+        double *f[5]; int mask[5];
+        for (int m = 0; m < 5; m++) { f[m] = ctx->p.prim[m]; mask[m] = 7; }
+        return fill_ghosts(ctx, f, mask, 5, "ghost fill", defer_z);
+    }
     float *f[5]; int mask[5];
     for (int m = 0; m < 5; m++) { f[m] = ctx->p.prim32[m]; mask[m] = 7; }
-    return fill_ghosts(ctx, f, mask, 5, "ghost fill");
+    return fill_ghosts(ctx, f, mask, 5, "ghost fill", defer_z);
 }
 
 // precision form: FP64 primitives (interior and ghosts) from the FP64
@@ -506,6 +541,10 @@ static int sweeps_auto(ocfd_b200_ctx *ctx) {
     if ((!w[0] || !w[1] || !w[2]) && ocfd::sweeps3_defers(p))
         CK(cudaMemsetAsync(p.defer_count, 0, 3 * sizeof(unsigned), ctx->stream), "deferred counters");
     for (int d = 0; d < 3; d++) {
+        if (d == 2) {
+            int rc = join_z(ctx);
+            if (rc) return rc;
+        }
         if (w[d]) {
             CK(ocfd::launch_sweep4_dir(p, d, ctx->stream), "inviscid sweeps");
             ctx->launches += 1;
@@ -540,7 +579,7 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
     }
     {
         TimerScope ts(ctx, T_GHOST);
-        int rc = ghost_prims(ctx);
+        int rc = ghost_prims(ctx, true);      // the z planes arrive while the x and y sweeps run
         if (rc) return rc;
     }
     {
@@ -552,23 +591,29 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
         if (p.mixed || (p.sweep_impl == 4 && ocfd::sweeps4_supported(p))) {
             int rc = sweeps_auto(ctx);
             if (rc) return rc;
-        }
-        else if (p.sweep_impl == 1) CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
-        else if (p.sweep_impl == 6) CK(ocfd::launch_sweeps4(p, ctx->stream), "inviscid sweeps");
-        else if (p.sweep_impl >= 4) CK(ocfd::launch_sweeps3(p, ctx->stream), "inviscid sweeps");
-        else                        CK(ocfd::launch_sweeps2(p, ctx->stream), "inviscid sweeps");
-        if (!(p.mixed || (p.sweep_impl == 4 && ocfd::sweeps4_supported(p))))
+        } else {            // the other variants launch the three directions together
+            int rc = join_z(ctx);
+            if (rc) return rc;
+            if (p.sweep_impl == 1)      CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
+            else if (p.sweep_impl == 6) CK(ocfd::launch_sweeps4(p, ctx->stream), "inviscid sweeps");
+            else if (p.sweep_impl >= 4) CK(ocfd::launch_sweeps3(p, ctx->stream), "inviscid sweeps");
+            else                        CK(ocfd::launch_sweeps2(p, ctx->stream), "inviscid sweeps");
             ctx->launches += p.sweep_impl == 6 ? 3 : (p.sweep_impl >= 4 ? ocfd::sweeps3_kernels(p) : 3);
+        }
     }
     {
         TimerScope ts(ctx, T_VIS);
         CK(ocfd::launch_vis_ev(p, ctx->stream), "viscous fluxes");
         void *evf[12]; int mask[12];
         ocfd::ev_ghost_fields(p, evf, mask);
+        // (forming the planes away from the slab faces while the Ev_z planes
+        // travel, and the two bands next to the faces after, measured slower
+        // than one launch after the exchange: the small band launches and the
+        // extra tail cost more than the exchange they hide)
         int rc = p.mixed ? fill_ghosts(ctx, reinterpret_cast<float *const *>(evf), mask, 12, "Ev ghost fill")
                          : fill_ghosts(ctx, reinterpret_cast<double *const *>(evf), mask, 12, "Ev ghost fill");
         if (rc) return rc;
-        CK(ocfd::launch_vis_div(p, fused_rk, ctx->stream), "viscous divergence");
+        CK(ocfd::launch_vis_div(p, fused_rk, 0, p.nz, ctx->stream), "viscous divergence");
         ctx->launches += 2;
     }
     if (fused_rk && p.ibc) {        // OCFD_bc: boundary values, then the faces
@@ -685,12 +730,25 @@ extern "C" int ocfd_b200_set_slab(ocfd_b200_ctx *ctx, int nranks, int rank, int 
     ctx->z_offset = z_offset;
     ctx->nz_global = nz_global;
     ctx->slab_count = nranks;
+    if (cudaStreamCreateWithFlags(&ctx->xstream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->xev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->xev[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, OCFD_ERR_CUDA, "exchange stream");
+    }
     // hz = 1/(NZ_GLOBAL - 1) (src/OCFD_init.cu:29-31); OCFD_bc re-projects
     // only the faces of the whole grid (src/OCFD_boundary.cu:78-95)
     p.hz = 1.0 / (nz_global - 1.0);
     p.inv_h[2] = 1.0 / p.hz;
     p.zface_lo = z_offset == 0;
     p.zface_hi = z_offset + p.nz == nz_global;
+    // z closures (DIF_BOUND, NON_REFLETION) act at the faces of the whole
+    // grid only, as the reference's npz == 0 / NPZ0-1 checks have them
+    if (!p.zface_lo) { p.bnd_lo[2] = 0; p.nonref_lo[2] = 0; }
+    if (!p.zface_hi) { p.bnd_hi[2] = 0; p.nonref_hi[2] = 0; }
+    p.has_bnd = 0;
+    for (int d = 0; d < 3; d++)
+        p.has_bnd |= p.bnd_lo[d] | p.bnd_hi[d] | (p.nonref_lo[d] == 1) | (p.nonref_hi[d] == 1);
     return OCFD_OK;
 }
 

@@ -406,11 +406,11 @@ __device__ __forceinline__ void cons_to_prim(const Params &p, const double f[5],
 // 32 x 8 tile of one z plane (grid: x tiles * y tiles, nz), so most y
 // neighbours of its cells are loaded by the same block and meet in L1.
 constexpr int VT_X = 32, VT_Y = 8;
-__device__ __forceinline__ bool tile_cell(const Params &p, int &i, int &j, int &k, long long &tid) {
+__device__ __forceinline__ bool tile_cell(const Params &p, int &i, int &j, int &k, long long &tid, int k0 = 0) {
     const int ntx = (p.nx + VT_X - 1) / VT_X;
     i = (int)(blockIdx.x % ntx) * VT_X + (int)(threadIdx.x % VT_X);
     j = (int)(blockIdx.x / ntx) * VT_Y + (int)(threadIdx.x / VT_X);
-    k = (int)blockIdx.y;
+    k = (int)blockIdx.y + k0;
     if (i >= p.nx || j >= p.ny) return false;
     tid = in_index(p, i, j, k);
     return true;
@@ -548,10 +548,10 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
 // RK = true: the stage's du is complete here, so the RK update, cons->prim
 // and the face re-projection follow in the same thread and du is not stored.
 template <bool UNI, bool RK, typename R>
-__global__ void __launch_bounds__(256, 6) k_vis_div(Params p, int krk) {
+__global__ void __launch_bounds__(256, 6) k_vis_div(Params p, int krk, int k0) {
     int i, j, k;
     long long tid;
-    if (!tile_cell(p, i, j, k, tid)) return;
+    if (!tile_cell(p, i, j, k, tid, k0)) return;
     long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
     const long long st[3] = { 1LL, p.ys, p.zs };
     const R hh[3] = { (R)p.hx, (R)p.hy, (R)p.hz };
@@ -790,14 +790,15 @@ static cudaError_t launch_vis_ev_t(const Params &p, cudaStream_t st) {
 }
 
 template <typename R>
-static cudaError_t launch_vis_div_t(const Params &p, int krk, cudaStream_t st) {
-    const dim3 nb((unsigned)(((p.nx + VT_X - 1) / VT_X) * ((p.ny + VT_Y - 1) / VT_Y)), (unsigned)p.nz);
+static cudaError_t launch_vis_div_t(const Params &p, int krk, int k0, int k1, cudaStream_t st) {
+    if (k1 <= k0) return cudaSuccess;
+    const dim3 nb((unsigned)(((p.nx + VT_X - 1) / VT_X) * ((p.ny + VT_Y - 1) / VT_Y)), (unsigned)(k1 - k0));
     if (krk == 0) {
-        if (p.uniform_metrics) k_vis_div<true, false, R><<<nb, 256, 0, st>>>(p, 0);
-        else                   k_vis_div<false, false, R><<<nb, 256, 0, st>>>(p, 0);
+        if (p.uniform_metrics) k_vis_div<true, false, R><<<nb, 256, 0, st>>>(p, 0, k0);
+        else                   k_vis_div<false, false, R><<<nb, 256, 0, st>>>(p, 0, k0);
     } else {
-        if (p.uniform_metrics) k_vis_div<true, true, R><<<nb, 256, 0, st>>>(p, krk);
-        else                   k_vis_div<false, true, R><<<nb, 256, 0, st>>>(p, krk);
+        if (p.uniform_metrics) k_vis_div<true, true, R><<<nb, 256, 0, st>>>(p, krk, k0);
+        else                   k_vis_div<false, true, R><<<nb, 256, 0, st>>>(p, krk, k0);
     }
     return cudaGetLastError();
 }
@@ -812,8 +813,9 @@ cudaError_t launch_vis_ev(const Params &p, cudaStream_t st) {
     return p.mixed ? launch_vis_ev_t<float>(p, st) : launch_vis_ev_t<double>(p, st);
 }
 
-cudaError_t launch_vis_div(const Params &p, int krk, cudaStream_t st) {
-    return p.mixed ? launch_vis_div_t<float>(p, krk, st) : launch_vis_div_t<double>(p, krk, st);
+// planes k0 .. k1-1 (the whole slab: 0, nz)
+cudaError_t launch_vis_div(const Params &p, int krk, int k0, int k1, cudaStream_t st) {
+    return p.mixed ? launch_vis_div_t<float>(p, krk, k0, k1, st) : launch_vis_div_t<double>(p, krk, k0, k1, st);
 }
 
 // base pointers of the 12 Ev fields (FP64, or FP32 in the precision form)

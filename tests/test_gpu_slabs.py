@@ -29,7 +29,8 @@ def _same(a, b):
     assert np.array_equal(a.primitives(), b.primitives())
 
 
-@pytest.mark.parametrize("name", ["tgv_weno7", "iso_hybrid", "iso_hybrid_fp32", "curvilinear", "ramp_bc_filter"])
+@pytest.mark.parametrize("name", ["tgv_weno7", "iso_hybrid", "iso_hybrid_fp32", "iso_hybrid_impl5", "curvilinear",
+                                  "ramp_bc_filter"])
 def test_one_slab_equals_single_gpu(name, gpu_lib):
     prep = None
     steps = 4
@@ -39,6 +40,8 @@ def test_one_slab_equals_single_gpu(name, gpu_lib):
         c = cases.isotropic_turbulence(24, seed=9, charteric=1, hy_dp_intv=(0.002, 0.02))
         if name.endswith("fp32"):
             prep = lambda s: s.set_precision(1)
+        elif name.endswith("impl5"):         # all three sweeps launched together
+            prep = lambda s: s.set_sweep_impl(5)
     elif name == "curvilinear":
         c = cases.random_smooth_case(20, 16, 12, seed=5, curvilinear=True, shock=True)
     else:
