@@ -293,6 +293,38 @@ def read_field_file(path: str, shape: Tuple[int, int, int]) -> Tuple[List[np.nda
     return fields, istep, tt
 
 
+# --------------------------------------------------------------------------
+# restart: Opencfd.msg names the field file a run starts from
+# --------------------------------------------------------------------------
+
+def read_restart_step(path: str = "Opencfd.msg") -> int:
+    """The restart step Opencfd.msg holds (read_file, src/OCFD_IO.c:38-58: one
+    native int read with fread); -1 when the file is absent."""
+    try:
+        with open(path, "rb") as fh:
+            raw = fh.read(4)
+    except FileNotFoundError:
+        return -1
+    if len(raw) < 4:
+        raise FormatError(f"{path}: shorter than one int")
+    return struct.unpack("<i", raw)[0]
+
+
+def write_restart_step(path: str, istep: int) -> None:
+    """Opencfd.msg for a restart from OCFD%08d.dat of step istep."""
+    with open(path, "wb") as fh:
+        fh.write(struct.pack("<i", int(istep)))
+
+
+def initial_field_file(directory: str = ".") -> str:
+    """The field file a run reads first: opencfd.dat, or OCFD%08d.dat of the
+    step in Opencfd.msg when that file exists and holds a step >= 0
+    (src/OCFD_IO.c:53-60)."""
+    step = read_restart_step(os.path.join(directory, "Opencfd.msg"))
+    name = "opencfd.dat" if step < 0 else f"OCFD{step:08d}.dat"
+    return os.path.join(directory, name)
+
+
 def write_metric_file(path: str, fields: Sequence[np.ndarray]) -> None:
     """Write OCFD3d-Jacobi.dat (13 blocks) or OCFD3d-Mesh.dat (3 blocks)."""
     if len(fields) not in (3, 13):

@@ -89,3 +89,25 @@ def test_config_unknown_scheme_raises(tmp_path):
     p.write_text("GRID_3D = 8 8 8\nSCHEME_INVIS = WENO9\nSCHEME_VIS = CD6\n")
     with pytest.raises(formats.FormatError):
         formats.read_config(str(p))
+
+
+def test_restart_message_selects_the_field_file(tmp_path):
+    """Opencfd.msg absent or negative: opencfd.dat; otherwise OCFD%08d.dat of
+    its step, and that file reads back with its step and time."""
+    d = str(tmp_path)
+    assert formats.initial_field_file(d).endswith("opencfd.dat")
+    formats.write_restart_step(os.path.join(d, "Opencfd.msg"), -1)
+    assert formats.initial_field_file(d).endswith("opencfd.dat")
+    formats.write_restart_step(os.path.join(d, "Opencfd.msg"), 1200)
+    assert formats.read_restart_step(os.path.join(d, "Opencfd.msg")) == 1200
+    path = formats.initial_field_file(d)
+    assert os.path.basename(path) == "OCFD00001200.dat"
+    rng = np.random.default_rng(0)
+    f = [rng.standard_normal((3, 4, 5)) for _ in range(5)]
+    formats.write_field_file(path, f, istep=1200, tt=0.25)
+    g, istep, tt = formats.read_field_file(path, (3, 4, 5))
+    assert istep == 1200 and tt == 0.25 and all(np.array_equal(a, b) for a, b in zip(f, g))
+    with open(os.path.join(d, "Opencfd.msg"), "wb") as fh:
+        fh.write(b"\x01\x02")
+    with pytest.raises(formats.FormatError):
+        formats.read_restart_step(os.path.join(d, "Opencfd.msg"))
