@@ -302,6 +302,9 @@ def run_ours(args, rank, world, dist):
         "stage_roofline": {"bytes_per_cell_stage": b_alg, "achieved_gbs": b_alg * cells / (stage_ms / 1e3) / 1e9,
                            "frac": b_alg * cells / (stage_ms / 1e3) / 1e9 / hbm},
         "kernel_ms_per_stage": {k: fam[k][0] / 3.0 for k in fam},
+        "fp64_flops": ({"flop_per_cell_stage": FP64_FLOP_PER_CELL_STAGE[args.workload],
+                        "achieved_tflops": FP64_FLOP_PER_CELL_STAGE[args.workload] * value / 1e3,
+                        "source": FLOP_SOURCE} if args.form == "fp64" else None),
         "e2e": {"value": e2e_val, "unit": METRIC, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                 "steps": e2e_steps, "api": "ocfd_b200_advance_host"},
         "gpu_launches": int(launches),
@@ -362,6 +365,14 @@ TRAFFIC_PER_CELL = {
     "viscous_rk_update": 385.6,     # k_vis_ev + k_vis_div (Ev ghost fill not captured)
 }
 TRAFFIC_SOURCE = "ncu capture at 160^3 scaled by cells (profiles/stage_traffic_iso160.txt)"
+
+# FP64 operations executed per cell and stage (2 x DFMA + DADD + DMUL, counted
+# by ncu over one stage's kernels: profiles/fp64_flops_iso160_tgv128_ramp256.txt);
+# times the measured rate, the FP64 rate the whole stage sustains.  The hybrid
+# count depends on how many faces the sensor flags (isotropic turbulence: UP7
+# almost everywhere).
+FP64_FLOP_PER_CELL_STAGE = {"iso": 2353.0, "tgv": 7353.0, "ramp": 10712.0}
+FLOP_SOURCE = "ncu executed FP64 instructions per stage (profiles/fp64_flops_iso160_tgv128_ramp256.txt)"
 
 
 def run_reference(args, rank, world):
