@@ -1731,4 +1731,3 @@ void oro_get_flags(const oro_state *s, int *sx, int *sy, int *sz) {
 }
 int oro_istep(const oro_state *s) { return s->istep; }
 double oro_tt(const oro_state *s) { return s->tt; }
-double oro_flops_last_rhs(const oro_state *s) { (void)s; return 0.0; }

@@ -109,8 +109,6 @@ void oro_get_du(const oro_state *s, double *du5);
 void oro_get_flags(const oro_state *s, int *sx, int *sy, int *sz);
 int  oro_istep(const oro_state *s);
 double oro_tt(const oro_state *s);
-/* FP64 operation counter of the last du_comput (instrumented build only; 0 otherwise). */
-double oro_flops_last_rhs(const oro_state *s);
 
 /* Point kernels exposed for unit tests (reference formulas, stencils as in
  * the reference: P side stencil[k] = f(i-3+k), k=0..7; M side f(i-4+k)). */
