@@ -182,6 +182,14 @@ int ocfd_b200_get_metrics(ocfd_b200_ctx *ctx, double *metrics13);
 int ocfd_b200_set_primitives(ocfd_b200_ctx *ctx, const double *prim5, int istep, double tt);
 int ocfd_b200_set_primitives_device(ocfd_b200_ctx *ctx, const double *prim5_dev, int istep, double tt);
 
+/* Whole steps as CUDA graphs (no counterpart in the reference; default on):
+ * a step whose stages need nothing from the host -- no kernel timing, no
+ * per-step flag-count read-back (the hybrid scheme's automatic walk choice),
+ * no boundary-condition family, no z split -- is captured once per
+ * time-level parity and replayed, which removes the per-kernel launch cost
+ * on small grids.  Any change of the parameters, the stream or the switch
+ * captures it again.  0 turns it off (every kernel launched one by one). */
+int ocfd_b200_set_graphs(ocfd_b200_ctx *ctx, int enabled);
 /* nsteps full SSP-RK3 steps (time-level swap + 3 stages each),
  * src/OCFD_NS_Solver.cu:63-89.  Asynchronous on the context stream. */
 int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps);

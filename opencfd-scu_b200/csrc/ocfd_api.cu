@@ -149,6 +149,18 @@ struct ocfd_b200_ctx {
     long long launches = 0;
     // timing
     bool timing = false;
+    // whole RK3 steps replayed from CUDA graphs (one per time-level parity,
+    // captured on first use and again whenever the parameter block, the
+    // stream or the switch set-up differs from the captured one)
+    struct StepGraph {
+        cudaGraphExec_t exec = nullptr;
+        Params key;
+        cudaStream_t stream = nullptr;
+        bool sw_on = false;
+        float sw_conf = 0.0f;
+        long long launches = 0;
+    } graph[2];
+    bool graphs_on = true;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     double t_ms[OCFD_TIMER_COUNT] = {0};
     long long t_n[OCFD_TIMER_COUNT] = {0};
@@ -204,6 +216,7 @@ static void free_all(ocfd_b200_ctx *c) {
     cudaFree(c->prec_buf);
     cudaFree(c->sw_w);
     cudaFree(c->sw_stats);
+    for (auto &g : c->graph) if (g.exec) { cudaGraphExecDestroy(g.exec); g.exec = nullptr; }
     if (c->xstream) cudaStreamSynchronize(c->xstream);
     ocfd::slab_destroy(c->slab);
     c->slab = nullptr;
@@ -1143,6 +1156,59 @@ static int run_filters(ocfd_b200_ctx *ctx) {
     return OCFD_OK;
 }
 
+// A step can run as one CUDA graph when nothing in it goes to the host: no
+// kernel timing, no per-step flag-count read-back for the walk choice, no
+// boundary-condition family (its wall law takes the time of each stage), no
+// slab exchange.  The filters run after the step, outside the graph.
+static bool step_graph_ok(const ocfd_b200_ctx *ctx) {
+    const Params &p = ctx->p;
+    const bool readback = p.scheme_invis == 310 && (p.sweep_impl == 4 || p.mixed) && ocfd::sweeps4_supported(p) &&
+                          p.flag_count;
+    return ctx->graphs_on && !ctx->timing && !readback && !p.ibc && !ctx->slab;
+}
+
+// the three stages of one step (time levels already swapped) from the graph
+// of this parity, captured first if it is missing or stale
+static int step_graph(ocfd_b200_ctx *ctx) {
+    auto &G = ctx->graph[ctx->p.f == ctx->cons_buf ? 0 : 1];
+    const bool fresh = G.exec && G.stream == ctx->stream && G.sw_on == ctx->sw_on &&
+                       G.sw_conf == ctx->sw_conf_logit && memcmp(&G.key, &ctx->p, sizeof(Params)) == 0;
+    if (fresh) {
+        CK(cudaGraphLaunch(G.exec, ctx->stream), "step graph");
+        ctx->launches += G.launches;
+        return OCFD_OK;
+    }
+    if (G.exec) { cudaGraphExecDestroy(G.exec); G.exec = nullptr; }
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "step graph capture");
+    const long long l0 = ctx->launches;
+    int rc = OCFD_OK;
+    for (int krk = 1; krk <= 3 && !rc; krk++) rc = rhs(ctx, krk, krk);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (rc || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (rc) return rc;
+        return cuda_fail(ctx, e, "step graph capture");
+    }
+    e = cudaGraphInstantiate(&G.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { G.exec = nullptr; return cuda_fail(ctx, e, "step graph instantiate"); }
+    memcpy(&G.key, &ctx->p, sizeof(Params));
+    G.stream = ctx->stream;
+    G.sw_on = ctx->sw_on;
+    G.sw_conf = ctx->sw_conf_logit;
+    G.launches = ctx->launches - l0;
+    CK(cudaGraphLaunch(G.exec, ctx->stream), "step graph");
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_set_graphs(ocfd_b200_ctx *ctx, int enabled) {
+    if (!ctx) return OCFD_ERR_ARG;
+    ctx->graphs_on = enabled != 0;
+    return OCFD_OK;
+}
+
 extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
     int rc = check_ready(ctx);
     if (rc) return rc;
@@ -1152,8 +1218,12 @@ extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
     if (ctx->p.mixed && nsteps > 0) ctx->prims64_stale = true;
     for (int n = 0; n < nsteps; n++) {
         ocfd_b200_swap_time_levels(ctx);
-        for (int krk = 1; krk <= 3; krk++)
-            if ((rc = rhs(ctx, krk, krk))) return rc;
+        if (step_graph_ok(ctx)) {
+            if ((rc = step_graph(ctx))) return rc;
+        } else {
+            for (int krk = 1; krk <= 3; krk++)
+                if ((rc = rhs(ctx, krk, krk))) return rc;
+        }
         ctx->istep++;
         ctx->tt += ctx->p.dt;
         if ((rc = run_filters(ctx))) return rc;
