@@ -188,7 +188,10 @@ int ocfd_b200_set_primitives_device(ocfd_b200_ctx *ctx, const double *prim5_dev,
  * no boundary-condition family, no z split -- is captured once per
  * time-level parity and replayed, which removes the per-kernel launch cost
  * on small grids.  Any change of the parameters, the stream or the switch
- * captures it again.  0 turns it off (every kernel launched one by one). */
+ * captures it again.  On a stream the caller is capturing, the kernels go
+ * into the caller's graph; on a stream that cannot be captured (the legacy
+ * default stream) steps launch one by one.  0 turns it off (every kernel
+ * launched one by one). */
 int ocfd_b200_set_graphs(ocfd_b200_ctx *ctx, int enabled);
 /* nsteps full SSP-RK3 steps (time-level swap + 3 stages each),
  * src/OCFD_NS_Solver.cu:63-89.  Asynchronous on the context stream. */

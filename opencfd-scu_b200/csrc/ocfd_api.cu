@@ -1169,7 +1169,22 @@ static bool step_graph_ok(const ocfd_b200_ctx *ctx) {
 
 // the three stages of one step (time levels already swapped) from the graph
 // of this parity, captured first if it is missing or stale
+static int step_launched(ocfd_b200_ctx *ctx) {
+    for (int krk = 1; krk <= 3; krk++) {
+        int rc = rhs(ctx, krk, krk);
+        if (rc) return rc;
+    }
+    return OCFD_OK;
+}
+
 static int step_graph(ocfd_b200_ctx *ctx) {
+    // a stream that the caller is capturing already takes the launches into
+    // the caller's graph
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return step_launched(ctx);
+    }
     auto &G = ctx->graph[ctx->p.f == ctx->cons_buf ? 0 : 1];
     const bool fresh = G.exec && G.stream == ctx->stream && G.sw_on == ctx->sw_on &&
                        G.sw_conf == ctx->sw_conf_logit && memcmp(&G.key, &ctx->p, sizeof(Params)) == 0;
@@ -1179,7 +1194,13 @@ static int step_graph(ocfd_b200_ctx *ctx) {
         return OCFD_OK;
     }
     if (G.exec) { cudaGraphExecDestroy(G.exec); G.exec = nullptr; }
-    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "step graph capture");
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        // a stream that cannot be captured (the legacy default stream):
+        // launch one by one from now on
+        cudaGetLastError();
+        ctx->graphs_on = false;
+        return step_launched(ctx);
+    }
     const long long l0 = ctx->launches;
     int rc = OCFD_OK;
     for (int krk = 1; krk <= 3 && !rc; krk++) rc = rhs(ctx, krk, krk);
@@ -1218,12 +1239,7 @@ extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
     if (ctx->p.mixed && nsteps > 0) ctx->prims64_stale = true;
     for (int n = 0; n < nsteps; n++) {
         ocfd_b200_swap_time_levels(ctx);
-        if (step_graph_ok(ctx)) {
-            if ((rc = step_graph(ctx))) return rc;
-        } else {
-            for (int krk = 1; krk <= 3; krk++)
-                if ((rc = rhs(ctx, krk, krk))) return rc;
-        }
+        if ((rc = step_graph_ok(ctx) ? step_graph(ctx) : step_launched(ctx))) return rc;
         ctx->istep++;
         ctx->tt += ctx->p.dt;
         if ((rc = run_filters(ctx))) return rc;

@@ -50,3 +50,15 @@ def test_graph_follows_parameter_changes(gpu_lib):
         s.set_primitives(c.prims, 0, 0.0)  # new state, same parameters
         s.step(2)
     assert np.array_equal(a.conserved(), b.conserved())
+
+
+def test_uncapturable_stream_launches(gpu_lib):
+    """On the legacy default stream (which cannot be captured) steps launch
+    their kernels one by one, with the same result."""
+    c = cases.taylor_green(16, seed=3)
+    a, b = _pair(c)
+    b.set_stream(1)                        # cudaStreamLegacy
+    a.step(3)
+    b.step(3)
+    b.synchronize()
+    assert np.array_equal(a.conserved(), b.conserved())
