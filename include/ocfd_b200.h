@@ -184,10 +184,11 @@ int ocfd_b200_set_primitives_device(ocfd_b200_ctx *ctx, const double *prim5_dev,
 
 /* Whole steps as CUDA graphs (no counterpart in the reference; default on):
  * a step whose stages need nothing from the host -- no kernel timing, no
- * per-step flag-count read-back (the hybrid scheme's automatic walk choice),
- * no boundary-condition family, no z split -- is captured once per
- * time-level parity and replayed, which removes the per-kernel launch cost
- * on small grids.  Any change of the parameters, the stream or the switch
+ * boundary-condition family, no z split -- is captured once per time-level
+ * parity and replayed, which removes the per-kernel launch cost on small
+ * grids.  With the hybrid scheme's automatic walk choice the first sensor
+ * pass and its read-back run first and the graph holds the rest of the step
+ * for the walks chosen.  Any change of the parameters, the stream or the switch
  * captures it again.  On a stream the caller is capturing, the kernels go
  * into the caller's graph; on a stream that cannot be captured (the legacy
  * default stream) steps launch one by one.  0 turns it off (every kernel

@@ -159,6 +159,7 @@ struct ocfd_b200_ctx {
         bool sw_on = false;
         float sw_conf = 0.0f;
         long long launches = 0;
+        int walk = -1;          // the walks chosen by the sensor pass before it (-1: none)
     } graph[2];
     bool graphs_on = true;
     cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -569,15 +570,22 @@ static int sweeps_auto(ocfd_b200_ctx *ctx) {
     return OCFD_OK;
 }
 
-static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
+// the hybrid scheme's sensor (or learned switch) pass of the first stage,
+// with the per-step read-back of its non-UP7 counts that picks the walks
+static bool needs_readback(const ocfd_b200_ctx *ctx) {
     const Params &p = ctx->p;
-    if (p.scheme_invis == 310 && krk == 1) {
+    return p.scheme_invis == 310 && (p.sweep_impl == 4 || p.mixed) && ocfd::sweeps4_supported(p) && p.flag_count;
+}
+
+static int rhs_sensor(ocfd_b200_ctx *ctx) {
+    const Params &p = ctx->p;
+    {
         TimerScope ts(ctx, T_SENSOR);
         if (ctx->sw_on) CK(ocfd::launch_switch_infer(p, ctx->sw_w, ctx->sw_conf_logit, ctx->sw_stats, ctx->stream),
                            "learned switch");
         else            CK(ocfd::launch_sensor(p, ctx->stream), "sensor");
         ctx->launches += 1;
-        if ((p.sweep_impl == 4 || p.mixed) && ocfd::sweeps4_supported(p) && p.flag_count) {
+        if (needs_readback(ctx)) {
             // the choice follows this pass's flags: one small read-back per step
             if (ctx->slab) {        // every slab takes the same walk: counts of the whole grid
                 std::string err;
@@ -589,6 +597,16 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk) {
             CK(cudaStreamSynchronize(ctx->stream), "flag counts");
             for (int d = 0; d < 3; d++) ctx->walk4[d] = walk4_wanted(ctx, d, ctx->h_flag_count[d]);
         }
+    }
+    return OCFD_OK;
+}
+
+// skip_sensor: the first stage's sensor pass has run already (step graphs)
+static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk, bool skip_sensor = false) {
+    const Params &p = ctx->p;
+    if (p.scheme_invis == 310 && krk == 1 && !skip_sensor) {
+        int rc = rhs_sensor(ctx);
+        if (rc) return rc;
     }
     {
         TimerScope ts(ctx, T_GHOST);
@@ -1156,37 +1174,44 @@ static int run_filters(ocfd_b200_ctx *ctx) {
     return OCFD_OK;
 }
 
-// A step can run as one CUDA graph when nothing in it goes to the host: no
-// kernel timing, no per-step flag-count read-back for the walk choice, no
-// boundary-condition family (its wall law takes the time of each stage), no
-// slab exchange.  The filters run after the step, outside the graph.
+// A step runs from a CUDA graph unless something in it goes to the host: no
+// kernel timing, no boundary-condition family (its wall law takes the time
+// of each stage), no slab exchange.  The hybrid scheme's flag-count
+// read-back comes before the graph; the filters run after the step.
 static bool step_graph_ok(const ocfd_b200_ctx *ctx) {
-    const Params &p = ctx->p;
-    const bool readback = p.scheme_invis == 310 && (p.sweep_impl == 4 || p.mixed) && ocfd::sweeps4_supported(p) &&
-                          p.flag_count;
-    return ctx->graphs_on && !ctx->timing && !readback && !p.ibc && !ctx->slab;
+    return ctx->graphs_on && !ctx->timing && !ctx->p.ibc && !ctx->slab;
 }
 
-// the three stages of one step (time levels already swapped) from the graph
-// of this parity, captured first if it is missing or stale
-static int step_launched(ocfd_b200_ctx *ctx) {
+// the three stages of one step, time levels already swapped (skip_sensor:
+// the first stage's sensor pass has run)
+static int step_launched(ocfd_b200_ctx *ctx, bool skip_sensor) {
     for (int krk = 1; krk <= 3; krk++) {
-        int rc = rhs(ctx, krk, krk);
+        int rc = rhs(ctx, krk, krk, skip_sensor);
         if (rc) return rc;
     }
     return OCFD_OK;
 }
 
+// The same from the graph of this parity, captured first if it is missing or
+// stale.  With the hybrid scheme's per-step read-back the sensor pass runs
+// first, outside the graph, and the graph holds the rest of the step for the
+// walks that pass chose.
 static int step_graph(ocfd_b200_ctx *ctx) {
+    const bool skip = needs_readback(ctx);
+    if (skip) {
+        int rc = rhs_sensor(ctx);
+        if (rc) return rc;
+    }
     // a stream that the caller is capturing already takes the launches into
     // the caller's graph
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
         cudaGetLastError();
-        return step_launched(ctx);
+        return step_launched(ctx, skip);
     }
+    const int walk = skip ? ctx->walk4[0] | ctx->walk4[1] << 1 | ctx->walk4[2] << 2 : -1;
     auto &G = ctx->graph[ctx->p.f == ctx->cons_buf ? 0 : 1];
-    const bool fresh = G.exec && G.stream == ctx->stream && G.sw_on == ctx->sw_on &&
+    const bool fresh = G.exec && G.stream == ctx->stream && G.sw_on == ctx->sw_on && G.walk == walk &&
                        G.sw_conf == ctx->sw_conf_logit && memcmp(&G.key, &ctx->p, sizeof(Params)) == 0;
     if (fresh) {
         CK(cudaGraphLaunch(G.exec, ctx->stream), "step graph");
@@ -1199,11 +1224,11 @@ static int step_graph(ocfd_b200_ctx *ctx) {
         // launch one by one from now on
         cudaGetLastError();
         ctx->graphs_on = false;
-        return step_launched(ctx);
+        return step_launched(ctx, skip);
     }
     const long long l0 = ctx->launches;
     int rc = OCFD_OK;
-    for (int krk = 1; krk <= 3 && !rc; krk++) rc = rhs(ctx, krk, krk);
+    for (int krk = 1; krk <= 3 && !rc; krk++) rc = rhs(ctx, krk, krk, skip);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
     if (rc || e != cudaSuccess) {
@@ -1219,6 +1244,7 @@ static int step_graph(ocfd_b200_ctx *ctx) {
     G.stream = ctx->stream;
     G.sw_on = ctx->sw_on;
     G.sw_conf = ctx->sw_conf_logit;
+    G.walk = walk;
     G.launches = ctx->launches - l0;
     CK(cudaGraphLaunch(G.exec, ctx->stream), "step graph");
     return OCFD_OK;
@@ -1239,7 +1265,7 @@ extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
     if (ctx->p.mixed && nsteps > 0) ctx->prims64_stale = true;
     for (int n = 0; n < nsteps; n++) {
         ocfd_b200_swap_time_levels(ctx);
-        if ((rc = step_graph_ok(ctx) ? step_graph(ctx) : step_launched(ctx))) return rc;
+        if ((rc = step_graph_ok(ctx) ? step_graph(ctx) : step_launched(ctx, false))) return rc;
         ctx->istep++;
         ctx->tt += ctx->p.dt;
         if ((rc = run_filters(ctx))) return rc;

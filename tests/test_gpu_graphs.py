@@ -1,10 +1,12 @@
 """Whole steps replayed from CUDA graphs give the same state, to the last
 bit, as the same kernels launched one by one; a change of the parameters
 between steps captures the graph again."""
+import os
+
 import numpy as np
 import pytest
 
-from ocfd_b200 import cases, lib
+from ocfd_b200 import cases, learned, lib
 
 pytestmark = pytest.mark.gpu
 
@@ -19,16 +21,26 @@ def _pair(c, prep=None):
     return a, b
 
 
-@pytest.mark.parametrize("name", ["tgv_weno7", "tgv_fp32", "iso_hybrid_inline", "curvilinear"])
+@pytest.mark.parametrize("name", ["tgv_weno7", "tgv_fp32", "iso_hybrid_inline", "iso_hybrid_auto", "iso_fp32_learned",
+                                  "curvilinear"])
 def test_graph_steps_equal_launched_steps(name, gpu_lib):
     prep = None
     if name.startswith("tgv"):
         c = cases.taylor_green(16, seed=3)
         if name.endswith("fp32"):
             prep = lambda s: s.set_precision(1)
-    elif name == "iso_hybrid_inline":          # variant 6: no per-step read-back, so a graph
+    elif name == "iso_hybrid_inline":          # variant 6: no per-step read-back
         c = cases.isotropic_turbulence(24, seed=9, charteric=1, hy_dp_intv=(0.002, 0.02))
         prep = lambda s: s.set_sweep_impl(6)
+    elif name == "iso_hybrid_auto":            # sensor and read-back before the graph
+        c = cases.isotropic_turbulence(24, seed=9, charteric=1, hy_dp_intv=(0.002, 0.02))
+    elif name == "iso_fp32_learned":           # the switch pass before the graph
+        c = cases.isotropic_turbulence(24, seed=9, charteric=1, hy_dp_intv=(0.002, 0.02))
+        w = learned.load_model(os.path.join(os.path.dirname(lib.__file__), "data", "switch_c1c3.npz"))
+
+        def prep(s):
+            s.set_precision(1)
+            s.set_switch(w, 0.9)
     else:
         c = cases.random_smooth_case(20, 16, 12, seed=5, curvilinear=True, shock=True)
     a, b = _pair(c, prep)
@@ -38,6 +50,10 @@ def test_graph_steps_equal_launched_steps(name, gpu_lib):
     assert np.array_equal(a.primitives(), b.primitives())
     assert a.launch_count() == b.launch_count()
     assert a.time() == b.time()
+    if c.cfg.scheme_invis == "SCHEME_HYBRIDAUTO":
+        assert a.sweep_walks() == b.sweep_walks()
+        for fa, fb in zip(a.flags(), b.flags()):
+            assert np.array_equal(fa, fb)
 
 
 def test_graph_follows_parameter_changes(gpu_lib):
