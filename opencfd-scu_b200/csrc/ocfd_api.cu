@@ -755,18 +755,20 @@ extern "C" int ocfd_b200_set_slab(ocfd_b200_ctx *ctx, int nranks, int rank, int 
     if (z_offset < 0 || nz_global < p.nz || z_offset + p.nz > nz_global)
         return fail(ctx, OCFD_ERR_ARG, "slab planes outside the grid");
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    // the exchange stream and its events first, so that a failure leaves the
+    // context as it was (a stream or event made here is released at destroy)
+    if ((!ctx->xstream && cudaStreamCreateWithFlags(&ctx->xstream, cudaStreamNonBlocking) != cudaSuccess) ||
+        (!ctx->xev[0] && cudaEventCreateWithFlags(&ctx->xev[0], cudaEventDisableTiming) != cudaSuccess) ||
+        (!ctx->xev[1] && cudaEventCreateWithFlags(&ctx->xev[1], cudaEventDisableTiming) != cudaSuccess)) {
+        cudaGetLastError();
+        return fail(ctx, OCFD_ERR_CUDA, "exchange stream");
+    }
     std::string err;
     ctx->slab = ocfd::slab_create(p, nranks, rank, rank_lo, rank_hi, id, err);
     if (!ctx->slab) return fail(ctx, OCFD_ERR_CUDA, err);
     ctx->z_offset = z_offset;
     ctx->nz_global = nz_global;
     ctx->slab_count = nranks;
-    if (cudaStreamCreateWithFlags(&ctx->xstream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->xev[0], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->xev[1], cudaEventDisableTiming) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(ctx, OCFD_ERR_CUDA, "exchange stream");
-    }
     // hz = 1/(NZ_GLOBAL - 1) (src/OCFD_init.cu:29-31); OCFD_bc re-projects
     // only the faces of the whole grid (src/OCFD_boundary.cu:78-95)
     p.hz = 1.0 / (nz_global - 1.0);
