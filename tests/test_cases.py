@@ -78,3 +78,36 @@ def test_isotropic_turbulence_reynolds_number():
     dudx = np.real(np.fft.ifftn(1j * KX * np.fft.fftn(u)))
     lam = math.sqrt(np.mean(u * u) / np.mean(dudx * dudx))
     assert c.cfg.re * lam == pytest.approx(100.0, rel=1e-12)
+
+
+def test_ramp_mesh_and_inflow():
+    """The 24-degree ramp: flat wall up to the corner at mid-length, then the
+    wall rises at the ramp angle; tanh wall-normal stretching with a first
+    cell of 0.01 boundary-layer thicknesses; periodic span; the inflow is the
+    1/7-power layer at the isothermal wall temperature."""
+    nx, ny, nz = 64, 32, 8
+    c = cases.ramp_case(nx, ny, nz, seed=1)
+    x, y, z = c.metrics
+    assert x.shape == (nz, ny, nx)
+    wall = y[0, 0, :]
+    xs = x[0, 0, :]
+    flat = xs <= 20.0
+    assert np.all(np.abs(wall[flat]) < 1e-12)
+    slope = np.diff(wall[~flat]) / np.diff(xs[~flat])
+    assert np.allclose(slope, math.tan(math.radians(24.0)), rtol=1e-12)
+    assert y[0, 1, 0] - y[0, 0, 0] == pytest.approx(0.01, rel=1e-6)      # first cell at x = 0
+    assert np.all(np.diff(y[0, :, 0]) > 0) and y[0, -1, 0] == pytest.approx(15.0)
+    assert np.all(np.diff(y[0, :, 0])[1:] > np.diff(y[0, :, 0])[:-1])    # stretched away from the wall
+    assert np.allclose(np.diff(z[:, 0, 0]), 1.0)                          # span 8, 8 planes
+    d_in, u_in, v_in, T_in = c.inlet
+    dist = y[0, :, 0]
+    assert np.allclose(u_in, np.clip(dist, 0, 1) ** (1 / 7))
+    # T linear in u from the wall temperature 2.5 to 1 at the edge, uniform pressure
+    assert np.allclose(T_in, 2.5 - 1.5 * u_in) and np.allclose(d_in * T_in, 1.0) and not v_in.any()
+    assert u_in[0] < 0.01 and u_in[-1] == 1.0
+    assert c.cfg.iperiodic == (0, 0, 1) and c.cfg.ibc == 108 and c.cfg.dif_bound[:4] == (1, 1, 1, 1)
+    # seeded fluctuations of about 2 %
+    d = c.prims[0]
+    dwall = y - y[:, :1, :]
+    base = 1.0 / (2.5 - 1.5 * np.clip(dwall, 0, 1) ** (1 / 7))
+    assert np.std(d / base - 1.0) == pytest.approx(0.02, rel=0.05)
