@@ -111,7 +111,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
-# The three plain-FP64 workloads (BASELINE configurations):
+# The three plain-FP64 workloads (the benchmark configurations):
 #   iso  decaying isotropic turbulence n^3 (default 256^3), hybrid UP7/WENO7/WENO5
 #        with the Jameson sensor and characteristic projection, CD6, periodic;
 #   tgv  Taylor-Green vortex n^3 (64^3), WENO7 + CD6, Mach 0.1, Re 1600;
@@ -335,7 +335,7 @@ DOM_BYTES = {
 # Grids whose metrics are fields (the ramp): the sweeps also read the
 # direction's 3 metrics at every split point and Ajac per cell (+4 words per
 # direction), k_vis_ev reads 9 metrics and Ajac, k_vis_div Ajac (+11 words);
-# the stage-level bound adds the 10 metric fields (SURVEY's B_alg = 200 B).
+# the stage-level bound adds the 10 metric fields (200 B per cell-stage).
 DOM_BYTES_FIELDS = {
     "inviscid_sweeps": (40 + 12) * 8.0,
     "viscous_rk_update": (53 + 11) * 8.0,

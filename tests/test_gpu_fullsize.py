@@ -10,7 +10,7 @@
 * C4: the compression ramp 512x128x64 (metrics from the mesh, IBC 108, the
   shock filter) against the reference build after 100 steps, and after the
   stated 500 steps within the reference's own one-ulp sensitivity.
-Tolerance: relative L2 <= 1e-12 per variable.
+Tolerance: relative L2 <= 1e-12 per variable (the parity bound).
 """
 import numpy as np
 import pytest
