@@ -199,6 +199,8 @@ def run_ours(args, rank, world, dist):
         cid = slabs.share_id(group=None) if dist else lib.slab_unique_id()
         slab = slabs.slab_spec(rank, world, case.cfg.nz * world, cid)
     solver = lib.Solver(case.cfg, case.prims, case.metrics, device=dev, inlet=case.inlet, slab=slab)
+    if args.no_graphs:                  # every kernel launched one by one
+        solver.set_graphs(False)
     if args.form != "fp64":             # precision form (and the learned switch)
         solver.set_precision(1)
     if args.form == "fp32-learned":
@@ -290,6 +292,7 @@ def run_ours(args, rank, world, dist):
                    "seed": 2024 if args.workload != "tgv" else 1234,
                    "l2": f"inputs larger than L2 (state ~{state_gb:.1f} GB/GPU)" if state_gb > 0.5
                          else f"state ~{state_gb:.2f} GB/GPU, partly L2-resident",
+                   "steps_as": "launched kernels" if args.no_graphs else "CUDA graphs where eligible",
                    "parallelism": (f"z slabs x{world} (grid {nx}x{ny}x{nz * world}, ghost planes over NCCL)"
                                    if args.decomp == "z" else f"replicas x{world}")},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
@@ -420,6 +423,8 @@ def main():
                     help="grid size (iso, tgv: n^3; ramp: 4n x n x n/2); 0 = the configuration's own")
     ap.add_argument("--decomp", choices=("replicas", "z"), default="replicas",
                     help="N > 1: independent replicas, or the z slabs of one grid (ghost planes over NCCL)")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="launch every kernel one by one instead of replaying whole steps as CUDA graphs")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--ref-steps", type=int, default=4)
     ap.add_argument("--cpu-sample", type=int, default=96)
