@@ -143,6 +143,22 @@ def cells_of(case) -> int:
     return case.cfg.nx * case.cfg.ny * case.cfg.nz
 
 
+def config_of(args, case, world: int) -> dict:
+    """The workload description both arms print (the reference arm runs the
+    same case, so the two dicts are equal)."""
+    nx, ny, nz = case.cfg.nx, case.cfg.ny, case.cfg.nz
+    cells = nx * ny * nz
+    state_gb = 8 * cells * (15 + 35 * (nx + 8) * (ny + 8) * (nz + 8) / cells) / 1e9
+    return {"workload": WORKLOADS[args.workload].format(nx=nx, ny=ny, nz=nz),
+            "grid": [nx, ny, nz], "stages_per_step": 3, "form": args.form,
+            "scheme": f"SCHEME_INVIS {case.cfg.scheme_invis}, CHARTERIC={case.cfg.charteric}",
+            "seed": 2024 if args.workload != "tgv" else 1234,
+            "l2": f"inputs larger than L2 (state ~{state_gb:.1f} GB/GPU)" if state_gb > 0.5
+                  else f"state ~{state_gb:.2f} GB/GPU, partly L2-resident",
+            "parallelism": (f"z slabs x{world} (grid {nx}x{ny}x{nz * world}, ghost planes over NCCL)"
+                            if args.decomp == "z" else f"replicas x{world}")}
+
+
 def cpu_baseline(workload: str, n_sample: int, steps: int = 0, budget_s: float = 12.0):
     """The OpenMP FP64 oracle timed on this host on a bounded sample: whole
     RK3 steps of the case at a reduced size until about budget_s seconds of
@@ -183,9 +199,93 @@ def aggregate_rate(cells: int, stages: int, seconds_max: float, world: int) -> f
     return world * cells * stages / seconds_max / 1e9
 
 
+def make_solver(args, case, dev, form, slab=None):
+    from ocfd_b200 import lib
+    solver = lib.Solver(case.cfg, case.prims, case.metrics, device=dev, inlet=case.inlet, slab=slab)
+    if args.no_graphs:                  # every kernel launched one by one
+        solver.set_graphs(False)
+    if form != "fp64":                  # precision form (and the learned switch)
+        solver.set_precision(1)
+    if form == "fp32-learned":
+        from ocfd_b200 import learned
+        solver.set_switch(learned.load_model(SWITCH_MODEL), 0.9)
+    return solver
+
+
+def timed_steps(solver, stream, steps, warmup, dist, dev, sample_clocks=True):
+    """W untimed steps, one timing pass (per-family device times, untimed),
+    then exactly `steps` steps between CUDA events on the solver's stream,
+    barrier + synchronize on both sides.  Returns (ms, launches, families,
+    clocks)."""
+    import torch
+    solver.step(warmup)
+    solver.synchronize()
+    solver.set_timing(True)
+    solver.step(1)
+    solver.synchronize()
+    fam = solver.timing()
+    solver.set_timing(False)
+    sampler = ClockSampler(dev) if sample_clocks else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    l0 = solver.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    solver.step(steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    launches = solver.launch_count() - l0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if sampler else None
+    return ev0.elapsed_time(ev1), launches, fam, clocks
+
+
+def rel_l2_per_variable(a, b):
+    """Relative L2 of each conserved variable; the momentum components
+    against the norm of the whole momentum vector (one may start near 0)."""
+    vec = float(np.sqrt(sum(np.linalg.norm(b[m]) ** 2 for m in (1, 2, 3))))
+    return [float(np.linalg.norm(a[m] - b[m]) / (vec if m in (1, 2, 3) else np.linalg.norm(b[m])))
+            for m in range(5)]
+
+
+def learned_leg(args, case, dev, ref_cons, ref_ms, steps_done):
+    """The precision form with the plain sensor and with the learned switch
+    on the same case, each timed like the main run (W warm-up steps, one
+    timing pass, `steps` timed steps), with the relative L2 of its conserved
+    state against the FP64 state after the same number of steps."""
+    import torch
+    out = {}
+    cells = cells_of(case)
+    for form in ("fp32", "fp32-learned"):
+        s = make_solver(args, case, dev, form)
+        stream = torch.cuda.Stream(device=dev)
+        s.set_stream(stream.cuda_stream)
+        ms, launches, fam, _ = timed_steps(s, stream, args.steps, args.warmup, None, dev, sample_clocks=False)
+        assert args.warmup + 1 + args.steps == steps_done
+        err = rel_l2_per_variable(s.conserved(), ref_cons)
+        leg = {"value": cells * 3 * args.steps / (ms / 1e3) / 1e9, "unit": METRIC,
+               "ms_per_step": ms / args.steps, "speedup_vs_fp64": ref_ms / ms,
+               "rel_l2_vs_fp64": err, "after_steps": steps_done,
+               "kernel_ms_per_stage": {k: v[0] / 3.0 for k, v in fam.items()}}
+        if form == "fp32-learned":
+            dec, plain, differ = s.switch_stats()
+            leg["switch_decisions"] = {"network": dec, "plain_sensor": plain, "network_differs": differ}
+        out[form] = leg
+        s.close()
+        del stream
+    out["switch_vs_plain_sensor"] = out["fp32"]["ms_per_step"] / out["fp32-learned"]["ms_per_step"]
+    return out
+
+
 def run_ours(args, rank, world, dist):
     import torch
-    from ocfd_b200 import lib
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
@@ -193,57 +293,24 @@ def run_ours(args, rank, world, dist):
     case = make_case(args.workload, n)
     slab = None
     if args.decomp == "z":
-        from ocfd_b200 import slabs
+        from ocfd_b200 import lib, slabs
         if args.workload == "ramp" and world > 1:
             raise SystemExit("--decomp z repeats the case in z; the ramp's mesh coordinates would not follow")
         cid = slabs.share_id(group=None) if dist else lib.slab_unique_id()
         slab = slabs.slab_spec(rank, world, case.cfg.nz * world, cid)
-    solver = lib.Solver(case.cfg, case.prims, case.metrics, device=dev, inlet=case.inlet, slab=slab)
-    if args.no_graphs:                  # every kernel launched one by one
-        solver.set_graphs(False)
-    if args.form != "fp64":             # precision form (and the learned switch)
-        solver.set_precision(1)
-    if args.form == "fp32-learned":
-        from ocfd_b200 import learned
-        solver.set_switch(learned.load_model(SWITCH_MODEL), 0.9)
+    solver = make_solver(args, case, dev, args.form, slab)
     stream = torch.cuda.Stream(device=dev)
     solver.set_stream(stream.cuda_stream)
     cells = cells_of(case)
     nx, ny, nz = case.cfg.nx, case.cfg.ny, case.cfg.nz
 
-    # warm-up
-    solver.step(args.warmup)
-    solver.synchronize()
-
-    # per-kernel timing pass (untimed region): device time per family
-    solver.set_timing(True)
-    solver.step(1)
-    solver.synchronize()
-    fam = solver.timing()
-    solver.set_timing(False)
-
-    # timed region
-    sampler = ClockSampler(dev)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    sampler.start()
-    time.sleep(0.3)
-    l0 = solver.launch_count()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    solver.step(args.steps)
-    ev1.record(stream)
-    ev1.synchronize()
-    launches = solver.launch_count() - l0
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = sampler.stop()
-    ms = ev0.elapsed_time(ev1)
+    ms, launches, fam, clocks = timed_steps(solver, stream, args.steps, args.warmup, dist, dev)
     ms_max = max_over_ranks(ms, dist, f"cuda:{dev}")
     value = aggregate_rate(cells, 3 * args.steps, ms_max / 1e3, world)
+    steps_done = args.warmup + 1 + args.steps
+    want_learned = (rank == 0 and world == 1 and args.learned and args.form == "fp64" and args.workload == "iso"
+                    and args.decomp == "replicas")
+    ref_cons = solver.conserved() if want_learned else None
 
     # end to end through the C ABI with host buffers (pinned), one RK3 step
     # per call: H2D of the primitives, the step, D2H of the primitives
@@ -263,45 +330,43 @@ def run_ours(args, rank, world, dist):
     e2e_s = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{dev}")
     e2e_val = aggregate_rate(cells, 3 * e2e_steps, e2e_s, world)
     nbytes = 5 * cells * 8
+    uniform = solver.uniform_metrics
+    if want_learned:
+        solver.close()
 
     if rank != 0:
         return None
     hbm, peak_kind = peaks()
-    # dominant kernel family and its roofline (HBM, algorithmic bytes)
-    fam_ms = {k: v[0] / max(v[1], 1) for k, v in fam.items() if v[1] > 0}
+    # dominant kernel family; its roofline uses the algorithmic bytes of a
+    # stage (read U^k and U^n, write U^k+1: 120 B per cell-stage; 200 B with
+    # the 10 metric fields of a curvilinear grid) over the family's time
     dom = max(fam, key=lambda k: fam[k][0])
     dom_ms_per_stage = fam[dom][0] / 3.0                  # one step = 3 stages
-    uniform = solver.uniform_metrics
-    dom_table = DOM_BYTES if uniform else DOM_BYTES_FIELDS
+    impl_table = DOM_BYTES if uniform else DOM_BYTES_FIELDS
     if args.form != "fp64":
-        dom_table = DOM_BYTES_FP32
+        impl_table = DOM_BYTES_FP32
     b_alg = B_ALG if uniform else B_ALG_FIELDS
-    dom_bytes = dom_table.get(dom, b_alg) * cells
-    achieved = dom_bytes / (dom_ms_per_stage / 1e3) / 1e9
+    achieved = b_alg * cells / (dom_ms_per_stage / 1e3) / 1e9
     stage_ms = ms_max / args.steps / 3.0
-    state_gb = 8 * cells * (15 + 35 * (nx + 8) * (ny + 8) * (nz + 8) / cells) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.form == "fp64" else "f32 stencils / f64 RK3 accumulation",
         "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.workload].format(nx=nx, ny=ny, nz=nz),
-                   "grid": [nx, ny, nz], "stages_per_step": 3, "form": args.form,
-                   "scheme": f"SCHEME_INVIS {case.cfg.scheme_invis}, CHARTERIC={case.cfg.charteric}",
-                   "seed": 2024 if args.workload != "tgv" else 1234,
-                   "l2": f"inputs larger than L2 (state ~{state_gb:.1f} GB/GPU)" if state_gb > 0.5
-                         else f"state ~{state_gb:.2f} GB/GPU, partly L2-resident",
-                   "steps_as": "launched kernels" if args.no_graphs else "CUDA graphs where eligible",
-                   "parallelism": (f"z slabs x{world} (grid {nx}x{ny}x{nz * world}, ghost planes over NCCL)"
-                                   if args.decomp == "z" else f"replicas x{world}")},
+        "config": config_of(args, case, world),
+        "execution": "launched kernels" if args.no_graphs else "whole steps as CUDA graphs where eligible",
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
+                     "algorithmic_bytes_per_cell_stage": b_alg,
                      "traffic": (TRAFFIC_PER_CELL[dom] * cells
                                  if (uniform and args.form == "fp64" and dom in TRAFFIC_PER_CELL) else None),
                      "traffic_source": TRAFFIC_SOURCE,
-                     "algorithmic_bytes_per_cell": dom_table.get(dom, b_alg),
                      "launch_ms": dom_ms_per_stage},
+        "implementation_bytes": {"bytes_per_cell": impl_table.get(dom, b_alg),
+                                 "gbs": impl_table.get(dom, b_alg) * cells / (dom_ms_per_stage / 1e3) / 1e9,
+                                 "note": "fields this implementation's kernels of the family read and write "
+                                         "once each per stage"},
         "stage_roofline": {"bytes_per_cell_stage": b_alg, "achieved_gbs": b_alg * cells / (stage_ms / 1e3) / 1e9,
                            "frac": b_alg * cells / (stage_ms / 1e3) / 1e9 / hbm},
         "kernel_ms_per_stage": {k: fam[k][0] / 3.0 for k in fam},
@@ -313,11 +378,15 @@ def run_ours(args, rank, world, dist):
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
+    if want_learned:
+        line["learned"] = learned_leg(args, case, dev, ref_cons, ms, steps_done)
     return line
 
 
-# Algorithmic bytes per cell for one stage's launches of each kernel family
-# on a uniform grid (metrics are constants there; every field touched once):
+# Bytes per cell that this implementation's kernels of each family move in
+# one stage, every field they touch counted once (reported beside the
+# roofline, which uses the stage's algorithmic bytes, B_ALG); uniform grid,
+# metrics constants:
 #   inviscid_sweeps: each of the x, y, z sweeps reads d,u,v,w,T; x writes du
 #                    (5), y and z read and write du (10 each)      -> 40 words
 #   viscous_rk_update: Ev kernel reads u,v,w,T, writes 12 Ev; divergence +
@@ -331,10 +400,6 @@ DOM_BYTES = {
     "sensor": 19.0,
 }
 
-# Measured DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell
-# for one stage's launches of each family, from one ncu capture of the same
-# kernels at 160^3 (profiles/stage_traffic_iso160.txt); the traffic scales with
-# the cells processed, so the bench line reports it times the cells of a launch.
 # Grids whose metrics are fields (the ramp): the sweeps also read the
 # direction's 3 metrics at every split point and Ajac per cell (+4 words per
 # direction), k_vis_ev reads 9 metrics and Ajac, k_vis_div Ajac (+11 words);
@@ -363,6 +428,10 @@ DOM_BYTES_FP32 = {
 SWITCH_MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "opencfd-scu_b200", "ocfd_b200", "data",
                             "switch_c1c3.npz")
 
+# Measured DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per cell
+# for one stage's launches of each family, from one ncu capture of the same
+# kernels at 160^3 (profiles/stage_traffic_iso160.txt); the traffic scales with
+# the cells processed, so the bench line reports it times the cells of a launch.
 TRAFFIC_PER_CELL = {
     "inviscid_sweeps": 304.6,       # 3 sweeps + 3 fix-ups
     "viscous_rk_update": 385.6,     # k_vis_ev + k_vis_div (Ev ghost fill not captured)
@@ -379,30 +448,32 @@ FLOP_SOURCE = "ncu executed FP64 instructions per stage (profiles/fp64_flops_iso
 
 
 def run_reference(args, rank, world):
-    """The reference's own CUDA build on the same workload (rank 0 only)."""
+    """The reference's own CUDA build on the same workload (rank 0 only):
+    the same case, W warm-up steps and exactly K timed steps."""
     if rank != 0:
         return None
     from oracle import ref_runner
     n = args.n
+    case = make_case(args.workload, n)
     if not ref_runner.available():
         c = cpu_baseline(args.workload, max(8, n // 4))
         return {"impl": "reference", "metric": METRIC, "value": c["value"], "unit": METRIC,
-                "n_gpus": world, "steps": 1, "warmup": 1, "higher_is_better": True,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "config": config_of(args, case, world),
                 "note": "reference build missing; CPU oracle port timed instead",
                 "cpu_baseline": c, "e2e": {"value": c["value"], "unit": METRIC,
                                             "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    case = make_case(args.workload, n)
-    ref_steps = max(1, min(args.steps, args.ref_steps))
-    secs, out = ref_runner.time_steps(case, args.warmup, ref_steps)
+    ref_steps = args.ref_steps if args.ref_steps > 0 else args.steps
+    secs, interval, _ = ref_runner.time_steps(case, args.warmup, ref_steps)
     v = cells_of(case) * 3 * ref_steps / secs / 1e9
-    nx, ny, nz = case.cfg.nx, case.cfg.ny, case.cfg.nz
-    return {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": 1,
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world,
             "steps": ref_steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / ref_steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.workload].format(nx=nx, ny=ny, nz=nz),
-                       "grid": [nx, ny, nz], "build": "reference sources, nvcc -O3 sm_100a, single-rank MPI shim",
-                       "timing": "reference's own MPI_Wtime interval print"},
+            "config": config_of(args, case, world),
+            "execution": "reference sources, nvcc -O3 sm_100a, single-rank MPI shim",
+            "timing": (f"the reference's own MPI_Wtime interval prints every {interval} steps; "
+                       f"the {ref_steps // interval} intervals after the {args.warmup} warm-up steps summed"),
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": 1, "kind": "reference",
                              "sample": f"{ref_steps} steps of the reference CUDA build on 1 B200, "
                                        f"driven by 1 host thread"},
@@ -412,8 +483,8 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="iso")
     ap.add_argument("--form", choices=("fp64", "fp32", "fp32-learned"), default="fp64",
@@ -426,7 +497,10 @@ def main():
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch every kernel one by one instead of replaying whole steps as CUDA graphs")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--ref-steps", type=int, default=4)
+    ap.add_argument("--ref-steps", type=int, default=0,
+                    help="timed steps of the reference arm (0: the same as --steps)")
+    ap.add_argument("--no-learned", dest="learned", action="store_false",
+                    help="skip the precision-form and learned-switch legs of the default run")
     ap.add_argument("--cpu-sample", type=int, default=96)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -11,7 +11,8 @@
  *  2. Reference-named entry points (du_comput, OCFD_time_advance, get_duvwT,
  *     get_Amu, OCFD_bc, Set_Scheme_HybridAuto) acting on a context bound with
  *     ocfd_b200_compat_bind().  These replace the reference's own objects for
- *     the RHS path; see INTEGRATION.md.
+ *     the RHS path; the reference's driver, configuration reader and I/O link
+ *     against them unchanged apart from its f/fn pointer swap.
  *
  * Arrays crossing the ABI are FP64, C order [nvar][nz][ny][nx] (x fastest),
  * interior cells only -- the order of the reference's record files
@@ -194,6 +195,8 @@ int ocfd_b200_set_primitives_device(ocfd_b200_ctx *ctx, const double *prim5_dev,
  * default stream) steps launch one by one.  0 turns it off (every kernel
  * launched one by one). */
 int ocfd_b200_set_graphs(ocfd_b200_ctx *ctx, int enabled);
+/* Step graphs captured so far (a replayed step adds none). */
+long long ocfd_b200_graph_captures(const ocfd_b200_ctx *ctx);
 /* nsteps full SSP-RK3 steps (time-level swap + 3 stages each),
  * src/OCFD_NS_Solver.cu:63-89.  Asynchronous on the context stream. */
 int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps);
@@ -294,8 +297,10 @@ long long ocfd_b200_launch_count(const ocfd_b200_ctx *ctx);
  * Partial sums go to one fixed device array shared by every call on a
  * device: at most OCFD_NOALLOC_MAX_FIELDS fields x 592 partials (37,888
  * bytes); nfield above the maximum returns OCFD_ERR_ARG with the reason in
- * ocfd_b200_last_error(NULL).  The first call on a device looks up that
- * array's address, so make it before any stream capture on that device.
+ * ocfd_b200_last_error(NULL).  Every call looks up that array's address on
+ * the current device (no allocation); the first call on a device can load
+ * the library's device code there, so make it before any stream capture on
+ * that device.
  * Calls that overlap in time on one device (other streams, other threads)
  * race on the shared array; order them.  For the same values the mean is
  * bitwise that of ocfd_b200_ana_residual. */

@@ -13,7 +13,6 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -162,6 +161,7 @@ struct ocfd_b200_ctx {
         int walk = -1;          // the walks chosen by the sensor pass before it (-1: none)
     } graph[2];
     bool graphs_on = true;
+    long long graph_captures = 0;       // step graphs captured so far
     cudaEvent_t ev[2] = {nullptr, nullptr};
     double t_ms[OCFD_TIMER_COUNT] = {0};
     long long t_n[OCFD_TIMER_COUNT] = {0};
@@ -1229,6 +1229,7 @@ static int step_graph(ocfd_b200_ctx *ctx) {
         return step_launched(ctx, skip);
     }
     const long long l0 = ctx->launches;
+    ctx->graph_captures += 1;
     int rc = OCFD_OK;
     for (int krk = 1; krk <= 3 && !rc; krk++) rc = rhs(ctx, krk, krk, skip);
     cudaGraph_t graph = nullptr;
@@ -1257,6 +1258,7 @@ extern "C" int ocfd_b200_set_graphs(ocfd_b200_ctx *ctx, int enabled) {
     ctx->graphs_on = enabled != 0;
     return OCFD_OK;
 }
+extern "C" long long ocfd_b200_graph_captures(const ocfd_b200_ctx *ctx) { return ctx ? ctx->graph_captures : 0; }
 
 extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
     int rc = check_ready(ctx);
@@ -1672,11 +1674,10 @@ namespace {
 constexpr int NA_BLOCKS = 592;        // partial sums per field (4 x 148 SMs)
 constexpr int NA_THREADS = 256;
 constexpr int NA_MAX_FIELDS = OCFD_NOALLOC_MAX_FIELDS;
-constexpr int NA_MAX_DEVICES = 64;
 
 // 8 fields x 592 partials x 8 bytes = 37,888 bytes per device.  Host code
-// never names this array directly; it reaches it through the address that
-// cudaGetSymbolAddress returns on each device.
+// never passes this array's name to a kernel; it passes the address that
+// cudaGetSymbolAddress returns on the current device.
 static __device__ __align__(256) double g_mean_scratch[NA_MAX_FIELDS * NA_BLOCKS];
 
 __global__ void __launch_bounds__(NA_THREADS) k_field_mean_partial(const double *fields, long long n,
@@ -1710,20 +1711,15 @@ __global__ void __launch_bounds__(NA_THREADS) k_field_mean_final(const double *p
     if (threadIdx.x == 0) means[blockIdx.x] = sh[0] / (double)n;
 }
 
-std::mutex g_na_mutex;
-double *g_na_scratch[NA_MAX_DEVICES] = {};
-
-// Address of this device's copy of g_mean_scratch, looked up once per device
-// (on the first call made with that device current) and cached.
-int noalloc_scratch(int dev, double **out) {
-    std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_scratch[dev]) {
-        double *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_mean_scratch);
-        if (e != cudaSuccess) return cuda_fail(nullptr, e, "field_means_noalloc: cudaGetSymbolAddress");
-        g_na_scratch[dev] = ptr;
-    }
-    *out = g_na_scratch[dev];
+// Address of the current device's copy of g_mean_scratch.  Looked up on every
+// call (the lookup allocates nothing): a cached address would go stale if the
+// caller reset the device or released its primary context, after which the
+// library's device code is loaded again and the array may sit elsewhere.
+int noalloc_scratch(double **out) {
+    double *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_mean_scratch);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "field_means_noalloc: cudaGetSymbolAddress");
+    *out = ptr;
     return OCFD_OK;
 }
 
@@ -1739,13 +1735,9 @@ extern "C" int ocfd_b200_field_means_noalloc(const double *fields, int nfield, l
                         std::to_string(NA_MAX_FIELDS) + " x " + std::to_string(NA_BLOCKS) + " partial sums)");
     if (n < 1 || n > (1LL << 40))
         return fail(nullptr, OCFD_ERR_ARG, "field_means_noalloc: n = " + std::to_string(n) + " is outside 1..2^40");
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(nullptr, e, "field_means_noalloc: cudaGetDevice");
-    if (dev < 0 || dev >= NA_MAX_DEVICES)
-        return fail(nullptr, OCFD_ERR_ARG, "field_means_noalloc: device ordinal above 63");
     double *scratch = nullptr;
-    int rc = noalloc_scratch(dev, &scratch);
+    int rc = noalloc_scratch(&scratch);
+    cudaError_t e;
     if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // every partial slot the final kernel reads is written by the first

@@ -30,7 +30,7 @@ EXPORTED = (
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
     "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics", "ocfd_b200_set_sweep_impl",
     "ocfd_b200_sweep_walks", "ocfd_b200_set_precision", "ocfd_b200_slab_unique_id", "ocfd_b200_set_slab",
-    "ocfd_b200_set_graphs",
+    "ocfd_b200_set_graphs", "ocfd_b200_graph_captures",
     "ocfd_b200_scheme_proportion", "ocfd_b200_mlp_nparam", "ocfd_b200_set_switch", "ocfd_b200_switch_stats", "ocfd_b200_switch_features",
     "ocfd_b200_mlp_last_error", "ocfd_b200_mlp_infer", "ocfd_b200_mlp_grad", "ocfd_b200_mlp_train",
     "ocfd_b200_set_mesh", "ocfd_b200_set_mesh_device", "ocfd_b200_get_metrics",
@@ -123,6 +123,7 @@ def load(path: Optional[str] = None):
         "ocfd_b200_set_precision": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_slab_unique_id": (ctypes.c_int, [ctypes.c_char_p]),
         "ocfd_b200_set_graphs": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_graph_captures": (ctypes.c_longlong, [P]),
         "ocfd_b200_set_slab": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                               ctypes.c_int, ctypes.c_int, ctypes.c_char_p]),
         "ocfd_b200_scheme_proportion": (ctypes.c_int, [P, D]),
@@ -485,3 +486,7 @@ class Solver:
 
     def launch_count(self) -> int:
         return int(self.L.ocfd_b200_launch_count(self.h))
+
+    def graph_captures(self) -> int:
+        """Step graphs captured so far; replayed steps add none."""
+        return int(self.L.ocfd_b200_graph_captures(self.h))

@@ -7,6 +7,7 @@ directory and parses what it prints or saves.
 """
 from __future__ import annotations
 
+import math
 import os
 import re
 import resource
@@ -79,14 +80,16 @@ def run_and_read(case, nsteps: int, timeout: float = 900.0):
 _INTERVAL = re.compile(r"^(\d+) steps GPU time ([0-9.eE+-]+)", re.M)
 
 
-def time_steps(case, warmup: int, steps: int, timeout: float = 1800.0) -> Tuple[float, str]:
-    """Seconds for `steps` RK3 steps after `warmup` steps, from the reference's
-    own MPI_Wtime interval print (src/OCFD_NS_Solver.cu:104-153).  The show
-    interval is `steps`; warmup is rounded up to a multiple of it."""
+def time_steps(case, warmup: int, steps: int, timeout: float = 1800.0) -> Tuple[float, int, str]:
+    """Seconds for exactly `steps` RK3 steps after exactly `warmup` steps, from
+    the reference's own MPI_Wtime interval print (src/OCFD_NS_Solver.cu:104-153).
+    The print interval is gcd(warmup, steps); the intervals after the warm-up
+    are summed (each interval excludes the analysis the print itself runs).
+    Returns (seconds, interval, stdout)."""
     cfg = case.cfg
-    nwarm = max(1, -(-warmup // steps)) * steps
-    cfg.set_steps(nwarm + steps)
-    cfg.kstep_show = steps
+    interval = math.gcd(max(1, warmup), steps)
+    cfg.set_steps(warmup + steps)
+    cfg.kstep_show = interval
     cfg.kstep_save = 10 ** 8
     wd = tempfile.mkdtemp(prefix="ocfd_ref_")
     try:
@@ -96,8 +99,10 @@ def time_steps(case, warmup: int, steps: int, timeout: float = 1800.0) -> Tuple[
         if p.returncode != 0:
             raise RuntimeError(f"reference exited {p.returncode}:\n{p.stdout[-3000:]}\n{p.stderr[-3000:]}")
         m = _INTERVAL.findall(p.stdout)
-        if not m:
-            raise RuntimeError("no interval timing in reference output:\n" + p.stdout[-3000:])
-        return float(m[-1][1]), p.stdout
+        need = steps // interval
+        if len(m) < need:
+            raise RuntimeError(f"{len(m)} interval prints in the reference output, {need} needed:\n"
+                               + p.stdout[-3000:])
+        return sum(float(t) for _, t in m[-need:]), interval, p.stdout
     finally:
         shutil.rmtree(wd, ignore_errors=True)

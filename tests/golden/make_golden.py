@@ -5,7 +5,10 @@ Runs the reference's own CUDA build (oracle/_ref/opencfd-scu.out, made by
 reference's own file interface (opencfd-scu.in, opencfd.dat,
 OCFD3d-Jacobi.dat -> OCFD%08d.dat), and stores inputs and outputs as .npz.
 
-    python tests/golden/make_golden.py --out gpurun_out/golden
+    python tests/golden/make_golden.py --out <directory>
+
+(default: a new temporary directory, printed at the end; copy the .npz files
+that should become fixtures into tests/golden/).
 
 Each case is run twice so that a non-deterministic reference result (the
 shared-memory race of the characteristic kernels) shows up as a difference
@@ -159,11 +162,14 @@ def bounded_cases():
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", default="", help="output directory (default: a new temporary directory)")
     ap.add_argument("--only", default="")
     args = ap.parse_args(argv)
     if not ref_runner.available():
         raise SystemExit(f"{ref_runner.REF_BIN} missing: build it with make -f oracle/ref.mk")
+    if not args.out:
+        import tempfile
+        args.out = tempfile.mkdtemp(prefix="ocfd_golden_")
     os.makedirs(args.out, exist_ok=True)
     summary = {}
     for name, case, nsteps in golden_cases():
@@ -188,6 +194,7 @@ def main(argv=None):
         print(name, summary[name], flush=True)
     with open(os.path.join(args.out, "summary.json"), "w") as fh:
         json.dump(summary, fh, indent=1)
+    print("fixtures written to", args.out, flush=True)
 
 
 if __name__ == "__main__":
