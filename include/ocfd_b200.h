@@ -116,10 +116,12 @@ int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl);
  * stencils run in FP32 on FP32 copies of the primitives, with the stage
  * RHS and the viscous fluxes stored in FP32; the conserved state, the RK3
  * update, cons->prim, the grid metrics and the reductions stay FP64.
- * Covers the characteristic hybrid scheme and WENO7 without a
- * boundary-condition family or filter (OCFD_ERR_UNSUPPORTED otherwise);
- * whole steps only (ocfd_b200_step).  Switching back recomputes the FP64
- * primitives from the conserved state. */
+ * With a boundary-condition family its values are formed in FP64 (and
+ * copied to the FP32 primitives); the shock filter forms its weights from an
+ * FP32 pressure and updates U in FP64.  Covers the characteristic hybrid
+ * scheme and WENO7 (OCFD_ERR_UNSUPPORTED otherwise); whole steps only
+ * (ocfd_b200_step).  Switching back recomputes the FP64 primitives from the
+ * conserved state. */
 int ocfd_b200_set_precision(ocfd_b200_ctx *ctx, int form);
 /* HybridAuto_scheme_Proportion (src/OCFD_Schemes_hybrid_auto.cu:745-829):
  * frac[3*d + t], the share of direction d's flag entries that are 1 (t=0),

@@ -799,17 +799,16 @@ extern "C" int ocfd_b200_set_precision(ocfd_b200_ctx *ctx, int form) {
     if (p.mixed) return OCFD_OK;
     if (!ocfd::sweeps4_supported(p))
         return fail(ctx, OCFD_ERR_UNSUPPORTED, "the precision form covers the characteristic hybrid scheme and WENO7");
-    if (p.ibc || ctx->nfilter)
-        return fail(ctx, OCFD_ERR_UNSUPPORTED, "the precision form has no boundary-condition family or filter");
     if (!ctx->prec_buf) {
-        const size_t n = 17 * (size_t)p.lapN + 5 * (size_t)p.N;
+        const size_t n = 18 * (size_t)p.lapN + 5 * (size_t)p.N;
         cudaError_t e = cudaMalloc((void **)&ctx->prec_buf, n * sizeof(float));
         if (e != cudaSuccess) { ctx->prec_buf = nullptr; return cuda_fail(ctx, e, "precision-form buffers"); }
         CK(cudaMemsetAsync(ctx->prec_buf, 0, n * sizeof(float), ctx->stream), "memset");
     }
     for (int m = 0; m < 5; m++) p.prim32[m] = ctx->prec_buf + (size_t)m * p.lapN;
     p.ev32 = ctx->prec_buf + 5 * (size_t)p.lapN;
-    p.du32 = ctx->prec_buf + 17 * (size_t)p.lapN;
+    p.pfil32 = ctx->prec_buf + 17 * (size_t)p.lapN;
+    p.du32 = ctx->prec_buf + 18 * (size_t)p.lapN;
     p.mixed = 1;
     if (ctx->have_state) {
         CK(ocfd::launch_prims_to_fp32(p, ctx->stream), "FP32 primitives");
@@ -1150,10 +1149,15 @@ static int run_filters(ocfd_b200_ctx *ctx) {
     {   // periodic exchange of p and pf_lap in the directions any filter uses
         double *f[6]; int mask[6];
         const int dm = (ctx->fjudge[0] ? 1 : 0) | (ctx->fjudge[1] ? 2 : 0) | (ctx->fjudge[2] ? 4 : 0);
-        f[0] = p.pfil; mask[0] = dm;
-        for (int m = 0; m < 5; m++) { f[1 + m] = p.flap + (size_t)m * p.lapN; mask[1 + m] = dm; }
-        int rc = fill_ghosts(ctx, f, mask, 6, "filter ghost fill");
+        int n = 0;
+        if (!p.mixed) { f[n] = p.pfil; mask[n++] = dm; }
+        for (int m = 0; m < 5; m++) { f[n] = p.flap + (size_t)m * p.lapN; mask[n++] = dm; }
+        int rc = fill_ghosts(ctx, f, mask, n, "filter ghost fill");
         if (rc) return rc;
+        if (p.mixed) {      // the precision form's FP32 pressure
+            float *f32[1] = { p.pfil32 };
+            if ((rc = fill_ghosts(ctx, f32, mask, 1, "filter ghost fill"))) return rc;
+        }
     }
     for (int m = 0; m < ctx->nfilter; m++) {
         if (!(ctx->tt <= ctx->frpar[m][2]) || ctx->istep % ctx->fpar[m][0] != 0) continue;
@@ -1264,8 +1268,6 @@ extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
     int rc = check_ready(ctx);
     if (rc) return rc;
     if (nsteps < 0) return fail(ctx, OCFD_ERR_ARG, "nsteps < 0");
-    if (ctx->p.mixed && (ctx->p.ibc || ctx->nfilter))
-        return fail(ctx, OCFD_ERR_UNSUPPORTED, "the precision form has no boundary-condition family or filter");
     if (ctx->p.mixed && nsteps > 0) ctx->prims64_stale = true;
     for (int n = 0; n < nsteps; n++) {
         ocfd_b200_swap_time_levels(ctx);

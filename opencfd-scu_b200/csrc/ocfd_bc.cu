@@ -9,6 +9,8 @@
 //          then T = TW with the pressure extrapolated to the wall (and the
 //          ghost rows mirrored: d, T even, u, v, w odd), or, for TW <= 0, T and
 //          p extrapolated.  The wall kernels act on their own (x, z) column.
+// In the precision form the values are formed in FP64 as above and also
+// stored in the FP32 primitives the stencils read.
 #include "ocfd_device.cuh"
 
 #include <cuda_runtime.h>
@@ -16,6 +18,13 @@
 namespace ocfd {
 
 namespace {
+
+// the five primitives of LAP-box point q into the FP32 copies (precision form)
+__device__ __forceinline__ void to_fp32(const Params &p, long long q) {
+    if (!p.mixed) return;
+#pragma unroll
+    for (int m = 0; m < 5; m++) p.prim32[m][q] = (float)p.prim[m][q];
+}
 
 __global__ void k_bc108_inlet(Params p) {
     const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -25,6 +34,7 @@ __global__ void k_bc108_inlet(Params p) {
     for (int i = 0; i <= OCFD_LAP; i++) {
         const long long q = lap_index(p, i, j + OCFD_LAP, k + OCFD_LAP);
         p.prim[0][q] = d; p.prim[1][q] = u; p.prim[2][q] = v; p.prim[3][q] = 0.; p.prim[4][q] = T;
+        to_fp32(p, q);
     }
 }
 
@@ -40,6 +50,7 @@ __global__ void k_bc108_top(Params p) {
     p.prim[2][q] = p.bc_ub1[2 * p.ny + j];
     p.prim[3][q] = 0.;
     p.prim[4][q] = p.bc_ub1[3 * p.ny + j];
+    to_fp32(p, q);
 }
 
 // do_wall_dist_kernel, then do_wall_Tp1_kernel / do_wall_Tp2_kernel
@@ -53,7 +64,10 @@ __global__ void k_bc108_wall(Params p, double ht) {
     u[q] = 0.;
     v[q] = p.bc_epsl * p.bc_fx[i] * p.bc_gz[k] * ht;
     w[q] = 0.;
-    if (p.bc_wall_mode == 0) return;                   // non-normal wall: not supported there either
+    if (p.bc_wall_mode == 0) {                         // non-normal wall: not supported there either
+        to_fp32(p, q);
+        return;
+    }
     if (p.bc_wall_mode == 1) {
         const double pw = (18. * d[q + sy] * T[q + sy] - 9. * d[q + 2 * sy] * T[q + 2 * sy]
                            + 2. * d[q + 3 * sy] * T[q + 3 * sy]) / 11.;
@@ -63,6 +77,7 @@ __global__ void k_bc108_wall(Params p, double ht) {
             const long long qg = lap_index(p, i + OCFD_LAP, g, k + OCFD_LAP);
             const long long qm = lap_index(p, i + OCFD_LAP, 2 * OCFD_LAP - g, k + OCFD_LAP);
             d[qg] = d[qm]; u[qg] = -u[qm]; v[qg] = -v[qm]; w[qg] = -w[qm]; T[qg] = T[qm];
+            to_fp32(p, qg);
         }
     } else {
         T[q] = (18. * T[q + sy] - 9. * T[q + 2 * sy] + 2. * T[q + 3 * sy]) / 11.;
@@ -70,6 +85,7 @@ __global__ void k_bc108_wall(Params p, double ht) {
                            + 2. * d[q + 3 * sy] * T[q + 3 * sy]) / 11.;
         d[q] = pw / T[q];
     }
+    to_fp32(p, q);
 }
 
 inline unsigned blocks(long long n) { return (unsigned)((n + 255) / 256); }

@@ -73,6 +73,9 @@ struct Params {
     // cons_to_pri leaves after the last stage (1 LAP-box field)
     double *flap;
     double *pfil;
+    // precision form: the filter's pressure in FP32 (1 LAP-box field; the
+    // filter's weights are formed from it, its U update stays FP64)
+    float *pfil32;
     // boundary-condition family (IBC; 0 none, 108 compression corner): the
     // inflow profile [4][ny] (d,u,v,T), wall blowing shapes fx [nx], gz [nz],
     // first x of the upper inflow row, wall treatment (0 none, 1 TW > 0,

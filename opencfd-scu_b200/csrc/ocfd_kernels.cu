@@ -519,19 +519,29 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
     }
     double d1, u1, v1, w1, T2;
     cons_to_prim(p, f, d1, u1, v1, w1, T2);
+    const bool face = (i == 0) || (i == p.nx - 1) || (j == 0) || (j == p.ny - 1) || (k == 0 && p.zface_lo) ||
+                      (k == p.nz - 1 && p.zface_hi);
     if (p.mixed) {      // the stencils of the precision form read FP32 primitives
         p.prim32[0][o] = (float)d1; p.prim32[1][o] = (float)u1; p.prim32[2][o] = (float)v1;
         p.prim32[3][o] = (float)w1; p.prim32[4][o] = (float)T2;
+        // the boundary-condition family works on FP64 primitives: its wall
+        // law reads the four rows next to the wall and the face re-projection
+        // reads the face cells
+        if (p.ibc && (face || j <= OCFD_LAP)) {
+            p.prim[0][o] = d1; p.prim[1][o] = u1; p.prim[2][o] = v1; p.prim[3][o] = w1; p.prim[4][o] = T2;
+        }
     } else {
         p.prim[0][o] = d1; p.prim[1][o] = u1; p.prim[2][o] = v1; p.prim[3][o] = w1; p.prim[4][o] = T2;
     }
     // cons_to_pri_kernel also leaves the pressure (src/commen_kernel.cu:107),
-    // which the filter after the step reads
-    if (krk == 3 && p.pfil) p.pfil[o] = T2 * d1 / (p.Gamma * p.Ama * p.Ama);
+    // which the filter after the step reads (FP32 in the precision form)
+    if (krk == 3 && p.pfil) {
+        const double pr = T2 * d1 / (p.Gamma * p.Ama * p.Ama);
+        if (p.mixed) p.pfil32[o] = (float)pr;
+        else         p.pfil[o] = pr;
+    }
     // with a boundary-condition family the faces are re-projected after it
     // sets the boundary values (k_bc_faces)
-    bool face = (i == 0) || (i == p.nx - 1) || (j == 0) || (j == p.ny - 1) || (k == 0 && p.zface_lo) ||
-                (k == p.nz - 1 && p.zface_hi);
     if (face && !p.ibc) {
         f[0] = d1;
         f[1] = u1 * d1;

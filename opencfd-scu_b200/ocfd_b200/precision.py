@@ -7,6 +7,10 @@ The FP64 form is the reference here: it agrees with the CPU oracle to the
 the oracle itself would take hours, so the FP64 GPU run stands in for it.
 
     python -m ocfd_b200.precision --n 256 --steps 50,100,200 --out prec.json
+    python -m ocfd_b200.precision --workload ramp --n 128 --steps 100,500
+
+(--workload ramp: the compression ramp 4n x n x n/2, IBC 108 and the shock
+filter every step.)
 """
 import argparse
 import json
@@ -78,8 +82,12 @@ def main(argv=None):
     ap.add_argument("--steps", default="50,100,200")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--out", default="")
+    ap.add_argument("--workload", choices=("iso", "ramp"), default="iso")
     a = ap.parse_args(argv)
-    case = cases.isotropic_turbulence(a.n, seed=a.seed, charteric=1)
+    if a.workload == "ramp":
+        case = cases.ramp_case(4 * a.n, a.n, a.n // 2, seed=a.seed)
+    else:
+        case = cases.isotropic_turbulence(a.n, seed=a.seed, charteric=1)
     res = compare_forms(case, [int(x) for x in a.steps.split(",")])
     txt = json.dumps(res, indent=1)
     if a.out:

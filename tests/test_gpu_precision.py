@@ -68,13 +68,38 @@ def test_precision_switch_round_trip(gpu_lib):
     assert ei.value.status == -2
 
 
-@pytest.mark.parametrize("maker", [
-    lambda: cases.random_smooth_case(12, 11, 10, seed=21, scheme_invis="UP7", shock=True),
-    lambda: cases.ramp_case(30, 18, 8, seed=66),
-], ids=["up7", "ramp_bc108_filter"])
-def test_precision_form_refuses_uncovered(maker, gpu_lib):
-    case = maker()
+def test_precision_form_refuses_uncovered(gpu_lib):
+    """Schemes outside the FP32 walks (here UP7 alone) are refused."""
+    case = cases.random_smooth_case(12, 11, 10, seed=21, scheme_invis="UP7", shock=True)
     s = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
     with pytest.raises(lib.OcfdError) as ei:
         s.set_precision(1)
     assert ei.value.status == -2
+
+
+@pytest.mark.parametrize("maker", [
+    lambda: cases.ramp_case(30, 18, 8, seed=66),
+    lambda: cases.ramp_case(30, 18, 8, seed=67, tw=-1.0, epsl=0.01, beta=0.5, mtmax=4),
+], ids=["ramp_bc108_tw_filter", "ramp_bc108_adiabatic_blowing_filter"])
+def test_fp32_form_tracks_fp64_on_the_ramp(maker, gpu_lib):
+    """The compression ramp (metrics from the mesh, closures in x and y,
+    IBC 108 inflow, top and wall, the shock filter every step) in the
+    precision form against the FP64 path after ten steps: the boundary
+    values are formed in FP64, the filter weights from the FP32 pressure."""
+    case = maker()
+    a = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+    b = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+    b.set_precision(1)
+    a.step(10)
+    b.step(10)
+    err = rel_l2(b.conserved(), a.conserved())
+    print("ramp FP32 vs FP64 rel L2 after 10 steps:", err)
+    assert np.all(np.isfinite(err)) and np.all(err > 0), err
+    assert np.all(err <= TOL_FP32_10STEPS), err
+    ep = rel_l2(b.primitives(), a.primitives())
+    assert np.all(ep <= TOL_FP32_10STEPS), ep
+    # the wall rows carry the boundary law exactly: no slip, T = Tw
+    pb = b.primitives()
+    assert np.all(pb[1][:, 0, :] == 0.0) and np.all(pb[3][:, 0, :] == 0.0)
+    if case.cfg.bc_rpara[0] > 0:
+        assert np.allclose(pb[4][:, 0, :], case.cfg.bc_rpara[0], rtol=1e-14)
