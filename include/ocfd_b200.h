@@ -102,7 +102,12 @@ int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx);
  * closure and line-end rule is formed in the walk (variant 6), except that a
  * hybrid direction whose sensor pass marked almost every face UP7 takes the
  * UP7 walk with its few other cells deferred (the choice is read back once
- * per step, after the sensor); 5 the walk with every face through one
+ * per step, after the sensor); in the precision form the y and z UP7 walks
+ * run as per-lane marches over pencil tiles staged in shared memory by the
+ * tensor copy engine, each lane keeping its face window in registers; 7 the
+ * same as 4 with every UP7 walk through the shared-memory ring; 8 the same
+ * as 4 with the y and z marches in FP64 as well (as fast as the ring there);
+ * 5 the walk with every face through one
  * in-loop dispatch; 6 the in-line walk alone (characteristic hybrid scheme
  * and WENO7 only); 2 one thread per (face, sign) in tiles
  * with the five characteristic fields in registers, register budget for 4
@@ -163,6 +168,21 @@ int ocfd_b200_mlp_train(float *params, const float *feat, const float *label, lo
 /* Bit d set: direction d currently takes the walk that forms every face in
  * line (variant 4 after the last sensor pass, or variant 6). */
 int ocfd_b200_sweep_walks(const ocfd_b200_ctx *ctx);
+/* Share of a direction's cells that the UP7 walk would defer (2 x its
+ * non-UP7 faces, plus closed line ends) above which variant 4 takes the
+ * in-line walk for that direction; default 0.002.  3 or more keeps the
+ * UP7 walk whatever the sensor marks (every other cell then goes to the fix-up
+ * kernel).  No reference counterpart (a tuning knob of this library). */
+int ocfd_b200_set_walk_threshold(ocfd_b200_ctx *ctx, double frac);
+/* Kernel of the viscous divergence + RK stage of whole steps: 2 stages the
+ * Ev tiles of each plane (x and y with their halos, z in a ring of planes)
+ * in shared memory by bulk tensor copies while the block marches along z;
+ * 1 reads every Ev value through the L1/L2 caches; 0 (default) the staged
+ * kernel in the precision form and the cached one in FP64, each the faster
+ * of the two there.  The same arithmetic (results equal bit for bit).  No reference counterpart
+ * (du_viscous_Jacobian3d_*_final, src/OCFD_NS_Jacobian3d.cu:80-440, is the
+ * computation both replace). */
+int ocfd_b200_set_viscous_impl(ocfd_b200_ctx *ctx, int impl);
 int ocfd_b200_set_metrics_device(ocfd_b200_ctx *ctx, const double *metrics13_dev);
 /* Mesh coordinates x,y,z, 3 interior fields (host or device memory), from
  * which the 13 metric fields are computed on the GPU.  Replaces the
@@ -312,6 +332,10 @@ int ocfd_b200_field_means_noalloc(const double *fields, int nfield, long long n,
 
 /* ---- reference-named entry points (act on the bound context) ---------- */
 int  ocfd_b200_compat_bind(ocfd_b200_ctx *ctx);
+/* A translation unit that also includes the reference's own headers, which
+ * declare these names with the reference's types, defines
+ * OCFD_B200_NO_REFERENCE_NAMES before including this header. */
+#ifndef OCFD_B200_NO_REFERENCE_NAMES
 void du_comput(int KRK);                    /* head/OCFD_Stream.h:10           */
 void OCFD_time_advance(int KRK);            /* src/OCFD_time.cu:96             */
 void get_duvwT(void);                       /* head/commen_kernel.h:17         */
@@ -319,6 +343,7 @@ void get_Amu(void);                         /* head/commen_kernel.h:20         *
 void OCFD_bc(void);                         /* src/OCFD_boundary.cu:18         */
 void Set_Scheme_HybridAuto(void *stream);   /* head/OCFD_Schemes_hybrid_auto.h:24 (cudaStream_t*) */
 void filtering(double *pf, double *pf_lap, double *pp);   /* src/OCFD_filtering.cu:75 */
+#endif
 
 #ifdef __cplusplus
 }

@@ -7,6 +7,7 @@
 #include "ocfd_b200.h"
 #include "ocfd_device.cuh"
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -18,6 +19,11 @@
 
 namespace ocfd {
 cudaError_t launch_sensor(const Params &p, cudaStream_t st);
+bool march_tensor_map(const Params &p, const void *base, int elem_bytes, int dir, CUtensorMap *out);
+bool march_supported(const Params &p, int dir);
+cudaError_t march_prepare();
+cudaError_t vdiv_prepare();
+cudaError_t launch_march_dir(const Params &p, const CUtensorMap &tm, int dir, cudaStream_t st);
 cudaError_t launch_ghost(const Params &p, double *const *fields, const int *dirmask, int nf, cudaStream_t st);
 cudaError_t launch_ghost32(const Params &p, float *const *fields, const int *dirmask, int nf, cudaStream_t st);
 cudaError_t launch_prims_to_fp32(const Params &p, cudaStream_t st);
@@ -120,8 +126,11 @@ struct ocfd_b200_ctx {
     // precision form: FP32 primitives (5 LAP fields), stage RHS (5 interior
     // fields) and viscous fluxes (12 LAP fields); the FP64 primitives are
     // brought up to date from the conserved state before they are read
+    // (with a filter the last stage has written their interior: only the
+    // ghosts are stale)
     float *prec_buf = nullptr;
     bool prims64_stale = false;
+    bool prims64_interior_ok = false;
     // learned scheme switch: parameter vector on the device, the confidence
     // threshold as a logit, decision counters
     float *sw_w = nullptr;
@@ -130,6 +139,17 @@ struct ocfd_b200_ctx {
     float sw_conf_logit = 0.0f;
     int walk4[3] = {1, 1, 1};
     double walk4_threshold = 0.002;     // deferred cells per cell above which the inline walk is used
+    // the UP7 walk of the y and z sweeps as per-lane marches over staged
+    // pencil tiles (ocfd_march.cu): tensor maps of the FP64 and FP32
+    // primitives per direction (y, z).  march: 0 the shared-memory ring walk
+    // everywhere (sweep variant 7), 1 the march in the precision form only
+    // (default: in FP64 the ring walk measured as fast), 2 the march in both
+    // forms (variant 8)
+    CUtensorMap tm64[2];
+    CUtensorMap tm32[2];
+    bool tm64_ok = false, tm32_ok = false;
+    bool vdiv_ok = true;        // the staged divergence kernel can be launched
+    int march = 1;
     // the grid split in z across GPUs: this rank's slab starts at global
     // plane z_offset of nz_global; ghost planes in z come from the
     // neighbouring slabs (null: one GPU holds the grid)
@@ -159,6 +179,7 @@ struct ocfd_b200_ctx {
         float sw_conf = 0.0f;
         long long launches = 0;
         int walk = -1;          // the walks chosen by the sensor pass before it (-1: none)
+        int march = 1;
     } graph[2];
     bool graphs_on = true;
     long long graph_captures = 0;       // step graphs captured so far
@@ -338,6 +359,19 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     p.flag_count = nullptr;
     if (ctx->defer_buf && cudaHostAlloc((void **)&ctx->h_flag_count, 64, cudaHostAllocDefault) == cudaSuccess)
         p.flag_count = ctx->defer_buf + 8;
+    // word 16 of the counter block: the kernels' error word
+    p.kerr = ctx->defer_buf ? reinterpret_cast<int *>(ctx->defer_buf + 16) : nullptr;
+    if (p.kerr && (e = cudaMemset(p.kerr, 0, sizeof(int))) != cudaSuccess) {
+        cuda_fail(nullptr, e, "error word");
+        free_all(ctx); delete ctx;
+        return OCFD_ERR_CUDA;
+    }
+    // the staged divergence kernel is used only when its shared-memory size is set
+    if (ocfd::vdiv_prepare() != cudaSuccess) { cudaGetLastError(); p.vis_impl = 1; ctx->vdiv_ok = false; }
+    ctx->tm64_ok = ocfd::march_prepare() == cudaSuccess &&
+                   ocfd::march_tensor_map(p, ctx->prim_buf, 8, 1, &ctx->tm64[0]) &&
+                   ocfd::march_tensor_map(p, ctx->prim_buf, 8, 2, &ctx->tm64[1]);
+    cudaGetLastError();
 
     if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = cudaEventCreate(&ctx->ev[0])) != cudaSuccess || (e = cudaEventCreate(&ctx->ev[1])) != cudaSuccess) {
@@ -377,9 +411,22 @@ extern "C" int ocfd_b200_set_stream(ocfd_b200_ctx *ctx, void *stream) {
 }
 extern "C" void *ocfd_b200_get_stream(const ocfd_b200_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
+// a kernel whose wait on a staged copy ran out leaves 1 in the error word
+static int check_kerr(ocfd_b200_ctx *ctx, int word) {
+    if (word == 0) return OCFD_OK;
+    int zero = 0;
+    cudaMemcpy(ctx->p.kerr, &zero, sizeof(int), cudaMemcpyHostToDevice);
+    return fail(ctx, OCFD_ERR_CUDA, "a sweep kernel gave up waiting for a staged tile (the step's result is invalid)");
+}
+
 extern "C" int ocfd_b200_synchronize(ocfd_b200_ctx *ctx) {
     if (!ctx) return OCFD_ERR_ARG;
     CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+    if (ctx->p.kerr) {
+        int w = 0;
+        CK(cudaMemcpy(&w, ctx->p.kerr, sizeof(int), cudaMemcpyDeviceToHost), "error word");
+        return check_kerr(ctx, w);
+    }
     return OCFD_OK;
 }
 
@@ -477,8 +524,10 @@ static int ghost_prims(ocfd_b200_ctx *ctx, bool defer_z = false) {
 // conserved state, before anything reads them
 static int refresh_prims64(ocfd_b200_ctx *ctx) {
     if (!ctx->prims64_stale) return OCFD_OK;
-    CK(ocfd::launch_c2p(ctx->p, ctx->stream), "cons_to_pri");
-    ctx->launches += 1;
+    if (!ctx->prims64_interior_ok) {
+        CK(ocfd::launch_c2p(ctx->p, ctx->stream), "cons_to_pri");
+        ctx->launches += 1;
+    }
     int rc = ghost_prims64(ctx);
     if (rc) return rc;
     ctx->prims64_stale = false;
@@ -562,6 +611,11 @@ static int sweeps_auto(ocfd_b200_ctx *ctx) {
         if (w[d]) {
             CK(ocfd::launch_sweep4_dir(p, d, ctx->stream), "inviscid sweeps");
             ctx->launches += 1;
+        } else if (d > 0 && ctx->march > (p.mixed ? 0 : 1) && ocfd::march_supported(p, d) &&
+                   (p.mixed ? ctx->tm32_ok : ctx->tm64_ok)) {
+            CK(ocfd::launch_march_dir(p, p.mixed ? ctx->tm32[d - 1] : ctx->tm64[d - 1], d, ctx->stream),
+               "inviscid sweeps");
+            ctx->launches += 2;
         } else {
             CK(ocfd::launch_sweep3_dir(p, d, ctx->stream), "inviscid sweeps");
             ctx->launches += ocfd::sweeps3_defers(p) ? 2 : 1;
@@ -592,9 +646,11 @@ static int rhs_sensor(ocfd_b200_ctx *ctx) {
                 if (ocfd::slab_allreduce(ctx->slab, p.flag_count, 3, 2, ctx->stream, err))
                     return fail(ctx, OCFD_ERR_CUDA, err);
             }
-            CK(cudaMemcpyAsync(ctx->h_flag_count, p.flag_count, 3 * sizeof(unsigned), cudaMemcpyDeviceToHost,
+            // the three counts and, 8 words on, the kernels' error word
+            CK(cudaMemcpyAsync(ctx->h_flag_count, p.flag_count, 9 * sizeof(unsigned), cudaMemcpyDeviceToHost,
                                ctx->stream), "flag counts");
             CK(cudaStreamSynchronize(ctx->stream), "flag counts");
+            if (int rc = check_kerr(ctx, (int)ctx->h_flag_count[8])) return rc;
             for (int d = 0; d < 3; d++) ctx->walk4[d] = walk4_wanted(ctx, d, ctx->h_flag_count[d]);
         }
     }
@@ -809,6 +865,8 @@ extern "C" int ocfd_b200_set_precision(ocfd_b200_ctx *ctx, int form) {
     p.ev32 = ctx->prec_buf + 5 * (size_t)p.lapN;
     p.pfil32 = ctx->prec_buf + 17 * (size_t)p.lapN;
     p.du32 = ctx->prec_buf + 18 * (size_t)p.lapN;
+    ctx->tm32_ok = ocfd::march_tensor_map(p, ctx->prec_buf, 4, 1, &ctx->tm32[0]) &&
+                   ocfd::march_tensor_map(p, ctx->prec_buf, 4, 2, &ctx->tm32[1]);
     p.mixed = 1;
     if (ctx->have_state) {
         CK(ocfd::launch_prims_to_fp32(p, ctx->stream), "FP32 primitives");
@@ -997,9 +1055,22 @@ extern "C" int ocfd_b200_sweep_walks(const ocfd_b200_ctx *ctx) {
     return ctx->walk4[0] | (ctx->walk4[1] << 1) | (ctx->walk4[2] << 2);
 }
 
+extern "C" int ocfd_b200_set_viscous_impl(ocfd_b200_ctx *ctx, int impl) {
+    if (!ctx || impl < 0 || impl > 2) return OCFD_ERR_ARG;
+    ctx->p.vis_impl = ctx->vdiv_ok ? impl : 1;
+    return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_set_walk_threshold(ocfd_b200_ctx *ctx, double frac) {
+    if (!ctx || !(frac >= 0.0)) return OCFD_ERR_ARG;
+    ctx->walk4_threshold = frac;
+    return OCFD_OK;
+}
+
 extern "C" int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl) {
-    if (!ctx || impl < 1 || impl > 6) return OCFD_ERR_ARG;
-    ctx->p.sweep_impl = impl;
+    if (!ctx || impl < 1 || impl > 8) return OCFD_ERR_ARG;
+    ctx->march = impl == 7 ? 0 : (impl == 8 ? 2 : 1);
+    ctx->p.sweep_impl = impl >= 7 ? 4 : impl;
     return OCFD_OK;
 }
 
@@ -1218,7 +1289,7 @@ static int step_graph(ocfd_b200_ctx *ctx) {
     const int walk = skip ? ctx->walk4[0] | ctx->walk4[1] << 1 | ctx->walk4[2] << 2 : -1;
     auto &G = ctx->graph[ctx->p.f == ctx->cons_buf ? 0 : 1];
     const bool fresh = G.exec && G.stream == ctx->stream && G.sw_on == ctx->sw_on && G.walk == walk &&
-                       G.sw_conf == ctx->sw_conf_logit && memcmp(&G.key, &ctx->p, sizeof(Params)) == 0;
+                       G.march == ctx->march && G.sw_conf == ctx->sw_conf_logit && memcmp(&G.key, &ctx->p, sizeof(Params)) == 0;
     if (fresh) {
         CK(cudaGraphLaunch(G.exec, ctx->stream), "step graph");
         ctx->launches += G.launches;
@@ -1249,6 +1320,7 @@ static int step_graph(ocfd_b200_ctx *ctx) {
     if (e != cudaSuccess) { G.exec = nullptr; return cuda_fail(ctx, e, "step graph instantiate"); }
     memcpy(&G.key, &ctx->p, sizeof(Params));
     G.stream = ctx->stream;
+    G.march = ctx->march;
     G.sw_on = ctx->sw_on;
     G.sw_conf = ctx->sw_conf_logit;
     G.walk = walk;
@@ -1268,7 +1340,10 @@ extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
     int rc = check_ready(ctx);
     if (rc) return rc;
     if (nsteps < 0) return fail(ctx, OCFD_ERR_ARG, "nsteps < 0");
-    if (ctx->p.mixed && nsteps > 0) ctx->prims64_stale = true;
+    if (ctx->p.mixed && nsteps > 0) {
+        ctx->prims64_stale = true;
+        ctx->prims64_interior_ok = ctx->p.flap != nullptr;
+    }
     for (int n = 0; n < nsteps; n++) {
         ocfd_b200_swap_time_levels(ctx);
         if ((rc = step_graph_ok(ctx) ? step_graph(ctx) : step_launched(ctx, false))) return rc;

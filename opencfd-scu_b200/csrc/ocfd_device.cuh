@@ -63,11 +63,18 @@ struct Params {
     DirConst dc[3];
     double inv_h[3], inv_Ama;   // reciprocals for div_const
     int sweep_impl;         // 1: per-(face,sign,field) threads; 2, 3: per-(face,sign) threads; 4, 5: warp rings
+    // viscous divergence + RK of whole steps: 0 Ev tiles staged in shared
+    // memory in the precision form, read through L1/L2 in FP64 (each the
+    // faster there); 1 read through L1/L2; 2 staged
+    int vis_impl;
     // cells whose du the call-free sweep leaves to the fix-up kernel, per
     // direction (interior cell indices; capacity N each), and their counts
     unsigned *defer[3];
     unsigned *defer_count;
     unsigned *flag_count;          // faces per direction whose hybrid flag is not 1 (sensor), or null
+    // set to 1 by a kernel whose wait on a staged copy ran out (the host
+    // reports it as an error at the next synchronisation)
+    int *kerr;
     // shock filter (null when no filter is set): U after the stage-3 update
     // before the face re-projection (5 LAP-box fields) and the pressure
     // cons_to_pri leaves after the last stage (1 LAP-box field)

@@ -16,6 +16,7 @@
 // 5-term dot product per thread; phase C forms du of each tile cell from
 // the two neighbouring face fluxes (no atomics).
 #include "ocfd_fp32.cuh"
+#include "ocfd_tma.cuh"
 
 #include <cuda_runtime.h>
 
@@ -495,21 +496,22 @@ __global__ void __launch_bounds__(256, sizeof(R) == 8 ? 5 : 6) k_vis_ev(Params p
 // RK stage (src/OCFD_time.cu:44-94) + cons_to_pri (src/commen_kernel.cu:77-109)
 // + pri_to_cons re-projection on the six faces (src/OCFD_boundary.cu:40-91)
 // for one cell, given its final du
-__device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid, int i, int j, int k,
-                                        const double du[5]) {
+// (fn0, fk0: U^n and U^k of the cell, read by the caller)
+__device__ __forceinline__ void rk_cell_pre(const Params &p, int krk, long long tid, int i, int j, int k,
+                                            const double du[5], const double fn0[5], const double fk0[5]) {
     const long long N = p.N;
     double f[5];
 #pragma unroll
     for (int m = 0; m < 5; m++) {
-        double fn = p.fn[m * N + tid];
+        double fn = fn0[m];
         if (krk == 1) {
             f[m] = fn + p.dt * du[m];
         } else if (krk == 2) {
             double t1 = 3.0 / 4.0, t2 = 1.0 / 4.0;
-            f[m] = t1 * fn + t2 * (p.f[m * N + tid] + p.dt * du[m]);
+            f[m] = t1 * fn + t2 * (fk0[m] + p.dt * du[m]);
         } else {
             double t1 = 1.0 / 3.0, t2 = 2.0 / 3.0;
-            f[m] = t1 * fn + t2 * (p.f[m * N + tid] + p.dt * du[m]);
+            f[m] = t1 * fn + t2 * (fk0[m] + p.dt * du[m]);
         }
     }
     long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
@@ -526,8 +528,10 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
         p.prim32[3][o] = (float)w1; p.prim32[4][o] = (float)T2;
         // the boundary-condition family works on FP64 primitives: its wall
         // law reads the four rows next to the wall and the face re-projection
-        // reads the face cells
-        if (p.ibc && (face || j <= OCFD_LAP)) {
+        // reads the face cells.  With a filter the step's FP64 primitives are
+        // the last stage's, before the filter changes U (cons_to_pri is not
+        // run after filtering), so the last stage writes them all.
+        if ((p.ibc && (face || j <= OCFD_LAP)) || (krk == 3 && p.flap)) {
             p.prim[0][o] = d1; p.prim[1][o] = u1; p.prim[2][o] = v1; p.prim[3][o] = w1; p.prim[4][o] = T2;
         }
     } else {
@@ -551,6 +555,16 @@ __device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid,
     }
 #pragma unroll
     for (int m = 0; m < 5; m++) p.f[m * N + tid] = f[m];
+}
+__device__ __forceinline__ void rk_cell(const Params &p, int krk, long long tid, int i, int j, int k,
+                                        const double du[5]) {
+    double fn0[5], fk0[5];
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+        fn0[m] = p.fn[m * p.N + tid];
+        fk0[m] = krk == 1 ? 0.0 : p.f[m * p.N + tid];
+    }
+    rk_cell_pre(p, krk, tid, i, j, k, du, fn0, fk0);
 }
 
 // du[1..4] += Ajac * d(Ev)/d(xi) for x, then y, then z
@@ -594,6 +608,364 @@ __global__ void __launch_bounds__(256, 6) k_vis_div(Params p, int krk, int k0) {
     } else {
 #pragma unroll
         for (int m = 0; m < 4; m++) du[(m + 1) * p.N + tid] = acc[m + 1];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The same divergence + RK stage with the Ev tiles staged in shared memory by
+// bulk tensor copies (k_vis_div reads every Ev value through L1/L2).  A block
+// owns a VX x VY tile of the x-y plane and marches along z over a segment of
+// planes: per plane it takes Ev_x with an x halo, Ev_y with a y halo (one
+// barrier for both, double-buffered) and Ev_z of plane k+H into a ring of
+// 2H+2 planes, so that every Ev value crosses L2 once per block and every
+// stencil read is a shared-memory read.  The Ev fields and their ghosts are
+// those k_vis_ev and the ghost fill leave; the arithmetic per cell is
+// k_vis_div's, in its order.  Blocks are persistent over (tile, segment)
+// items.  H: half-width of the derivative stencil (3: CD6, 4: CD8).
+// ---------------------------------------------------------------------------
+constexpr int VX = 32, VY = 8, VXH = 4;      // tile; x halo of the Ev_x box (keeps its x start even)
+
+template <typename R, int H>
+struct VdivTiles {
+    static constexpr int NZS = 2 * H + 2;                  // Ev_z ring slots
+    static constexpr int ZE = 4 * VY * VX;                 // [field][y][x]
+    static constexpr int XE = 4 * VY * (VX + 2 * VXH);
+    static constexpr int YE = 4 * (VY + 2 * H) * VX;
+    static constexpr size_t bytes = (size_t)(NZS * ZE + 2 * XE + 2 * YE) * sizeof(R);
+};
+
+// d0 / d0b of k_vis_div from a window v[0..2H] (v[H] the cell), same expressions
+template <typename R, int H>
+__device__ __forceinline__ R d0w(const R *v, R h, R ih, bool c8) {
+    R t;
+    if (c8) t = cd8(v[H - 4], v[H - 3], v[H - 2], v[H - 1], v[H + 1], v[H + 2], v[H + 3], v[H + 4]);
+    else    t = cd6(v[H - 3], v[H - 2], v[H - 1], v[H + 1], v[H + 2], v[H + 3]);
+    return div_const(t, h, ih);
+}
+template <typename R, int H>
+__device__ __forceinline__ R d0bw(const R *v, R h, R ih, bool c8, int X, int n, bool lo, bool hi) {
+    if (lo && X <= 3) {
+        R t;
+        if (X == 0)      t = (v[H + 1] - v[H]);
+        else if (X == 1) t = (v[H + 1] - v[H - 1]) * (R)0.5;
+        else if (X == 2) t = (v[H - 2] - (R)8.0 * v[H - 1] + (R)8.0 * v[H + 1] - v[H + 2]) / (R)12.0;
+        else             t = (v[H + 3] - v[H - 3] - (R)9.0 * (v[H + 2] - v[H - 2])
+                             + (R)45.0 * (v[H + 1] - v[H - 1])) / (R)60.0;
+        return div_const(t, h, ih);
+    }
+    if (hi && X >= n - 4) {
+        R t;
+        const int q = X - n;
+        if (q == -1)      t = (v[H] - v[H - 1]);
+        else if (q == -2) t = (v[H + 1] - v[H - 1]) * (R)0.5;
+        else if (q == -3) t = (v[H - 2] - (R)8.0 * v[H - 1] + (R)8.0 * v[H + 1] - v[H + 2]) / (R)12.0;
+        else              t = (v[H + 3] - v[H - 3] - (R)9.0 * (v[H + 2] - v[H - 2])
+                              + (R)45.0 * (v[H + 1] - v[H - 1])) / (R)60.0;
+        return div_const(t, h, ih);
+    }
+    return d0w<R, H>(v, h, ih, c8);
+}
+
+template <bool UNI, typename R, int H>
+__global__ void __launch_bounds__(VX * VY, 2)
+k_vdiv(const __grid_constant__ Params p, const __grid_constant__ CUtensorMap tmx,
+       const __grid_constant__ CUtensorMap tmy, const __grid_constant__ CUtensorMap tmz, int krk, int seg_len) {
+    using T = VdivTiles<R, H>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ unsigned long long zbar[T::NZS], xybar[2];
+    R *zring = reinterpret_cast<R *>(smem_raw);
+    R *xbuf = zring + T::NZS * T::ZE;                  // [2][XE]
+    R *ybuf = xbuf + 2 * T::XE;                        // [2][YE]
+    const int tid = threadIdx.x;
+    const int ti = tid % VX, tj = tid / VX;
+    const int ntx = (p.nx + VX - 1) / VX, nty = (p.ny + VY - 1) / VY;
+    const int nseg = (p.nz + seg_len - 1) / seg_len;
+    const long long nitems = (long long)ntx * nty * nseg;
+    const bool c8 = p.scheme_vis == 204;
+    const long long N = p.N;
+    const R hh[3] = { (R)p.hx, (R)p.hy, (R)p.hz };
+    const R ihh[3] = { (R)p.inv_h[0], (R)p.inv_h[1], (R)p.inv_h[2] };
+    if (tid == 0) {
+        for (int s = 0; s < T::NZS; s++) tma::mbar_init(&zbar[s], 1);
+        tma::mbar_init(&xybar[0], 1);
+        tma::mbar_init(&xybar[1], 1);
+        tma::fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned zph = 0, xyph = 0;             // parity of each barrier's next phase
+    unsigned zpend = 0, xypend = 0;         // barriers with a copy issued and not yet waited for
+    bool failed = false;
+    auto slot = [](int q) { return (q + T::NZS) % T::NZS; };      // q >= -H
+    for (long long item = blockIdx.x; item < nitems && !failed; item += gridDim.x) {
+        const int tile = (int)(item % ((long long)ntx * nty)), sg = (int)(item / ((long long)ntx * nty));
+        const int x0 = (tile % ntx) * VX, y0 = (tile / ntx) * VY;
+        const int k0 = sg * seg_len, k1 = min(p.nz, k0 + seg_len);
+        const int i = x0 + ti, j = y0 + tj;
+        const bool valid = i < p.nx && j < p.ny;
+        // thread 0 issues: Ev_z of plane q into its ring slot; Ev_x and Ev_y of plane k into buffer b
+        auto issue_z = [&](int q) {
+            const int s = slot(q);
+            tma::mbar_expect_tx(&zbar[s], (unsigned)(T::ZE * sizeof(R)));
+            tma::load_4d(zring + s * T::ZE, &tmz, OCFD_LAP + x0, OCFD_LAP + y0, OCFD_LAP + q, 0, &zbar[s]);
+        };
+        auto issue_xy = [&](int k, int b) {
+            tma::mbar_expect_tx(&xybar[b], (unsigned)((T::XE + T::YE) * sizeof(R)));
+            tma::load_4d(xbuf + b * T::XE, &tmx, OCFD_LAP + x0 - VXH, OCFD_LAP + y0, OCFD_LAP + k, 0, &xybar[b]);
+            tma::load_4d(ybuf + b * T::YE, &tmy, OCFD_LAP + x0, OCFD_LAP + y0 - H, OCFD_LAP + k, 0, &xybar[b]);
+        };
+        if (tid == 0) {
+            for (int q = k0 - H; q <= k0 + H + 1 && q <= k1 - 1 + H; q++) { issue_z(q); zpend |= 1u << slot(q); }
+            issue_xy(k0, 0); xypend |= 1u;
+            if (k0 + 1 < k1) { issue_xy(k0 + 1, 1); xypend |= 2u; }
+        }
+        // the bookkeeping of thread 0 is replayed by every thread
+        if (tid != 0) {
+            for (int q = k0 - H; q <= k0 + H + 1 && q <= k1 - 1 + H; q++) zpend |= 1u << slot(q);
+            xypend |= 1u;
+            if (k0 + 1 < k1) xypend |= 2u;
+        }
+        for (int k = k0; k < k1; k++) {
+            const int b = (k - k0) & 1;
+            const long long ci = valid ? in_index(p, i, j, k) : 0;
+            // this cell's state, read before the waits; the next plane's
+            // cell into L1 meanwhile
+            R acc[5];
+            double fn0[5], fk0[5];
+            if (valid) {
+                const R *du = du_r<R>(p);
+#pragma unroll
+                for (int m = 0; m < 5; m++) {
+                    acc[m] = du[m * N + ci];
+                    fn0[m] = p.fn[m * N + ci];
+                    fk0[m] = krk == 1 ? 0.0 : p.f[m * N + ci];
+                }
+                if (k + 1 < k1) {
+                    const long long cn = ci + (long long)p.nx * p.ny;
+#pragma unroll
+                    for (int m = 0; m < 5; m++) {
+                        tma::prefetch_l1(du + m * N + cn);
+                        tma::prefetch_l1(p.fn + m * N + cn);
+                        if (krk != 1) tma::prefetch_l1(p.f + m * N + cn);
+                    }
+                }
+            }
+            // planes k-H .. k+H of Ev_z, and Ev_x / Ev_y of plane k
+            for (int q = k - H; q <= k + H; q++) {
+                const int s = slot(q);
+                if (zpend & (1u << s)) {
+                    if (!tma::mbar_wait(&zbar[s], (zph >> s) & 1u)) failed = true;
+                    zph ^= 1u << s;
+                    zpend &= ~(1u << s);
+                }
+            }
+            if (xypend & (1u << b)) {
+                if (!tma::mbar_wait(&xybar[b], (xyph >> b) & 1u)) failed = true;
+                xyph ^= 1u << b;
+                xypend &= ~(1u << b);
+            }
+            if (valid && !failed) {
+                const long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+                const R ajac = (R)metric<UNI>(p, M_AJAC, o);
+                const R *xb = xbuf + b * T::XE, *yb = ybuf + b * T::YE;
+                // the 12 derivatives first (shared memory only), then their
+                // sums into du in k_vis_div's order, so that the first sum
+                // does not wait on du's load
+                R dv[3][4];
+#pragma unroll
+                for (int dd = 0; dd < 3; dd++) {
+#pragma unroll
+                    for (int m = 0; m < 4; m++) {
+                        R v[2 * H + 1];
+#pragma unroll
+                        for (int t = 0; t <= 2 * H; t++) {
+                            if (dd == 0)      v[t] = xb[(m * VY + tj) * (VX + 2 * VXH) + ti + VXH - H + t];
+                            else if (dd == 1) v[t] = yb[(m * (VY + 2 * H) + tj + t) * VX + ti];
+                            else              v[t] = zring[slot(k - H + t) * T::ZE + (m * VY + tj) * VX + ti];
+                        }
+                        if (!p.has_bnd) {
+                            dv[dd][m] = d0w<R, H>(v, hh[dd], ihh[dd], c8);
+                        } else {
+                            const int X = dd == 0 ? i : (dd == 1 ? j : k), n = dd == 0 ? p.nx : (dd == 1 ? p.ny : p.nz);
+                            dv[dd][m] = d0bw<R, H>(v, hh[dd], ihh[dd], c8, X, n, p.bnd_lo[dd], p.bnd_hi[dd]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int dd = 0; dd < 3; dd++)
+#pragma unroll
+                    for (int m = 0; m < 4; m++) acc[m + 1] += ajac * dv[dd][m];
+                double a64[5];
+#pragma unroll
+                for (int m = 0; m < 5; m++) a64[m] = (double)acc[m];
+                rk_cell_pre(p, krk, ci, i, j, k, a64, fn0, fk0);
+            }
+            // plane k-H's slot and buffer b are free; a wait that ran out
+            // anywhere in the block ends the block's work
+            if (__syncthreads_or(failed)) { failed = true; break; }
+            if (k + H + 2 <= k1 - 1 + H) {
+                if (tid == 0) issue_z(k + H + 2);
+                zpend |= 1u << slot(k + H + 2);
+            }
+            if (k + 2 < k1) {
+                if (tid == 0) issue_xy(k + 2, b);
+                xypend |= 1u << b;
+            }
+        }
+    }
+    if (failed) {
+        if (tid == 0) atomicExch(p.kerr, 1);
+        // copies still in flight land before the block's shared memory goes away
+        for (int s = 0; s < T::NZS; s++)
+            if (zpend & (1u << s)) tma::mbar_wait(&zbar[s], (zph >> s) & 1u);
+        for (int b = 0; b < 2; b++)
+            if (xypend & (1u << b)) tma::mbar_wait(&xybar[b], (xyph >> b) & 1u);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_vis_ev with the primitives staged in shared memory: a block owns a
+// VX x VY tile and marches along z; each plane of u, v, w, T arrives with
+// its x and y halos (one bulk tensor copy per plane) into a ring of 2H+2
+// planes, so the 12 derivative stencils read shared memory only and every
+// primitive crosses L2 once per block.  Same arithmetic as k_vis_ev.
+// ---------------------------------------------------------------------------
+template <typename R, int H>
+struct VevTiles {
+    static constexpr int NZS = 2 * H + 2;
+    static constexpr int PX = VX + 2 * VXH, PY = VY + 2 * H;     // plane box (x halo even)
+    static constexpr int PE = 4 * PY * PX;                         // [field][y][x]
+    static constexpr size_t bytes = (size_t)NZS * PE * sizeof(R);
+};
+
+template <bool UNI, typename R, int H>
+__global__ void __launch_bounds__(VX * VY, sizeof(R) == 8 ? 1 : 3)
+k_vev(const __grid_constant__ Params p, const __grid_constant__ CUtensorMap tmq, int seg_len) {
+    using T = VevTiles<R, H>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ unsigned long long zbar[T::NZS];
+    R *ring = reinterpret_cast<R *>(smem_raw);
+    const int tid = threadIdx.x;
+    const int ti = tid % VX, tj = tid / VX;
+    const int ntx = (p.nx + VX - 1) / VX, nty = (p.ny + VY - 1) / VY;
+    const int nseg = (p.nz + seg_len - 1) / seg_len;
+    const long long nitems = (long long)ntx * nty * nseg;
+    const bool c8 = p.scheme_vis == 204;
+    if (tid == 0) {
+        for (int s = 0; s < T::NZS; s++) tma::mbar_init(&zbar[s], 1);
+        tma::fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned zph = 0, zpend = 0;
+    bool failed = false;
+    auto slot = [](int q) { return (q + T::NZS) % T::NZS; };      // q >= -H
+    // value of field f (0 u, 1 v, 2 w, 3 T) at tile offset (dx, dy) of plane q
+    auto at = [&](int q, int f, int dy, int dx) -> R {
+        return ring[slot(q) * T::PE + (f * T::PY + tj + H + dy) * T::PX + ti + VXH + dx];
+    };
+    for (long long item = blockIdx.x; item < nitems && !failed; item += gridDim.x) {
+        const int tile = (int)(item % ((long long)ntx * nty)), sg = (int)(item / ((long long)ntx * nty));
+        const int x0 = (tile % ntx) * VX, y0 = (tile / ntx) * VY;
+        const int k0 = sg * seg_len, k1 = min(p.nz, k0 + seg_len);
+        const int i = x0 + ti, j = y0 + tj;
+        const bool valid = i < p.nx && j < p.ny;
+        auto issue = [&](int q) {
+            const int s = slot(q);
+            tma::mbar_expect_tx(&zbar[s], (unsigned)(T::PE * sizeof(R)));
+            tma::load_4d(ring + s * T::PE, &tmq, OCFD_LAP + x0 - VXH, OCFD_LAP + y0 - H, OCFD_LAP + q, 0, &zbar[s]);
+        };
+        for (int q = k0 - H; q <= k0 + H + 1 && q <= k1 - 1 + H; q++) {
+            if (tid == 0) issue(q);
+            zpend |= 1u << slot(q);
+        }
+        for (int k = k0; k < k1; k++) {
+            for (int q = k - H; q <= k + H; q++) {
+                const int s = slot(q);
+                if (zpend & (1u << s)) {
+                    if (!tma::mbar_wait(&zbar[s], (zph >> s) & 1u)) failed = true;
+                    zph ^= 1u << s;
+                    zpend &= ~(1u << s);
+                }
+            }
+            if (valid && !failed) {
+                const long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+                R Akx = (R)metric<UNI>(p, M_AKX, o), Aix = (R)metric<UNI>(p, M_AIX, o), Asx = (R)metric<UNI>(p, M_ASX, o);
+                R Aky = (R)metric<UNI>(p, M_AKY, o), Aiy = (R)metric<UNI>(p, M_AIY, o), Asy = (R)metric<UNI>(p, M_ASY, o);
+                R Akz = (R)metric<UNI>(p, M_AKZ, o), Aiz = (R)metric<UNI>(p, M_AIZ, o), Asz = (R)metric<UNI>(p, M_ASZ, o);
+                R Tc = at(k, 3, 0, 0);
+                R Amu = (R)p.amu_C0 * sqrt_r(Tc * Tc * Tc) / ((R)p.Tsb + Tc);      // get_Amu_kernal
+                const R ihx = (R)p.inv_h[0], ihy = (R)p.inv_h[1], ihz = (R)p.inv_h[2];
+                const R hx = (R)p.hx, hy = (R)p.hy, hz = (R)p.hz;
+                R dk[4], di[4], ds[4];         // d/dxi, d/deta, d/dzeta of u, v, w, T
+#pragma unroll
+                for (int f = 0; f < 4; f++) {
+                    R vx[2 * H + 1], vy[2 * H + 1], vz[2 * H + 1];
+#pragma unroll
+                    for (int t = 0; t <= 2 * H; t++) {
+                        vx[t] = at(k, f, 0, t - H);
+                        vy[t] = at(k, f, t - H, 0);
+                        vz[t] = at(k - H + t, f, 0, 0);
+                    }
+                    if (!p.has_bnd) {
+                        dk[f] = d0w<R, H>(vx, hx, ihx, c8);
+                        di[f] = d0w<R, H>(vy, hy, ihy, c8);
+                        ds[f] = d0w<R, H>(vz, hz, ihz, c8);
+                    } else {
+                        dk[f] = d0bw<R, H>(vx, hx, ihx, c8, i, p.nx, p.bnd_lo[0], p.bnd_hi[0]);
+                        di[f] = d0bw<R, H>(vy, hy, ihy, c8, j, p.ny, p.bnd_lo[1], p.bnd_hi[1]);
+                        ds[f] = d0bw<R, H>(vz, hz, ihz, c8, k, p.nz, p.bnd_lo[2], p.bnd_hi[2]);
+                    }
+                }
+                const R uk = dk[0], ui = di[0], us = ds[0], vk = dk[1], vi = di[1], vs = ds[1];
+                const R wk = dk[2], wi = di[2], ws = ds[2], Tk = dk[3], Ti = di[3], Ts = ds[3];
+                R ux = uk*Akx + ui*Aix + us*Asx;
+                R vx = vk*Akx + vi*Aix + vs*Asx;
+                R wx = wk*Akx + wi*Aix + ws*Asx;
+                R uy = uk*Aky + ui*Aiy + us*Asy;
+                R vy = vk*Aky + vi*Aiy + vs*Asy;
+                R wy = wk*Aky + wi*Aiy + ws*Asy;
+                R uz = uk*Akz + ui*Aiz + us*Asz;
+                R vz = vk*Akz + vi*Aiz + vs*Asz;
+                R wz = wk*Akz + wi*Aiz + ws*Asz;
+                R div = ux + vy + wz;
+                R s11 = ((R)2.0*ux - (R)(2.0/3.0)*div) * Amu;
+                R s22 = ((R)2.0*vy - (R)(2.0/3.0)*div) * Amu;
+                R s33 = ((R)2.0*wz - (R)(2.0/3.0)*div) * Amu;
+                R s12 = (uy + vx) * Amu;
+                R s13 = (uz + wx) * Amu;
+                R s23 = (vz + wy) * Amu;
+                R uu = at(k, 0, 0, 0), vv = at(k, 1, 0, 0), ww = at(k, 2, 0, 0);
+                R Amuk = Amu * (R)p.vis_c;
+                R Tx = Tk*Akx + Ti*Aix + Ts*Asx;
+                R Ty = Tk*Aky + Ti*Aiy + Ts*Asy;
+                R Tz = Tk*Akz + Ti*Aiz + Ts*Asz;
+                R E1 = uu*s11 + vv*s12 + ww*s13 + Amuk*Tx;
+                R E2 = uu*s12 + vv*s22 + ww*s23 + Amuk*Ty;
+                R E3 = uu*s13 + vv*s23 + ww*s33 + Amuk*Tz;
+                R Aj1 = (R)metric<UNI>(p, M_AJAC, o);
+                R *const evb = ev_r<R>(p);
+#pragma unroll
+                for (int dd = 0; dd < 3; dd++) {
+                    R akx = (R)metric<UNI>(p, M_AKX + 3 * dd, o) * Aj1;
+                    R aky = (R)metric<UNI>(p, M_AKX + 3 * dd + 1, o) * Aj1;
+                    R akz = (R)metric<UNI>(p, M_AKX + 3 * dd + 2, o) * Aj1;
+                    R *ev = evb + (long long)(4 * dd) * p.lapN;
+                    ev[o]              = (akx*s11 + aky*s12 + akz*s13);
+                    ev[p.lapN + o]     = (akx*s12 + aky*s22 + akz*s23);
+                    ev[2 * p.lapN + o] = (akx*s13 + aky*s23 + akz*s33);
+                    ev[3 * p.lapN + o] = (akx*E1  + aky*E2  + akz*E3);
+                }
+            }
+            if (__syncthreads_or(failed)) { failed = true; break; }
+            if (k + H + 2 <= k1 - 1 + H) {          // into the slot of plane k-H, read for the last time
+                if (tid == 0) issue(k + H + 2);
+                zpend |= 1u << slot(k + H + 2);
+            }
+        }
+    }
+    if (failed) {
+        if (tid == 0) atomicExch(p.kerr, 1);
+        for (int s = 0; s < T::NZS; s++)
+            if (zpend & (1u << s)) tma::mbar_wait(&zbar[s], (zph >> s) & 1u);
     }
 }
 
@@ -819,12 +1191,131 @@ static cudaError_t launch_vis_div_t(const Params &p, int krk, int k0, int k1, cu
 // k_vis_div.  krk = 0: viscous terms into du; krk = 1..3: viscous terms,
 // then the RK stage update in the same kernel (du is not written).  FP32
 // stencils in the precision form.
+template <typename R, int H>
+static bool launch_vev_h(const Params &p, cudaStream_t st, cudaError_t &err);
 cudaError_t launch_vis_ev(const Params &p, cudaStream_t st) {
+    const bool staged = p.vis_impl == 2 || (p.vis_impl == 0 && p.mixed);
+    if (staged && p.kerr) {
+        cudaError_t e = cudaSuccess;
+        const bool c8 = p.scheme_vis == 204;
+        const bool done = p.mixed ? (c8 ? launch_vev_h<float, 4>(p, st, e) : launch_vev_h<float, 3>(p, st, e))
+                                  : (c8 ? launch_vev_h<double, 4>(p, st, e) : launch_vev_h<double, 3>(p, st, e));
+        if (done) return e;
+    }
     return p.mixed ? launch_vis_ev_t<float>(p, st) : launch_vis_ev_t<double>(p, st);
+}
+
+// persistent grid of the staged viscous kernels: blocks per SM from their
+// shared memory, and the segment length along z with the fewest plane steps
+// on the busiest block (two steps of ring fill counted per item)
+static void staged_grid(const Params &p, size_t smem_bytes, unsigned &nb, int &seg) {
+    static int nsm = 0;
+    if (!nsm) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            nsm = 148;
+        }
+    }
+    long long bps = (long long)(225 * 1024) / (long long)smem_bytes;
+    if (bps < 1) bps = 1;
+    if (bps > 4) bps = 4;
+    const long long grid = (long long)nsm * bps;
+    const long long tiles = (long long)((p.nx + VX - 1) / VX) * ((p.ny + VY - 1) / VY);
+    int best = p.nz;
+    long long best_cost = -1;
+    for (int sl = 8; sl <= p.nz + 7; sl += 8) {
+        const int len = sl < p.nz ? sl : p.nz;
+        const long long items = tiles * ((p.nz + len - 1) / len);
+        const long long cost = (items + grid - 1) / grid * (len + 2);
+        if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = len; }
+        if (len == p.nz) break;
+    }
+    const long long items = tiles * ((p.nz + best - 1) / best);
+    nb = (unsigned)(items < grid ? items : grid);
+    seg = best;
+}
+
+// the staged Ev kernel; false when the tensor map cannot be formed
+template <typename R, int H>
+static bool launch_vev_h(const Params &p, cudaStream_t st, cudaError_t &err) {
+    using T = VevTiles<R, H>;
+    const unsigned long long eb = sizeof(R);
+    const unsigned long long dims[4] = { (unsigned long long)p.ys, (unsigned long long)(p.ny + 2 * OCFD_LAP),
+                                         (unsigned long long)(p.nz + 2 * OCFD_LAP), 4 };
+    const unsigned long long strides[3] = { p.ys * eb, p.zs * eb, p.lapN * eb };
+    const unsigned bq[4] = { (unsigned)T::PX, (unsigned)T::PY, 1, 4 };
+    // (host code: the primitives of the form, u first)
+    const R *prim1 = sizeof(R) == 4 ? reinterpret_cast<const R *>(p.prim32[1]) : reinterpret_cast<const R *>(p.prim[1]);
+    if (p.prim[2] - p.prim[1] != p.lapN && sizeof(R) == 8) return false;
+    if (sizeof(R) == 4 && p.prim32[2] - p.prim32[1] != p.lapN) return false;
+    CUtensorMap tmq;
+    if (!encode_map_4d(prim1, (int)eb, dims, strides, bq, &tmq)) return false;
+    unsigned nb;
+    int seg;
+    staged_grid(p, T::bytes, nb, seg);
+    auto kern = p.uniform_metrics ? k_vev<true, R, H> : k_vev<false, R, H>;
+    kern<<<nb, VX * VY, T::bytes, st>>>(p, tmq, seg);
+    err = cudaGetLastError();
+    return true;
+}
+
+// the staged divergence + RK stage over the whole slab; false when the tensor
+// maps cannot be formed (the caller then uses k_vis_div)
+template <typename R, int H>
+static bool launch_vdiv_h(const Params &p, int krk, cudaStream_t st, cudaError_t &err) {
+    using T = VdivTiles<R, H>;
+    const unsigned long long eb = sizeof(R);
+    const unsigned long long dims[4] = { (unsigned long long)p.ys, (unsigned long long)(p.ny + 2 * OCFD_LAP),
+                                         (unsigned long long)(p.nz + 2 * OCFD_LAP), 4 };
+    const unsigned long long strides[3] = { p.ys * eb, p.zs * eb, p.lapN * eb };
+    const unsigned bx[4] = { VX + 2 * VXH, VY, 1, 4 }, by[4] = { VX, VY + 2 * H, 1, 4 }, bz[4] = { VX, VY, 1, 4 };
+    // (host code: the Ev base of the form, not the device accessor ev_r)
+    const R *ev = sizeof(R) == 4 ? reinterpret_cast<const R *>(p.ev32) : reinterpret_cast<const R *>(p.ev);
+    CUtensorMap tmx, tmy, tmz;
+    if (!encode_map_4d(ev, (int)eb, dims, strides, bx, &tmx) ||
+        !encode_map_4d(ev + 4 * p.lapN, (int)eb, dims, strides, by, &tmy) ||
+        !encode_map_4d(ev + 8 * p.lapN, (int)eb, dims, strides, bz, &tmz))
+        return false;
+    unsigned nb;
+    int best;
+    staged_grid(p, T::bytes, nb, best);
+    if (T::bytes * 2 > 225 * 1024 && nb > 0) {}     // one block per SM
+    auto kern = p.uniform_metrics ? k_vdiv<true, R, H> : k_vdiv<false, R, H>;
+    kern<<<nb, VX * VY, T::bytes, st>>>(p, tmx, tmy, tmz, krk, best);
+    err = cudaGetLastError();
+    return true;
+}
+
+// the dynamic shared-memory size of every staged-divergence instance, set on
+// the current device before the first launch (and before any stream capture)
+cudaError_t vdiv_prepare() {
+    cudaError_t e = cudaSuccess;
+    auto one = [&](auto kern, size_t bytes) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    };
+    one(k_vdiv<true, double, 3>, VdivTiles<double, 3>::bytes);  one(k_vdiv<false, double, 3>, VdivTiles<double, 3>::bytes);
+    one(k_vdiv<true, double, 4>, VdivTiles<double, 4>::bytes);  one(k_vdiv<false, double, 4>, VdivTiles<double, 4>::bytes);
+    one(k_vdiv<true, float, 3>, VdivTiles<float, 3>::bytes);    one(k_vdiv<false, float, 3>, VdivTiles<float, 3>::bytes);
+    one(k_vdiv<true, float, 4>, VdivTiles<float, 4>::bytes);    one(k_vdiv<false, float, 4>, VdivTiles<float, 4>::bytes);
+    one(k_vev<true, double, 3>, VevTiles<double, 3>::bytes);    one(k_vev<false, double, 3>, VevTiles<double, 3>::bytes);
+    one(k_vev<true, double, 4>, VevTiles<double, 4>::bytes);    one(k_vev<false, double, 4>, VevTiles<double, 4>::bytes);
+    one(k_vev<true, float, 3>, VevTiles<float, 3>::bytes);      one(k_vev<false, float, 3>, VevTiles<float, 3>::bytes);
+    one(k_vev<true, float, 4>, VevTiles<float, 4>::bytes);      one(k_vev<false, float, 4>, VevTiles<float, 4>::bytes);
+    return e;
 }
 
 // planes k0 .. k1-1 (the whole slab: 0, nz)
 cudaError_t launch_vis_div(const Params &p, int krk, int k0, int k1, cudaStream_t st) {
+    const bool staged = p.vis_impl == 2 || (p.vis_impl == 0 && p.mixed);
+    if (krk > 0 && k0 == 0 && k1 == p.nz && staged && p.kerr) {
+        cudaError_t e = cudaSuccess;
+        const bool c8 = p.scheme_vis == 204;
+        const bool done = p.mixed ? (c8 ? launch_vdiv_h<float, 4>(p, krk, st, e) : launch_vdiv_h<float, 3>(p, krk, st, e))
+                                  : (c8 ? launch_vdiv_h<double, 4>(p, krk, st, e) : launch_vdiv_h<double, 3>(p, krk, st, e));
+        if (done) return e;
+    }
     return p.mixed ? launch_vis_div_t<float>(p, krk, k0, k1, st) : launch_vis_div_t<double>(p, krk, k0, k1, st);
 }
 

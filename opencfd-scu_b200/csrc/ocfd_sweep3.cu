@@ -185,69 +185,122 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
     }
 }
 
-// Cells the FAST sweep deferred: each thread takes one cell, splits the 9
-// points X-4 .. X+4 of its line, forms the fluxes of faces X-1/2 and X+1/2
-// (UP7 or the out-of-line routine, as the inline path would) and adds the
-// cell's du in the same order.
+// Cells the FAST sweep deferred, one warp per cell (few cells, each with the
+// longest arithmetic of the path, so the work of a cell is spread over
+// lanes): lanes 0..8 split the points X-4 .. X+4 into the warp's window;
+// lane (face, value) forms a value of the fluxes of faces X-1/2 and X+1/2 --
+// UP7, or the out-of-line routine's component-wise reconstruction or
+// closure; for a characteristic face lane (face, sign, field c) projects on
+// field c, reconstructs and takes column c of R, and lane (face, sign, m)
+// sums the products over c in the routine's order (face_generic); lanes 0..4
+// then add the cell's du, field by field, in the same order as the walk.
+constexpr int FIXW = 4;        // warps (cells in flight) per block
+
 template <int DIR, bool UNI, bool EPS0>
-__global__ void __launch_bounds__(128) k_sweep3_fix(const __grid_constant__ Params p) {
+__global__ void __launch_bounds__(32 * FIXW) k_sweep3_fix(const __grid_constant__ Params p) {
+    __shared__ double win_s[FIXW][90];          // [point X-4+t][sign * 5 + field]
+    __shared__ double res_s[FIXW][20];          // characteristic faces: reconstruction of (face, sign, c)
+    __shared__ double rc_s[FIXW][20][5];        //   and column c of R
+    __shared__ double out_s[FIXW][2][10];       // fluxes of faces X-1/2 and X+1/2
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned cnt = p.defer_count[DIR];
     const long long sd = DIR == 0 ? 1LL : (DIR == 1 ? p.ys : p.zs);
-    const bool hybrid = p.scheme_invis == 310;
+    const int scheme = p.scheme_invis;
+    const bool hybrid = scheme == 310;
+    const bool char_scheme = p.charteric && (scheme == 304 || scheme == 305 || scheme == 310);
+    const bool lo = p.bnd_lo[DIR], hi = p.bnd_hi[DIR];
+    const bool bnd = lo || hi;
     const double h = DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz), ih = p.inv_h[DIR];
-    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
+    const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
+    double *win = win_s[w];
+    for (unsigned e = blockIdx.x * FIXW + w; e < cnt; e += gridDim.x * FIXW) {
         const long long ci = p.defer[DIR][e];
         const int i = (int)(ci % p.nx);
         const long long r = ci / p.nx;
         const int j = (int)(r % p.ny), k = (int)(r / p.ny);
         const int X = DIR == 0 ? i : (DIR == 1 ? j : k);
         const long long oX = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
-        double win[90];                       // [point X-4+t][sign * 5 + field]
-        for (int t = 0; t < 9; t++) {
-            const long long o = oX + (long long)(t - 4) * sd;
+        if (lane < 9) {
+            const long long o = oX + (long long)(lane - 4) * sd;
             double q5[5], fp[5], fm[5];
             load5(p, o, q5);
             split_point<DIR, UNI, EPS0>(p, o, q5[0], q5[1], q5[2], q5[3], q5[4], fp, fm);
 #pragma unroll
-            for (int m = 0; m < 5; m++) { win[t * 10 + m] = fp[m]; win[t * 10 + 5 + m] = fm[m]; }
+            for (int m = 0; m < 5; m++) { win[lane * 10 + m] = fp[m]; win[lane * 10 + 5 + m] = fm[m]; }
         }
+        __syncwarp();
         // flag of face F+1/2 is entry F+1 of the direction's flag array
-        auto flag_at = [&](int e1) -> int {
-            if (!hybrid) return 2;
-            long long q = DIR == 0 ? (long long)e1 + (long long)(p.nx + 1) * ((long long)j + (long long)p.ny * k)
-                        : DIR == 1 ? (long long)i + (long long)p.nx * ((long long)e1 + (long long)(p.ny + 1) * k)
-                                   : (long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * e1);
-            return p.flag[DIR][q];
-        };
-        const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
-        double cur[10], prv[10];
-        for (int side = 0; side < 2; side++) {          // 0: face X-1/2, 1: face X+1/2
-            const int hf = flag_at(X + side);
-            const int F = X - 1 + side;
-            double *out = side ? cur : prv;
-            if (up7_face(p, hf) && !near_closure(p, DIR, F, n)) {
-                for (int sv = 0; sv < 10; sv++) {
-                    double vals[8];
+        const int side = lane / 10, q = lane - 10 * (lane / 10);
+        const int e1 = X + (side & 1);
+        int hf = 2;
+        if (hybrid) {
+            const long long qq = DIR == 0 ? (long long)e1 + (long long)(p.nx + 1) * ((long long)j + (long long)p.ny * k)
+                               : DIR == 1 ? (long long)i + (long long)p.nx * ((long long)e1 + (long long)(p.ny + 1) * k)
+                                          : (long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * e1);
+            hf = p.flag[DIR][qq];
+        }
+        const int F = X - 1 + (side & 1);
+        const bool up7 = up7_face(p, hf) && !near_closure(p, DIR, F, n);
+        const bool gchar = !up7 && char_scheme && !(hybrid && hf == 1);
+        const Win wv{win, 10, 1, 15, side & 1};
+        if (lane < 20) {
+            const int sign = q >= 5, mc = q - 5 * sign;
+            int KA, KB;
+            extents(scheme, char_scheme, sign, KA, KB);
+            if (up7) {
+                double vals[8];
 #pragma unroll
-                    for (int t = 0; t < 8; t++) vals[t] = win[(side + t) * 10 + sv];
-                    out[sv] = sv < 5 ? up7_p_q(vals) : up7_m_q(vals);
-                }
-            } else {
-                face_generic<UNI>(p, DIR, Win{win, 10, 1, 15, side}, hf, oX + (long long)(side - 1) * sd, sd,
-                                  F, n, out);
+                for (int t = 0; t < 8; t++) vals[t] = win[(side + t) * 10 + q];
+                out_s[w][side][q] = q < 5 ? up7_p_q(vals) : up7_m_q(vals);
+            } else if (p.charteric && !char_scheme) {       // the reference adds nothing
+                out_s[w][side][q] = 0.0;
+            } else if (!gchar) {                             // component-wise
+                double vals[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) vals[t] = wv.at(q, t);
+                int hq = hf;
+                if (hybrid && !char_scheme && mc > 0 && p.nochar_comp_flag) hq = p.nochar_comp_flag;
+                double o;
+                if (!(bnd && closure(sign, lo, hi, KA, KB, F, n, vals, o))) o = recon_one(p, scheme, hq, sign, vals);
+                out_s[w][side][q] = o;
+            } else {                                         // characteristic field c = mc of this sign
+                double rec[FP_N], Lr[5], Rc[5], vals[8];
+                const long long o0 = oX + (long long)(side - 1) * sd;
+                face_record<UNI>(p, DIR, o0, o0 + sd, rec);
+                L_row(rec, 1, mc, Lr);
+#pragma unroll
+                for (int t = 0; t < 8; t++)
+                    vals[t] = dot5(Lr, wv.at(sign * 5 + 0, t), wv.at(sign * 5 + 1, t), wv.at(sign * 5 + 2, t),
+                                   wv.at(sign * 5 + 3, t), wv.at(sign * 5 + 4, t));
+                double res;
+                if (!(bnd && closure(sign, lo, hi, KA, KB, F, n, vals, res)))
+                    res = recon_one(p, scheme, hf, sign, vals);
+                R_col(rec, 1, mc, Rc);
+                res_s[w][lane] = res;
+#pragma unroll
+                for (int m = 0; m < 5; m++) rc_s[w][lane][m] = Rc[m];
             }
         }
-        const double aj = metric<UNI>(p, M_AJAC, oX);
-        // du of the cell: x+ then x- for every field (put_du_p_kernel /
-        // put_du_m_kernel, src/OCFD_Schemes.cu:293-381; the characteristic
-        // kernels' put_du_character_{p,m}_kernel, src/OCFD_flux_charteric.cu:16-118,
-        // and OCFD_bound_character_kernel_{p,m}, :121-319)
-        const int scheme = p.scheme_invis;
-        const bool char_kernel = p.charteric && (scheme == 304 || scheme == 305 || scheme == 310);
-        const bool lo = p.bnd_lo[DIR], hi = p.bnd_hi[DIR];
-        const bool only_lo = lo && !hi, only_hi = hi && !lo;     // flag 1..6, not 7..9
-        const bool first = X == 0, last = X == n - 1;
-        for (int m = 0; m < 5; m++) {
+        __syncwarp();
+        if (lane < 20 && gchar) {        // lane (face, sign, field m): the sum over c in order
+            const int sign = q >= 5, m = q - 5 * sign, b0 = side * 10 + sign * 5;
+            double o = rc_s[w][b0][m] * res_s[w][b0];
+#pragma unroll
+            for (int c = 1; c < 5; c++) o = o + rc_s[w][b0 + c][m] * res_s[w][b0 + c];
+            out_s[w][side][q] = o;
+        }
+        __syncwarp();
+        if (lane < 5) {
+            // du of the cell: x+ then x- for field m (put_du_p_kernel /
+            // put_du_m_kernel, src/OCFD_Schemes.cu:293-381; the characteristic
+            // kernels' put_du_character_{p,m}_kernel, src/OCFD_flux_charteric.cu:16-118,
+            // and OCFD_bound_character_kernel_{p,m}, :121-319)
+            const int m = lane;
+            const double *cur = out_s[w][1], *prv = out_s[w][0];
+            const double aj = metric<UNI>(p, M_AJAC, oX);
+            const bool char_kernel = char_scheme;
+            const bool only_lo = lo && !hi, only_hi = hi && !lo;     // flag 1..6, not 7..9
+            const bool first = X == 0, last = X == n - 1;
             double acc = DIR == 0 ? 0.0 : p.du[m * p.N + ci];
             // P side
             if (!char_kernel ? (first && p.nonref_lo[DIR] == 1) : (only_lo && p.nonref_lo[DIR] == 1 && first)) {
@@ -286,6 +339,7 @@ __global__ void __launch_bounds__(128) k_sweep3_fix(const __grid_constant__ Para
             }
             p.du[m * p.N + ci] = acc;
         }
+        __syncwarp();                    // the window and fluxes are reused by the next cell
     }
 }
 
@@ -313,7 +367,7 @@ cudaError_t launch_dir(const Params &p, cudaStream_t st) {
     if (sizeof(R) == 4) return launch_sweep4_fix(p, DIR, st);
     // the deferred-cell count is only known on the device: a fixed grid
     // that strides over it (usually a few thousand cells, often none)
-    k_sweep3_fix<DIR, UNI, EPS0><<<2 * 148, 128, 0, st>>>(p);
+    k_sweep3_fix<DIR, UNI, EPS0><<<2 * 148, 32 * FIXW, 0, st>>>(p);
     return cudaGetLastError();
 }
 
@@ -369,6 +423,26 @@ cudaError_t dir3(const Params &p, int dir, cudaStream_t st) {
     return launch_dir<2, UNI, EPS0, 5, false>(p, st);
 }
 }  // namespace
+
+// the fix-up of one direction's deferred cells (FP64)
+cudaError_t launch_sweep3_fix(const Params &p, int dir, cudaStream_t st) {
+    if (p.uniform_metrics) {
+        if (p.epsl_sw == 0.0) {
+            if (dir == 0) k_sweep3_fix<0, true, true><<<2 * 148, 32 * FIXW, 0, st>>>(p);
+            else if (dir == 1) k_sweep3_fix<1, true, true><<<2 * 148, 32 * FIXW, 0, st>>>(p);
+            else k_sweep3_fix<2, true, true><<<2 * 148, 32 * FIXW, 0, st>>>(p);
+        } else {
+            if (dir == 0) k_sweep3_fix<0, true, false><<<2 * 148, 32 * FIXW, 0, st>>>(p);
+            else if (dir == 1) k_sweep3_fix<1, true, false><<<2 * 148, 32 * FIXW, 0, st>>>(p);
+            else k_sweep3_fix<2, true, false><<<2 * 148, 32 * FIXW, 0, st>>>(p);
+        }
+    } else {
+        if (dir == 0) k_sweep3_fix<0, false, false><<<2 * 148, 32 * FIXW, 0, st>>>(p);
+        else if (dir == 1) k_sweep3_fix<1, false, false><<<2 * 148, 32 * FIXW, 0, st>>>(p);
+        else k_sweep3_fix<2, false, false><<<2 * 148, 32 * FIXW, 0, st>>>(p);
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t launch_sweep3_dir(const Params &p, int dir, cudaStream_t st) {
     if (p.uniform_metrics)

@@ -29,7 +29,7 @@ EXPORTED = (
     "ocfd_b200_create", "ocfd_b200_destroy", "ocfd_b200_set_stream", "ocfd_b200_get_stream",
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
     "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics", "ocfd_b200_set_sweep_impl",
-    "ocfd_b200_sweep_walks", "ocfd_b200_set_precision", "ocfd_b200_slab_unique_id", "ocfd_b200_set_slab",
+    "ocfd_b200_sweep_walks", "ocfd_b200_set_walk_threshold", "ocfd_b200_set_viscous_impl", "ocfd_b200_set_precision", "ocfd_b200_slab_unique_id", "ocfd_b200_set_slab",
     "ocfd_b200_set_graphs", "ocfd_b200_graph_captures",
     "ocfd_b200_scheme_proportion", "ocfd_b200_mlp_nparam", "ocfd_b200_set_switch", "ocfd_b200_switch_stats", "ocfd_b200_switch_features",
     "ocfd_b200_mlp_last_error", "ocfd_b200_mlp_infer", "ocfd_b200_mlp_grad", "ocfd_b200_mlp_train",
@@ -120,6 +120,8 @@ def load(path: Optional[str] = None):
         "ocfd_b200_uniform_metrics": (ctypes.c_int, [P]),
         "ocfd_b200_set_sweep_impl": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_sweep_walks": (ctypes.c_int, [P]),
+        "ocfd_b200_set_walk_threshold": (ctypes.c_int, [P, ctypes.c_double]),
+        "ocfd_b200_set_viscous_impl": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_set_precision": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_slab_unique_id": (ctypes.c_int, [ctypes.c_char_p]),
         "ocfd_b200_set_graphs": (ctypes.c_int, [P, ctypes.c_int]),
@@ -378,6 +380,16 @@ class Solver:
     def sweep_walks(self) -> int:
         """Bit d set: direction d takes the walk that forms every face in line."""
         return int(self.L.ocfd_b200_sweep_walks(self.h))
+
+    def set_viscous_impl(self, impl: int):
+        """0: the faster kernel of the form (default); 1: Ev read through the caches; 2: Ev tiles staged in shared memory."""
+        self._check(self.L.ocfd_b200_set_viscous_impl(self.h, impl), "set_viscous_impl")
+
+    def set_walk_threshold(self, frac: float):
+        """Deferred-cell fraction above which a hybrid direction takes the
+        in-line walk (default 0.002; 3 or more keeps every direction on the
+        UP7 walk with its other cells deferred)."""
+        self._check(self.L.ocfd_b200_set_walk_threshold(self.h, float(frac)), "set_walk_threshold")
 
     @property
     def uniform_metrics(self) -> bool:

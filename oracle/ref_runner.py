@@ -23,6 +23,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 REF_BIN = os.path.join(HERE, "_ref", "opencfd-scu.out")
+# the reference's program with its RHS-path calls served by libocfd_b200 (oracle/dropin.mk)
+DROPIN_BIN = os.path.join(HERE, "_ref", "dropin", "opencfd-scu-dropin.out")
 
 sys.path.insert(0, os.path.join(ROOT, "opencfd-scu_b200"))
 from ocfd_b200 import formats  # noqa: E402
@@ -39,8 +41,8 @@ def _big_stack():
         pass
 
 
-def available() -> bool:
-    return os.path.exists(REF_BIN) and os.access(REF_BIN, os.X_OK)
+def available(binary: str = REF_BIN) -> bool:
+    return os.path.exists(binary) and os.access(binary, os.X_OK)
 
 
 def _write_inputs(case, workdir: str) -> None:
@@ -55,7 +57,7 @@ def _write_inputs(case, workdir: str) -> None:
         formats.write_inlet_file(os.path.join(workdir, "flow1d-inlet.dat"), inlet)
 
 
-def run_and_read(case, nsteps: int, timeout: float = 900.0):
+def run_and_read(case, nsteps: int, timeout: float = 900.0, binary: str = REF_BIN):
     """Run nsteps steps and return (prims[5,nz,ny,nx], Istep, tt, wall_s, stdout)."""
     cfg = case.cfg
     cfg.set_steps(nsteps)
@@ -65,7 +67,7 @@ def run_and_read(case, nsteps: int, timeout: float = 900.0):
     try:
         _write_inputs(case, wd)
         t0 = time.time()
-        p = subprocess.run([REF_BIN], cwd=wd, capture_output=True, text=True, timeout=timeout,
+        p = subprocess.run([binary], cwd=wd, capture_output=True, text=True, timeout=timeout,
                            preexec_fn=_big_stack)
         wall = time.time() - t0
         if p.returncode != 0:

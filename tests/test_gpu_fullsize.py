@@ -10,6 +10,10 @@
 * C4: the compression ramp 512x128x64 (metrics from the mesh, IBC 108, the
   shock filter) against the reference build after 100 steps, and after the
   stated 500 steps within the reference's own one-ulp sensitivity.
+* C3 and the precision half of C4: the FP32-stencil form against the FP64
+  path at the stated steps (50, 100, 200 on the C2 input; 100 and 500 on the
+  ramp), relative L2 and L-infinity per conserved variable, bounded from
+  the first measurements with a stated margin.
 Tolerance: relative L2 <= 1e-12 per variable (the parity bound).
 """
 import numpy as np
@@ -101,25 +105,40 @@ def test_c2_iso256_repeatable(iso256):
     assert np.array_equal(s2.primitives(), s.primitives())
 
 
+def _matches_reference(rr, got, make, nsteps, runs=3):
+    """The reference build at this size does not always repeat itself: the
+    shared-memory race of its characteristic y/z kernels can fire (measured:
+    one 3-step run 1e-6 and one 200-step run 2e-5 away from other runs of the
+    same input, which agree with each other and with the library to 5e-16).
+    The library's state must match a reference run to 1e-12; up to `runs`
+    runs are taken, and if none matches, the library must lie within twice
+    the largest distance between them."""
+    refs = []
+    for _ in range(runs):
+        ref, istep, *_ = rr.run_and_read(make(), nsteps, timeout=1800.0)
+        assert istep == nsteps
+        if np.all(rel_l2(got, ref) <= TOL):
+            return
+        refs.append(ref)
+    spread = np.max([rel_l2(a, b) for n, a in enumerate(refs) for b in refs[n + 1:]], axis=0)
+    errs = [rel_l2(got, r) for r in refs]
+    assert all(np.all(e <= np.maximum(TOL, 2.0 * spread)) for e in errs), (errs, spread)
+
+
 def test_c2_iso256_vs_reference(iso256):
     rr = _ref_runner()
     case, s, _ = iso256
-    ref, istep, tt, wall, _ = rr.run_and_read(cases.isotropic_turbulence(256, seed=2024, charteric=1), 3)
-    err = rel_l2(s.primitives(), ref)
-    assert np.all(err <= TOL), err
+    _matches_reference(rr, s.primitives(), lambda: cases.isotropic_turbulence(256, seed=2024, charteric=1), 3)
 
 
 def test_c2_iso256_200_steps_vs_reference():
-    """C2 for its stated 200 steps against the reference build."""
+    """C2 for its stated 200 steps against the reference build (see
+    _matches_reference for the reference's own run-to-run spread)."""
     rr = _ref_runner()
     case = cases.isotropic_turbulence(256, seed=2024, charteric=1)
     s = lib.Solver(case.cfg, case.prims, case.metrics)
     s.step(200)
-    ref, istep, tt, wall, _ = rr.run_and_read(cases.isotropic_turbulence(256, seed=2024, charteric=1), 200,
-                                               timeout=1800.0)
-    assert istep == 200
-    err = rel_l2(s.primitives(), ref)
-    assert np.all(err <= TOL), err
+    _matches_reference(rr, s.primitives(), lambda: cases.isotropic_turbulence(256, seed=2024, charteric=1), 200)
 
 
 @pytest.fixture(scope="module")
@@ -127,13 +146,13 @@ def ramp500():
     case = cases.ramp_case(512, 128, 64, seed=2024)
     s = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
     s.step(100)
-    p100 = s.primitives()
+    p100, c100 = s.primitives(), s.conserved()
     s.step(400)
-    return case, s, p100
+    return case, s, p100, c100
 
 
 def test_c4_ramp_500_steps_stays_physical(ramp500):
-    case, s, _ = ramp500
+    case, s, _, _ = ramp500
     nnan, nneg, mean_t = s.check_state()
     assert nnan == 0 and nneg == 0
     p = s.primitives()
@@ -148,7 +167,7 @@ def test_c4_ramp_100_steps_vs_reference(ramp500):
     state must match one of the two runs to 1e-12, or lie within twice the
     two runs' own distance from each other."""
     rr = _ref_runner()
-    case, s, p100 = ramp500
+    case, s, p100, _ = ramp500
     runs = []
     for _ in range(2):
         ref, istep, *_ = rr.run_and_read(cases.ramp_case(512, 128, 64, seed=2024), 100, timeout=1800.0)
@@ -168,7 +187,7 @@ def test_c4_ramp_500_steps_within_reference_sensitivity(ramp500):
     run.  The library's 500-step state must sit within that spread of the
     reference's (it matches to 1e-15 at 100 steps, above)."""
     rr = _ref_runner()
-    case, s, _ = ramp500
+    case, s, _, _ = ramp500
     ref, istep, *_ = rr.run_and_read(cases.ramp_case(512, 128, 64, seed=2024), 500, timeout=1800.0)
     pert = cases.ramp_case(512, 128, 64, seed=2024)
     d = pert.prims[0].copy()
@@ -193,3 +212,62 @@ def test_c3_precision_form_256_50_steps(iso256):
     b.step(50)
     err = rel_l2(b.conserved(), a.conserved())
     assert np.all(err <= 1e-6) and np.all(err > 0), err
+
+
+def form_errors(test, ref):
+    """Relative L2 and L-infinity per conserved variable; the momentum
+    components are measured against the momentum vector (its L2 norm, its
+    largest magnitude), since the spanwise component is a small fluctuation."""
+    mom_l2 = np.sqrt(sum(np.linalg.norm(ref[m]) ** 2 for m in (1, 2, 3)))
+    mom_max = np.sqrt(ref[1] ** 2 + ref[2] ** 2 + ref[3] ** 2).max()
+    l2, linf = [], []
+    for m in range(5):
+        d = test[m] - ref[m]
+        l2.append(np.linalg.norm(d) / (mom_l2 if m in (1, 2, 3) else np.linalg.norm(ref[m])))
+        linf.append(np.abs(d).max() / (mom_max if m in (1, 2, 3) else np.abs(ref[m]).max()))
+    return np.array(l2), np.array(linf)
+
+
+def test_c3_precision_form_256_100_200_steps(iso256):
+    """C3 at its stated steps: the precision form against the FP64 path on
+    the C2 input.  Measured (per-variable norms): relative L2 <= 5.4e-7 and
+    L-infinity <= 2.5e-4 at step 100, <= 4.2e-6 and <= 7.1e-4 at step 200
+    (shocklets form between 100 and 200 and a few faces fall on the other
+    side of a sensor threshold in FP32).  Bounds: 5x those."""
+    case, _, _ = iso256
+    a = lib.Solver(case.cfg, case.prims, case.metrics)
+    b = lib.Solver(case.cfg, case.prims, case.metrics)
+    b.set_precision(1)
+    for steps, tol_l2, tol_inf in ((100, 2.7e-6, 1.3e-3), (200, 2.1e-5, 3.6e-3)):
+        a.step(steps - a.time()[0])
+        b.step(steps - b.time()[0])
+        l2, linf = form_errors(b.conserved(), a.conserved())
+        print(f"C3 step {steps}: rel L2 {l2}, rel Linf {linf}")
+        assert np.all(l2 > 0), l2
+        assert np.all(l2 <= tol_l2), (steps, l2)
+        assert np.all(linf <= tol_inf), (steps, linf)
+
+
+def test_c4_precision_form_ramp_100_500_steps(ramp500):
+    """The ramp in the precision form (boundary values formed in FP64, the
+    filter weights from the FP32 pressure, its update in FP64) against the
+    FP64 path at steps 100 and 500.  The shocked ramp flow amplifies any
+    perturbation (the reference run from a one-ulp change ends 5e-7 away
+    after 500 steps); FP32 stencils perturb every cell by ~1e-7 each stage.
+    Bounds: relative L2 1e-4 at step 100 and 5e-3 at step 500, L-infinity
+    5e-2 and 0.2."""
+    case, s64, _, c100 = ramp500
+    b = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+    b.set_precision(1)
+    b.step(100)
+    l2, linf = form_errors(b.conserved(), c100)
+    print(f"C4 precision form step 100: rel L2 {l2}, rel Linf {linf}")
+    assert np.all(l2 > 0) and np.all(l2 <= 1e-4), l2
+    assert np.all(linf <= 5e-2), linf
+    b.step(400)
+    l2, linf = form_errors(b.conserved(), s64.conserved())
+    print(f"C4 precision form step 500: rel L2 {l2}, rel Linf {linf}")
+    assert np.all(l2 <= 5e-3), l2
+    assert np.all(linf <= 0.2), linf
+    nnan, nneg, _ = b.check_state()
+    assert nnan == 0 and nneg == 0

@@ -221,6 +221,95 @@ def test_inline_walk_matches_dispatch(name, case, gpu_lib):
     assert np.all(rel_l2(a.primitives(), b.primitives()) <= 1e-14), name
 
 
+def _march_cases():
+    """Hybrid-scheme cases for the UP7 walk: periodic boxes (x narrower than
+    a warp, odd sizes, x wider than a warp), a curvilinear grid with a shock,
+    and closed faces in every direction or in one.  With the walk threshold
+    at 3 every direction stays on the UP7 walk, so shocked cases defer many
+    cells to the fix-up kernel."""
+    out = [
+        ("iso24_hybrid_char", cases.isotropic_turbulence(24, seed=5, charteric=1)),
+        ("iso40_hybrid_char", cases.isotropic_turbulence(40, seed=6, charteric=1)),
+        ("rnd17x18x13_hybrid_char_curv_shock",
+         cases.random_smooth_case(17, 18, 13, seed=65, scheme_invis="SCHEME_HYBRIDAUTO", charteric=1,
+                                  shock=True, curvilinear=True)),
+        ("rnd37x20x19_hybrid_char_shock",
+         cases.random_smooth_case(37, 20, 19, seed=8, scheme_invis="SCHEME_HYBRIDAUTO", charteric=1, shock=True)),
+    ]
+    out += [(n, c) for n, c in bounded_cases() if n.startswith("bnd_hybrid")]
+    return out
+
+
+@pytest.mark.parametrize("name,case", _march_cases(), ids=[n for n, _ in _march_cases()])
+def test_march_matches_ring_walk(name, case, gpu_lib):
+    """The y and z UP7 walks run as per-lane marches over staged pencil tiles
+    (variant 8; variant 4 in the precision form) or through the shared-memory
+    ring (variant 7).  Same face and cell arithmetic and the same deferred
+    cells, so the same state to the last bit, in FP64 and in the precision
+    form; and the FP64 state matches the in-loop dispatch (variant 5) to the
+    walk-equivalence bound."""
+    for form in (0, 1):
+        a = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+        b = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+        a.set_sweep_impl(8)
+        b.set_sweep_impl(7)
+        for s in (a, b):
+            s.set_walk_threshold(3.0)
+            if form:
+                s.set_precision(1)
+        a.step(3)
+        b.step(3)
+        assert a.sweep_walks() == 0 and b.sweep_walks() == 0
+        assert np.array_equal(a.conserved(), b.conserved()), (name, form, rel_l2(a.conserved(), b.conserved()))
+        if form == 0:
+            c = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+            c.set_sweep_impl(5)
+            c.step(3)
+            assert np.all(rel_l2(a.primitives(), c.primitives()) <= 1e-14), name
+
+
+def _viscous_cases():
+    """Viscous-kernel cases: CD6 and CD8, uniform and curvilinear metrics,
+    closed faces, a width that is not a multiple of the 32-cell tile, the
+    ramp with its boundary conditions and filter."""
+    out = [
+        ("tgv24_cd6", cases.taylor_green(24, seed=3)),
+        ("iso40_hybrid_char", cases.isotropic_turbulence(40, seed=6, charteric=1)),
+        ("rnd_weno7_cd8", cases.random_smooth_case(37, 11, 10, seed=22, scheme_vis="CD8")),
+        ("rnd_weno7_curv", cases.random_smooth_case(19, 13, 11, seed=3, curvilinear=True)),
+        ("ramp_bc108", cases.ramp_case(30, 18, 8, seed=66)),
+    ]
+    out += [(n, c) for n, c in bounded_cases() if n in ("bnd_weno7_cd8_one", "bnd_hybrid_char_both")]
+    return out
+
+
+@pytest.mark.parametrize("name,case", _viscous_cases(), ids=[n for n, _ in _viscous_cases()])
+def test_staged_viscous_matches_cached(name, case, gpu_lib):
+    """The viscous kernels with their stencil inputs staged in shared memory
+    (variant 2: the primitives of the Ev kernel, the Ev tiles of the
+    divergence + RK kernel) against the kernels that read them through the
+    caches:
+    the same arithmetic in the same order, so the same state to the last bit,
+    in FP64 and (where the form covers the scheme) in the precision form."""
+    forms = [0, 1] if case.cfg.scheme_invis in ("SCHEME_HYBRIDAUTO", "WENO7") and \
+        (case.cfg.charteric or case.cfg.scheme_invis == "WENO7") else [0]
+    for form in forms:
+        a = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+        b = lib.Solver(case.cfg, case.prims, case.metrics, inlet=case.inlet)
+        a.set_viscous_impl(2)
+        b.set_viscous_impl(1)
+        if form:
+            try:
+                a.set_precision(1)
+            except lib.OcfdError:
+                continue
+            b.set_precision(1)
+        a.step(3)
+        b.step(3)
+        assert np.array_equal(a.conserved(), b.conserved()), (name, form, rel_l2(a.conserved(), b.conserved()))
+        assert np.array_equal(a.primitives(), b.primitives()), (name, form)
+
+
 def test_walk_choice_follows_sensor(gpu_lib):
     """Variant 4 picks a walk per direction after each sensor pass: the UP7
     walk where (almost) every face is UP7, the in-line walk where many are
