@@ -667,6 +667,7 @@ __device__ __forceinline__ R d0bw(const R *v, R h, R ih, bool c8, int X, int n, 
 }
 
 template <bool UNI, typename R, int H>
+// (two blocks per SM: a budget for three spills and measured 14 % slower in FP32)
 __global__ void __launch_bounds__(VX * VY, 2)
 k_vdiv(const __grid_constant__ Params p, const __grid_constant__ CUtensorMap tmx,
        const __grid_constant__ CUtensorMap tmy, const __grid_constant__ CUtensorMap tmz, int krk, int seg_len) {
@@ -1208,7 +1209,8 @@ cudaError_t launch_vis_ev(const Params &p, cudaStream_t st) {
 // persistent grid of the staged viscous kernels: blocks per SM from their
 // shared memory, and the segment length along z with the fewest plane steps
 // on the busiest block (two steps of ring fill counted per item)
-static void staged_grid(const Params &p, size_t smem_bytes, unsigned &nb, int &seg) {
+template <typename K>
+static void staged_grid(const Params &p, K kern, size_t smem_bytes, unsigned &nb, int &seg) {
     static int nsm = 0;
     if (!nsm) {
         int dev = 0;
@@ -1218,9 +1220,13 @@ static void staged_grid(const Params &p, size_t smem_bytes, unsigned &nb, int &s
             nsm = 148;
         }
     }
-    long long bps = (long long)(225 * 1024) / (long long)smem_bytes;
-    if (bps < 1) bps = 1;
-    if (bps > 4) bps = 4;
+    // resident blocks per SM of this kernel (registers and shared memory)
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, VX * VY, smem_bytes) != cudaSuccess || occ < 1) {
+        cudaGetLastError();
+        occ = 1;
+    }
+    const long long bps = occ;
     const long long grid = (long long)nsm * bps;
     const long long tiles = (long long)((p.nx + VX - 1) / VX) * ((p.ny + VY - 1) / VY);
     int best = p.nz;
@@ -1254,8 +1260,8 @@ static bool launch_vev_h(const Params &p, cudaStream_t st, cudaError_t &err) {
     if (!encode_map_4d(prim1, (int)eb, dims, strides, bq, &tmq)) return false;
     unsigned nb;
     int seg;
-    staged_grid(p, T::bytes, nb, seg);
     auto kern = p.uniform_metrics ? k_vev<true, R, H> : k_vev<false, R, H>;
+    staged_grid(p, kern, T::bytes, nb, seg);
     kern<<<nb, VX * VY, T::bytes, st>>>(p, tmq, seg);
     err = cudaGetLastError();
     return true;
@@ -1280,9 +1286,8 @@ static bool launch_vdiv_h(const Params &p, int krk, cudaStream_t st, cudaError_t
         return false;
     unsigned nb;
     int best;
-    staged_grid(p, T::bytes, nb, best);
-    if (T::bytes * 2 > 225 * 1024 && nb > 0) {}     // one block per SM
     auto kern = p.uniform_metrics ? k_vdiv<true, R, H> : k_vdiv<false, R, H>;
+    staged_grid(p, kern, T::bytes, nb, best);
     kern<<<nb, VX * VY, T::bytes, st>>>(p, tmx, tmy, tmz, krk, best);
     err = cudaGetLastError();
     return true;

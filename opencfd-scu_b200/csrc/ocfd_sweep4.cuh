@@ -318,12 +318,24 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep4(const __grid_constant_
     }
 }
 
-// Cells the call-free UP7 walk left (precision form): each thread takes one
-// cell, splits the 9 points X-4 .. X+4 of its line into a private 16-slot
-// ring, forms faces X-1/2 and X+1/2 with the walk's own face routine and
-// adds the cell's du in the same order.
-template <int DIR, bool UNI, bool EPS0, int KIND, typename R>
-__global__ void __launch_bounds__(128) k_sweep4_fix(const __grid_constant__ Params p) {
+// Cells the call-free UP7 walk left (precision form, the characteristic
+// hybrid scheme), one warp per cell: lanes 0..8 split the points X-4 .. X+4
+// into the warp's window; lane (face, value) forms a value of the fluxes of
+// faces X-1/2 and X+1/2 where the face is UP7 (with its closure when one is
+// in reach); for a characteristic face lane (face, sign, field c) projects,
+// reconstructs (WENO7 on flag 2, else WENO5, or the closure) and takes
+// column c of R, and lane (face, sign, m) sums the products over c in
+// char_sign's order; lanes 0..4 add the cell's du as the walk does.  The
+// arithmetic of every value is face4's.
+constexpr int FIX4W = 4;       // warps (cells in flight) per block
+
+template <int DIR, bool UNI, bool EPS0, typename R>
+__global__ void __launch_bounds__(32 * FIX4W) k_sweep4_fix(const __grid_constant__ Params p) {
+    __shared__ R win_s[FIX4W][90];              // [point X-4+t][sign * 5 + field]
+    __shared__ R res_s[FIX4W][20];
+    __shared__ R rc_s[FIX4W][20][5];
+    __shared__ R out_s[FIX4W][2][10];           // fluxes of faces X-1/2 and X+1/2
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned cnt = p.defer_count[DIR];
     const long long sd = DIR == 0 ? 1LL : (DIR == 1 ? p.ys : p.zs);
     const R h = (R)(DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz)), ih = (R)p.inv_h[DIR];
@@ -331,43 +343,121 @@ __global__ void __launch_bounds__(128) k_sweep4_fix(const __grid_constant__ Para
     const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
     R *__restrict__ du = du_r<R>(p);
     const long long N = p.N;
-    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
+    R *win = win_s[w];
+    // value sv of point Q of the cell's window (point X-4 is entry 0)
+    for (unsigned e = blockIdx.x * FIX4W + w; e < cnt; e += gridDim.x * FIX4W) {
         const long long ci = p.defer[DIR][e];
         const int i = (int)(ci % p.nx);
         const long long r = ci / p.nx;
         const int j = (int)(r % p.ny), k = (int)(r / p.ny);
         const int X = DIR == 0 ? i : (DIR == 1 ? j : k);
         const long long oX = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
-        R win[10 * 16];
-        for (int t = -4; t <= 4; t++) {
-            R q5[5];
-            const long long o = oX + (long long)t * sd;
+        auto wv = [&](int sv, int Q) -> R { return win[(Q - X + 4) * 10 + sv]; };
+        if (lane < 9) {
+            const long long o = oX + (long long)(lane - 4) * sd;
+            R q5[5], fp[5], fm[5];
             load5(p, o, q5);
-            ring_put<DIR, 16, 1, UNI, EPS0>(p, win, 0, X + t, o, q5);
-        }
-        // flag of face F+1/2 is entry F+1 of the direction's flag array
-        auto flag_at = [&](int e1) -> int {
-            if (KIND != K_HYBC) return 2;
-            long long q = DIR == 0 ? (long long)e1 + (long long)(p.nx + 1) * ((long long)j + (long long)p.ny * k)
-                        : DIR == 1 ? (long long)i + (long long)p.nx * ((long long)e1 + (long long)(p.ny + 1) * k)
-                                   : (long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * e1);
-            return p.flag[DIR][q];
-        };
-        R prv[10], cur[10];
-        face4<KIND, 16, 1, UNI, false>(p, DIR, win, 0, X - 1, n, flag_at(X), oX - sd, sd, lo, hi, prv);
-        face4<KIND, 16, 1, UNI, false>(p, DIR, win, 0, X, n, flag_at(X + 1), oX, sd, lo, hi, cur);
-        const R aj = (R)metric<UNI>(p, M_AJAC, oX);
-        if (p.has_bnd && rule_cell(p, DIR, X, n)) {
-            du_rule_cell<DIR, KIND, 16, 1>(p, win, 0, X, n, du, ci, aj, h, ih, cur, prv);
-        } else {
-            R old[5];
-            if (DIR != 0) {
+            split_point<DIR, UNI, EPS0>(p, o, q5[0], q5[1], q5[2], q5[3], q5[4], fp, fm);
 #pragma unroll
-                for (int m = 0; m < 5; m++) old[m] = du[m * N + ci];
-            }
-            if (DIR == 0) add_du<true>(du, N, ci, aj, h, ih, cur, prv, old);
-            else          add_du<false>(du, N, ci, aj, h, ih, cur, prv, old);
+            for (int m = 0; m < 5; m++) { win[lane * 10 + m] = fp[m]; win[lane * 10 + 5 + m] = fm[m]; }
         }
+        __syncwarp();
+        const int side = (lane / 10) & 1, q = lane - 10 * (lane / 10);
+        const int e1 = X + side;
+        const long long qq = DIR == 0 ? (long long)e1 + (long long)(p.nx + 1) * ((long long)j + (long long)p.ny * k)
+                           : DIR == 1 ? (long long)i + (long long)p.nx * ((long long)e1 + (long long)(p.ny + 1) * k)
+                                      : (long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * e1);
+        const int hflag = p.flag[DIR][qq];
+        const int F = X - 1 + side;
+        const bool near = (lo && F <= 3) || (hi && F >= n - 5);
+        const bool charf = hflag != 1;
+        if (lane < 20) {
+            const int sign = q >= 5, mc = q - 5 * sign;
+            if (!charf) {                                     // UP7 on the flux components
+                R vals[8];
+#pragma unroll
+                for (int t = 0; t < 8; t++) vals[t] = wv(q, F - 3 + t);
+                R o;
+                if (!(near && closure(sign, lo, hi, sign ? 4 : 3, sign ? 3 : 4, F, n, vals, o)))
+                    o = sign ? up7_m_q(vals) : up7_p_q(vals);
+                out_s[w][side][q] = o;
+            } else {                                          // characteristic field c = mc of this sign
+                R rec[FP_N], Lr[5], Rc[5], vals[8];
+                const long long o0 = oX + (long long)(side - 1) * sd;
+                face_record<UNI>(p, DIR, o0, o0 + sd, rec);
+                L_row(rec, 1, mc, Lr);
+                const int K0 = sign, K1 = sign + 6;
+#pragma unroll
+                for (int t = 0; t < 8; t++)
+                    vals[t] = (t >= K0 && t <= K1) ? dot5(Lr, wv(sign * 5 + 0, F - 3 + t), wv(sign * 5 + 1, F - 3 + t),
+                                                          wv(sign * 5 + 2, F - 3 + t), wv(sign * 5 + 3, F - 3 + t),
+                                                          wv(sign * 5 + 4, F - 3 + t))
+                                                   : (R)0.0;
+                R res;
+                if (!(near && closure(sign, lo, hi, sign ? 4 : 3, sign ? 3 : 4, F, n, vals, res)))
+                    res = hflag == 2 ? (sign ? weno7_m(vals) : weno7_p(vals)) : (sign ? weno5_m(vals) : weno5_p(vals));
+                R_col(rec, 1, mc, Rc);
+                res_s[w][lane] = res;
+#pragma unroll
+                for (int m = 0; m < 5; m++) rc_s[w][lane][m] = Rc[m];
+            }
+        }
+        __syncwarp();
+        if (lane < 20 && charf) {            // lane (face, sign, field m): the sum over c in order
+            const int sign = q >= 5, m = q - 5 * sign, b0 = side * 10 + sign * 5;
+            R o = rc_s[w][b0][m] * res_s[w][b0];
+#pragma unroll
+            for (int c = 1; c < 5; c++) o = o + rc_s[w][b0 + c][m] * res_s[w][b0 + c];
+            out_s[w][side][q] = o;
+        }
+        __syncwarp();
+        if (lane < 5) {
+            const int m = lane;
+            const R *cur = out_s[w][1], *prv = out_s[w][0];
+            const R aj = (R)metric<UNI>(p, M_AJAC, oX);
+            R acc = DIR == 0 ? (R)0.0 : (R)du[m * N + ci];
+            if (p.has_bnd && rule_cell(p, DIR, X, n)) {       // du_rule_cell, field m
+                const bool only_lo = lo && !hi, only_hi = hi && !lo;
+                const bool first = X == 0, last = X == n - 1;
+                if (only_lo && p.nonref_lo[DIR] == 1 && first) {
+                    acc += (R)0.0;
+                } else if ((only_lo && first) || (only_hi && last)) {
+                    R tmp;
+                    if (first) {
+                        tmp = wv(m, X + 1) - wv(m, X);
+                    } else {
+                        const R f0 = wv(m, X), f1 = wv(m, X - 1), f2 = wv(m, X - 2);
+                        const R tr = f0 + (R)0.5 * minmod2(f0 - f1, f0 - f1);
+                        const R tl = f1 + (R)0.5 * minmod2(f0 - f1, f1 - f2);
+                        tmp = tr - tl;
+                    }
+                    acc += div_const(-aj * tmp, h, ih);
+                } else {
+                    acc += div_const(-aj * (cur[m] - prv[m]), h, ih);
+                }
+                if (only_hi && p.nonref_hi[DIR] == 1 && last) {
+                    acc += (R)0.0;
+                } else if ((DIR != 1 && only_lo && first) || (only_hi && last)) {
+                    R tmp;
+                    if (first) {
+                        const R f0 = wv(5 + m, X), f1 = wv(5 + m, X + 1), f2 = wv(5 + m, X + 2);
+                        const R tr = f1 - (R)0.5 * minmod2(f2 - f1, f1 - f0);
+                        const R tl = f0 - (R)0.5 * minmod2(f1 - f0, f1 - f0);
+                        tmp = tr - tl;
+                    } else {
+                        tmp = wv(5 + m, X) - wv(5 + m, X - 1);
+                    }
+                    acc += div_const(-aj * tmp, h, ih);
+                } else {
+                    acc += div_const(-aj * (cur[5 + m] - prv[5 + m]), h, ih);
+                }
+            } else {                                          // add_du, field m
+                acc += div_const(-aj * (cur[m] - prv[m]), h, ih);
+                acc += div_const(-aj * (cur[5 + m] - prv[5 + m]), h, ih);
+            }
+            du[m * N + ci] = acc;
+        }
+        __syncwarp();
     }
 }
 

@@ -155,20 +155,25 @@ def _timed(s: "lib.Solver", n: int) -> float:
 
 
 def evaluate(params: np.ndarray, n: int = 512, steps: int = 100, confidence: float = 0.9,
-             seed: int = 2024) -> dict:
+             seed: int = 2024, workload: str = "iso") -> dict:
     """Plain FP64 against the precision form with the learned switch, and the
-    precision form with the plain sensor, on isotropic turbulence n^3."""
-    c = cases.isotropic_turbulence(n, seed=seed, charteric=1)
-    ncell = n ** 3
+    precision form with the plain sensor: isotropic turbulence n^3, or the
+    compression ramp 4n x n x n/2 (IBC 108, the shock filter), where the
+    plain sensor marks most faces for the characteristic WENO schemes."""
+    if workload == "ramp":
+        c = cases.ramp_case(4 * n, n, n // 2, seed=seed)
+    else:
+        c = cases.isotropic_turbulence(n, seed=seed, charteric=1)
+    ncell = c.cfg.nx * c.cfg.ny * c.cfg.nz
     out = {"case": c.description, "steps": steps, "confidence": confidence}
-    ref = lib.Solver(c.cfg, c.prims, c.metrics)
+    ref = lib.Solver(c.cfg, c.prims, c.metrics, inlet=c.inlet)
     ref.step(1)                                   # first launches outside the timing
     t_ref = _timed(ref, steps - 1)
     u_ref, p_ref = ref.conserved(), ref.primitives()
     ref.close()
     runs = {}
     for name, use in (("fp32_plain_sensor", False), ("fp32_learned", True)):
-        s = lib.Solver(c.cfg, c.prims, c.metrics)
+        s = lib.Solver(c.cfg, c.prims, c.metrics, inlet=c.inlet)
         s.set_precision(1)
         if use:
             s.set_switch(params, confidence)
@@ -179,6 +184,7 @@ def evaluate(params: np.ndarray, n: int = 512, steps: int = 100, confidence: flo
              "rel_l2": [float(np.linalg.norm(u[m] - u_ref[m]) / np.linalg.norm(u_ref[m])) for m in range(5)]}
         pres = pr[0] * pr[4]
         r["shock"] = shock_error(p_ref[0] * p_ref[4], pres)
+        r["non_up7_faces"] = [float(np.mean(f != 1)) for f in s.flags()]
         if use:
             sure, unsure, differ = s.switch_stats()
             r["switch"] = {"network_cells": sure, "plain_fallback_cells": unsure, "network_differs_from_plain": differ}
@@ -187,6 +193,7 @@ def evaluate(params: np.ndarray, n: int = 512, steps: int = 100, confidence: flo
     out["fp64_plain"] = {"ms_per_step": t_ref, "gcell_stage_per_s": ncell * 3 / t_ref / 1e6}
     out.update(runs)
     out["speedup_learned_fp32_vs_fp64"] = t_ref / runs["fp32_learned"]["ms_per_step"]
+    out["switch_vs_plain_sensor"] = runs["fp32_plain_sensor"]["ms_per_step"] / runs["fp32_learned"]["ms_per_step"]
     return out
 
 
@@ -202,6 +209,7 @@ def main(argv=None):
     e.add_argument("--n", type=int, default=512)
     e.add_argument("--steps", type=int, default=100)
     e.add_argument("--out", default="")
+    e.add_argument("--workload", choices=("iso", "ramp"), default="iso")
     a = ap.parse_args(argv)
     if a.cmd == "train":
         data = dataset(iso_n=a.iso_n)
@@ -211,7 +219,7 @@ def main(argv=None):
         save(a.out, res["params"], meta)
         print(json.dumps(meta, indent=1))
     else:
-        res = evaluate(load_model(a.model), a.n, a.steps)
+        res = evaluate(load_model(a.model), a.n, a.steps, workload=a.workload)
         txt = json.dumps(res, indent=1)
         if a.out:
             with open(a.out, "w") as f:
