@@ -24,6 +24,7 @@
 #ifndef OCFD_B200_H
 #define OCFD_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -104,16 +105,14 @@ int ocfd_b200_uniform_metrics(const ocfd_b200_ctx *ctx);
  * UP7 walk with its few other cells deferred (the choice is read back once
  * per step, after the sensor); in the precision form the y and z UP7 walks
  * run as per-lane marches over pencil tiles staged in shared memory by the
- * tensor copy engine, each lane keeping its face window in registers; 7 the
- * same as 4 with every UP7 walk through the shared-memory ring; 8 the same
- * as 4 with the y and z marches in FP64 as well (as fast as the ring there);
- * 5 the walk with every face through one
- * in-loop dispatch; 6 the in-line walk alone (characteristic hybrid scheme
- * and WENO7 only); 2 one thread per (face, sign) in tiles
- * with the five characteristic fields in registers, register budget for 4
- * blocks per SM; 3 the same with a budget for 3 blocks; 1 one thread per
- * (face, sign, field).  All agree to the parity bound (WENO weights
- * amplify the different multiply-add contractions). */
+ * tensor copy engine, each lane keeping its face window in registers.
+ * 5: the walk with every face through one in-loop dispatch (the path of the
+ * schemes other than UP7, WENO7 and the hybrid scheme in variant 4 too);
+ * 6: the in-line walk alone (characteristic hybrid scheme and WENO7 only);
+ * 7: as 4 with every UP7 walk through the shared-memory ring; 8: as 4 with
+ * the y and z marches in FP64 as well (as fast as the ring there).  All
+ * agree to the parity bound (WENO weights amplify the different multiply-add
+ * contractions); 4, 7 and 8 agree bit for bit.  Other values: OCFD_ERR_ARG. */
 int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl);
 /* Arithmetic form of the stencils.  0 (default): FP64 throughout, the
  * reference's own arithmetic.  1, the precision form: the Steger-Warming
@@ -133,6 +132,20 @@ int ocfd_b200_set_precision(ocfd_b200_ctx *ctx, int form);
  * 2 (t=1) or any other value (t=2), for the flags the last sensor pass
  * wrote. */
 int ocfd_b200_scheme_proportion(ocfd_b200_ctx *ctx, double frac[9]);
+/* get_Q (src/OCFD_ana.cu:317-456): the Q criterion
+ * Q = (ux vy + ux wz + vy wz - uy vx - uz wx - vz wy) Ajac^2 of the current
+ * primitives, the velocity derivatives by the viscous scheme's central
+ * differences (with the DIF_BOUND closures) through the metrics, into a host
+ * array [nz][ny][nx].  The reference's kernel stores Q at ghost offsets in a
+ * field allocated without ghosts; this is the interior value it computes. */
+int ocfd_b200_q_criterion(ocfd_b200_ctx *ctx, double *q);
+/* init_time_average / ana_time_average (src/OCFD_ana.cu:224-316): reset != 0
+ * zeroes the running means of d, u, v, w, T; reset = 0 adds the current
+ * primitives as one more sample, m = (n m + x) / (n + 1).  get_time_average
+ * copies the means to a host array [5][nz][ny][nx] (mean5 may be NULL) and
+ * the number of samples to *count. */
+int ocfd_b200_time_average(ocfd_b200_ctx *ctx, int reset);
+int ocfd_b200_get_time_average(ocfd_b200_ctx *ctx, double *mean5, int *count);
 /* Learned scheme switch (hybrid scheme).  A 14 -> 32 -> 32 -> 1 ReLU network
  * over normalised pressure and density differences on the sensor's 7-point
  * stencil takes the place of the plain sensor's choice
@@ -282,6 +295,23 @@ int ocfd_b200_bc(ocfd_b200_ctx *ctx);                      /* src/OCFD_boundary.
 int ocfd_b200_slab_unique_id(unsigned char id[OCFD_SLAB_ID_BYTES]);
 int ocfd_b200_set_slab(ocfd_b200_ctx *ctx, int nranks, int rank, int rank_lo, int rank_hi, int z_offset,
                        int nz_global, const unsigned char id[OCFD_SLAB_ID_BYTES]);
+/* The same split with the exchange carried by the caller instead of NCCL,
+ * as the reference carries it through host memory and MPI_Sendrecv
+ * (exchange_boundary_z_packed_dev, src/OCFD_mpi_dev.cu:271-310): a driver
+ * with its own MPI between ranks whose GPUs have no NCCL path, or several
+ * slab processes sharing one GPU (no kernel of one waits on another's).
+ * The library packs the ghost planes, copies them to pinned host memory and
+ * calls fn(user, 0, send, recv, count, type): send holds count elements for
+ * rank_lo (this slab's lowest interior planes) then count for rank_hi (its
+ * highest); fn must fill recv with rank_lo's count (that rank's highest
+ * planes) then rank_hi's (its lowest), pairing the transfers as two
+ * Sendrecv would.  The analysis sums call fn(user, 1, buf, buf, count,
+ * type): sum buf over all ranks in place.  type: 0 FP64, 1 uint64, 2 uint32,
+ * 3 FP32.  fn returns 0 on success.  Whole steps then run launched (no step
+ * graph). */
+typedef int (*ocfd_b200_slab_transport)(void *user, int op, void *send, void *recv, size_t count, int type);
+int ocfd_b200_set_slab_host(ocfd_b200_ctx *ctx, int nranks, int rank, int rank_lo, int rank_hi, int z_offset,
+                            int nz_global, ocfd_b200_slab_transport fn, void *user);
 
 /* Read-back (synchronous). */
 int ocfd_b200_get_primitives(ocfd_b200_ctx *ctx, double *prim5);

@@ -19,6 +19,8 @@
 
 namespace ocfd {
 cudaError_t launch_sensor(const Params &p, cudaStream_t st);
+cudaError_t launch_q_criterion(const Params &p, double *q, cudaStream_t st);
+cudaError_t launch_time_average(const Params &p, double *mean5, int n, cudaStream_t st);
 bool march_tensor_map(const Params &p, const void *base, int elem_bytes, int dir, CUtensorMap *out);
 bool march_supported(const Params &p, int dir);
 cudaError_t march_prepare();
@@ -28,7 +30,6 @@ cudaError_t launch_ghost(const Params &p, double *const *fields, const int *dirm
 cudaError_t launch_ghost32(const Params &p, float *const *fields, const int *dirmask, int nf, cudaStream_t st);
 cudaError_t launch_prims_to_fp32(const Params &p, cudaStream_t st);
 cudaError_t launch_flag_hist(const Params &p, unsigned long long *counts, cudaStream_t st);
-cudaError_t launch_sweeps(const Params &p, cudaStream_t st);
 cudaError_t launch_vis_ev(const Params &p, cudaStream_t st);
 cudaError_t launch_vis_div(const Params &p, int krk, int k0, int k1, cudaStream_t st);
 void ev_ghost_fields(const Params &p, void *fields[12], int dirmask[12]);
@@ -50,9 +51,10 @@ void slab_destroy(Slab *s);
 int slab_exchange(Slab *s, const Params &p, double *const *f, int nf, cudaStream_t st, std::string &err);
 int slab_exchange32(Slab *s, const Params &p, float *const *f, int nf, cudaStream_t st, std::string &err);
 int slab_allreduce(Slab *s, void *buf, size_t count, int type, cudaStream_t st, std::string &err);
+Slab *slab_create_host(const Params &p, int nranks, int rank, int lo, int hi, SlabTransport fn, void *user,
+                       std::string &err);
 int slab_launches_per_exchange();
 int reduce_scratch_doubles();
-cudaError_t launch_sweeps2(const Params &p, cudaStream_t st);
 cudaError_t launch_sweeps3(const Params &p, cudaStream_t st);
 cudaError_t launch_sweeps4(const Params &p, cudaStream_t st);
 bool sweeps4_supported(const Params &p);
@@ -72,7 +74,8 @@ cudaError_t launch_switch_features(const Params &p, long long first, long long c
                                    cudaStream_t st);
 cudaError_t launch_switch_infer(const Params &p, const float *w, float conf_logit, unsigned long long *stats,
                                 cudaStream_t st);
-cudaError_t launch_mlp_infer(const float *w, const float *feat, long long n, float *logit, cudaStream_t st);
+cudaError_t launch_mlp_infer(const float *w, const float *feat, long long n, float *logit, int *err,
+                             cudaStream_t st);
 cudaError_t launch_mlp_grad(const float *w, const float *feat, const float *label, const int *idx, long long n,
                             float pos_w, float *part, float *lpart, float *grad, double *loss, cudaStream_t st);
 cudaError_t launch_mlp_adam(float *w, const float *grad, float *m1, float *m2, float scale, float lr, int t,
@@ -149,6 +152,10 @@ struct ocfd_b200_ctx {
     CUtensorMap tm32[2];
     bool tm64_ok = false, tm32_ok = false;
     bool vdiv_ok = true;        // the staged divergence kernel can be launched
+    // running time averages of d, u, v, w, T (5 interior fields, allocated on
+    // first use) and the number of samples in them
+    double *avg_buf = nullptr;
+    int avg_n = 0;
     int march = 1;
     // the grid split in z across GPUs: this rank's slab starts at global
     // plane z_offset of nz_global; ghost planes in z come from the
@@ -232,6 +239,7 @@ extern "C" const char *ocfd_b200_last_error(const ocfd_b200_ctx *ctx) {
 static void free_all(ocfd_b200_ctx *c) {
     cudaFree(c->prim_buf); cudaFree(c->met_buf); cudaFree(c->cons_buf);
     cudaFree(c->ev_buf); cudaFree(c->flag_buf); cudaFree(c->stage_buf);
+    cudaFree(c->avg_buf);
     cudaFree(c->red_buf); cudaFree(c->defer_buf); cudaFree(c->filter_buf); cudaFree(c->bc_buf);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->h_flag_count) cudaFreeHost(c->h_flag_count);
@@ -416,7 +424,9 @@ static int check_kerr(ocfd_b200_ctx *ctx, int word) {
     if (word == 0) return OCFD_OK;
     int zero = 0;
     cudaMemcpy(ctx->p.kerr, &zero, sizeof(int), cudaMemcpyHostToDevice);
-    return fail(ctx, OCFD_ERR_CUDA, "a sweep kernel gave up waiting for a staged tile (the step's result is invalid)");
+    return fail(ctx, OCFD_ERR_CUDA, word == 2 ? "the learned switch gave up waiting for a tensor-core product "
+                                                 "(the step's result is invalid)"
+                                               : "a kernel gave up waiting for a staged tile (the step's result is invalid)");
 }
 
 extern "C" int ocfd_b200_synchronize(ocfd_b200_ctx *ctx) {
@@ -671,8 +681,6 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk, bool skip_sensor = fal
     }
     {
         TimerScope ts(ctx, T_SWEEP);
-        if (p.has_bnd && p.sweep_impl < 4)
-            return fail(ctx, OCFD_ERR_UNSUPPORTED, "sweep variants 1-3 have no boundary closures (use 4 or 5)");
         if (p.sweep_impl == 6 && !ocfd::sweeps4_supported(p))
             return fail(ctx, OCFD_ERR_UNSUPPORTED, "sweep variant 6 covers the characteristic hybrid scheme and WENO7");
         if (p.mixed || (p.sweep_impl == 4 && ocfd::sweeps4_supported(p))) {
@@ -681,11 +689,9 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk, bool skip_sensor = fal
         } else {            // the other variants launch the three directions together
             int rc = join_z(ctx);
             if (rc) return rc;
-            if (p.sweep_impl == 1)      CK(ocfd::launch_sweeps(p, ctx->stream), "inviscid sweeps");
-            else if (p.sweep_impl == 6) CK(ocfd::launch_sweeps4(p, ctx->stream), "inviscid sweeps");
-            else if (p.sweep_impl >= 4) CK(ocfd::launch_sweeps3(p, ctx->stream), "inviscid sweeps");
-            else                        CK(ocfd::launch_sweeps2(p, ctx->stream), "inviscid sweeps");
-            ctx->launches += p.sweep_impl == 6 ? 3 : (p.sweep_impl >= 4 ? ocfd::sweeps3_kernels(p) : 3);
+            if (p.sweep_impl == 6) CK(ocfd::launch_sweeps4(p, ctx->stream), "inviscid sweeps");
+            else                   CK(ocfd::launch_sweeps3(p, ctx->stream), "inviscid sweeps");
+            ctx->launches += p.sweep_impl == 6 ? 3 : ocfd::sweeps3_kernels(p);
         }
     }
     {
@@ -795,9 +801,9 @@ extern "C" int ocfd_b200_slab_unique_id(unsigned char id[OCFD_SLAB_ID_BYTES]) {
     return OCFD_OK;
 }
 
-extern "C" int ocfd_b200_set_slab(ocfd_b200_ctx *ctx, int nranks, int rank, int rank_lo, int rank_hi, int z_offset,
-                                  int nz_global, const unsigned char id[OCFD_SLAB_ID_BYTES]) {
-    if (!ctx || !id) return OCFD_ERR_ARG;
+static int set_slab_impl(ocfd_b200_ctx *ctx, int nranks, int rank, int rank_lo, int rank_hi, int z_offset,
+                         int nz_global, const unsigned char *id, ocfd::SlabTransport fn, void *user) {
+    if (!ctx || (!id && !fn)) return OCFD_ERR_ARG;
     Params &p = ctx->p;
     if (ctx->slab) return fail(ctx, OCFD_ERR_STATE, "the slab is already set");
     if (ctx->have_metrics || ctx->have_state || ctx->nfilter)
@@ -820,7 +826,8 @@ extern "C" int ocfd_b200_set_slab(ocfd_b200_ctx *ctx, int nranks, int rank, int 
         return fail(ctx, OCFD_ERR_CUDA, "exchange stream");
     }
     std::string err;
-    ctx->slab = ocfd::slab_create(p, nranks, rank, rank_lo, rank_hi, id, err);
+    ctx->slab = fn ? ocfd::slab_create_host(p, nranks, rank, rank_lo, rank_hi, fn, user, err)
+                   : ocfd::slab_create(p, nranks, rank, rank_lo, rank_hi, id, err);
     if (!ctx->slab) return fail(ctx, OCFD_ERR_CUDA, err);
     ctx->z_offset = z_offset;
     ctx->nz_global = nz_global;
@@ -839,6 +846,19 @@ extern "C" int ocfd_b200_set_slab(ocfd_b200_ctx *ctx, int nranks, int rank, int 
     for (int d = 0; d < 3; d++)
         p.has_bnd |= p.bnd_lo[d] | p.bnd_hi[d] | (p.nonref_lo[d] == 1) | (p.nonref_hi[d] == 1);
     return OCFD_OK;
+}
+
+extern "C" int ocfd_b200_set_slab(ocfd_b200_ctx *ctx, int nranks, int rank, int rank_lo, int rank_hi, int z_offset,
+                                  int nz_global, const unsigned char id[OCFD_SLAB_ID_BYTES]) {
+    if (!id) return OCFD_ERR_ARG;
+    return set_slab_impl(ctx, nranks, rank, rank_lo, rank_hi, z_offset, nz_global, id, nullptr, nullptr);
+}
+
+// the same with the caller's host transport in place of NCCL
+extern "C" int ocfd_b200_set_slab_host(ocfd_b200_ctx *ctx, int nranks, int rank, int rank_lo, int rank_hi,
+                                       int z_offset, int nz_global, ocfd_b200_slab_transport fn, void *user) {
+    if (!fn) return OCFD_ERR_ARG;
+    return set_slab_impl(ctx, nranks, rank, rank_lo, rank_hi, z_offset, nz_global, nullptr, fn, user);
 }
 
 extern "C" int ocfd_b200_set_precision(ocfd_b200_ctx *ctx, int form) {
@@ -957,14 +977,22 @@ extern "C" int ocfd_b200_mlp_infer(const float *params, const float *feat, long 
     if (!params || !feat || !logit || n < 0) return OCFD_ERR_ARG;
     if (n == 0) return OCFD_OK;
     const int np = ocfd::mlp_nparam();
-    DevBuf w, f, z;
+    DevBuf w, f, z, err;
     MCK(w.alloc(sizeof(float) * np), "alloc");
     MCK(f.alloc(sizeof(float) * 14 * (size_t)n), "alloc");
     MCK(z.alloc(sizeof(float) * (size_t)n), "alloc");
+    MCK(err.alloc(sizeof(int)), "alloc");
+    MCK(cudaMemset(err.p, 0, sizeof(int)), "memset");
     MCK(cudaMemcpy(w.p, params, sizeof(float) * np, cudaMemcpyHostToDevice), "copy");
     MCK(cudaMemcpy(f.p, feat, sizeof(float) * 14 * (size_t)n, cudaMemcpyHostToDevice), "copy");
-    MCK(ocfd::launch_mlp_infer(w.as<float>(), f.as<float>(), n, z.as<float>(), 0), "mlp_infer");
+    MCK(ocfd::launch_mlp_infer(w.as<float>(), f.as<float>(), n, z.as<float>(), err.as<int>(), 0), "mlp_infer");
     MCK(cudaMemcpy(logit, z.p, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost), "copy");
+    int ew = 0;
+    MCK(cudaMemcpy(&ew, err.p, sizeof(int), cudaMemcpyDeviceToHost), "copy");
+    if (ew) {
+        g_mlp_err = "mlp_infer: a tensor-core product did not complete within the wait limit";
+        return OCFD_ERR_CUDA;
+    }
     return OCFD_OK;
 }
 
@@ -1068,7 +1096,7 @@ extern "C" int ocfd_b200_set_walk_threshold(ocfd_b200_ctx *ctx, double frac) {
 }
 
 extern "C" int ocfd_b200_set_sweep_impl(ocfd_b200_ctx *ctx, int impl) {
-    if (!ctx || impl < 1 || impl > 8) return OCFD_ERR_ARG;
+    if (!ctx || impl < 4 || impl > 8) return OCFD_ERR_ARG;
     ctx->march = impl == 7 ? 0 : (impl == 8 ? 2 : 1);
     ctx->p.sweep_impl = impl >= 7 ? 4 : impl;
     return OCFD_OK;
@@ -1632,6 +1660,58 @@ extern "C" int ocfd_b200_check_state(ocfd_b200_ctx *ctx, long long *n_nan, long 
     if (n_nan) *n_nan = (long long)c[0];
     if (n_neg_t) *n_neg_t = (long long)c[1];
     if (mean_t) *mean_t = host[0];
+    return OCFD_OK;
+}
+
+// get_Q (src/OCFD_ana.cu:317-456) of the current primitives, ghosts filled
+// first; q: host array [nz][ny][nx]
+extern "C" int ocfd_b200_q_criterion(ocfd_b200_ctx *ctx, double *q) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (!q) return fail(ctx, OCFD_ERR_ARG, "null output");
+    if ((rc = refresh_prims64(ctx))) return rc;
+    if ((rc = ghost_prims64(ctx))) return rc;
+    CK(ocfd::launch_q_criterion(ctx->p, ctx->stage_buf, ctx->stream), "Q criterion");
+    ctx->launches += 1;
+    CK(cudaMemcpyAsync(q, ctx->stage_buf, sizeof(double) * (size_t)ctx->p.N, cudaMemcpyDeviceToHost, ctx->stream),
+       "Q read-back");
+    CK(cudaStreamSynchronize(ctx->stream), "Q criterion");
+    return OCFD_OK;
+}
+
+// init_time_average / ana_time_average (src/OCFD_ana.cu:224-316): reset the
+// running means, or add the current primitives as one more sample
+extern "C" int ocfd_b200_time_average(ocfd_b200_ctx *ctx, int reset) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    const size_t bytes = 5 * sizeof(double) * (size_t)ctx->p.N;
+    if (!ctx->avg_buf) {
+        cudaError_t e = cudaMalloc((void **)&ctx->avg_buf, bytes);
+        if (e != cudaSuccess) { ctx->avg_buf = nullptr; cudaGetLastError(); return fail(ctx, OCFD_ERR_NOMEM, "time averages"); }
+        reset = 1;
+    }
+    if (reset) {
+        CK(cudaMemsetAsync(ctx->avg_buf, 0, bytes, ctx->stream), "time averages");
+        ctx->avg_n = 0;
+        return OCFD_OK;
+    }
+    if ((rc = refresh_prims64(ctx))) return rc;
+    CK(ocfd::launch_time_average(ctx->p, ctx->avg_buf, ctx->avg_n, ctx->stream), "time average");
+    ctx->launches += 1;
+    ctx->avg_n += 1;
+    return OCFD_OK;
+}
+
+// the running means of d, u, v, w, T (host [5][nz][ny][nx]) and their sample count
+extern "C" int ocfd_b200_get_time_average(ocfd_b200_ctx *ctx, double *mean5, int *count) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (count) *count = ctx->avg_n;
+    if (!mean5) return OCFD_OK;
+    if (!ctx->avg_buf) return fail(ctx, OCFD_ERR_STATE, "no time averages taken");
+    CK(cudaMemcpyAsync(mean5, ctx->avg_buf, 5 * sizeof(double) * (size_t)ctx->p.N, cudaMemcpyDeviceToHost,
+                       ctx->stream), "time average read-back");
+    CK(cudaStreamSynchronize(ctx->stream), "time average");
     return OCFD_OK;
 }
 

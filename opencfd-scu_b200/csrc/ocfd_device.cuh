@@ -62,7 +62,7 @@ struct Params {
     double mc[13];
     DirConst dc[3];
     double inv_h[3], inv_Ama;   // reciprocals for div_const
-    int sweep_impl;         // 1: per-(face,sign,field) threads; 2, 3: per-(face,sign) threads; 4, 5: warp rings
+    int sweep_impl;         // 4: the walks chosen per direction (default); 5: every face through the in-loop dispatch; 6: the in-line walk
     // viscous divergence + RK of whole steps: 0 Ev tiles staged in shared
     // memory in the precision form, read through L1/L2 in FP64 (each the
     // faster there); 1 read through L1/L2; 2 staged
@@ -92,6 +92,11 @@ struct Params {
     int bc_xbegin, bc_wall_mode;
     double bc_tw, bc_epsl;
 };
+
+// host transport of the z split (ocfd_b200_slab_transport in the C ABI):
+// op 0 swaps the packed ghost planes with the neighbour ranks, op 1 sums a
+// buffer over the ranks in place; type 0 FP64, 1 uint64, 2 uint32, 3 FP32
+typedef int (*SlabTransport)(void *user, int op, void *send, void *recv, size_t count, int type);
 
 enum { M_AXX = 0, M_AYY, M_AZZ, M_AKX, M_AKY, M_AKZ, M_AIX, M_AIY, M_AIZ,
        M_ASX, M_ASY, M_ASZ, M_AJAC };

@@ -4,17 +4,10 @@
 // src/OCFD_Stream.cu:28-54):
 //   [KRK=1, hybrid] sensor        -> int8 face flags            (k_sensor)
 //   ghost fill of d,u,v,w,T        (periodic wrap on device)    (k_ghost_prim)
-//   inviscid x, y, z sweeps        -> du (single writer, fixed order)  (k_sweep<DIR>)
+//   inviscid x, y, z sweeps        -> du (single writer, fixed order)  (ocfd_sweep3/4.cu, ocfd_march.cu)
 //   viscous gradients, Ev, Ev ghosts, divergence -> du         (k_vis_*)
-//   RK stage + cons->prim + face re-projection                 (k_rk_update)
-//
-// Each sweep block owns a tile of TS cells along the sweep direction and R
-// rows across it.  Phase A computes the Steger-Warming split of every tile
-// point once into shared memory; phase B runs one thread per
-// (face, sign, component) -- for characteristic schemes the component is the
-// characteristic field, so the 5x5 projection of the 8-point stencil is a
-// 5-term dot product per thread; phase C forms du of each tile cell from
-// the two neighbouring face fluxes (no atomics).
+//   RK stage + cons->prim + face re-projection                 (fused into k_vis_div / k_vdiv)
+// and the reductions of the analysis after the path.
 #include "ocfd_fp32.cuh"
 #include "ocfd_tma.cuh"
 
@@ -120,230 +113,33 @@ __global__ void k_ghost(Params p, GhostList<T> g) {
     }
 }
 
-// ---------------------------------------------------------------------------
-// inviscid sweep along DIR
-// ---------------------------------------------------------------------------
-template <int DIR> struct SweepShape;
-template <> struct SweepShape<0> { static constexpr int TS = 64, R = 2, THREADS = 128; };
-template <> struct SweepShape<1> { static constexpr int TS = 16, R = 16, THREADS = 256; };
-template <> struct SweepShape<2> { static constexpr int TS = 16, R = 16, THREADS = 256; };
-
-template <int DIR> __device__ __forceinline__ int ndir(const Params &p) { return DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz); }
-template <int DIR> __device__ __forceinline__ int nrow(const Params &p) { return DIR == 0 ? p.ny : p.nx; }
-template <int DIR> __device__ __forceinline__ long long sdir(const Params &p) { return DIR == 0 ? 1LL : (DIR == 1 ? p.ys : p.zs); }
-template <int DIR> __device__ __forceinline__ long long srow(const Params &p) { return DIR == 0 ? p.ys : 1LL; }
-template <int DIR> __device__ __forceinline__ long long s3rd(const Params &p) { return DIR == 2 ? p.ys : p.zs; }
-template <int DIR> __device__ __forceinline__ double hdir(const Params &p) { return DIR == 0 ? p.hx : (DIR == 1 ? p.hy : p.hz); }
-
-// reconstruction of one (face, sign) from the stencil v[0..7] = f(F-3..F+4)
-__device__ __forceinline__ double recon(const Params &p, int scheme, int hflag, int sign, const double *v) {
-    if (sign == 0) {
-        switch (scheme) {
-        case 301: return up7_p(v);
-        case 302: return weno5_p(v);
-        case 303: return weno7_p(v);
-        case 304: return symbo_p(0, p.tv_lim, p.tv_max, v);
-        case 305: return symbo_p(1, p.tv_lim, p.tv_max, v);
-        case 306: return nnd2_p(v);
-        case 307: return omp6_p(0, v);
-        case 308: return omp6_p(1, v);
-        case 309: return omp6_p(2, v);
-        default:  // 310, style 2 (OCFD_HybridAuto_*_Jameson_kernel)
-            if (hflag == 1) return up7_p(v);
-            if (hflag == 2) return weno7_p(v);
-            return weno5_p(v);
-        }
-    } else {
-        switch (scheme) {
-        case 301: return up7_m(v);
-        case 302: return weno5_m(v);
-        case 303: return weno7_m(v);
-        case 304: return symbo_m(0, p.tv_lim, p.tv_max, v);
-        case 305: return symbo_m(1, p.tv_lim, p.tv_max, v);
-        case 306: return nnd2_m(v);
-        case 307: return omp6_m(0, v);
-        case 308: return omp6_m(1, v);
-        case 309: return omp6_m(2, v);
-        default:
-            if (hflag == 1) return up7_m(v);
-            if (hflag == 2) return weno7_m(v);
-            return weno5_m(v);
-        }
+// per-direction constants of a uniform grid, formed on the device with the
+// same code the field path uses (sw_split's |A| and A/|A|, the face basis)
+__global__ void k_dirconst(Params p, DirConst *out) {
+    for (int dd = 0; dd < 3; dd++) {
+        int mA = M_AKX + 3 * dd;
+        double A1 = p.mc[mA], A2 = p.mc[mA + 1], A3 = p.mc[mA + 2];
+        DirConst c;
+        c.A[0] = A1; c.A[1] = A2; c.A[2] = A3;
+        double ss = sqrt(A1 * A1 + A2 * A2 + A3 * A3);
+        c.ss = ss;
+        double inv = 1.0 / ss;
+        c.An[0] = A1 * inv; c.An[1] = A2 * inv; c.An[2] = A3 * inv;
+        CharPara cp;
+        // face average of a constant metric is the constant itself
+        char_para(0.0, 0.0, 0.0, 1.0, (A1 + A1) * 0.5, (A2 + A2) * 0.5, (A3 + A3) * 0.5, p.Gamma, cp);
+        c.n[0] = cp.n1; c.n[1] = cp.n2; c.n[2] = cp.n3;
+        c.l[0] = cp.l1; c.l[1] = cp.l2; c.l[2] = cp.l3;
+        c.m[0] = cp.m1; c.m[1] = cp.m2; c.m[2] = cp.m3;
+        out[dd] = c;
     }
 }
 
-template <int DIR, bool UNI>
-__global__ void __launch_bounds__(SweepShape<DIR>::THREADS)
-k_sweep(Params p) {
-    constexpr int TS = SweepShape<DIR>::TS, R = SweepShape<DIR>::R;
-    constexpr int NP = (TS + 8) * R;      // split points
-    constexpr int NF = (TS + 1) * R;      // faces
-    constexpr int NC = TS * R;            // cells
-    extern __shared__ double smem[];
-    double *spl = smem;                   // [10][NP]: f+ 0..4, f- 5..9
-    double *hat = smem + 10 * NP;         // [10][NF]: sign*5 + comp
-    double *cps = hat + 10 * NF;          // [NCP][NF]: face eigen-system (characteristic schemes)
-
-    const int n = ndir<DIR>(p), nr = nrow<DIR>(p);
-    const int s0 = blockIdx.x * TS;       // first interior cell of the tile (along DIR)
-    const int r0 = blockIdx.y * R;        // first row
-    const int c3 = blockIdx.z;            // third coordinate (interior)
-    const long long sd = sdir<DIR>(p), sr = srow<DIR>(p);
-    const long long base = lap_index(p, 0, 0, 0) + (long long)(c3 + OCFD_LAP) * s3rd<DIR>(p)
-                         + (long long)(r0 + OCFD_LAP) * sr + (long long)(s0) * sd;
-    // base points at LAP coordinate (s0 along DIR), i.e. interior cell s0-4
-    const double *d = p.prim[0], *u = p.prim[1], *v = p.prim[2], *w = p.prim[3], *T = p.prim[4];
-    const int mA = M_AKX + 3 * DIR;
-
-    // ---- phase A: split fluxes at interior-relative points s0-4 .. s0+TS+3
-    for (int q = threadIdx.x; q < NP; q += blockDim.x) {
-        int s, r;
-        if (DIR == 0) { s = q % (TS + 8); r = q / (TS + 8); }
-        else          { r = q % R; s = q / R; }
-        if (r0 + r >= nr || s0 + s - 4 > n + 3) continue;
-        long long o = base + (long long)s * sd + (long long)r * sr;
-        double cc = sqrt(T[o]) / p.Ama;
-        double fp[5], fm[5];
-        sw_split(d[o] * p.tmp0, u[o], v[o], w[o], cc, metric<UNI>(p, mA, o), metric<UNI>(p, mA + 1, o),
-                 metric<UNI>(p, mA + 2, o), p.Gamma, p.epsl_sw, p.split_C1, p.split_C3, fp, fm);
-        int pi = s + (TS + 8) * r;
-#pragma unroll
-        for (int m = 0; m < 5; m++) { spl[m * NP + pi] = fp[m]; spl[(5 + m) * NP + pi] = fm[m]; }
-    }
-
-    const int scheme = p.scheme_invis;
-    const bool char_scheme = p.charteric && (scheme == 304 || scheme == 305 || scheme == 310);
-    const bool comp_none = p.charteric && !char_scheme;   // reference adds nothing
-    const int8_t *flags = p.flag[DIR];
-
-    // ---- phase A2: face-averaged eigen-system, once per face
-    //      (get_para_charteric_{p,m}_kernel, src/OCFD_flux_charteric.cu:321-520)
-    if (char_scheme) {
-        for (int fi = threadIdx.x; fi < NF; fi += blockDim.x) {
-            int fs, r;
-            if (DIR == 0) { fs = fi % (TS + 1); r = fi / (TS + 1); }
-            else          { r = fi % R; fs = fi / R; }
-            int F = s0 - 1 + fs;
-            if (r0 + r >= nr || F > n - 1) continue;
-            long long o0 = base + (long long)(fs + 3) * sd + (long long)r * sr;   // cell F
-            long long o1 = o0 + sd;                                                // cell F+1
-            CharPara cp;
-            double c0v = sqrt(T[o0]) / p.Ama, c1v = sqrt(T[o1]) / p.Ama;
-            char_para((u[o0] + u[o1]) * 0.5, (v[o0] + v[o1]) * 0.5, (w[o0] + w[o1]) * 0.5,
-                      (c0v + c1v) * 0.5,
-                      (metric<UNI>(p, mA, o0) + metric<UNI>(p, mA, o1)) * 0.5,
-                      (metric<UNI>(p, mA + 1, o0) + metric<UNI>(p, mA + 1, o1)) * 0.5,
-                      (metric<UNI>(p, mA + 2, o0) + metric<UNI>(p, mA + 2, o1)) * 0.5, p.Gamma, cp);
-            store_para(cp, cps, fi, NF);
-        }
-    }
-    __syncthreads();
-
-    // ---- phase B1: one thread per (face, sign, component / characteristic)
-    for (int t = threadIdx.x; t < 10 * NF; t += blockDim.x) {
-        int fi = t % NF, rem = t / NF;          // rem = sign*5 + c
-        int sign = rem / 5, c = rem - 5 * sign;
-        int fs, r;
-        if (DIR == 0) { fs = fi % (TS + 1); r = fi / (TS + 1); }
-        else          { r = fi % R; fs = fi / R; }
-        int F = s0 - 1 + fs;                    // face F+1/2, interior-relative
-        if (r0 + r >= nr || F > n - 1) continue;
-        int hflag = 0;
-        if (scheme == 310) {
-            // flag of the face's left cell F (both signs)
-            long long fq;
-            if (DIR == 0)      fq = (long long)(F + 1) + (long long)(p.nx + 1) * ((long long)(r0 + r) + (long long)p.ny * c3);
-            else if (DIR == 1) fq = (long long)(r0 + r) + (long long)p.nx * ((long long)(F + 1) + (long long)(p.ny + 1) * c3);
-            else               fq = (long long)(r0 + r) + (long long)p.nx * ((long long)c3 + (long long)p.ny * (F + 1));
-            hflag = flags[fq];
-        }
-        const double *sp = spl + (sign * 5) * NP + fs + (TS + 8) * r;   // stencil start f(F-3)
-        double vals[8];
-        double res;
-        if (comp_none) {
-            res = 0.0;
-        } else if (char_scheme && !(scheme == 310 && hflag == 1)) {
-            // project the 8-point stencil on characteristic field c
-            CharPara cp;
-            load_para(cp, cps, fi, NF);
-            double Lr[5];
-            char_L_row(cp, c, Lr);
-#pragma unroll
-            for (int k = 0; k < 8; k++)
-                vals[k] = dot5(Lr, sp[k], sp[NP + k], sp[2 * NP + k], sp[3 * NP + k], sp[4 * NP + k]);
-            res = recon(p, scheme, hflag, sign, vals);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 8; k++) vals[k] = sp[c * NP + k];
-            int hf = hflag;
-            if (scheme == 310 && !char_scheme && c > 0 && p.nochar_comp_flag) hf = p.nochar_comp_flag;
-            res = recon(p, scheme, hf, sign, vals);
-        }
-        hat[rem * NF + fi] = res;
-    }
-    __syncthreads();
-
-    // ---- phase B2: back-projection R * F^_char (characteristic faces only)
-    if (char_scheme) {
-        double *outb = spl;   // the split values are no longer needed
-        for (int t = threadIdx.x; t < 10 * NF; t += blockDim.x) {
-            int fi = t % NF, rem = t / NF;
-            int sign = rem / 5, m = rem - 5 * sign;
-            int fs, r;
-            if (DIR == 0) { fs = fi % (TS + 1); r = fi / (TS + 1); }
-            else          { r = fi % R; fs = fi / R; }
-            int F = s0 - 1 + fs;
-            if (r0 + r >= nr || F > n - 1) continue;
-            int hflag = 2;
-            if (scheme == 310) {
-                long long fq;
-                if (DIR == 0)      fq = (long long)(F + 1) + (long long)(p.nx + 1) * ((long long)(r0 + r) + (long long)p.ny * c3);
-                else if (DIR == 1) fq = (long long)(r0 + r) + (long long)p.nx * ((long long)(F + 1) + (long long)(p.ny + 1) * c3);
-                else               fq = (long long)(r0 + r) + (long long)p.nx * ((long long)c3 + (long long)p.ny * (F + 1));
-                hflag = flags[fq];
-            }
-            const double *h = hat + (sign * 5) * NF + fi;
-            double res;
-            if (scheme == 310 && hflag == 1) {
-                res = h[m * NF];
-            } else {
-                CharPara cp;
-                load_para(cp, cps, fi, NF);
-                double Rr[5];
-                char_R_row(cp, m, Rr);
-                res = dot5(Rr, h[0], h[NF], h[2 * NF], h[3 * NF], h[4 * NF]);
-            }
-            outb[rem * NF + fi] = res;
-        }
-        __syncthreads();
-    }
-    const double *fl = char_scheme ? spl : hat;
-
-    // ---- phase C: du of each tile cell (x+ then x- for every component)
-    const double h = hdir<DIR>(p);
-    for (int t = threadIdx.x; t < NC; t += blockDim.x) {
-        int s, r;
-        if (DIR == 0) { s = t % TS; r = t / TS; }
-        else          { r = t % R; s = t / R; }
-        int X = s0 + s;
-        if (r0 + r >= nr || X > n - 1) continue;
-        long long o = base + (long long)(s + 4) * sd + (long long)r * sr;
-        double aj = metric<UNI>(p, M_AJAC, o);
-        int i, j, k;
-        if (DIR == 0)      { i = X; j = r0 + r; k = c3; }
-        else if (DIR == 1) { i = r0 + r; j = X; k = c3; }
-        else               { i = r0 + r; j = c3; k = X; }
-        long long ci = in_index(p, i, j, k);
-        int fr = (DIR == 0) ? (s + 1) + (TS + 1) * r : r + R * (s + 1);
-        int fl_ = (DIR == 0) ? s + (TS + 1) * r : r + R * s;
-#pragma unroll
-        for (int m = 0; m < 5; m++) {
-            double acc = (DIR == 0) ? 0.0 : p.du[m * p.N + ci];
-            acc += -aj * (fl[m * NF + fr] - fl[m * NF + fl_]) / h;
-            acc += -aj * (fl[(5 + m) * NF + fr] - fl[(5 + m) * NF + fl_]) / h;
-            p.du[m * p.N + ci] = acc;
-        }
-    }
+cudaError_t compute_dirconst(Params &p, DirConst *dev_scratch, cudaStream_t st) {
+    k_dirconst<<<1, 1, 0, st>>>(p, dev_scratch);
+    cudaError_t e = cudaMemcpyAsync(p.dc, dev_scratch, sizeof(DirConst) * 3, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(st);
 }
 
 // ---------------------------------------------------------------------------
@@ -970,6 +766,66 @@ k_vev(const __grid_constant__ Params p, const __grid_constant__ CUtensorMap tmq,
     }
 }
 
+// ---------------------------------------------------------------------------
+// analysis after the path (src/OCFD_ana.cu)
+// ---------------------------------------------------------------------------
+
+// get_Q (src/OCFD_ana.cu:317-456): the derivatives of u, v, w along the three
+// grid directions (OCFD_d{x,y,z}0 with the D0_bound closures, as in the Ev
+// kernel), the velocity gradient through the metrics and
+// Q = (ux vy + ux wz + vy wz - uy vx - uz wx - vz wy) Ajac^2, interior cells
+// into q[nz][ny][nx].  The ghosts of u, v, w are the caller's to fill.
+template <bool UNI>
+__global__ void __launch_bounds__(256) k_qcrit(Params p, double *q) {
+    int i, j, k;
+    long long tid;
+    if (!tile_cell(p, i, j, k, tid)) return;
+    const long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+    const bool c8 = p.scheme_vis == 204;
+    const double *U = p.prim[1], *V = p.prim[2], *W = p.prim[3];
+    const double ih[3] = { p.inv_h[0], p.inv_h[1], p.inv_h[2] }, hh[3] = { p.hx, p.hy, p.hz };
+    const long long st[3] = { 1LL, p.ys, p.zs };
+    const int X[3] = { i, j, k }, n[3] = { p.nx, p.ny, p.nz };
+    double g[3][3];                      // g[field][direction]: uk ui us, vk vi vs, wk wi ws
+    const double *F[3] = { U, V, W };
+#pragma unroll
+    for (int m = 0; m < 3; m++)
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+            g[m][d] = p.has_bnd ? d0b(F[m], o, st[d], hh[d], ih[d], c8, X[d], n[d], p.bnd_lo[d], p.bnd_hi[d])
+                                : d0(F[m], o, st[d], hh[d], ih[d], c8);
+    const double Akx = metric<UNI>(p, M_AKX, o), Aix = metric<UNI>(p, M_AIX, o), Asx = metric<UNI>(p, M_ASX, o);
+    const double Aky = metric<UNI>(p, M_AKY, o), Aiy = metric<UNI>(p, M_AIY, o), Asy = metric<UNI>(p, M_ASY, o);
+    const double Akz = metric<UNI>(p, M_AKZ, o), Aiz = metric<UNI>(p, M_AIZ, o), Asz = metric<UNI>(p, M_ASZ, o);
+    const double ux = g[0][0]*Akx + g[0][1]*Aix + g[0][2]*Asx;
+    const double vx = g[1][0]*Akx + g[1][1]*Aix + g[1][2]*Asx;
+    const double wx = g[2][0]*Akx + g[2][1]*Aix + g[2][2]*Asx;
+    const double uy = g[0][0]*Aky + g[0][1]*Aiy + g[0][2]*Asy;
+    const double vy = g[1][0]*Aky + g[1][1]*Aiy + g[1][2]*Asy;
+    const double wy = g[2][0]*Aky + g[2][1]*Aiy + g[2][2]*Asy;
+    const double uz = g[0][0]*Akz + g[0][1]*Aiz + g[0][2]*Asz;
+    const double vz = g[1][0]*Akz + g[1][1]*Aiz + g[1][2]*Asz;
+    const double wz = g[2][0]*Akz + g[2][1]*Aiz + g[2][2]*Asz;
+    const double aj = metric<UNI>(p, M_AJAC, o);
+    q[tid] = (ux*vy + ux*wz + vy*wz - uy*vx - uz*wx - vz*wy) * aj * aj;
+}
+
+// ana_time_average (src/OCFD_ana.cu:238-306): m = (n m + x) / (n + 1) for
+// d, u, v, w, T of every interior cell, n the number of samples so far
+__global__ void k_time_average(Params p, double *mean5, int n) {
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= p.N) return;
+    const int i = (int)(tid % p.nx);
+    const long long r = tid / p.nx;
+    const int j = (int)(r % p.ny), k = (int)(r / p.ny);
+    const long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+        double *a = mean5 + m * p.N + tid;
+        *a = (n * *a + p.prim[m][o]) / (n + 1.);
+    }
+}
+
 // RK stage + cons->prim + face re-projection over the whole grid (du given)
 __global__ void k_rk_update(Params p, int krk) {
     long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1106,26 +962,6 @@ __global__ void k_fill(double *f, long long n, double v) {
 // ---------------------------------------------------------------------------
 static inline unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
-template <int DIR, bool UNI>
-static cudaError_t launch_sweep(const Params &p, cudaStream_t st) {
-    using S = SweepShape<DIR>;
-    constexpr int NP = (S::TS + 8) * S::R, NF = (S::TS + 1) * S::R;
-    const bool chars = p.charteric && (p.scheme_invis == 304 || p.scheme_invis == 305 || p.scheme_invis == 310);
-    size_t smem = sizeof(double) * (10 * NP + 10 * NF + (chars ? NCP * NF : 0));
-    int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
-    int nr = DIR == 0 ? p.ny : p.nx;
-    int n3 = DIR == 2 ? p.ny : p.nz;
-    static size_t attr_bytes = 0;
-    if (smem > attr_bytes) {
-        cudaError_t e = cudaFuncSetAttribute(k_sweep<DIR, UNI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_bytes = smem;
-    }
-    dim3 grid((n + S::TS - 1) / S::TS, (nr + S::R - 1) / S::R, n3);
-    k_sweep<DIR, UNI><<<grid, S::THREADS, smem, st>>>(p);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_sensor(const Params &p, cudaStream_t st) {
     const long long n = (long long)(p.nx + 1) * (p.ny + 1) * (p.nz + 1);
     if (p.flag_count) {
@@ -1153,16 +989,7 @@ cudaError_t launch_ghost32(const Params &p, float *const *fields, const int *dir
     return launch_ghost_t<float>(p, fields, dirmask, nf, st);
 }
 
-template <bool UNI>
-static cudaError_t launch_sweeps_t(const Params &p, cudaStream_t st) {
-    cudaError_t e;
-    if ((e = launch_sweep<0, UNI>(p, st)) != cudaSuccess) return e;
-    if ((e = launch_sweep<1, UNI>(p, st)) != cudaSuccess) return e;
-    return launch_sweep<2, UNI>(p, st);
-}
-cudaError_t launch_sweeps(const Params &p, cudaStream_t st) {
-    return p.uniform_metrics ? launch_sweeps_t<true>(p, st) : launch_sweeps_t<false>(p, st);
-}
+
 
 template <typename R>
 static cudaError_t launch_vis_ev_t(const Params &p, cudaStream_t st) {
@@ -1334,6 +1161,18 @@ void ev_ghost_fields(const Params &p, void *fields[12], int dirmask[12]) {
             fields[4 * dd + m] = evb + (size_t)(4 * dd + m) * (size_t)p.lapN * es;
             dirmask[4 * dd + m] = 1 << dd;
         }
+}
+
+cudaError_t launch_q_criterion(const Params &p, double *q, cudaStream_t st) {
+    const dim3 nb((unsigned)(((p.nx + VT_X - 1) / VT_X) * ((p.ny + VT_Y - 1) / VT_Y)), (unsigned)p.nz);
+    if (p.uniform_metrics) k_qcrit<true><<<nb, 256, 0, st>>>(p, q);
+    else                   k_qcrit<false><<<nb, 256, 0, st>>>(p, q);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_time_average(const Params &p, double *mean5, int n, cudaStream_t st) {
+    k_time_average<<<blocks_for(p.N, 256), 256, 0, st>>>(p, mean5, n);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_rk(const Params &p, int krk, cudaStream_t st) {

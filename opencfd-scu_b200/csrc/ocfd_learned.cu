@@ -17,15 +17,17 @@
 //
 // Network: 14 -> 32 -> 32 -> 1 with ReLU, inputs standardised by (mu,
 // sigma); parameter vector mu[14] sigma[14] W1[32][14] b1[32] W2[32][32]
-// b2[32] W3[32] b3.  Inference runs the two hidden layers on the tensor
-// cores (mma.sync m16n8k16, BF16 operands, FP32 accumulation), one warp per
-// 32 cells; the output layer is an FP32 dot product.  A cell whose
+// b2[32] W3[32] b3.  Inference runs the two hidden layers as tcgen05
+// products of 128 cells (one block) at a time: BF16 operands in shared
+// memory, FP32 accumulators in tensor memory, issued by one thread; the
+// output layer is an FP32 dot product.  A cell whose
 // confidence max(s, 1-s), s = sigmoid(logit), is below the threshold keeps
 // the plain flag; otherwise flag 1 for s < 1/2 and max(2, plain flag) for
 // s >= 1/2.  Training runs in FP32: per-block forward and backward passes
 // with the activations in shared memory, a fixed-order reduction of the
 // block gradients, and Adam.
 #include "ocfd_fp32.cuh"
+#include "ocfd_tma.cuh"
 
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -102,154 +104,235 @@ __global__ void k_switch_features(Params p, long long first, long long count, fl
 }
 
 // ---------------------------------------------------------------------------
-// tensor-core MLP of one warp: 32 rows of standardised features in, 32
-// logits out (lane L gets row L)
+// tensor-core MLP of one block (tcgen05): 128 rows of standardised features
+// in, 128 logits out, thread t holding row t.  The block's features are
+// written as the A operand of the first product in shared memory, one
+// thread issues tcgen05.mma into a 128 x 32 FP32 accumulator in tensor
+// memory (TMEM lane t = row t), each warp reads its 32 lanes back with
+// tcgen05.ld, and the ReLU'd hidden layer goes back to shared memory as the
+// A operand of the second product (two K = 16 steps).  The weights sit in
+// shared memory as the B operands for the whole launch.
 // ---------------------------------------------------------------------------
+namespace umma {
+
+constexpr int ROWS = 128;             // rows per product: the MMA's M, one TMEM lane each
+constexpr unsigned TMEM_COLS = 32;    // the accumulator's columns (N = 32, FP32)
+// kind::f16 instruction descriptor: D FP32 (bits 4-5 = 1), A and B BF16
+// (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at
+// bits 17-22, M >> 4 at bits 24-28
+constexpr unsigned IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(MLP_H >> 3) << 17) |
+                           ((unsigned)(ROWS >> 4) << 24);
+
+// Element offset of (row, k) in a K-major BF16 operand of K = 16 without
+// swizzling: core matrices of 8 rows x 8 elements (128 contiguous bytes,
+// 16 per row), the two K halves of an 8-row group 128 B apart (the
+// descriptor's leading byte offset), 8-row groups 256 B apart (its stride
+// byte offset).
+__host__ __device__ constexpr int cm(int row, int k) {
+    return (row >> 3) * 128 + (k >> 3) * 64 + (row & 7) * 8 + (k & 7);
+}
+constexpr unsigned LBO = 128, SBO = 256;
+
+struct __align__(128) Smem {
+    __nv_bfloat16 w1[MLP_H * 16];         // B of layer 1: row n = W1[n][0..13], 0, 0
+    __nv_bfloat16 w2[2][MLP_H * 16];      // B of layer 2, K steps 0..15 and 16..31
+    __nv_bfloat16 a1[ROWS * 16];          // A of layer 1: the standardised features
+    __nv_bfloat16 a2[2][ROWS * 16];       // A of layer 2: the hidden layer, K steps
+    float b1[MLP_H], b2[MLP_H], w3[MLP_H], mu[16], isg[16];
+    unsigned long long bar;               // completion of the block's products
+    float b3;
+    unsigned tmem;                        // TMEM address of the accumulator
+};
+static_assert(sizeof(Smem) < 16384, "one block's shared memory");
+
+// shared-memory matrix descriptor: start address, leading and stride byte
+// offsets (all >> 4), version 1 (bits 46-47), no swizzle (bits 61-63 = 0)
+__device__ __forceinline__ unsigned long long desc(const void *ptr) {
+    const unsigned a = tma::smem_u32(ptr);
+    return (unsigned long long)((a >> 4) & 0x3FFFu) | ((unsigned long long)(LBO >> 4) << 16) |
+           ((unsigned long long)(SBO >> 4) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// D (+)= A B over K = 16, issued by one thread
+__device__ __forceinline__ void mma(unsigned tmem_d, unsigned long long a, unsigned long long b, bool accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(IDESC), "r"((unsigned)accumulate)
+        : "memory");
+}
+// one arrival on bar once the products this thread issued are complete
+__device__ __forceinline__ void commit(unsigned long long *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     tma::smem_u32(bar))
+                 : "memory");
+}
+// this warp's 32 lanes x 32 columns of the accumulator (thread = lane = row)
+__device__ __forceinline__ void load_row(unsigned taddr, float (&v)[32]) {
+    unsigned r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int c = 0; c < 32; c++) v[c] = __uint_as_float(r[c]);
+}
+
 __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<unsigned *>(&v);
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
-    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-                 "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+// The block's set-up: weights into shared memory as B operands, the
+// standardisation constants, the mbarrier, and 32 TMEM columns (warp 0).
+// Every thread of the 128-thread block calls it.
+__device__ void setup(Smem &s, const float *__restrict__ w) {
+    const int t = threadIdx.x;
+    for (int q = t; q < MLP_H * 16; q += ROWS) {          // B[k][n] = W1[n][k]
+        const int n = q >> 4, k = q & 15;
+        s.w1[cm(n, k)] = __float2bfloat16_rn(k < MLP_IN ? w[OFF_W1 + n * MLP_IN + k] : 0.0f);
+    }
+    for (int q = t; q < MLP_H * MLP_H; q += ROWS) {       // B[k][n] = W2[n][k]
+        const int n = q >> 5, k = q & 31;
+        s.w2[k >> 4][cm(n, k & 15)] = __float2bfloat16_rn(w[OFF_W2 + n * MLP_H + k]);
+    }
+    if (t < MLP_H) { s.b1[t] = w[OFF_B1 + t]; s.b2[t] = w[OFF_B2 + t]; s.w3[t] = w[OFF_W3 + t]; }
+    if (t < 16) {
+        s.mu[t] = t < MLP_IN ? w[OFF_MU + t] : 0.0f;
+        s.isg[t] = t < MLP_IN ? 1.0f / w[OFF_SG + t] : 0.0f;
+    }
+    if (t == 0) {
+        s.b3 = w[OFF_B3];
+        tma::mbar_init(&s.bar, 1);
+        tma::fence_mbar_init();
+    }
+    if (t < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         tma::smem_u32(&s.tmem)), "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    before_sync();
+    __syncthreads();
+    after_sync();
 }
 
-// one lane's share of the network for the tensor-core products: B operands
-// of layer 1 (n-tiles 0..3) and layer 2 (n-tiles 0..3, k-steps 0..1) as
-// BF16 pairs, and the biases / output weights of its accumulator columns
-struct MlpFrag {
-    unsigned w1[4][2], w2[4][2][2];
-    float b1[4][2], b2[4][2], w3[4][2], b3;
-};
+// The block's teardown: a product still outstanding after a wait ran out is
+// waited for once more (bounded), then warp 0 frees the TMEM columns.
+__device__ void teardown(Smem &s, bool good, unsigned phase) {
+    if (!__syncthreads_and(good) && threadIdx.x == 0) tma::mbar_wait(&s.bar, phase);
+    before_sync();
+    __syncthreads();
+    after_sync();
+    if (threadIdx.x < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s.tmem), "r"(TMEM_COLS)
+                     : "memory");
+}
 
-__device__ __forceinline__ void load_frags(const float *__restrict__ w, MlpFrag &fr) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+// The network on the block's 128 rows.  x: this thread's standardised
+// features.  good: this thread's last wait completed; phase: the mbarrier
+// parity to wait for next.  Returns false for every thread of the block
+// once a wait has run out (the block then stops), else this row's logit in z.
+__device__ bool mlp(Smem &s, const float (&x)[MLP_IN], bool &good, unsigned &phase, float &z) {
+    const int t = threadIdx.x;
+    const unsigned trow = s.tmem + ((unsigned)(t & ~31) << 16);    // this warp's TMEM lanes
+    uint4 c0, c1;
+    c0.x = pack_bf16(x[0], x[1]);   c0.y = pack_bf16(x[2], x[3]);
+    c0.z = pack_bf16(x[4], x[5]);   c0.w = pack_bf16(x[6], x[7]);
+    c1.x = pack_bf16(x[8], x[9]);   c1.y = pack_bf16(x[10], x[11]);
+    c1.z = pack_bf16(x[12], x[13]); c1.w = 0u;
+    *reinterpret_cast<uint4 *>(s.a1 + cm(t, 0)) = c0;
+    *reinterpret_cast<uint4 *>(s.a1 + cm(t, 8)) = c1;
+    fence_async_smem();
+    before_sync();
+    if (!__syncthreads_and(good)) return false;
+    after_sync();
+    // layer 1: Z1 = X W1^T
+    if (t == 0) {
+        mma(s.tmem, desc(s.a1), desc(s.w1), false);
+        commit(&s.bar);
+    }
+    good = tma::mbar_wait(&s.bar, phase);
+    phase ^= 1u;
+    after_sync();
+    float v[32];
+    load_row(trow, v);
+    // ReLU(Z1 + b1) as BF16, hidden units 0..15 into K step 0, 16..31 into step 1
 #pragma unroll
-    for (int nt = 0; nt < 4; nt++) {
-        const int n = nt * 8 + g;
-        const float *W1 = w + OFF_W1 + n * MLP_IN;
-        fr.w1[nt][0] = pack_bf16(W1[2 * t], W1[2 * t + 1]);
-        fr.w1[nt][1] = 2 * t + 8 < MLP_IN ? pack_bf16(W1[2 * t + 8], W1[2 * t + 9]) : 0u;
-        const float *W2 = w + OFF_W2 + n * MLP_H;
-#pragma unroll
-        for (int kk = 0; kk < 2; kk++) {
-            fr.w2[nt][kk][0] = pack_bf16(W2[kk * 16 + 2 * t], W2[kk * 16 + 2 * t + 1]);
-            fr.w2[nt][kk][1] = pack_bf16(W2[kk * 16 + 2 * t + 8], W2[kk * 16 + 2 * t + 9]);
-        }
+    for (int ks = 0; ks < 2; ks++)
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            fr.b1[nt][h] = w[OFF_B1 + nt * 8 + 2 * t + h];
-            fr.b2[nt][h] = w[OFF_B2 + nt * 8 + 2 * t + h];
-            fr.w3[nt][h] = w[OFF_W3 + nt * 8 + 2 * t + h];
+            const int u = ks * 16 + h * 8;
+            uint4 c;
+            c.x = pack_bf16(fmaxf(v[u + 0] + s.b1[u + 0], 0.0f), fmaxf(v[u + 1] + s.b1[u + 1], 0.0f));
+            c.y = pack_bf16(fmaxf(v[u + 2] + s.b1[u + 2], 0.0f), fmaxf(v[u + 3] + s.b1[u + 3], 0.0f));
+            c.z = pack_bf16(fmaxf(v[u + 4] + s.b1[u + 4], 0.0f), fmaxf(v[u + 5] + s.b1[u + 5], 0.0f));
+            c.w = pack_bf16(fmaxf(v[u + 6] + s.b1[u + 6], 0.0f), fmaxf(v[u + 7] + s.b1[u + 7], 0.0f));
+            *reinterpret_cast<uint4 *>(s.a2[ks] + cm(t, h * 8)) = c;
         }
+    fence_async_smem();
+    before_sync();
+    if (!__syncthreads_and(good)) return false;
+    after_sync();
+    // layer 2: Z2 = H W2^T over two K steps
+    if (t == 0) {
+        mma(s.tmem, desc(s.a2[0]), desc(s.w2[0]), false);
+        mma(s.tmem, desc(s.a2[1]), desc(s.w2[1]), true);
+        commit(&s.bar);
     }
-    fr.b3 = w[OFF_B3];
+    good = tma::mbar_wait(&s.bar, phase);
+    phase ^= 1u;
+    after_sync();
+    load_row(trow, v);
+    // output layer in FP32
+    float acc = s.b3;
+#pragma unroll
+    for (int c = 0; c < 32; c++) acc += fmaxf(v[c] + s.b2[c], 0.0f) * s.w3[c];
+    z = acc;
+    return true;
 }
 
-// x: this lane's 14 standardised features; sA: 32 x 16 bf16 (one warp's
-// staging), sL: 32 floats; returns this lane's logit
-__device__ __forceinline__ float warp_mlp(const MlpFrag &fr, const float (&x)[MLP_IN],
-                                          __nv_bfloat16 *sA, float *sL) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    __syncwarp();                       // the previous tile's reads of sA / sL are done
-#pragma unroll
-    for (int m = 0; m < 16; m += 2) {
-        const unsigned v = pack_bf16(m < MLP_IN ? x[m] : 0.0f, m + 1 < MLP_IN ? x[m + 1] : 0.0f);
-        *reinterpret_cast<unsigned *>(sA + lane * 16 + m) = v;
-    }
-    __syncwarp();
-    // layer 1: Z1 (32 x 32) = X (32 x 16) W1^T + b1; B[k][n] = W1[n][k]
-    float z1[2][4][4];
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++) {
-        const __nv_bfloat16 *row0 = sA + (mt * 16 + g) * 16, *row1 = sA + (mt * 16 + g + 8) * 16;
-        unsigned a[4];
-        a[0] = *reinterpret_cast<const unsigned *>(row0 + 2 * t);
-        a[1] = *reinterpret_cast<const unsigned *>(row1 + 2 * t);
-        a[2] = *reinterpret_cast<const unsigned *>(row0 + 2 * t + 8);
-        a[3] = *reinterpret_cast<const unsigned *>(row1 + 2 * t + 8);
-#pragma unroll
-        for (int nt = 0; nt < 4; nt++) {
-            z1[mt][nt][0] = fr.b1[nt][0]; z1[mt][nt][1] = fr.b1[nt][1];
-            z1[mt][nt][2] = fr.b1[nt][0]; z1[mt][nt][3] = fr.b1[nt][1];
-            mma_bf16(z1[mt][nt], a, fr.w1[nt][0], fr.w1[nt][1]);
-        }
-    }
-    // ReLU; the accumulator tiles of n-tiles 2kk and 2kk+1 are the A operand
-    // of k-step kk of layer 2
-    unsigned a2[2][2][4];
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-        for (int kk = 0; kk < 2; kk++) {
-            const float *lo = z1[mt][2 * kk], *hi = z1[mt][2 * kk + 1];
-            a2[mt][kk][0] = pack_bf16(fmaxf(lo[0], 0.0f), fmaxf(lo[1], 0.0f));
-            a2[mt][kk][1] = pack_bf16(fmaxf(lo[2], 0.0f), fmaxf(lo[3], 0.0f));
-            a2[mt][kk][2] = pack_bf16(fmaxf(hi[0], 0.0f), fmaxf(hi[1], 0.0f));
-            a2[mt][kk][3] = pack_bf16(fmaxf(hi[2], 0.0f), fmaxf(hi[3], 0.0f));
-        }
-    // layer 2 and the output layer's partial dot products
-    float part[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};     // [m-tile][row g / g+8]
-#pragma unroll
-    for (int nt = 0; nt < 4; nt++) {
-#pragma unroll
-        for (int mt = 0; mt < 2; mt++) {
-            float z[4] = {fr.b2[nt][0], fr.b2[nt][1], fr.b2[nt][0], fr.b2[nt][1]};
-            mma_bf16(z, a2[mt][0], fr.w2[nt][0][0], fr.w2[nt][0][1]);
-            mma_bf16(z, a2[mt][1], fr.w2[nt][1][0], fr.w2[nt][1][1]);
-            part[mt][0] += fmaxf(z[0], 0.0f) * fr.w3[nt][0] + fmaxf(z[1], 0.0f) * fr.w3[nt][1];
-            part[mt][1] += fmaxf(z[2], 0.0f) * fr.w3[nt][0] + fmaxf(z[3], 0.0f) * fr.w3[nt][1];
-        }
-    }
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            float v = part[mt][h];
-            v += __shfl_xor_sync(0xffffffffu, v, 1);
-            v += __shfl_xor_sync(0xffffffffu, v, 2);
-            if (t == 0) sL[mt * 16 + h * 8 + g] = v;
-        }
-    __syncwarp();
-    return sL[lane] + fr.b3;
-}
+}  // namespace umma
 
 // (f - mu) / sigma, as a product with the block's reciprocals of sigma
-__device__ __forceinline__ void standardise(const float *mu, const float *isg, const float (&f)[MLP_IN],
-                                            float (&x)[MLP_IN]) {
+__device__ __forceinline__ void standardise(const umma::Smem &s, const float (&f)[MLP_IN], float (&x)[MLP_IN]) {
 #pragma unroll
-    for (int m = 0; m < MLP_IN; m++) x[m] = (f[m] - mu[m]) * isg[m];
+    for (int m = 0; m < MLP_IN; m++) x[m] = (f[m] - s.mu[m]) * s.isg[m];
 }
 
-// the block's copy of the standardisation constants (mu, 1 / sigma)
-__device__ __forceinline__ void load_standard(const float *__restrict__ w, float *sMu, float *sIsg) {
-    if (threadIdx.x < MLP_IN) { sMu[threadIdx.x] = w[OFF_MU + threadIdx.x]; sIsg[threadIdx.x] = 1.0f / w[OFF_SG + threadIdx.x]; }
-    __syncthreads();
-}
-
-// logits of n raw feature rows (the network alone, for checks); each warp
-// loads its weight fragments once and walks 32-row tiles
-__global__ void __launch_bounds__(128) k_mlp_infer(const float *__restrict__ w, const float *__restrict__ feat,
-                                                   long long n, float *logit) {
-    __shared__ __align__(16) __nv_bfloat16 sA[4][32 * 16];
-    __shared__ float sL[4][32], sMu[MLP_IN], sIsg[MLP_IN];
-    load_standard(w, sMu, sIsg);
-    MlpFrag fr;
-    load_frags(w, fr);
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long ntile = (n + 31) / 32, nw = (long long)gridDim.x * 4;
-    for (long long tile = (long long)blockIdx.x * 4 + wid; tile < ntile; tile += nw) {
-        const long long row = tile * 32 + lane;
+// Logits of n raw feature rows (the network alone, for checks): persistent
+// blocks of 128 threads over 128-row tiles.  err: set when a wait ran out.
+__global__ void __launch_bounds__(umma::ROWS) k_mlp_infer(const float *__restrict__ w, const float *__restrict__ feat,
+                                                          long long n, float *logit, int *err) {
+    __shared__ umma::Smem s;
+    umma::setup(s, w);
+    bool good = true;
+    unsigned phase = 0;
+    const long long ntile = (n + umma::ROWS - 1) / umma::ROWS;
+    for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+        const long long row = tile * umma::ROWS + threadIdx.x;
         float f[MLP_IN], x[MLP_IN];
 #pragma unroll
         for (int m = 0; m < MLP_IN; m++) f[m] = row < n ? feat[row * MLP_IN + m] : 0.0f;
-        standardise(sMu, sIsg, f, x);
-        const float z = warp_mlp(fr, x, sA[wid], sL[wid]);
+        standardise(s, f, x);
+        float z;
+        if (!umma::mlp(s, x, good, phase, z)) break;
         if (row < n) logit[row] = z;
     }
+    if (!good) atomicExch(err, 2);
+    umma::teardown(s, good, phase);
 }
 
 // The learned switch over the extended box: cell (i, j, k), each of -1 ..
@@ -257,22 +340,22 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const float *__restrict__ w, 
 // the y array and entry k+1 of the z array.  conf_logit = ln(c / (1 - c))
 // for confidence threshold c.  stats (optional): cells decided by the
 // network, cells left to the plain flag, network flags that differ from the
-// plain flag.
+// plain flag.  Persistent blocks of 128 cells per tile, consecutive cells
+// along x on consecutive threads.
 template <typename R>
-__global__ void __launch_bounds__(128) k_switch_infer(Params p, const float *__restrict__ w, float conf_logit,
-                                                      unsigned long long *stats) {
-    __shared__ __align__(16) __nv_bfloat16 sA[4][32 * 16];
-    __shared__ float sL[4][32], sMu[MLP_IN], sIsg[MLP_IN];
-    load_standard(w, sMu, sIsg);
-    MlpFrag fr;
-    load_frags(w, fr);
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(umma::ROWS) k_switch_infer(Params p, const float *__restrict__ w, float conf_logit,
+                                                             unsigned long long *stats) {
+    __shared__ umma::Smem s;
+    umma::setup(s, w);
+    const int lane = threadIdx.x & 31;
     const long long ex = p.nx + 1, ey = p.ny + 1, ez = p.nz + 1, total = ex * ey * ez;
-    const long long ntile = (total + 31) / 32, nw = (long long)gridDim.x * 4;
+    const long long ntile = (total + umma::ROWS - 1) / umma::ROWS;
     const long long om[3] = {-1LL, -p.ys, -p.zs}, op[3] = {1LL, p.ys, p.zs};
     unsigned long long n_sure = 0, n_unsure = 0, n_differ = 0;
-    for (long long tile = (long long)blockIdx.x * 4 + wid; tile < ntile; tile += nw) {
-        const long long tid = tile * 32 + lane;
+    bool good = true;
+    unsigned phase = 0;
+    for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+        const long long tid = tile * umma::ROWS + threadIdx.x;
         const bool live = tid < total;
         int i = 0, j = 0, k = 0;
         float f[MLP_IN] = {};
@@ -284,8 +367,9 @@ __global__ void __launch_bounds__(128) k_switch_infer(Params p, const float *__r
             switch_features<R>(p, lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP), om, op, f, dp);
         }
         float x[MLP_IN];
-        standardise(sMu, sIsg, f, x);
-        const float z = warp_mlp(fr, x, sA[wid], sL[wid]);
+        standardise(s, f, x);
+        float z;
+        if (!umma::mlp(s, x, good, phase, z)) break;
         const int plain = plain_flag(p, dp);
         const bool sure = fabsf(z) >= conf_logit;
         const int kp = sure ? (z >= 0.0f ? max(2, plain) : 1) : plain;
@@ -314,6 +398,8 @@ __global__ void __launch_bounds__(128) k_switch_infer(Params p, const float *__r
         atomicAdd(stats + 1, n_unsure);
         atomicAdd(stats + 2, n_differ);
     }
+    if (!good && p.kerr) atomicExch(p.kerr, 2);
+    umma::teardown(s, good, phase);
 }
 
 // ---------------------------------------------------------------------------
@@ -443,24 +529,36 @@ cudaError_t launch_switch_features(const Params &p, long long first, long long c
     return cudaGetLastError();
 }
 
+// persistent blocks: as many as are resident at once, at most one per tile
+template <typename K>
+static unsigned resident_blocks(K kern, long long tiles) {
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, umma::ROWS, 0) != cudaSuccess || per < 1) {
+        cudaGetLastError();
+        per = 1;
+    }
+    const long long nb = (long long)sms * per;
+    return (unsigned)(tiles < nb ? tiles : nb);
+}
+
 cudaError_t launch_switch_infer(const Params &p, const float *w, float conf_logit, unsigned long long *stats,
                                 cudaStream_t st) {
     if (p.flag_count) {
         cudaError_t e = cudaMemsetAsync(p.flag_count, 0, 3 * sizeof(unsigned), st);
         if (e != cudaSuccess) return e;
     }
-    // persistent warps: a few resident blocks per SM, each warp over many tiles
     const long long n = (long long)(p.nx + 1) * (p.ny + 1) * (p.nz + 1);
-    const long long need = (n + 127) / 128;
-    const unsigned nb = (unsigned)(need < 148 * 4 ? need : 148 * 4);
-    if (p.mixed) k_switch_infer<float><<<nb, 128, 0, st>>>(p, w, conf_logit, stats);
-    else         k_switch_infer<double><<<nb, 128, 0, st>>>(p, w, conf_logit, stats);
+    const long long tiles = (n + umma::ROWS - 1) / umma::ROWS;
+    if (p.mixed) k_switch_infer<float><<<resident_blocks(k_switch_infer<float>, tiles), umma::ROWS, 0, st>>>(p, w, conf_logit, stats);
+    else         k_switch_infer<double><<<resident_blocks(k_switch_infer<double>, tiles), umma::ROWS, 0, st>>>(p, w, conf_logit, stats);
     return cudaGetLastError();
 }
 
-cudaError_t launch_mlp_infer(const float *w, const float *feat, long long n, float *logit, cudaStream_t st) {
-    const long long need = (n + 127) / 128;
-    k_mlp_infer<<<(unsigned)(need < 148 * 8 ? need : 148 * 8), 128, 0, st>>>(w, feat, n, logit);
+cudaError_t launch_mlp_infer(const float *w, const float *feat, long long n, float *logit, int *err, cudaStream_t st) {
+    const long long tiles = (n + umma::ROWS - 1) / umma::ROWS;
+    k_mlp_infer<<<resident_blocks(k_mlp_infer, tiles), umma::ROWS, 0, st>>>(w, feat, n, logit, err);
     return cudaGetLastError();
 }
 

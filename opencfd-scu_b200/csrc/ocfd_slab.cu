@@ -14,7 +14,11 @@
 //
 // NCCL is opened at run time (dlopen of libnccl.so.2; in a process that has
 // imported torch this is torch's own copy), so the library loads and runs
-// single-GPU without it.  The reductions of the analysis step
+// single-GPU without it.  A host transport can stand in for NCCL
+// (ocfd_b200_set_slab_host): the packed planes then go through pinned host
+// memory and a caller's function, as the reference's MPI_Sendrecv does --
+// for ranks without NCCL between their GPUs, and for tests that run several
+// slabs on one GPU (each process's kernels then never wait on another's).  The reductions of the analysis step
 // (ana_residual, src/OCFD_ana.cu:76-105, an MPI_Allreduce there) go through
 // the same communicator.
 #include "ocfd_device.cuh"
@@ -130,6 +134,11 @@ struct Slab {
     int nranks = 1, rank = 0, lo = 0, hi = 0;
     unsigned char *buf = nullptr;   // send (2 sides) then receive (2 sides)
     size_t side_bytes = 0;          // MAXF FP64 fields x L planes
+    // host transport (instead of NCCL): the caller's function and its
+    // pinned staging copy of buf
+    SlabTransport fn = nullptr;
+    void *user = nullptr;
+    unsigned char *hbuf = nullptr;
 };
 
 int slab_unique_id(unsigned char id[128], std::string &err) {
@@ -169,11 +178,45 @@ Slab *slab_create(const Params &p, int nranks, int rank, int lo, int hi, const u
     return s;
 }
 
+Slab *slab_create_host(const Params &p, int nranks, int rank, int lo, int hi, SlabTransport fn, void *user,
+                       std::string &err) {
+    Slab *s = new Slab();
+    s->nranks = nranks; s->rank = rank; s->lo = lo; s->hi = hi;
+    s->fn = fn; s->user = user;
+    s->side_bytes = sizeof(double) * (size_t)MAXF * OCFD_LAP * (size_t)p.nx * p.ny;
+    cudaError_t e = cudaMalloc(&s->buf, 4 * s->side_bytes);
+    if (e == cudaSuccess) e = cudaHostAlloc((void **)&s->hbuf, 4 * s->side_bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        err = std::string("slab exchange buffers: ") + cudaGetErrorString(e);
+        cudaFree(s->buf);
+        delete s;
+        return nullptr;
+    }
+    return s;
+}
+
 void slab_destroy(Slab *s) {
     if (!s) return;
     if (s->comm) nccl().CommDestroy(s->comm);
     cudaFree(s->buf);
+    if (s->hbuf) cudaFreeHost(s->hbuf);
     delete s;
+}
+
+// the packed planes (or a reduction buffer) through the host transport:
+// device -> pinned host, the caller's function, pinned host -> device
+static int host_round_trip(Slab *s, int op, const void *dsend, void *drecv, size_t count, size_t elem, int type,
+                           cudaStream_t st, std::string &err) {
+    const size_t nsend = (op == 0 ? 2 : 1) * count * elem;
+    unsigned char *hs = s->hbuf, *hr = op == 0 ? s->hbuf + 2 * s->side_bytes : s->hbuf;
+    cudaError_t e = cudaMemcpyAsync(hs, dsend, nsend, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) { err = std::string("host transport staging: ") + cudaGetErrorString(e); return -1; }
+    if (s->fn(s->user, op, hs, hr, count, type) != 0) { err = "host transport: the caller's function failed"; return -1; }
+    e = cudaMemcpyAsync(drecv, hr, nsend, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) { err = std::string("host transport staging: ") + cudaGetErrorString(e); return -1; }
+    return 0;
 }
 
 template <typename T>
@@ -197,6 +240,13 @@ static int exchange_t(Slab *s, const Params &p, T *const *f, int nf, cudaStream_
     // that neighbour's first receive from below, and the same for the
     // second pair, also when both neighbours are one rank (2 slabs) or this
     // rank itself (1 slab: the periodic wrap)
+    if (s->fn) {
+        if (host_round_trip(s, 0, send, recv, count, sizeof(T), sizeof(T) == 8 ? 0 : 3, st, err)) return -1;
+        k_halo_unpack<T><<<nb, 256, 0, st>>>(p, g, recv);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) { err = std::string("halo unpack: ") + cudaGetErrorString(e); return -1; }
+        return 0;
+    }
     ncclResult_t r = a.GroupStart();
     if (r == ncclSuccess) r = a.Send(send + count, count, nccl_type<T>(), s->hi, s->comm, st);
     if (r == ncclSuccess) r = a.Send(send, count, nccl_type<T>(), s->lo, s->comm, st);
@@ -221,6 +271,11 @@ int slab_exchange32(Slab *s, const Params &p, float *const *f, int nf, cudaStrea
 
 // in-place sum over the ranks; type 0 FP64, 1 uint64, 2 uint32
 int slab_allreduce(Slab *s, void *buf, size_t count, int type, cudaStream_t st, std::string &err) {
+    if (s->fn) {
+        const size_t elem = type == 2 ? 4 : 8;
+        if (count * elem > 2 * s->side_bytes) { err = "host transport: reduction larger than its buffer"; return -1; }
+        return host_round_trip(s, 1, buf, buf, count, elem, type, st, err);
+    }
     const ncclDataType_t t = type == 0 ? ncclFloat64 : (type == 1 ? ncclUint64 : ncclUint32);
     ncclResult_t r = nccl().AllReduce(buf, buf, count, t, ncclSum, s->comm, st);
     if (r != ncclSuccess) { err = nccl_msg("ncclAllReduce", r); return -1; }

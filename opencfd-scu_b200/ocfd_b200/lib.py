@@ -29,7 +29,7 @@ EXPORTED = (
     "ocfd_b200_create", "ocfd_b200_destroy", "ocfd_b200_set_stream", "ocfd_b200_get_stream",
     "ocfd_b200_synchronize", "ocfd_b200_set_metrics", "ocfd_b200_set_metrics_device",
     "ocfd_b200_set_metric_mode", "ocfd_b200_uniform_metrics", "ocfd_b200_set_sweep_impl",
-    "ocfd_b200_sweep_walks", "ocfd_b200_set_walk_threshold", "ocfd_b200_set_viscous_impl", "ocfd_b200_set_precision", "ocfd_b200_slab_unique_id", "ocfd_b200_set_slab",
+    "ocfd_b200_sweep_walks", "ocfd_b200_set_walk_threshold", "ocfd_b200_q_criterion", "ocfd_b200_time_average", "ocfd_b200_get_time_average", "ocfd_b200_set_viscous_impl", "ocfd_b200_set_precision", "ocfd_b200_slab_unique_id", "ocfd_b200_set_slab", "ocfd_b200_set_slab_host",
     "ocfd_b200_set_graphs", "ocfd_b200_graph_captures",
     "ocfd_b200_scheme_proportion", "ocfd_b200_mlp_nparam", "ocfd_b200_set_switch", "ocfd_b200_switch_stats", "ocfd_b200_switch_features",
     "ocfd_b200_mlp_last_error", "ocfd_b200_mlp_infer", "ocfd_b200_mlp_grad", "ocfd_b200_mlp_train",
@@ -122,8 +122,13 @@ def load(path: Optional[str] = None):
         "ocfd_b200_sweep_walks": (ctypes.c_int, [P]),
         "ocfd_b200_set_walk_threshold": (ctypes.c_int, [P, ctypes.c_double]),
         "ocfd_b200_set_viscous_impl": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_q_criterion": (ctypes.c_int, [P, D]),
+        "ocfd_b200_time_average": (ctypes.c_int, [P, ctypes.c_int]),
+        "ocfd_b200_get_time_average": (ctypes.c_int, [P, D, ctypes.POINTER(ctypes.c_int)]),
         "ocfd_b200_set_precision": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_slab_unique_id": (ctypes.c_int, [ctypes.c_char_p]),
+        "ocfd_b200_set_slab_host": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                   ctypes.c_int, ctypes.c_int, SLAB_TRANSPORT, ctypes.c_void_p]),
         "ocfd_b200_set_graphs": (ctypes.c_int, [P, ctypes.c_int]),
         "ocfd_b200_graph_captures": (ctypes.c_longlong, [P]),
         "ocfd_b200_set_slab": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -232,9 +237,22 @@ def mlp_train(params: np.ndarray, feat: np.ndarray, label: np.ndarray, epochs: i
 SLAB_ID_BYTES = 128
 
 
+def _torch_nccl_first():
+    """The library opens NCCL by its soname (libnccl.so.2) into the process's
+    global symbols.  torch links against its own, newer copy; loaded first,
+    an older system copy would shadow it and break torch's later import.  So
+    torch (where installed) is imported before the library touches NCCL,
+    and the library then shares torch's copy."""
+    try:
+        import torch  # noqa: F401
+    except ImportError:
+        pass
+
+
 def slab_unique_id() -> bytes:
     """The communicator id one rank makes for a z-split run (NCCL's unique
     id, 128 bytes) and hands to the others."""
+    _torch_nccl_first()
     L = load()
     buf = ctypes.create_string_buffer(SLAB_ID_BYTES)
     rc = L.ocfd_b200_slab_unique_id(buf)
@@ -261,12 +279,17 @@ def make_config(cfg: CaseConfig, device: int = 0) -> Config:
     return c
 
 
+# ocfd_b200_slab_transport: (user, op, send, recv, count, type) -> status
+SLAB_TRANSPORT = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_size_t, ctypes.c_int)
+
+
 class Solver:
     """One B200 solver context.  Same call surface as the reference driver."""
 
     def __init__(self, cfg: CaseConfig, prims: Optional[Sequence[np.ndarray]] = None,
                  metrics: Optional[Sequence[np.ndarray]] = None, device: int = 0,
-                 istep: int = 0, tt: float = 0.0, metric_mode: int = 0, inlet=None, slab=None):
+                 istep: int = 0, tt: float = 0.0, metric_mode: int = 0, inlet=None, slab=None, transport=None):
         self.L = load()
         self.cfg = cfg
         self.shape = (cfg.nz, cfg.ny, cfg.nx)
@@ -277,7 +300,13 @@ class Solver:
             raise OcfdError(rc, "ocfd_b200_create", (self.L.ocfd_b200_last_error(None) or b"").decode())
         self.h = h
         self.slab = slab
-        if slab is not None:        # slabs.SlabSpec: before the filters, metrics and state
+        self.transport = transport              # kept alive with the context
+        if slab is not None and transport is not None:     # exchange through the caller (slabs.HostTransport)
+            self._check(self.L.ocfd_b200_set_slab_host(self.h, slab.nranks, slab.rank, slab.rank_lo, slab.rank_hi,
+                                                       slab.z_offset, slab.nz_global, transport.fn, None),
+                        "set_slab_host")
+        elif slab is not None:      # slabs.SlabSpec: before the filters, metrics and state
+            _torch_nccl_first()
             self._check(self.L.ocfd_b200_set_slab(self.h, slab.nranks, slab.rank, slab.rank_lo, slab.rank_hi,
                                                   slab.z_offset, slab.nz_global, slab.comm_id), "set_slab")
         if metric_mode:
@@ -380,6 +409,22 @@ class Solver:
     def sweep_walks(self) -> int:
         """Bit d set: direction d takes the walk that forms every face in line."""
         return int(self.L.ocfd_b200_sweep_walks(self.h))
+
+    def q_criterion(self) -> np.ndarray:
+        """Q of the current primitives (get_Q, src/OCFD_ana.cu:317-456), [nz][ny][nx]."""
+        out = np.empty(self.shape, dtype=np.float64)
+        self._check(self.L.ocfd_b200_q_criterion(self.h, _dp(out)), "q_criterion")
+        return out
+
+    def time_average(self, reset: bool = False):
+        """Add the current primitives to the running means (or reset them)."""
+        self._check(self.L.ocfd_b200_time_average(self.h, int(bool(reset))), "time_average")
+
+    def get_time_average(self) -> Tuple[np.ndarray, int]:
+        out = np.empty((5,) + self.shape, dtype=np.float64)
+        n = ctypes.c_int()
+        self._check(self.L.ocfd_b200_get_time_average(self.h, _dp(out), ctypes.byref(n)), "get_time_average")
+        return out, n.value
 
     def set_viscous_impl(self, impl: int):
         """0: the faster kernel of the form (default); 1: Ev read through the caches; 2: Ev tiles staged in shared memory."""

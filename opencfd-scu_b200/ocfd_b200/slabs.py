@@ -17,6 +17,7 @@ torch.distributed carries only that host traffic (any backend).
     run.solver.step(100)
     u = gather_z(run.solver.conserved(), dist.get_rank(), dist.get_world_size())   # rank 0: whole grid
 """
+import ctypes
 import dataclasses
 from typing import Callable, List, Optional, Tuple
 
@@ -90,15 +91,71 @@ def gather_z(local: np.ndarray, rank: int, nranks: int, group=None, axis: int = 
     return np.concatenate(parts, axis=axis)
 
 
-class SlabRun:
-    """One rank's solver on its slab of a whole-grid case."""
+class HostTransport:
+    """The z split's exchange carried through host memory by
+    torch.distributed point-to-point messages and all-reduce (a backend that
+    moves CPU tensors, e.g. gloo), in place of NCCL: what the reference does
+    with MPI_Sendrecv (src/OCFD_mpi_dev.cu:271-310).  Each slab process may
+    then use any GPU, the same one as its neighbours included; no kernel of
+    one process waits on another's.  Messages going up carry tag 1, going
+    down tag 0, so that two slabs (the same rank above and below) pair their
+    messages correctly."""
 
-    def __init__(self, case: Case, rank: int, nranks: int, comm_id: bytes, device: int = 0, **solver_kw):
-        self.spec = slab_spec(rank, nranks, case.cfg.nz, comm_id)
+    _DT = {0: np.float64, 1: np.uint64, 2: np.uint32, 3: np.float32}
+    _CT = {0: ctypes.c_double, 1: ctypes.c_uint64, 2: ctypes.c_uint32, 3: ctypes.c_float}
+
+    def __init__(self, rank: int, rank_lo: int, rank_hi: int, group=None):
+        self.rank, self.lo, self.hi, self.group = rank, rank_lo, rank_hi, group
+        self.fn = lib.SLAB_TRANSPORT(self._call)
+        self.error: Optional[BaseException] = None
+
+    def _array(self, ptr, n, type_):
+        return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(self._CT[type_])), shape=(n,))
+
+    def _call(self, user, op, send, recv, count, type_):
+        import torch
+        import torch.distributed as dist
+        try:
+            if op == 0:
+                s = self._array(send, 2 * count, type_)
+                r = self._array(recv, 2 * count, type_)
+                if self.lo == self.rank and self.hi == self.rank:      # one slab: the periodic wrap
+                    r[:count] = s[count:]
+                    r[count:] = s[:count]
+                    return 0
+                down, up = torch.from_numpy(s[:count]), torch.from_numpy(s[count:])
+                from_lo, from_hi = torch.from_numpy(r[:count]), torch.from_numpy(r[count:])
+                reqs = [dist.isend(up, self.hi, group=self.group, tag=1),
+                        dist.isend(down, self.lo, group=self.group, tag=0),
+                        dist.irecv(from_lo, self.lo, group=self.group, tag=1),
+                        dist.irecv(from_hi, self.hi, group=self.group, tag=0)]
+                for q in reqs:
+                    q.wait()
+                return 0
+            # op 1: sum over the ranks in place (counts as signed integers of
+            # the same width: every sum here is far below 2^31)
+            a = self._array(send, count, type_)
+            view = {0: np.float64, 1: np.int64, 2: np.int32, 3: np.float32}[type_]
+            t = torch.from_numpy(a.view(view))
+            dist.all_reduce(t, group=self.group)
+            return 0
+        except BaseException as e:       # reported by the library as a failed exchange
+            self.error = e
+            return 1
+
+
+class SlabRun:
+    """One rank's solver on its slab of a whole-grid case.  comm_id: the NCCL
+    id (share_id); None: the exchange goes through HostTransport."""
+
+    def __init__(self, case: Case, rank: int, nranks: int, comm_id: Optional[bytes], device: int = 0,
+                 group=None, **solver_kw):
+        self.spec = slab_spec(rank, nranks, case.cfg.nz, comm_id if comm_id is not None else b"")
         nz = part_z(case.cfg.nz, nranks)[rank][1]
         self.case = slab_case(case, self.spec.z_offset, nz)
+        transport = HostTransport(rank, self.spec.rank_lo, self.spec.rank_hi, group) if comm_id is None else None
         self.solver = lib.Solver(self.case.cfg, self.case.prims, self.case.metrics, device=device,
-                                 inlet=self.case.inlet, slab=self.spec, **solver_kw)
+                                 inlet=self.case.inlet, slab=self.spec, transport=transport, **solver_kw)
 
     def close(self):
         self.solver.close()

@@ -1488,6 +1488,45 @@ static void d0(oro_state *s, const double *f, double *out, int dir) {
             }
 }
 
+/* get_Q (src/OCFD_ana.cu:317-456): the derivatives of u, v, w along the
+ * three grid directions (OCFD_d{x,y,z}0 with the D0_bound closures), the
+ * velocity gradient through the metrics (get_Q_kernal :317-389) and
+ * Q = (ux vy + ux wz + vy wz - uy vx - uz wx - vz wy) Ajac^2 at every
+ * interior cell.  (The reference kernel stores Q at LAP offsets into a field
+ * allocated without ghosts; this is the interior value it computes.)  The
+ * ghosts of u, v, w are exchanged first. */
+void oro_q_criterion(oro_state *s, double *q) {
+    exchange_xyz(s, s->u);
+    exchange_xyz(s, s->v);
+    exchange_xyz(s, s->w);
+    const double *pr[3] = { s->u, s->v, s->w };
+    for (int m = 0; m < 3; m++)
+        for (int dir = 0; dir < 3; dir++) d0(s, pr[m], s->grad[3 * m + dir], dir);
+#pragma omp parallel for
+    for (int k = 0; k < s->nz; k++)
+        for (int j = 0; j < s->ny; j++)
+            for (int i = 0; i < s->nx; i++) {
+                size_t p = L(s, i + LAP, j + LAP, k + LAP), c = I(s, i, j, k);
+                double Akx = s->A[AKX][p], Aix = s->A[AIX][p], Asx = s->A[ASX][p];
+                double Aky = s->A[AKY][p], Aiy = s->A[AIY][p], Asy = s->A[ASY][p];
+                double Akz = s->A[AKZ][p], Aiz = s->A[AIZ][p], Asz = s->A[ASZ][p];
+                double uk = s->grad[0][c], ui = s->grad[1][c], us = s->grad[2][c];
+                double vk = s->grad[3][c], vi = s->grad[4][c], vs = s->grad[5][c];
+                double wk = s->grad[6][c], wi = s->grad[7][c], ws = s->grad[8][c];
+                double ux = uk*Akx + ui*Aix + us*Asx;
+                double vx = vk*Akx + vi*Aix + vs*Asx;
+                double wx = wk*Akx + wi*Aix + ws*Asx;
+                double uy = uk*Aky + ui*Aiy + us*Asy;
+                double vy = vk*Aky + vi*Aiy + vs*Asy;
+                double wy = wk*Aky + wi*Aiy + ws*Asy;
+                double uz = uk*Akz + ui*Aiz + us*Asz;
+                double vz = vk*Akz + vi*Aiz + vs*Asz;
+                double wz = wk*Akz + wi*Aiz + ws*Asz;
+                double aj = s->A[AJAC][p];
+                q[c] = (ux*vy + ux*wz + vy*wz - uy*vx - uz*wx - vz*wy) * aj * aj;
+            }
+}
+
 static void viscous(oro_state *s) {
     /* du_viscous_Jacobian3d_init (:58-77) */
     const double *pr[4] = { s->u, s->v, s->w, s->T };

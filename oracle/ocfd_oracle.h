@@ -107,6 +107,9 @@ void oro_get_conserved(const oro_state *s, double *f5);
 void oro_get_conserved_n(const oro_state *s, double *f5);
 void oro_get_du(const oro_state *s, double *du5);
 void oro_get_flags(const oro_state *s, int *sx, int *sy, int *sz);
+/* Q criterion of the current primitives, interior [nz][ny][nx]: get_Q
+ * (src/OCFD_ana.cu:317-456) after the ghost exchange of u, v, w. */
+void oro_q_criterion(oro_state *s, double *q);
 int  oro_istep(const oro_state *s);
 double oro_tt(const oro_state *s);
 

@@ -76,7 +76,7 @@ def lib():
         for name in ("oro_du_comput", "oro_time_advance", "oro_step"):
             getattr(L, name).argtypes = [P, ctypes.c_int]
         for name in ("oro_get_primitives", "oro_get_pressure", "oro_get_conserved",
-                     "oro_get_conserved_n", "oro_get_du"):
+                     "oro_get_conserved_n", "oro_get_du", "oro_q_criterion"):
             getattr(L, name).argtypes = [P, D]
         IP = ctypes.POINTER(ctypes.c_int)
         L.oro_get_flags.argtypes = [P, IP, IP, IP]
@@ -230,6 +230,12 @@ class Oracle:
     def pressure(self) -> np.ndarray:
         out = np.empty(self.shape, dtype=np.float64)
         self.L.oro_get_pressure(self.h, _dp(out))
+        return out
+
+    def q_criterion(self) -> np.ndarray:
+        """Q of the current primitives (get_Q, src/OCFD_ana.cu:317-456)."""
+        out = np.empty(self.shape, dtype=np.float64)
+        self.L.oro_q_criterion(self.h, _dp(out))
         return out
 
     def flags(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:

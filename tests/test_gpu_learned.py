@@ -7,10 +7,17 @@ plain FP64 run)."""
 import numpy as np
 import pytest
 
+import os
+
 from ocfd_b200 import cases, learned, lib
 from oracle import mlp_oracle as mo
 
 pytestmark = pytest.mark.gpu
+
+# the network the package ships (trained on the plain solver's labels of
+# Taylor-Green 64^3 and isotropic turbulence 256^3)
+MODEL = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "opencfd-scu_b200", "ocfd_b200",
+                     "data", "switch_c1c3.npz")
 
 
 def random_params(rng, scale=0.4):
@@ -155,3 +162,61 @@ def test_trained_switch_tracks_plain_run(gpu_lib):
     pa, pb = a.primitives(), b.primitives()
     sh = learned.shock_error(pa[0] * pa[4], pb[0] * pb[4], q=0.9)
     assert sh["max_cells"] <= 1, sh
+
+
+def _vec_rel_l2(test, ref):
+    """Relative L2 per conserved variable; the momentum components against
+    the momentum vector's norm (the spanwise one is a small fluctuation)."""
+    mom = np.sqrt(sum(np.linalg.norm(ref[m]) ** 2 for m in (1, 2, 3)))
+    return np.array([np.linalg.norm(test[m] - ref[m]) / (mom if m in (1, 2, 3) else np.linalg.norm(ref[m]))
+                     for m in range(5)])
+
+
+@pytest.mark.parametrize("which", ["iso128", "ramp256x64x32"])
+def test_shipped_switch_cost_and_accuracy(which, gpu_lib):
+    """What the shipped network changes, against the same precision form with
+    the plain sensor: the time per step of each (recorded; the network pass
+    costs more than the sensor formula it replaces, so the ratio is at or
+    below 1 -- on these flows both mark the same faces, so the walks do the
+    same work), and the state against the plain FP64 run: within 1e-3
+    relative L2 and shock positions within one cell.  Isotropic turbulence
+    is the flow the network was trained on; the ramp (IBC 108, the filter,
+    half the faces non-UP7) is not."""
+    import time
+
+    if which == "iso128":
+        c = cases.isotropic_turbulence(128, seed=2024, charteric=1)
+        steps = 30
+    else:
+        c = cases.ramp_case(256, 64, 32, seed=2024)
+        steps = 50
+    w = learned.load_model(MODEL)
+    ref = lib.Solver(c.cfg, c.prims, c.metrics, inlet=c.inlet)
+    ref.step(steps)
+    u_ref, p_ref = ref.conserved(), ref.primitives()
+    ms = {}
+    out = {}
+    for name, use in (("plain", False), ("switch", True)):
+        s = lib.Solver(c.cfg, c.prims, c.metrics, inlet=c.inlet)
+        s.set_precision(1)
+        if use:
+            s.set_switch(w, 0.9)
+        s.step(2)
+        s.synchronize()
+        t0 = time.perf_counter()
+        s.step(steps - 2)
+        s.synchronize()
+        ms[name] = (time.perf_counter() - t0) * 1e3 / (steps - 2)
+        out[name] = (s.conserved(), s.primitives())
+        if use:
+            sure, unsure, differ = s.switch_stats()
+    err = _vec_rel_l2(out["switch"][0], u_ref)
+    pr = out["switch"][1]
+    sh = learned.shock_error(p_ref[0] * p_ref[4], pr[0] * pr[4], q=0.99)
+    print(f"{which}: ms/step plain sensor {ms['plain']:.3f}, switch {ms['switch']:.3f} "
+          f"(ratio {ms['plain'] / ms['switch']:.3f}); rel L2 vs FP64 {err}; shock {sh}; "
+          f"network cells {sure}, plain fallbacks {unsure}, differing {differ}")
+    assert sure > 0.9 * (sure + unsure)
+    assert np.all(err <= 1e-3), err
+    assert sh["max_cells"] <= 1, sh
+    assert ms["plain"] / ms["switch"] > 0.5

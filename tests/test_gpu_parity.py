@@ -180,19 +180,18 @@ def test_matches_reference_golden(path, gpu_lib):
 @pytest.mark.parametrize("name,case", bounded_cases(), ids=[n for n, _ in bounded_cases()])
 def test_bounded_sweep_variants(name, case, gpu_lib):
     """Cells next to closed faces go through the fix-up kernel (variant 4) or
-    the in-loop dispatch (variant 5): same results; the tiled variants have
-    no closures and refuse the case."""
+    the in-loop dispatch (variant 5): same results; a variant number that
+    does not exist is refused."""
     a = lib.Solver(case.cfg, case.prims, case.metrics)
     b = lib.Solver(case.cfg, case.prims, case.metrics)
     b.set_sweep_impl(5)
     a.step(2)
     b.step(2)
     assert np.all(rel_l2(a.primitives(), b.primitives()) <= 1e-13), name
-    c = lib.Solver(case.cfg, case.prims, case.metrics)
-    c.set_sweep_impl(2)
-    with pytest.raises(lib.OcfdError) as ei:
-        c.step(1)
-    assert ei.value.status == -2
+    for bad in (0, 2, 9):
+        with pytest.raises(lib.OcfdError) as ei:
+            a.set_sweep_impl(bad)
+        assert ei.value.status == -1
 
 
 def _walk4_supported(cfg):

@@ -124,3 +124,32 @@ def test_symbo_limiter_linear_branch_p_only():
     assert np.isfinite(lp) and np.isfinite(np_)
     # linear data: every candidate stencil is exact, so both give the face value
     assert abs(lp - np_) < 1e-12
+
+
+def test_oracle_q_criterion_matches_its_formula():
+    """The oracle's Q (get_Q, src/OCFD_ana.cu:317-456) on a periodic grid
+    against the same formula in numpy: sixth-order central derivatives with
+    the periodic wrap, the metrics, Q = (ux vy + ux wz + vy wz - uy vx -
+    uz wx - vz wy) Ajac^2."""
+    from ocfd_b200 import cases
+    case = cases.random_smooth_case(12, 11, 10, seed=5, curvilinear=True)
+    o = oro.Oracle(case.cfg, case.prims, case.metrics)
+    q = o.q_criterion()
+    prims = np.asarray(case.prims)
+    met = np.asarray(case.metrics)
+    nz, ny, nx = prims.shape[1:]
+    h = [1.0 / (n - 1.0) for n in (nx, ny, nz)]
+    axis = [2, 1, 0]
+
+    def d(f, dir_):
+        a = axis[dir_]
+        r = lambda k: np.roll(f, -k, axis=a)
+        return (45.0 * (r(1) - r(-1)) - 9.0 * (r(2) - r(-2)) + (r(3) - r(-3))) / 60.0 / h[dir_]
+
+    g = [[d(prims[m], dd) for dd in range(3)] for m in (1, 2, 3)]
+    Akx, Aky, Akz, Aix, Aiy, Aiz, Asx, Asy, Asz, Aj = (met[k] for k in (3, 4, 5, 6, 7, 8, 9, 10, 11, 12))
+    grad = [[g[m][0] * A0 + g[m][1] * A1 + g[m][2] * A2 for (A0, A1, A2) in ((Akx, Aix, Asx), (Aky, Aiy, Asy), (Akz, Aiz, Asz))]
+            for m in range(3)]
+    (ux, uy, uz), (vx, vy, vz), (wx, wy, wz) = grad
+    want = (ux * vy + ux * wz + vy * wz - uy * vx - uz * wx - vz * wy) * Aj * Aj
+    assert np.linalg.norm(q - want) / np.linalg.norm(want) < 1e-12

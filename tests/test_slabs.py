@@ -119,3 +119,58 @@ def test_id_from_rank0_and_gather_over_gloo(world):
         assert made == ([0] if rank == 0 else [])      # only rank 0 makes the id
         assert (lo, hi) == slabs.neighbours(rank, world)
         assert ok
+
+
+def _transport_worker(rank, world, port, q):
+    """The host transport's two operations as the library calls them, on
+    host buffers: the ghost-plane swap (each rank's lowest planes to the
+    rank below, highest to the rank above) and the in-place sums."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    from datetime import timedelta
+    import ctypes
+    import numpy as np
+    import torch.distributed as dist
+    from ocfd_b200 import slabs
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        lo, hi = slabs.neighbours(rank, world)
+        t = slabs.HostTransport(rank, lo, hi)
+        count = 5
+        send = np.concatenate([np.full(count, 100.0 * rank + 1.0), np.full(count, 100.0 * rank + 2.0)])
+        recv = np.zeros(2 * count)
+        rc = t.fn(None, 0, send.ctypes.data, recv.ctypes.data, count, 0)
+        ok_swap = (rc == 0 and np.all(recv[:count] == 100.0 * lo + 2.0)      # the lower rank's highest planes
+                   and np.all(recv[count:] == 100.0 * hi + 1.0))             # the upper rank's lowest planes
+        f32 = np.full(2 * count, rank, dtype=np.float32)
+        r32 = np.zeros(2 * count, dtype=np.float32)
+        ok_f32 = t.fn(None, 0, f32.ctypes.data, r32.ctypes.data, count, 3) == 0 and \
+            np.all(r32[:count] == lo) and np.all(r32[count:] == hi)
+        acc = np.array([rank + 0.5, 2.0 * rank])
+        c64 = np.array([rank + 1, 10], dtype=np.uint64)
+        c32 = np.array([rank, 3, 7], dtype=np.uint32)
+        ok_sum = (t.fn(None, 1, acc.ctypes.data, acc.ctypes.data, 2, 0) == 0 and
+                  t.fn(None, 1, c64.ctypes.data, c64.ctypes.data, 2, 1) == 0 and
+                  t.fn(None, 1, c32.ctypes.data, c32.ctypes.data, 3, 2) == 0)
+        n = world
+        ok_sum = ok_sum and np.allclose(acc, [n * (n - 1) / 2 + 0.5 * n, n * (n - 1)]) and \
+            list(c64) == [n * (n + 1) // 2, 10 * n] and list(c32) == [n * (n - 1) // 2, 3 * n, 7 * n]
+        q.put((rank, bool(ok_swap), bool(ok_f32), bool(ok_sum)))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_host_transport_over_gloo(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_transport_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=180) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, ok_swap, ok_f32, ok_sum in res:
+        assert ok_swap and ok_f32 and ok_sum, (rank, ok_swap, ok_f32, ok_sum)
