@@ -249,7 +249,10 @@ int ocfd_b200_advance_host(ocfd_b200_ctx *ctx, const double *prim5_in, double *p
  * X_DIST_END, BETA, X_WALL_BEGIN, X_UP_BOUNDARY_BEGIN, SLZ; inlet4 is the
  * flow1d-inlet.dat profile [4][ny] (d,u,v,T), needed when INLET_BOUNDARY = 1.
  * Call after the metrics (the wall and top coordinates are read from them)
- * and before set_primitives; MZMAX > 0 (random phases) is not built. */
+ * and before set_primitives.  MZMAX > 0 sums MZMAX spanwise modes whose
+ * phases are the first MZMAX draws of the C library's rand() from its initial
+ * state, as the reference's set-up takes them (it seeds nothing first,
+ * src/OCFD_boundary_init.c:444-499); MZMAX <= 4096. */
 int ocfd_b200_set_bc(ocfd_b200_ctx *ctx, int ibc, const int *npara, int nnpara, const double *rpara,
                      int nrpara, const double *inlet4);
 

@@ -9,6 +9,7 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cmath>
 #include <cstdio>
@@ -553,12 +554,17 @@ static int ghost_metrics(ocfd_b200_ctx *ctx) {
     return fill_ghosts(ctx, fj, mj, 1, "metric ghost fill");
 }
 
+// A kernel family of one stage: an NVTX range named for it (seen by a
+// profiler attached to the process, free otherwise) and, with timing on,
+// CUDA events around it on the solver stream.
 struct TimerScope {
     ocfd_b200_ctx *c; int which; bool on;
     TimerScope(ocfd_b200_ctx *cc, int w) : c(cc), which(w), on(cc->timing) {
+        nvtxRangePushA(kTimerNames[w]);
         if (on) cudaEventRecord(c->ev[0], c->stream);
     }
     ~TimerScope() {
+        nvtxRangePop();
         if (!on) return;
         cudaEventRecord(c->ev[1], c->stream);
         if (cudaEventSynchronize(c->ev[1]) == cudaSuccess) {
@@ -1373,11 +1379,16 @@ extern "C" int ocfd_b200_step(ocfd_b200_ctx *ctx, int nsteps) {
         ctx->prims64_interior_ok = ctx->p.flap != nullptr;
     }
     for (int n = 0; n < nsteps; n++) {
+        nvtxRangePushA("ocfd_b200_step");
         ocfd_b200_swap_time_levels(ctx);
-        if ((rc = step_graph_ok(ctx) ? step_graph(ctx) : step_launched(ctx, false))) return rc;
-        ctx->istep++;
-        ctx->tt += ctx->p.dt;
-        if ((rc = run_filters(ctx))) return rc;
+        rc = step_graph_ok(ctx) ? step_graph(ctx) : step_launched(ctx, false);
+        if (!rc) {
+            ctx->istep++;
+            ctx->tt += ctx->p.dt;
+            rc = run_filters(ctx);
+        }
+        nvtxRangePop();
+        if (rc) return rc;
     }
     return OCFD_OK;
 }
@@ -1395,6 +1406,29 @@ extern "C" int ocfd_b200_set_time(ocfd_b200_ctx *ctx, int istep, double tt) {
     return OCFD_OK;
 }
 
+// The first n values of the C library's rand() in its initial state (as
+// after srand(1)): the additive generator r[i] = r[i-3] + r[i-31] mod 2^32
+// over a table filled by r[i] = 16807 r[i-1] mod (2^31 - 1) from r[0] = 1,
+// r[31..33] = r[0..2], the values up to r[343] discarded, each output
+// r[i] >> 1 (the published description of the GNU C library's TYPE_3
+// random()).
+static std::vector<int> libc_rand_initial(int n) {
+    std::vector<unsigned> r((size_t)344 + n);
+    r[0] = 1u;
+    for (int i = 1; i < 31; i++) {
+        long long w = (16807LL * (long long)r[i - 1]) % 2147483647LL;
+        if (w < 0) w += 2147483647LL;
+        r[i] = (unsigned)w;
+    }
+    for (int i = 31; i < 34; i++) r[i] = r[i - 31];
+    std::vector<int> out((size_t)n);
+    for (int i = 34; i < 344 + n; i++) {
+        r[i] = r[i - 31] + r[i - 3];
+        if (i >= 344) out[i - 344] = (int)(r[i] >> 1);
+    }
+    return out;
+}
+
 // IBC and BC_NPARA / BC_RPARA (bc_parameter, src/OCFD_boundary_init.c:50-93)
 // with the set-up of bc_user_Compression_conner_init (:376-438)
 extern "C" int ocfd_b200_set_bc(ocfd_b200_ctx *ctx, int ibc, const int *npara, int nnpara, const double *rpara,
@@ -1408,8 +1442,7 @@ extern "C" int ocfd_b200_set_bc(ocfd_b200_ctx *ctx, int ibc, const int *npara, i
         return fail(ctx, OCFD_ERR_ARG, "IBC 108 needs 4 BC_NPARA and 8 BC_RPARA values");
     if (!ctx->have_metrics) return fail(ctx, OCFD_ERR_STATE, "set the metrics or mesh before the boundary conditions");
     const int MZ = npara[0], MT = npara[1], inlet_file = npara[2], not_normal = npara[3];
-    if (MZ > 0)
-        return fail(ctx, OCFD_ERR_UNSUPPORTED, "MZMAX > 0 draws random spanwise phases (rand()); use MZMAX <= 0");
+    if (MZ > 4096) return fail(ctx, OCFD_ERR_ARG, "MZMAX must be <= 4096");
     if (MT > 64) return fail(ctx, OCFD_ERR_ARG, "MTMAX must be <= 64");
     if (inlet_file == 1 && !inlet4) return fail(ctx, OCFD_ERR_ARG, "INLET_BOUNDARY = 1 needs the inflow profile");
     const double TW = rpara[0], EPSL = rpara[1], DB = rpara[2], DE = rpara[3], BETA = rpara[4];
@@ -1444,9 +1477,32 @@ extern "C" int ocfd_b200_set_bc(ocfd_b200_ctx *ctx, int ibc, const int *npara, i
             fx[i] = 0.;
         }
     }
+    // MZMAX > 0: MZMAX spanwise modes of weights 1, 1/1.25, ... (normalised)
+    // and phases rand() / RAND_MAX, the first draws of the C library's
+    // generator in its initial state -- the reference seeds nothing before
+    // (get_xs_blow_suction_multiwave, src/OCFD_boundary_init.c:444-499)
+    std::vector<double> faiz, zl;
+    if (MZ > 0) {
+        std::vector<int> draws = libc_rand_initial(MZ);
+        faiz.resize(MZ);
+        zl.resize(MZ);
+        double ztmp = 0.;
+        for (int m = 0; m < MZ; m++) {
+            faiz[m] = draws[m] / 2147483647.0;
+            zl[m] = m == 0 ? 1. : zl[m - 1] / 1.25;
+            ztmp = ztmp + zl[m];
+        }
+        for (int m = 0; m < MZ; m++) zl[m] = zl[m] / ztmp;
+    }
     for (int k = 0; k < nz; k++) {
         const double za = hz[(size_t)nx * ny * k];                      // x = 0, y = 0
-        gz[k] = MZ == 0 ? 1. : sin(-2. * PI * MZ * (za / SL));
+        const double seta = za / SL;
+        if (MZ > 0) {
+            gz[k] = 0.;
+            for (int m = 0; m < MZ; m++) gz[k] = gz[k] + zl[m] * sin(2. * PI * (m + 1) * (seta + faiz[m]));
+        } else {
+            gz[k] = MZ == 0 ? 1. : sin(-2. * PI * MZ * seta);
+        }
     }
     free(hx); free(hz);
     double Ttmp = 0.;

@@ -20,6 +20,7 @@
 #include "ocfd_oracle.h"
 
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 #include <stdio.h>
@@ -157,10 +158,29 @@ void oro_set_inlet(oro_state *s, const double *ub1) {
     memcpy(s->ub1, ub1, 4 * (size_t)s->ny * sizeof(double));
 }
 
+/* rand() of the GNU C library from its initial state (srand(1)): a table
+ * t[0] = 1, t[i] = 16807 t[i-1] mod 2147483647 (i < 31), t[31..33] =
+ * t[0..2], then t[i] = t[i-3] + t[i-31] mod 2^32; draws are t[i] >> 1 for
+ * i >= 344.  A ring of the last 34 values is enough. */
+void oro_libc_rand(int n, int *out) {
+    uint32_t t[34];
+    t[0] = 1u;
+    for (int i = 1; i < 31; i++) t[i] = (uint32_t)((16807ULL * t[i - 1]) % 2147483647ULL);
+    for (int i = 31; i < 34; i++) t[i] = t[i - 31];
+    int got = 0;
+    for (long i = 34; got < n; i++) {
+        uint32_t v = t[(i - 31) % 34] + t[(i - 3) % 34];
+        t[i % 34] = v;
+        if (i >= 344) out[got++] = (int)(v >> 1);
+    }
+}
+
 /* x_begin, the blowing shapes fx (x) and gz (z) and the frequency weights TM,
  * from the wall and top coordinates (get_xs_blow_suction_multiwave,
  * get_fait_multifrequancy, src/OCFD_boundary_init.c:376-521).  MZMAX > 0
- * draws random phases with rand() and is not restated. */
+ * takes its MZMAX phases from the first rand() draws of the C library in its
+ * initial state (nothing seeds it before, :444-499), restated by
+ * oro_libc_rand. */
 static void bc108_init(oro_state *s) {
     const double PI = 3.14159265358979323846;
     const double *Axx = s->A[AXX], *Azz = s->A[AZZ];
@@ -178,12 +198,35 @@ static void bc108_init(oro_state *s) {
             s->bfx[i] = 0.;
         }
     }
+    double *faiz = NULL, *zl = NULL;
+    if (MZ > 0) {
+        int *draw = (int *)malloc(sizeof(int) * (size_t)MZ);
+        faiz = (double *)malloc(sizeof(double) * (size_t)MZ);
+        zl = (double *)malloc(sizeof(double) * (size_t)MZ);
+        oro_libc_rand(MZ, draw);
+        double ztmp = 0.;
+        for (int m = 0; m < MZ; m++) {
+            faiz[m] = draw[m] / (double)2147483647;     /* RAND_MAX */
+            zl[m] = m == 0 ? 1. : zl[m - 1] / 1.25;
+            ztmp += zl[m];
+        }
+        for (int m = 0; m < MZ; m++) zl[m] = zl[m] / ztmp;
+        free(draw);
+    }
     for (int k = 0; k < s->nz; k++) {
         double za = Azz[L(s, LAP, LAP, k + LAP)];
         double seta = za / SL;
-        if (MZ == 0) s->bgz[k] = 1.;
-        else s->bgz[k] = sin(-2. * PI * MZ * seta);      /* MZ < 0 */
+        if (MZ > 0) {
+            s->bgz[k] = 0.;
+            for (int m = 0; m < MZ; m++) s->bgz[k] = s->bgz[k] + zl[m] * sin(2. * PI * (m + 1) * (seta + faiz[m]));
+        } else if (MZ == 0) {
+            s->bgz[k] = 1.;
+        } else {
+            s->bgz[k] = sin(-2. * PI * MZ * seta);
+        }
     }
+    free(faiz);
+    free(zl);
     double Ttmp = 0.;
     for (int k = 0; k < MT && k < 64; k++) {
         s->TM[0] = 1.;

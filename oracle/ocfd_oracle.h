@@ -110,6 +110,8 @@ void oro_get_flags(const oro_state *s, int *sx, int *sy, int *sz);
 /* Q criterion of the current primitives, interior [nz][ny][nx]: get_Q
  * (src/OCFD_ana.cu:317-456) after the ghost exchange of u, v, w. */
 void oro_q_criterion(oro_state *s, double *q);
+/* the first n draws of the C library's rand() from its initial state */
+void oro_libc_rand(int n, int *out);
 int  oro_istep(const oro_state *s);
 double oro_tt(const oro_state *s);
 

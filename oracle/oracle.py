@@ -80,6 +80,7 @@ def lib():
             getattr(L, name).argtypes = [P, D]
         IP = ctypes.POINTER(ctypes.c_int)
         L.oro_get_flags.argtypes = [P, IP, IP, IP]
+        L.oro_libc_rand.argtypes = [ctypes.c_int, IP]
         L.oro_istep.argtypes = [P]
         L.oro_istep.restype = ctypes.c_int
         L.oro_tt.argtypes = [P]
@@ -255,6 +256,14 @@ class Oracle:
     @property
     def tt(self) -> float:
         return self.L.oro_tt(self.h)
+
+
+def libc_rand(n: int) -> np.ndarray:
+    """The first n draws of the C library's rand() from its initial state,
+    as the oracle restates it (the spanwise phases of IBC 108, MZMAX > 0)."""
+    out = np.zeros(n, dtype=np.int32)
+    lib().oro_libc_rand(int(n), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    return out
 
 
 def point(name: str, stencil: Sequence[float], *args) -> float:

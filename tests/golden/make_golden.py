@@ -67,7 +67,8 @@ def golden_cases():
 def ramp_cases():
     """The compression-corner boundary family (IBC 108) on a small ramp mesh:
     isothermal wall with the inflow profile file, hybrid scheme and filter;
-    adiabatic wall with time-dependent wall blowing; the default profile."""
+    adiabatic wall with time-dependent wall blowing; the default profile;
+    blowing with random-phase spanwise modes."""
     out = []
     c = cases.ramp_case(32, 20, 8, seed=91)
     out.append(("ramp32x20x8_bc108_tw_filter", c, 3))
@@ -79,6 +80,13 @@ def ramp_cases():
     c.cfg.bc_npara = (0, 0, 0, 0)            # INLET_BOUNDARY 0: d = u = T = 1, v = 0
     c.inlet = None
     out.append(("ramp28x18x8_bc108_default_inlet", c, 3))
+    # three spanwise modes with phases from rand() (MZMAX = 3), a span of 8
+    # cells over SLZ = 2 so that the modes vary across it
+    c = cases.ramp_case(30, 18, 8, seed=94, tw=-1.0, epsl=0.05, beta=40.0, mtmax=3,
+                        scheme_invis="WENO7", charteric=0, filters=())
+    c.cfg.bc_npara = (3, 3, 1, 0)
+    c.cfg.bc_rpara = (-1.0, 0.05, 4.0, 30.0, 40.0, 0.0, 30.0, 2.0)
+    out.append(("ramp30x18x8_bc108_mz3_blowing", c, 3))
     return out
 
 

@@ -153,3 +153,16 @@ def test_oracle_q_criterion_matches_its_formula():
     (ux, uy, uz), (vx, vy, vz), (wx, wy, wz) = grad
     want = (ux * vy + ux * wz + vy * wz - uy * vx - uz * wx - vz * wy) * Aj * Aj
     assert np.linalg.norm(q - want) / np.linalg.norm(want) < 1e-12
+
+
+def test_libc_rand_restatement():
+    """The oracle's restatement of rand() from the C library's initial state
+    (the phases of IBC 108's spanwise modes, MZMAX > 0) equals this host's
+    own rand() after srand(1), draw for draw."""
+    import ctypes
+    libc = ctypes.CDLL(None)
+    libc.srand(1)
+    want = np.array([libc.rand() for _ in range(1000)], dtype=np.int64)
+    got = oro.libc_rand(1000).astype(np.int64)
+    assert np.array_equal(got, want)
+    assert got[0] == 1804289383 and got[1] == 846930886
