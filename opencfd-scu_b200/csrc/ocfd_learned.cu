@@ -529,15 +529,33 @@ cudaError_t launch_switch_features(const Params &p, long long first, long long c
     return cudaGetLastError();
 }
 
-// persistent blocks: as many as are resident at once, at most one per tile
+// Persistent blocks: as many as fit on the SMs at once (registers, shared
+// memory, threads; 32 TMEM columns each, so at most 16 by tensor memory), at
+// most one per tile.  Counted from the kernel's attributes: the runtime's
+// occupancy query gave one block per SM for these kernels, which left 4
+// warps per SM to hide the feature loads.
 template <typename K>
 static unsigned resident_blocks(K kern, long long tiles) {
-    int dev = 0, sms = 148, per = 1;
+    int dev = 0, sms = 148, regs_sm = 65536, smem_sm = 233472, smem_rsv = 1024, thr_sm = 2048;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, umma::ROWS, 0) != cudaSuccess || per < 1) {
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    int per = 1;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, reinterpret_cast<const void *>(kern)) == cudaSuccess) {
+        const int regs = (fa.numRegs + 7) / 8 * 8;
+        const int by_regs = regs_sm / (umma::ROWS * (regs > 0 ? regs : 1));
+        const int by_smem = smem_sm / ((int)fa.sharedSizeBytes + smem_rsv);
+        const int by_thr = thr_sm / umma::ROWS;
+        per = by_regs < by_smem ? by_regs : by_smem;
+        if (per > by_thr) per = by_thr;
+        if (per > (int)(512 / umma::TMEM_COLS)) per = (int)(512 / umma::TMEM_COLS);
+        if (per < 1) per = 1;
+    } else {
         cudaGetLastError();
-        per = 1;
     }
     const long long nb = (long long)sms * per;
     return (unsigned)(tiles < nb ? tiles : nb);
