@@ -425,6 +425,14 @@ static int check_kerr(ocfd_b200_ctx *ctx, int word) {
     if (word == 0) return OCFD_OK;
     int zero = 0;
     cudaMemcpy(ctx->p.kerr, &zero, sizeof(int), cudaMemcpyHostToDevice);
+    if (word == 3) {
+        int at[3] = {0, 0, 0};
+        cudaMemcpy(at, ctx->p.kerr + 1, sizeof(at), cudaMemcpyDeviceToHost);
+        const long long v = (long long)(unsigned)at[1] | (long long)at[2] << 32;
+        return fail(ctx, OCFD_ERR_CUDA, "bounds-checked build: a kernel formed an index outside its array "
+                                        "(check at source line " + std::to_string(at[0]) + ", value " +
+                                        std::to_string(v) + "; the access was redirected, the result is invalid)");
+    }
     return fail(ctx, OCFD_ERR_CUDA, word == 2 ? "the learned switch gave up waiting for a tensor-core product "
                                                  "(the step's result is invalid)"
                                                : "a kernel gave up waiting for a staged tile (the step's result is invalid)");

@@ -101,8 +101,38 @@ typedef int (*SlabTransport)(void *user, int op, void *send, void *recv, size_t 
 enum { M_AXX = 0, M_AYY, M_AZZ, M_AKX, M_AKY, M_AKZ, M_AIX, M_AIY, M_AIZ,
        M_ASX, M_ASY, M_ASZ, M_AJAC };
 
+// Bounds-checked build (make bounds: -DOCFD_BOUNDS, libocfd_b200_bounds.so).
+// The index helpers and the walks' global accesses check their indexes; one
+// outside its array sets error word 3 and is replaced by 0, so that the
+// access stays inside the allocation and the call that ran the kernel
+// reports the error.  The default build compiles the checks away.
+#ifdef OCFD_BOUNDS
+// the first failed check also leaves, after the error word, the source line
+// of the check and the offending value (an index, or packed coordinates)
+__device__ __forceinline__ bool bounds_ok(const Params &p, bool ok, int line, long long value) {
+    if (!ok && p.kerr && atomicCAS(p.kerr, 0, 3) == 0) {
+        p.kerr[1] = line;
+        p.kerr[2] = (int)(value & 0xffffffffLL);
+        p.kerr[3] = (int)(value >> 32);
+    }
+    return ok;
+}
+__device__ __forceinline__ long long bounds_idx(const Params &p, long long q, long long n, int line) {
+    return bounds_ok(p, q >= 0 && q < n, line, q) ? q : 0;
+}
+#define OCFD_IDX(p, q, n) ::ocfd::bounds_idx((p), (q), (n), __LINE__)
+#else
+#define OCFD_IDX(p, q, n) (q)
+#endif
+
 __device__ __forceinline__ long long lap_index(const Params &p, int i, int j, int k) {
     // i,j,k are LAP-box coordinates (0 .. n+2*LAP-1)
+#ifdef OCFD_BOUNDS
+    if (!bounds_ok(p, i >= 0 && j >= 0 && k >= 0 && i < p.nx + 2 * OCFD_LAP && j < p.ny + 2 * OCFD_LAP &&
+                          k < p.nz + 2 * OCFD_LAP, __LINE__,
+                   (long long)(i & 0xfffff) | (long long)(j & 0xfffff) << 20 | (long long)(k & 0xfffff) << 40))
+        return 0;
+#endif
     return (long long)i + p.ys * j + p.zs * k;
 }
 // metric m at LAP offset o; UNI selects the constant of a uniform grid (the
@@ -110,11 +140,29 @@ __device__ __forceinline__ long long lap_index(const Params &p, int i, int j, in
 template <bool UNI>
 __device__ __forceinline__ double metric(const Params &p, int m, long long o) {
     if (UNI) return p.mc[m];
-    return p.met[m][o];
+    return p.met[m][OCFD_IDX(p, o, p.lapN)];
 }
 
 __device__ __forceinline__ long long in_index(const Params &p, int i, int j, int k) {
+#ifdef OCFD_BOUNDS
+    if (!bounds_ok(p, i >= 0 && j >= 0 && k >= 0 && i < p.nx && j < p.ny && k < p.nz, __LINE__,
+                   (long long)(i & 0xfffff) | (long long)(j & 0xfffff) << 20 | (long long)(k & 0xfffff) << 40))
+        return 0;
+#endif
     return (long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * k);
+}
+// entries of direction d's hybrid flag array ((n_d + 1) along d)
+__device__ __forceinline__ long long flag_entries(const Params &p, int d) {
+    return (long long)(p.nx + (d == 0)) * (p.ny + (d == 1)) * (p.nz + (d == 2));
+}
+// entry q of direction d's flag array from a pointer fl into it (checked in
+// the bounds build, where an entry outside the array reads as flag 2)
+__device__ __forceinline__ int flag_at(const Params &p, int d, const int8_t *fl, long long q) {
+#ifdef OCFD_BOUNDS
+    const long long a = (long long)(fl - p.flag[d]) + q;
+    if (!bounds_ok(p, a >= 0 && a < flag_entries(p, d), __LINE__, a)) return 2;
+#endif
+    return (int)fl[q];
 }
 
 // x / c for a run-time constant c with inv = RN(1/c): the product plus one

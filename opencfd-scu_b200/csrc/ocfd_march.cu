@@ -114,7 +114,7 @@ k_march(const __grid_constant__ Params p, const __grid_constant__ CUtensorMap tm
 #pragma unroll
         for (int t = 0; t < CH; t++) {
             const int e = P0 + c * CH + t - 3;
-            hf[t] = (hybrid && colok && e >= y0 && e <= y1) ? (int)fl[(long long)e * fst] : 2;
+            hf[t] = (hybrid && colok && e >= y0 && e <= y1) ? flag_at(p, DIR, fl, (long long)e * fst) : 2;
         }
     };
     // the chunk's flags, one byte each (flags are small integers)
@@ -210,14 +210,14 @@ k_march(const __grid_constant__ Params p, const __grid_constant__ CUtensorMap tm
                     if (F >= y0) {               // cell F: faces F-1/2 (prv) and F+1/2 (cur)
                         bool defer = colok && (slow || prv_slow);
                         if (p.has_bnd) defer = defer || (colok && rule_cell(p, DIR, F, n));
-                        const long long ci = cb + (long long)F * cst;
+                        const long long ci = OCFD_IDX(p, cb + (long long)F * cst, N);
                         const unsigned mask = __ballot_sync(FULL, defer);
                         if (mask) {              // one atomic per warp
                             const int leader = __ffs(mask) - 1;
                             unsigned slot = 0;
                             if (lane == leader) slot = atomicAdd(p.defer_count + DIR, (unsigned)__popc(mask));
                             slot = __shfl_sync(FULL, slot, leader);
-                            if (defer) p.defer[DIR][slot + __popc(mask & ((1u << lane) - 1u))] = (unsigned)ci;
+                            if (defer) p.defer[DIR][OCFD_IDX(p, (long long)slot + __popc(mask & ((1u << lane) - 1u)), p.N)] = (unsigned)ci;
                         }
                         if (colok && !defer) {
                             const R aj = (R)metric<UNI>(p, M_AJAC, base + (long long)F * sd);

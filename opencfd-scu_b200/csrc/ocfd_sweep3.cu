@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
     for (int m = 0; m < 10; m++) cur[m] = (R)0.0;
     int slow = 0, carry_slow = 0;
     if (ly == 0 && colok) {
-        const int hf = hybrid ? (int)fl[(long long)y0 * fst] : 2;
+        const int hf = hybrid ? flag_at(p, DIR, fl, (long long)y0 * fst) : 2;
         if constexpr (FAST) {
             slow = !up7_face(p, hf) || near_closure(p, DIR, y0 - 1, n);
             if (!slow) face_up7<RING, LC>(ring, col, y0 - 1, cur);
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
     R nq[5] = {(R)0.0, (R)0.0, (R)0.0, (R)0.0, (R)0.0};
     int nflag = 2;
     if (colok && y0 + 4 + ly <= y1 + 3) load5(p, base + (long long)(y0 + 4 + ly) * sd, nq);
-    if (hybrid && colok && y0 + ly < y1) nflag = fl[(long long)(y0 + ly + 1) * fst];
+    if (hybrid && colok && y0 + ly < y1) nflag = flag_at(p, DIR, fl, (long long)(y0 + ly + 1) * fst);
 
     for (int Y0 = y0; Y0 < y1; Y0 += LY) {
         const int P = Y0 + 4 + ly;
@@ -135,9 +135,10 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
         if (colok && P <= y1 + 3) ring_put<DIR, RING, LC, UNI, EPS0>(p, ring, col, P, base + (long long)P * sd, nq);
         const int hflag = nflag;
         if (colok && P + LY <= y1 + 3) load5(p, base + (long long)(P + LY) * sd, nq);
-        if (hybrid && colok && F + LY < y1) nflag = fl[(long long)(F + LY + 1) * fst];
+        if (hybrid && colok && F + LY < y1) nflag = flag_at(p, DIR, fl, (long long)(F + LY + 1) * fst);
         __syncwarp();
-        const long long ci = cb + (long long)F * cst;
+        // (lanes past the segment's end form an index they never use)
+        const long long ci = valid ? OCFD_IDX(p, cb + (long long)F * cst, N) : 0;
         R old[5];
         if (DIR != 0 && valid) {
 #pragma unroll
@@ -173,7 +174,7 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep3(const __grid_constant_
                 unsigned slot = 0;
                 if (lane == leader) slot = atomicAdd(p.defer_count + DIR, (unsigned)__popc(mask));
                 slot = __shfl_sync(FULL, slot, leader);
-                if (defer) p.defer[DIR][slot + __popc(mask & ((1u << lane) - 1u))] = (unsigned)ci;
+                if (defer) p.defer[DIR][OCFD_IDX(p, (long long)slot + __popc(mask & ((1u << lane) - 1u)), p.N)] = (unsigned)ci;
             }
         }
         if (valid && !defer) {
@@ -214,7 +215,7 @@ __global__ void __launch_bounds__(32 * FIXW) k_sweep3_fix(const __grid_constant_
     const int n = DIR == 0 ? p.nx : (DIR == 1 ? p.ny : p.nz);
     double *win = win_s[w];
     for (unsigned e = blockIdx.x * FIXW + w; e < cnt; e += gridDim.x * FIXW) {
-        const long long ci = p.defer[DIR][e];
+        const long long ci = OCFD_IDX(p, (long long)p.defer[DIR][e], p.N);
         const int i = (int)(ci % p.nx);
         const long long r = ci / p.nx;
         const int j = (int)(r % p.ny), k = (int)(r / p.ny);
@@ -237,7 +238,7 @@ __global__ void __launch_bounds__(32 * FIXW) k_sweep3_fix(const __grid_constant_
             const long long qq = DIR == 0 ? (long long)e1 + (long long)(p.nx + 1) * ((long long)j + (long long)p.ny * k)
                                : DIR == 1 ? (long long)i + (long long)p.nx * ((long long)e1 + (long long)(p.ny + 1) * k)
                                           : (long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * e1);
-            hf = p.flag[DIR][qq];
+            hf = flag_at(p, DIR, p.flag[DIR], qq);
         }
         const int F = X - 1 + (side & 1);
         const bool up7 = up7_face(p, hf) && !near_closure(p, DIR, F, n);

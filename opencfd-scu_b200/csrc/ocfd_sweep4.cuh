@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep4(const __grid_constant_
     }
     __syncwarp();
     if (ly == 0 && colok) {
-        const int hf = KIND == K_HYBC ? (int)fl[(long long)y0 * fst] : 2;
+        const int hf = KIND == K_HYBC ? flag_at(p, DIR, fl, (long long)y0 * fst) : 2;
         R cur[10];
         face4<KIND, RING, LC, UNI, SPLIT>(p, DIR, ring, col, y0 - 1, n, hf, base + (long long)(y0 - 1) * sd, sd, lo, hi, cur);
 #pragma unroll
@@ -287,7 +287,7 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep4(const __grid_constant_
             load5(p, o, q5);
             ring_put<DIR, RING, LC, UNI, EPS0>(p, ring, col, P, o, q5);
         }
-        const int hflag = (KIND == K_HYBC && valid) ? (int)fl[(long long)(F + 1) * fst] : 2;
+        const int hflag = (KIND == K_HYBC && valid) ? flag_at(p, DIR, fl, (long long)(F + 1) * fst) : 2;
         __syncwarp();
         R cur[10];
         if (valid) {
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(32 * SW, MINB) k_sweep4(const __grid_constant_
             R prv[10];
 #pragma unroll
             for (int sv = 0; sv < 10; sv++) prv[sv] = fbuf[(sv * FR + ((F - 1) & (FR - 1))) * LC + col];
-            const long long ci = cb + (long long)F * cst;
+            const long long ci = OCFD_IDX(p, cb + (long long)F * cst, N);
             const R aj = (R)metric<UNI>(p, M_AJAC, base + (long long)F * sd);
             if (p.has_bnd && rule_cell(p, DIR, F, n)) {
                 du_rule_cell<DIR, KIND, RING, LC>(p, ring, col, F, n, du, ci, aj, h, ih, cur, prv);
@@ -346,7 +346,7 @@ __global__ void __launch_bounds__(32 * FIX4W) k_sweep4_fix(const __grid_constant
     R *win = win_s[w];
     // value sv of point Q of the cell's window (point X-4 is entry 0)
     for (unsigned e = blockIdx.x * FIX4W + w; e < cnt; e += gridDim.x * FIX4W) {
-        const long long ci = p.defer[DIR][e];
+        const long long ci = OCFD_IDX(p, (long long)p.defer[DIR][e], p.N);
         const int i = (int)(ci % p.nx);
         const long long r = ci / p.nx;
         const int j = (int)(r % p.ny), k = (int)(r / p.ny);
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(32 * FIX4W) k_sweep4_fix(const __grid_constant
         const long long qq = DIR == 0 ? (long long)e1 + (long long)(p.nx + 1) * ((long long)j + (long long)p.ny * k)
                            : DIR == 1 ? (long long)i + (long long)p.nx * ((long long)e1 + (long long)(p.ny + 1) * k)
                                       : (long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * e1);
-        const int hflag = p.flag[DIR][qq];
+        const int hflag = flag_at(p, DIR, p.flag[DIR], qq);
         const int F = X - 1 + side;
         const bool near = (lo && F <= 3) || (hi && F >= n - 5);
         const bool charf = hflag != 1;

@@ -212,6 +212,7 @@ __device__ __forceinline__ void ring_put(const Params &p, R *ring, int col, int 
 
 template <typename R>
 __device__ __forceinline__ void load5(const Params &p, long long o, R (&q5)[5]) {
+    o = OCFD_IDX(p, o, p.lapN);
 #pragma unroll
     for (int m = 0; m < 5; m++) q5[m] = __ldg(prim_r<R>(p, m) + o);
 }
