@@ -42,6 +42,13 @@ constexpr int OFF_MU = 0, OFF_SG = 14, OFF_W1 = 28, OFF_B1 = OFF_W1 + MLP_H * ML
 // ---------------------------------------------------------------------------
 // features
 // ---------------------------------------------------------------------------
+// quotient of a feature that only the network reads: exact in FP64 (the
+// training features), the two-instruction approximate quotient in FP32 (its
+// error, a few units in the last place, is far below the BF16 rounding the
+// network's input takes)
+template <typename R> __device__ __forceinline__ R feat_div(R a, R b) { return a / b; }
+template <> __device__ __forceinline__ float feat_div<float>(float a, float b) { return __fdividef(a, b); }
+
 // om[a], op[a]: offsets of the minus / plus neighbour along direction a
 template <typename R>
 __device__ __forceinline__ void switch_features(const Params &p, long long c, const long long (&om)[3],
@@ -57,9 +64,9 @@ __device__ __forceinline__ void switch_features(const Params &p, long long c, co
         const R t = fabs(-Pm + 2*P0 - Pp)/den;          // k_sensor's term
         dp = a == 0 ? t : dp + t;
         f[a] = (float)t;
-        f[3 + a] = (float)((Pp - Pm) / den);
+        f[3 + a] = (float)feat_div(Pp - Pm, den);
         const R Dm = d[c + om[a]], Dp = d[c + op[a]];
-        const R rdd = (R)1 / (Dm + 2*D0 + Dp);
+        const R rdd = feat_div((R)1, Dm + 2*D0 + Dp);
         f[6 + a] = (float)(fabs(-Dm + 2*D0 - Dp) * rdd);
         f[9 + a] = (float)((Dp - Dm) * rdd);
     }
