@@ -237,9 +237,10 @@ __device__ void setup(Smem &s, const float *__restrict__ w) {
 }
 
 // The block's teardown: a product still outstanding after a wait ran out is
-// waited for once more (bounded), then warp 0 frees the TMEM columns.
+// waited for once more (bounded; phase has moved past the parity that ran
+// out), then warp 0 frees the TMEM columns.
 __device__ void teardown(Smem &s, bool good, unsigned phase) {
-    if (!__syncthreads_and(good) && threadIdx.x == 0) tma::mbar_wait(&s.bar, phase);
+    if (!__syncthreads_and(good) && threadIdx.x == 0) tma::mbar_wait(&s.bar, phase ^ 1u);
     before_sync();
     __syncthreads();
     after_sync();
