@@ -550,15 +550,21 @@ k_vdiv(const __grid_constant__ Params p, const __grid_constant__ CUtensorMap tmx
             for (int q = k - H; q <= k + H; q++) {
                 const int s = slot(q);
                 if (zpend & (1u << s)) {
-                    if (!tma::mbar_wait(&zbar[s], (zph >> s) & 1u)) failed = true;
-                    zph ^= 1u << s;
-                    zpend &= ~(1u << s);
+                    if (tma::mbar_wait(&zbar[s], (zph >> s) & 1u)) {
+                        zph ^= 1u << s;
+                        zpend &= ~(1u << s);
+                    } else {
+                        failed = true;          // still pending: waited for again on the way out
+                    }
                 }
             }
             if (xypend & (1u << b)) {
-                if (!tma::mbar_wait(&xybar[b], (xyph >> b) & 1u)) failed = true;
-                xyph ^= 1u << b;
-                xypend &= ~(1u << b);
+                if (tma::mbar_wait(&xybar[b], (xyph >> b) & 1u)) {
+                    xyph ^= 1u << b;
+                    xypend &= ~(1u << b);
+                } else {
+                    failed = true;
+                }
             }
             if (valid && !failed) {
                 const long long o = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
@@ -678,9 +684,12 @@ k_vev(const __grid_constant__ Params p, const __grid_constant__ CUtensorMap tmq,
             for (int q = k - H; q <= k + H; q++) {
                 const int s = slot(q);
                 if (zpend & (1u << s)) {
-                    if (!tma::mbar_wait(&zbar[s], (zph >> s) & 1u)) failed = true;
-                    zph ^= 1u << s;
-                    zpend &= ~(1u << s);
+                    if (tma::mbar_wait(&zbar[s], (zph >> s) & 1u)) {
+                        zph ^= 1u << s;
+                        zpend &= ~(1u << s);
+                    } else {
+                        failed = true;          // still pending: waited for again on the way out
+                    }
                 }
             }
             if (valid && !failed) {
