@@ -2,7 +2,7 @@
 //
 // One stage (reference driver order, src/OCFD_NS_Solver.cu:76-89 and
 // src/OCFD_Stream.cu:28-54):
-//   [KRK=1, hybrid] sensor        -> int8 face flags            (k_sensor)
+//   [KRK=1, hybrid] sensor        -> int8 face flags            (k_sensor_march)
 //   ghost fill of d,u,v,w,T        (periodic wrap on device)    (k_ghost_prim)
 //   inviscid x, y, z sweeps        -> du (single writer, fixed order)  (ocfd_sweep3/4.cu, ocfd_march.cu)
 //   viscous gradients, Ev, Ev ghosts, divergence -> du         (k_vis_*)
@@ -20,49 +20,63 @@ namespace ocfd {
 // (src/OCFD_Schemes_hybrid_auto.cu:48-68, :611-703).  Flag q along DIR
 // belongs to cell q-1; P = p00*d*T is formed on the fly from the LAP-box d,T
 // as they stand before this stage's ghost fill.  The three arrays' entries
-// of one cell share its value, so one thread per cell of the extended box
-// (-1 .. n-1 in each direction) forms it once and writes the entries the
-// cell owns: entry i+1 of the x array (j, k interior), j+1 of the y array,
-// k+1 of the z array.
+// of one cell share its value, so each cell of the extended box (-1 .. n-1
+// in each direction) forms it once and writes the entries it owns: entry
+// i+1 of the x array (j, k interior), j+1 of the y array, k+1 of the z
+// array.
 // ---------------------------------------------------------------------------
+// Each thread marches along z through a segment of its (i, j) column of the
+// extended box: a block covers a 32 x 8 tile of (i, j), P of the column's
+// planes k-1, k, k+1 stays in registers, and the x and y neighbours of
+// plane k are read through L1 from the rows the block's own warps load (10
+// loads a cell instead of the 26 of one thread per cell).  The sum of the
+// three terms is formed in the reference's order.
+constexpr int SEN_X = 32, SEN_Y = 8;
 template <typename R>
-__global__ void k_sensor(Params p) {
-    const long long ex = p.nx + 1, ey = p.ny + 1, ez = p.nz + 1;
-    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= ex * ey * ez) return;
-    const int i = (int)(tid % ex) - 1;
-    const long long r = tid / ex;
-    const int j = (int)(r % ey) - 1, k = (int)(r / ey) - 1;
-    const bool inx = j >= 0 && k >= 0, iny = i >= 0 && k >= 0, inz = i >= 0 && j >= 0;
-    int kp = 1;
-    if (inx || iny || inz) {
-        const R *d = prim_r<R>(p, 0), *T = prim_r<R>(p, 4);
-        const long long c = lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP);
-        const R p00 = (R)p.p00;
-        auto P = [&](long long o) { return p00 * d[o] * T[o]; };
-        R P0 = P(c);
-        R Pm = P(c - 1), Pp = P(c + 1);
-        R dp0 = fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
-        Pm = P(c - p.ys); Pp = P(c + p.ys);
-        dp0 += fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
-        Pm = P(c - p.zs); Pp = P(c + p.zs);
-        dp0 += fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
-        if (dp0 > (R)p.dp1) kp += 1;
-        if (dp0 > (R)p.dp2) kp += 1;
-        if (inx) p.flag[0][(long long)(i + 1) + ex * ((long long)j + (long long)p.ny * k)] = (int8_t)kp;
-        if (iny) p.flag[1][(long long)i + (long long)p.nx * ((long long)(j + 1) + ey * k)] = (int8_t)kp;
-        if (inz) p.flag[2][(long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * (k + 1))] = (int8_t)kp;
-    }
-    if (p.flag_count) {            // faces per direction whose flag is not 1
-        const unsigned act = __activemask();
-        const int lane = threadIdx.x & 31;
-        const bool non1 = kp != 1;
-        const unsigned mx = __ballot_sync(act, non1 && inx), my = __ballot_sync(act, non1 && iny),
-                       mz = __ballot_sync(act, non1 && inz);
-        if (lane == __ffs(act) - 1) {
-            if (mx) atomicAdd(p.flag_count + 0, (unsigned)__popc(mx));
-            if (my) atomicAdd(p.flag_count + 1, (unsigned)__popc(my));
-            if (mz) atomicAdd(p.flag_count + 2, (unsigned)__popc(mz));
+__global__ void __launch_bounds__(SEN_X * SEN_Y) k_sensor_march(Params p, int seg) {
+    const int ex = p.nx + 1, ey = p.ny + 1, ez = p.nz + 1;
+    const int ntx = (ex + SEN_X - 1) / SEN_X;
+    const int i = (int)(blockIdx.x % ntx) * SEN_X + (int)(threadIdx.x % SEN_X) - 1;
+    const int j = (int)(blockIdx.x / ntx) * SEN_Y + (int)(threadIdx.x / SEN_X) - 1;
+    const int ka = (int)blockIdx.y * seg - 1, kb = min(ez - 1, ka + seg);   // planes ka .. kb-1
+    const bool col = i < ex - 1 && j < ey - 1;              // i, j in -1 .. n-1
+    const R *d = prim_r<R>(p, 0), *T = prim_r<R>(p, 4);
+    const R p00 = (R)p.p00;
+    auto P = [&](long long o) { return p00 * d[o] * T[o]; };
+    const int lane = threadIdx.x & 31;
+    // a column with i and j both ghost owns no entry; it still takes part in
+    // the warp's ballots
+    const bool any = col && (i >= 0 || j >= 0);
+    long long c = any ? lap_index(p, i + OCFD_LAP, j + OCFD_LAP, ka + OCFD_LAP) : 0;
+    R Pz0 = (R)0, Pz1 = (R)0;
+    if (any) { Pz0 = P(c - p.zs); Pz1 = P(c); }
+    for (int k = ka; k < kb; k++, c += p.zs) {
+        int kp = 1;
+        bool inx = false, iny = false, inz = false;
+        if (any) {
+            inx = j >= 0 && k >= 0; iny = i >= 0 && k >= 0; inz = i >= 0 && j >= 0;
+            const R P0 = Pz1, Pzm = Pz0, Pzp = P(c + p.zs);
+            R Pm = P(c - 1), Pp = P(c + 1);
+            R dp0 = fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
+            Pm = P(c - p.ys); Pp = P(c + p.ys);
+            dp0 += fabs(-Pm + 2*P0 - Pp)/(Pm + 2*P0 + Pp);
+            dp0 += fabs(-Pzm + 2*P0 - Pzp)/(Pzm + 2*P0 + Pzp);
+            if (dp0 > (R)p.dp1) kp += 1;
+            if (dp0 > (R)p.dp2) kp += 1;
+            if (inx) p.flag[0][(long long)(i + 1) + (long long)ex * ((long long)j + (long long)p.ny * k)] = (int8_t)kp;
+            if (iny) p.flag[1][(long long)i + (long long)p.nx * ((long long)(j + 1) + (long long)ey * k)] = (int8_t)kp;
+            if (inz) p.flag[2][(long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * (k + 1))] = (int8_t)kp;
+            Pz0 = P0; Pz1 = Pzp;
+        }
+        if (p.flag_count) {        // faces per direction whose flag is not 1
+            const bool non1 = kp != 1;
+            const unsigned mx = __ballot_sync(0xffffffffu, non1 && inx), my = __ballot_sync(0xffffffffu, non1 && iny),
+                           mz = __ballot_sync(0xffffffffu, non1 && inz);
+            if (lane == 0) {
+                if (mx) atomicAdd(p.flag_count + 0, (unsigned)__popc(mx));
+                if (my) atomicAdd(p.flag_count + 1, (unsigned)__popc(my));
+                if (mz) atomicAdd(p.flag_count + 2, (unsigned)__popc(mz));
+            }
         }
     }
 }
@@ -977,8 +991,19 @@ cudaError_t launch_sensor(const Params &p, cudaStream_t st) {
         cudaError_t e = cudaMemsetAsync(p.flag_count, 0, 3 * sizeof(unsigned), st);
         if (e != cudaSuccess) return e;
     }
-    if (p.mixed) k_sensor<float><<<blocks_for(n, 256), 256, 0, st>>>(p);
-    else         k_sensor<double><<<blocks_for(n, 256), 256, 0, st>>>(p);
+    (void)n;
+    // tiles of the extended box's (i, j), z split into segments so that
+    // there are about eight blocks per SM
+    const int ntiles = ((p.nx + 1 + SEN_X - 1) / SEN_X) * ((p.ny + 1 + SEN_Y - 1) / SEN_Y);
+    const int ez = p.nz + 1;
+    int nseg = (148 * 8 + ntiles - 1) / ntiles;
+    if (nseg > ez) nseg = ez;
+    if (nseg < 1) nseg = 1;
+    const int seg = (ez + nseg - 1) / nseg;
+    nseg = (ez + seg - 1) / seg;
+    const dim3 grid((unsigned)ntiles, (unsigned)nseg);
+    if (p.mixed) k_sensor_march<float><<<grid, SEN_X * SEN_Y, 0, st>>>(p, seg);
+    else         k_sensor_march<double><<<grid, SEN_X * SEN_Y, 0, st>>>(p, seg);
     return cudaGetLastError();
 }
 

@@ -13,7 +13,7 @@
 //                          (P+ - P-) / (P- + 2P0 + P+), and the same for D;
 //   the sums of the three second-difference terms of P and of D.
 // The sum for P is the plain sensor's value, formed in the same order and
-// precision as k_sensor, so the fallback flag is the plain flag exactly.
+// precision as k_sensor_march, so the fallback flag is the plain flag exactly.
 //
 // Network: 14 -> 32 -> 32 -> 1 with ReLU, inputs standardised by (mu,
 // sigma); parameter vector mu[14] sigma[14] W1[32][14] b1[32] W2[32][32]
@@ -61,7 +61,7 @@ __device__ __forceinline__ void switch_features(const Params &p, long long c, co
     for (int a = 0; a < 3; a++) {
         const R Pm = P(c + om[a]), Pp = P(c + op[a]);
         const R den = Pm + 2*P0 + Pp;
-        const R t = fabs(-Pm + 2*P0 - Pp)/den;          // k_sensor's term
+        const R t = fabs(-Pm + 2*P0 - Pp)/den;          // the sensor's term
         dp = a == 0 ? t : dp + t;
         f[a] = (float)t;
         f[3 + a] = (float)feat_div(Pp - Pm, den);
