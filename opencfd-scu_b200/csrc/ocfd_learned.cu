@@ -49,6 +49,26 @@ constexpr int OFF_MU = 0, OFF_SG = 14, OFF_W1 = 28, OFF_B1 = OFF_W1 + MLP_H * ML
 template <typename R> __device__ __forceinline__ R feat_div(R a, R b) { return a / b; }
 template <> __device__ __forceinline__ float feat_div<float>(float a, float b) { return __fdividef(a, b); }
 
+// The 14 features and the sensor's sum dp of a cell from P = p00 d T and d
+// at the cell (P0, D0) and at its minus / plus neighbours along x, y, z
+template <typename R>
+__device__ __forceinline__ void features_of(R P0, R D0, const R (&Pm)[3], const R (&Pp)[3], const R (&Dm)[3],
+                                            const R (&Dp)[3], float f[MLP_IN], R &dp) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const R den = Pm[a] + 2*P0 + Pp[a];
+        const R t = fabs(-Pm[a] + 2*P0 - Pp[a])/den;    // the sensor's term
+        dp = a == 0 ? t : dp + t;
+        f[a] = (float)t;
+        f[3 + a] = (float)feat_div(Pp[a] - Pm[a], den);
+        const R rdd = feat_div((R)1, Dm[a] + 2*D0 + Dp[a]);
+        f[6 + a] = (float)(fabs(-Dm[a] + 2*D0 - Dp[a]) * rdd);
+        f[9 + a] = (float)((Dp[a] - Dm[a]) * rdd);
+    }
+    f[12] = f[0] + f[1] + f[2];
+    f[13] = f[6] + f[7] + f[8];
+}
+
 // om[a], op[a]: offsets of the minus / plus neighbour along direction a
 template <typename R>
 __device__ __forceinline__ void switch_features(const Params &p, long long c, const long long (&om)[3],
@@ -56,22 +76,13 @@ __device__ __forceinline__ void switch_features(const Params &p, long long c, co
     const R *d = prim_r<R>(p, 0), *T = prim_r<R>(p, 4);
     const R p00 = (R)p.p00;
     auto P = [&](long long o) { return p00 * d[o] * T[o]; };
-    const R P0 = P(c), D0 = d[c];
+    R Pm[3], Pp[3], Dm[3], Dp[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const R Pm = P(c + om[a]), Pp = P(c + op[a]);
-        const R den = Pm + 2*P0 + Pp;
-        const R t = fabs(-Pm + 2*P0 - Pp)/den;          // the sensor's term
-        dp = a == 0 ? t : dp + t;
-        f[a] = (float)t;
-        f[3 + a] = (float)feat_div(Pp - Pm, den);
-        const R Dm = d[c + om[a]], Dp = d[c + op[a]];
-        const R rdd = feat_div((R)1, Dm + 2*D0 + Dp);
-        f[6 + a] = (float)(fabs(-Dm + 2*D0 - Dp) * rdd);
-        f[9 + a] = (float)((Dp - Dm) * rdd);
+        Pm[a] = P(c + om[a]); Pp[a] = P(c + op[a]);
+        Dm[a] = d[c + om[a]]; Dp[a] = d[c + op[a]];
     }
-    f[12] = f[0] + f[1] + f[2];
-    f[13] = f[6] + f[7] + f[8];
+    features_of<R>(P(c), d[c], Pm, Pp, Dm, Dp, f, dp);
 }
 
 template <typename R>
@@ -348,31 +359,42 @@ __global__ void __launch_bounds__(umma::ROWS) k_mlp_infer(const float *__restric
 // the y array and entry k+1 of the z array.  conf_logit = ln(c / (1 - c))
 // for confidence threshold c.  stats (optional): cells decided by the
 // network, cells left to the plain flag, network flags that differ from the
-// plain flag.  Persistent blocks of 128 cells per tile, consecutive cells
-// along x on consecutive threads.
+// plain flag.  A block covers a 32 x 4 tile of (i, j) -- the 128 rows of one
+// product -- and marches along z through a segment of planes: P and d of
+// the column's planes k-1, k, k+1 stay in registers, the x and y neighbours
+// come through L1 from the rows the block's own warps load.
+constexpr int SWX = 32, SWY = umma::ROWS / SWX;
 template <typename R>
 __global__ void __launch_bounds__(umma::ROWS) k_switch_infer(Params p, const float *__restrict__ w, float conf_logit,
-                                                             unsigned long long *stats) {
+                                                             unsigned long long *stats, int seg) {
     __shared__ umma::Smem s;
     umma::setup(s, w);
     const int lane = threadIdx.x & 31;
-    const long long ex = p.nx + 1, ey = p.ny + 1, ez = p.nz + 1, total = ex * ey * ez;
-    const long long ntile = (total + umma::ROWS - 1) / umma::ROWS;
-    const long long om[3] = {-1LL, -p.ys, -p.zs}, op[3] = {1LL, p.ys, p.zs};
+    const int ex = p.nx + 1, ey = p.ny + 1, ez = p.nz + 1;
+    const int ntx = (ex + SWX - 1) / SWX;
+    const int i = (int)(blockIdx.x % ntx) * SWX + (int)(threadIdx.x % SWX) - 1;
+    const int j = (int)(blockIdx.x / ntx) * SWY + (int)(threadIdx.x / SWX) - 1;
+    const int ka = (int)blockIdx.y * seg - 1, kb = min(ez - 1, ka + seg);   // planes ka .. kb-1
+    const bool any = i < ex - 1 && j < ey - 1;          // a cell of the extended box
+    const R *d = prim_r<R>(p, 0), *T = prim_r<R>(p, 4);
+    const R p00 = (R)p.p00;
+    auto P = [&](long long o) { return p00 * d[o] * T[o]; };
+    long long c = any ? lap_index(p, i + OCFD_LAP, j + OCFD_LAP, ka + OCFD_LAP) : 0;
+    R Pz0 = (R)0, Pz1 = (R)0, Dz0 = (R)0, Dz1 = (R)0;
+    if (any) { Pz0 = P(c - p.zs); Pz1 = P(c); Dz0 = d[c - p.zs]; Dz1 = d[c]; }
     unsigned long long n_sure = 0, n_unsure = 0, n_differ = 0;
     bool good = true;
     unsigned phase = 0;
-    for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
-        const long long tid = tile * umma::ROWS + threadIdx.x;
-        const bool live = tid < total;
-        int i = 0, j = 0, k = 0;
+    for (int k = ka; k < kb; k++, c += p.zs) {
         float f[MLP_IN] = {};
         R dp = (R)0;
-        if (live) {
-            i = (int)(tid % ex) - 1;
-            const long long r = tid / ex;
-            j = (int)(r % ey) - 1; k = (int)(r / ey) - 1;
-            switch_features<R>(p, lap_index(p, i + OCFD_LAP, j + OCFD_LAP, k + OCFD_LAP), om, op, f, dp);
+        if (any) {
+            R Pm[3], Pp[3], Dm[3], Dp[3];
+            Pm[0] = P(c - 1);      Pp[0] = P(c + 1);      Dm[0] = d[c - 1];      Dp[0] = d[c + 1];
+            Pm[1] = P(c - p.ys);   Pp[1] = P(c + p.ys);   Dm[1] = d[c - p.ys];   Dp[1] = d[c + p.ys];
+            Pm[2] = Pz0;           Pp[2] = P(c + p.zs);   Dm[2] = Dz0;           Dp[2] = d[c + p.zs];
+            features_of<R>(Pz1, Dz1, Pm, Pp, Dm, Dp, f, dp);
+            Pz0 = Pz1; Pz1 = Pp[2]; Dz0 = Dz1; Dz1 = Dp[2];
         }
         float x[MLP_IN];
         standardise(s, f, x);
@@ -381,9 +403,9 @@ __global__ void __launch_bounds__(umma::ROWS) k_switch_infer(Params p, const flo
         const int plain = plain_flag(p, dp);
         const bool sure = fabsf(z) >= conf_logit;
         const int kp = sure ? (z >= 0.0f ? max(2, plain) : 1) : plain;
-        const bool inx = live && j >= 0 && k >= 0, iny = live && i >= 0 && k >= 0, inz = live && i >= 0 && j >= 0;
-        if (inx) p.flag[0][(long long)(i + 1) + ex * ((long long)j + (long long)p.ny * k)] = (int8_t)kp;
-        if (iny) p.flag[1][(long long)i + (long long)p.nx * ((long long)(j + 1) + ey * k)] = (int8_t)kp;
+        const bool inx = any && j >= 0 && k >= 0, iny = any && i >= 0 && k >= 0, inz = any && i >= 0 && j >= 0;
+        if (inx) p.flag[0][(long long)(i + 1) + (long long)ex * ((long long)j + (long long)p.ny * k)] = (int8_t)kp;
+        if (iny) p.flag[1][(long long)i + (long long)p.nx * ((long long)(j + 1) + (long long)ey * k)] = (int8_t)kp;
         if (inz) p.flag[2][(long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * (k + 1))] = (int8_t)kp;
         if (p.flag_count) {          // faces per direction whose flag is not 1
             const bool non1 = kp != 1;
@@ -396,8 +418,8 @@ __global__ void __launch_bounds__(umma::ROWS) k_switch_infer(Params p, const flo
             }
         }
         if (stats) {
-            const unsigned ms = __ballot_sync(0xffffffffu, live && sure), mu = __ballot_sync(0xffffffffu, live && !sure),
-                           md = __ballot_sync(0xffffffffu, live && sure && kp != plain);
+            const unsigned ms = __ballot_sync(0xffffffffu, any && sure), mu = __ballot_sync(0xffffffffu, any && !sure),
+                           md = __ballot_sync(0xffffffffu, any && sure && kp != plain);
             n_sure += __popc(ms); n_unsure += __popc(mu); n_differ += __popc(md);
         }
     }
@@ -575,10 +597,20 @@ cudaError_t launch_switch_infer(const Params &p, const float *w, float conf_logi
         cudaError_t e = cudaMemsetAsync(p.flag_count, 0, 3 * sizeof(unsigned), st);
         if (e != cudaSuccess) return e;
     }
-    const long long n = (long long)(p.nx + 1) * (p.ny + 1) * (p.nz + 1);
-    const long long tiles = (n + umma::ROWS - 1) / umma::ROWS;
-    if (p.mixed) k_switch_infer<float><<<resident_blocks(k_switch_infer<float>, tiles), umma::ROWS, 0, st>>>(p, w, conf_logit, stats);
-    else         k_switch_infer<double><<<resident_blocks(k_switch_infer<double>, tiles), umma::ROWS, 0, st>>>(p, w, conf_logit, stats);
+    // tiles of the extended box's (i, j), z split into as many segments as
+    // keep the grid within one wave of resident blocks
+    const int ntiles = ((p.nx + 1 + SWX - 1) / SWX) * ((p.ny + 1 + SWY - 1) / SWY);
+    const int ez = p.nz + 1;
+    const long long want = p.mixed ? resident_blocks(k_switch_infer<float>, 1LL << 40)
+                                   : resident_blocks(k_switch_infer<double>, 1LL << 40);
+    int nseg = (int)(want / ntiles);
+    if (nseg > ez) nseg = ez;
+    if (nseg < 1) nseg = 1;
+    const int seg = (ez + nseg - 1) / nseg;
+    nseg = (ez + seg - 1) / seg;
+    const dim3 grid((unsigned)ntiles, (unsigned)nseg);
+    if (p.mixed) k_switch_infer<float><<<grid, umma::ROWS, 0, st>>>(p, w, conf_logit, stats, seg);
+    else         k_switch_infer<double><<<grid, umma::ROWS, 0, st>>>(p, w, conf_logit, stats, seg);
     return cudaGetLastError();
 }
 
