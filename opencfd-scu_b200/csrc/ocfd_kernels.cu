@@ -92,37 +92,38 @@ template <typename T> struct GhostList { T *f[12]; int dirmask[12]; int n; };
 
 template <typename T>
 __global__ void k_ghost(Params p, GhostList<T> g) {
-    const int L = OCFD_LAP;
-    long long sx = 2LL * L * p.ny * p.nz, sy = 2LL * L * p.nx * p.nz, sz = 2LL * L * p.nx * p.ny;
-    long long per = sx + sy + sz;
-    long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= per * g.n) return;
-    int fi = (int)(tid / per);
-    long long q = tid - (long long)fi * per;
-    T *f = g.f[fi];
-    int mask = g.dirmask[fi];
+    // one field per grid row; element q of its ghost slabs (x, then y, then
+    // z), decomposed with 32-bit arithmetic (a field's slabs hold fewer than
+    // 2^31 elements)
+    constexpr unsigned L = OCFD_LAP, L2 = 2 * OCFD_LAP;
+    const unsigned nx = (unsigned)p.nx, ny = (unsigned)p.ny, nz = (unsigned)p.nz;
+    const unsigned sx = L2 * ny * nz, sy = L2 * nx * nz, sz = L2 * nx * ny;
+    unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= sx + sy + sz) return;
+    T *f = g.f[blockIdx.y];
+    const int mask = g.dirmask[blockIdx.y];
     if (q < sx) {
         if (!(mask & 1) || !p.periodic[0]) return;
-        int i = (int)(q % (2 * L)); long long r = q / (2 * L);
-        int j = (int)(r % p.ny) + L, k = (int)(r / p.ny) + L;
-        int dst = i < L ? i : p.nx + i;              // 0..L-1  or  nx+L..nx+2L-1
-        int src = i < L ? p.nx + i : i;              // wrap
+        const unsigned i = q % L2, r = q / L2;
+        const unsigned j = r % ny + L, k = r / ny + L;
+        const unsigned dst = i < L ? i : nx + i;             // 0..L-1  or  nx+L..nx+2L-1
+        const unsigned src = i < L ? nx + i : i;             // wrap
         f[lap_index(p, dst, j, k)] = f[lap_index(p, src, j, k)];
     } else if (q < sx + sy) {
         if (!(mask & 2) || !p.periodic[1]) return;
         q -= sx;
-        int i = (int)(q % p.nx) + L; long long r = q / p.nx;
-        int jj = (int)(r % (2 * L)); int k = (int)(r / (2 * L)) + L;
-        int dst = jj < L ? jj : p.ny + jj;
-        int src = jj < L ? p.ny + jj : jj;
+        const unsigned i = q % nx + L, r = q / nx;
+        const unsigned jj = r % L2, k = r / L2 + L;
+        const unsigned dst = jj < L ? jj : ny + jj;
+        const unsigned src = jj < L ? ny + jj : jj;
         f[lap_index(p, i, dst, k)] = f[lap_index(p, i, src, k)];
     } else {
         if (!(mask & 4) || !p.periodic[2]) return;
         q -= sx + sy;
-        int i = (int)(q % p.nx) + L; long long r = q / p.nx;
-        int j = (int)(r % p.ny) + L; int kk = (int)(r / p.ny);
-        int dst = kk < L ? kk : p.nz + kk;
-        int src = kk < L ? p.nz + kk : kk;
+        const unsigned i = q % nx + L, r = q / nx;
+        const unsigned j = r % ny + L, kk = r / ny;
+        const unsigned dst = kk < L ? kk : nz + kk;
+        const unsigned src = kk < L ? nz + kk : kk;
         f[lap_index(p, i, j, dst)] = f[lap_index(p, i, j, src)];
     }
 }
@@ -1009,11 +1010,14 @@ cudaError_t launch_sensor(const Params &p, cudaStream_t st) {
 
 template <typename T>
 static cudaError_t launch_ghost_t(const Params &p, T *const *fields, const int *dirmask, int nf, cudaStream_t st) {
+    const long long per = 2LL * OCFD_LAP * ((long long)p.ny * p.nz + (long long)p.nx * p.nz + (long long)p.nx * p.ny);
+    if (nf <= 0) return cudaSuccess;
+    if (per >= (1LL << 31) || nf > 12) return cudaErrorInvalidValue;
     GhostList<T> g;
     g.n = nf;
     for (int i = 0; i < nf; i++) { g.f[i] = fields[i]; g.dirmask[i] = dirmask[i]; }
-    long long per = 2LL * OCFD_LAP * ((long long)p.ny * p.nz + (long long)p.nx * p.nz + (long long)p.nx * p.ny);
-    k_ghost<T><<<blocks_for(per * nf, 256), 256, 0, st>>>(p, g);
+    const dim3 grid((unsigned)((per + 255) / 256), (unsigned)nf);
+    k_ghost<T><<<grid, 256, 0, st>>>(p, g);
     return cudaGetLastError();
 }
 cudaError_t launch_ghost(const Params &p, double *const *fields, const int *dirmask, int nf, cudaStream_t st) {
