@@ -55,8 +55,7 @@ __device__ __forceinline__ void char_sign(const R *ring, int col, int F, int n, 
         for (int k = 0; k < 8; k++)
             fv[m][k] = (k >= K0 && k <= K1) ? rv<RING, LC>(ring, col, S * 5 + m, F - 3 + k) : (R)0.0;
     R o5[5];
-#pragma unroll
-    for (int c = 0; c < 5; c++) {
+    auto one = [&](int c) {
         R Lr[5], vals[8], Rc[5];
         L_row(rec, 1, c, Lr);
 #pragma unroll
@@ -75,6 +74,18 @@ __device__ __forceinline__ void char_sign(const R *ring, int col, int F, int n, 
 #pragma unroll
             for (int m = 0; m < 5; m++) o5[m] = o5[m] + Rc[m] * res;
         }
+    };
+    // the general form in FP32 keeps one copy of the field loop's body: its
+    // five unrolled copies (a reconstruction, a closure and a WENO5 each)
+    // left the walk waiting on instruction fetch (10 % slower on the ramp);
+    // in FP64 the unrolled copies keep the walk's values in registers and
+    // measured faster
+    if constexpr (HOT || sizeof(R) == 8) {
+#pragma unroll
+        for (int c = 0; c < 5; c++) one(c);
+    } else {
+#pragma unroll 1
+        for (int c = 0; c < 5; c++) one(c);
     }
 #pragma unroll
     for (int m = 0; m < 5; m++) out[S * 5 + m] = o5[m];
