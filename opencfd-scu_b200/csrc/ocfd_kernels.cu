@@ -50,6 +50,7 @@ __global__ void __launch_bounds__(SEN_X * SEN_Y) k_sensor_march(Params p, int se
     long long c = any ? lap_index(p, i + OCFD_LAP, j + OCFD_LAP, ka + OCFD_LAP) : 0;
     R Pz0 = (R)0, Pz1 = (R)0;
     if (any) { Pz0 = P(c - p.zs); Pz1 = P(c); }
+    unsigned nx1 = 0, ny1 = 0, nz1 = 0;
     for (int k = ka; k < kb; k++, c += p.zs) {
         int kp = 1;
         bool inx = false, iny = false, inz = false;
@@ -68,15 +69,19 @@ __global__ void __launch_bounds__(SEN_X * SEN_Y) k_sensor_march(Params p, int se
             if (inz) p.flag[2][(long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * (k + 1))] = (int8_t)kp;
             Pz0 = P0; Pz1 = Pzp;
         }
-        if (p.flag_count) {        // faces per direction whose flag is not 1
-            const bool non1 = kp != 1;
-            const unsigned mx = __ballot_sync(0xffffffffu, non1 && inx), my = __ballot_sync(0xffffffffu, non1 && iny),
-                           mz = __ballot_sync(0xffffffffu, non1 && inz);
-            if (lane == 0) {
-                if (mx) atomicAdd(p.flag_count + 0, (unsigned)__popc(mx));
-                if (my) atomicAdd(p.flag_count + 1, (unsigned)__popc(my));
-                if (mz) atomicAdd(p.flag_count + 2, (unsigned)__popc(mz));
-            }
+        const bool non1 = kp != 1;
+        nx1 += non1 && inx; ny1 += non1 && iny; nz1 += non1 && inz;
+    }
+    // faces per direction whose flag is not 1: one sum per warp for the
+    // whole segment (an atomic per warp and plane queued on three words)
+    if (p.flag_count) {
+        nx1 = __reduce_add_sync(0xffffffffu, nx1);
+        ny1 = __reduce_add_sync(0xffffffffu, ny1);
+        nz1 = __reduce_add_sync(0xffffffffu, nz1);
+        if (lane == 0) {
+            if (nx1) atomicAdd(p.flag_count + 0, nx1);
+            if (ny1) atomicAdd(p.flag_count + 1, ny1);
+            if (nz1) atomicAdd(p.flag_count + 2, nz1);
         }
     }
 }

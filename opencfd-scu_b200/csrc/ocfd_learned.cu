@@ -383,6 +383,7 @@ __global__ void __launch_bounds__(umma::ROWS) k_switch_infer(Params p, const flo
     R Pz0 = (R)0, Pz1 = (R)0, Dz0 = (R)0, Dz1 = (R)0;
     if (any) { Pz0 = P(c - p.zs); Pz1 = P(c); Dz0 = d[c - p.zs]; Dz1 = d[c]; }
     unsigned long long n_sure = 0, n_unsure = 0, n_differ = 0;
+    unsigned nx1 = 0, ny1 = 0, nz1 = 0;
     bool good = true;
     unsigned phase = 0;
     for (int k = ka; k < kb; k++, c += p.zs) {
@@ -407,16 +408,8 @@ __global__ void __launch_bounds__(umma::ROWS) k_switch_infer(Params p, const flo
         if (inx) p.flag[0][(long long)(i + 1) + (long long)ex * ((long long)j + (long long)p.ny * k)] = (int8_t)kp;
         if (iny) p.flag[1][(long long)i + (long long)p.nx * ((long long)(j + 1) + (long long)ey * k)] = (int8_t)kp;
         if (inz) p.flag[2][(long long)i + (long long)p.nx * ((long long)j + (long long)p.ny * (k + 1))] = (int8_t)kp;
-        if (p.flag_count) {          // faces per direction whose flag is not 1
-            const bool non1 = kp != 1;
-            const unsigned mx = __ballot_sync(0xffffffffu, non1 && inx), my = __ballot_sync(0xffffffffu, non1 && iny),
-                           mz = __ballot_sync(0xffffffffu, non1 && inz);
-            if (lane == 0) {
-                if (mx) atomicAdd(p.flag_count + 0, (unsigned)__popc(mx));
-                if (my) atomicAdd(p.flag_count + 1, (unsigned)__popc(my));
-                if (mz) atomicAdd(p.flag_count + 2, (unsigned)__popc(mz));
-            }
-        }
+        const bool non1 = kp != 1;
+        nx1 += non1 && inx; ny1 += non1 && iny; nz1 += non1 && inz;
         if (stats) {
             const unsigned ms = __ballot_sync(0xffffffffu, any && sure), mu = __ballot_sync(0xffffffffu, any && !sure),
                            md = __ballot_sync(0xffffffffu, any && sure && kp != plain);
@@ -427,6 +420,18 @@ __global__ void __launch_bounds__(umma::ROWS) k_switch_infer(Params p, const flo
         atomicAdd(stats + 0, n_sure);
         atomicAdd(stats + 1, n_unsure);
         atomicAdd(stats + 2, n_differ);
+    }
+    // faces per direction whose flag is not 1: one sum per warp for the
+    // whole segment
+    if (p.flag_count) {
+        nx1 = __reduce_add_sync(0xffffffffu, nx1);
+        ny1 = __reduce_add_sync(0xffffffffu, ny1);
+        nz1 = __reduce_add_sync(0xffffffffu, nz1);
+        if (lane == 0) {
+            if (nx1) atomicAdd(p.flag_count + 0, nx1);
+            if (ny1) atomicAdd(p.flag_count + 1, ny1);
+            if (nz1) atomicAdd(p.flag_count + 2, nz1);
+        }
     }
     if (!good && p.kerr) atomicExch(p.kerr, 2);
     umma::teardown(s, good, phase);
