@@ -82,6 +82,12 @@ int ocfd_b200_destroy(ocfd_b200_ctx *ctx);
  * context's own stream. */
 int ocfd_b200_set_stream(ocfd_b200_ctx *ctx, void *stream);
 void *ocfd_b200_get_stream(const ocfd_b200_ctx *ctx);
+/* Waits for the context's stream, then reads the kernels' error word: a
+ * wait on a staged tile or on a tensor-core product that ran out of its
+ * bound (the kernel stopped; the step's result is invalid), or, in the
+ * bounds-checked build, an index outside its array, returns OCFD_ERR_CUDA
+ * with the cause in ocfd_b200_last_error and clears the word.  The hybrid
+ * scheme's per-step read-back checks the same word. */
 int ocfd_b200_synchronize(ocfd_b200_ctx *ctx);
 
 /* Grid metrics, 13 interior fields (host or device memory).  Replaces the
