@@ -167,6 +167,10 @@ struct ocfd_b200_ctx {
     // sweeps (which read no z ghosts) run; the z sweep waits for it
     cudaStream_t xstream = nullptr;
     cudaEvent_t xev[2] = {nullptr, nullptr};
+    // single-GPU steps: the viscous fluxes (they read only the primitives)
+    // run on vstream beside the inviscid sweeps; vev fork and join it
+    cudaStream_t vstream = nullptr;
+    cudaEvent_t vev[2] = {nullptr, nullptr};
     bool x_pending = false;
     bool have_metrics = false;
     int metric_mode = 0;          // 0 auto-detect uniform grids, 1 always read the fields
@@ -253,6 +257,9 @@ static void free_all(ocfd_b200_ctx *c) {
     c->slab = nullptr;
     for (auto &e : c->xev) if (e) cudaEventDestroy(e);
     if (c->xstream) cudaStreamDestroy(c->xstream);
+    if (c->vstream) cudaStreamSynchronize(c->vstream);
+    for (auto &e : c->vev) if (e) cudaEventDestroy(e);
+    if (c->vstream) cudaStreamDestroy(c->vstream);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
 }
@@ -383,7 +390,10 @@ extern "C" int ocfd_b200_create(const ocfd_b200_config *cfg, ocfd_b200_ctx **out
     cudaGetLastError();
 
     if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreate(&ctx->ev[0])) != cudaSuccess || (e = cudaEventCreate(&ctx->ev[1])) != cudaSuccess) {
+        (e = cudaEventCreate(&ctx->ev[0])) != cudaSuccess || (e = cudaEventCreate(&ctx->ev[1])) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&ctx->vstream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->vev[0], cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->vev[1], cudaEventDisableTiming)) != cudaSuccess) {
         cuda_fail(nullptr, e, "stream/event create");
         free_all(ctx); delete ctx;
         return OCFD_ERR_CUDA;
@@ -693,6 +703,22 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk, bool skip_sensor = fal
         int rc = ghost_prims(ctx, true);      // the z planes arrive while the x and y sweeps run
         if (rc) return rc;
     }
+    // On one GPU the viscous fluxes and their ghost fill (they read the
+    // primitives only) go to a second stream beside the inviscid sweeps; the
+    // divergence kernel waits for both.  Timed runs keep the families apart.
+    const bool side = ctx->vstream && !ctx->slab && !ctx->timing;
+    void *evf[12]; int evmask[12];
+    ocfd::ev_ghost_fields(p, evf, evmask);
+    if (side) {
+        CK(cudaEventRecord(ctx->vev[0], ctx->stream), "viscous fork");
+        CK(cudaStreamWaitEvent(ctx->vstream, ctx->vev[0], 0), "viscous fork");
+        CK(ocfd::launch_vis_ev(p, ctx->vstream), "viscous fluxes");
+        CK(p.mixed ? ghost_launch(p, reinterpret_cast<float *const *>(evf), evmask, 12, ctx->vstream)
+                   : ghost_launch(p, reinterpret_cast<double *const *>(evf), evmask, 12, ctx->vstream),
+           "Ev ghost fill");
+        CK(cudaEventRecord(ctx->vev[1], ctx->vstream), "viscous join");
+        ctx->launches += 2;
+    }
     {
         TimerScope ts(ctx, T_SWEEP);
         if (p.sweep_impl == 6 && !ocfd::sweeps4_supported(p))
@@ -710,18 +736,21 @@ static int rhs(ocfd_b200_ctx *ctx, int krk, int fused_rk, bool skip_sensor = fal
     }
     {
         TimerScope ts(ctx, T_VIS);
-        CK(ocfd::launch_vis_ev(p, ctx->stream), "viscous fluxes");
-        void *evf[12]; int mask[12];
-        ocfd::ev_ghost_fields(p, evf, mask);
-        // (forming the planes away from the slab faces while the Ev_z planes
-        // travel, and the two bands next to the faces after, measured slower
-        // than one launch after the exchange: the small band launches and the
-        // extra tail cost more than the exchange they hide)
-        int rc = p.mixed ? fill_ghosts(ctx, reinterpret_cast<float *const *>(evf), mask, 12, "Ev ghost fill")
-                         : fill_ghosts(ctx, reinterpret_cast<double *const *>(evf), mask, 12, "Ev ghost fill");
-        if (rc) return rc;
+        if (side) {
+            CK(cudaStreamWaitEvent(ctx->stream, ctx->vev[1], 0), "viscous join");
+        } else {
+            CK(ocfd::launch_vis_ev(p, ctx->stream), "viscous fluxes");
+            // (forming the planes away from the slab faces while the Ev_z planes
+            // travel, and the two bands next to the faces after, measured slower
+            // than one launch after the exchange: the small band launches and the
+            // extra tail cost more than the exchange they hide)
+            int rc = p.mixed ? fill_ghosts(ctx, reinterpret_cast<float *const *>(evf), evmask, 12, "Ev ghost fill")
+                             : fill_ghosts(ctx, reinterpret_cast<double *const *>(evf), evmask, 12, "Ev ghost fill");
+            if (rc) return rc;
+            ctx->launches += 1;
+        }
         CK(ocfd::launch_vis_div(p, fused_rk, 0, p.nz, ctx->stream), "viscous divergence");
-        ctx->launches += 2;
+        ctx->launches += 1;
     }
     if (fused_rk && p.ibc) {        // OCFD_bc: boundary values, then the faces
         int rc = apply_bc(ctx);
